@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Pair-count throughput of the post-growth analysis path on one B200.
+
+Workload (the exact-count configuration of the analysis path): mixed-type
+cover-shaped synthetic data, n = 50,000 samples, p = 54 (10 continuous + one-hot
+groups of 4 and 40), 7 imbalanced classes; a forest of 1,000 trees (mtry 7,
+nodesize 1) grown by the library's restatement of the reference's grower.
+
+One step = one full analysis pass through the C ABI with device-resident
+inputs and outputs: leaf routing of every (tree, sample) with OOB votes, the
+per-tree leaf member lists, the exact INT32 upper-triangle pair counts S, and
+permutation importance over all 54 features (overall and local).
+metric = pair updates per second (sum over trees and leaves of
+#OOB x #in-bag members; counted exactly by the kernel) of that step.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun (N > 1) every rank runs an independent replica on its own GPU
+(the path needs no exchange between replicas); value is the sum over ranks,
+timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_SAMPLES = 50_000
+N_TREES = 1000
+MTRY = 7
+WORKLOAD = ("exact pair counts + varimp: n=50000 p=54 (10 continuous + one-hot 4 + one-hot 40) c=7, "
+            "ntree=1000 mtry=7 nodesize=1, INT32 upper-triangle S (n(n+1)/2) + all 54 feature permutations")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_forest(n, T, rank, ws, barrier):
+    """Data + forest; rank 0 grows, other ranks read its export."""
+    from rfx_b200 import abi, synth
+    from rfx_b200.forest import Forest
+
+    X, y = synth.mixed_cover(n)
+    cat = synth.detect_categorical(X)
+    path = os.path.join(tempfile.gettempdir(), f"rfx_bench_forest_{n}_{T}_{os.getpid() if ws == 1 else 'dist'}.npz")
+    t0 = time.time()
+    if rank == 0:
+        f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
+        if ws > 1:
+            f.save(path)
+    barrier()
+    if rank != 0:
+        f = Forest.load(path)
+    barrier()
+    if rank == 0 and ws > 1 and os.path.exists(path):
+        os.remove(path)
+    return X, y, f, time.time() - t0
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.remove(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_run(X, y, f, budget_s=15.0, min_trees=2):
+    """The reference's CPU path on a bounded sample of trees.
+
+    Per tree, as grow_tree_single does: cpu_testreebag, the vote loop,
+    cpu_varimp (OpenMP over features) and find_terminal_node, all from
+    oracle/_ref (the reference's own sources); the pair counts use the
+    oracle's restatement of cpu_proximity's dense branch, because the shipped
+    cpu_proximity takes its sparse branch above n = 5000 and its n*n int32
+    size overflows at n = 50,000.  Returns (pair updates/s, dict)."""
+    from oracle import oracle as orc, reference as ref
+
+    cores = os.cpu_count() or 1
+    if ref.available():
+        ref.set_threads(cores)
+        kind = "reference"
+    else:
+        kind = "port"
+    done = 0
+    t_total = 0.0
+    U = 0
+    while done < min_trees or t_total < budget_s:
+        if done >= f.ntree:
+            break
+        sub = f.subset([done])
+        t0 = time.perf_counter()
+        if kind == "reference":
+            ref.analyse_trees(X, y, sub, do_imp=True, impn=True, do_prox=False)
+            out = orc.analyse(X, y, sub, do_imp=False, impn=False, do_prox=True)
+        else:
+            out = orc.analyse(X, y, sub, do_imp=True, impn=True, do_prox=True)
+        t_total += time.perf_counter() - t0
+        U += int(out["S"].astype(np.int64).sum())
+        del out
+        done += 1
+    return U / t_total, {"cores": cores if kind == "reference" else 1, "kind": kind,
+                         "sample": f"{done} of {f.ntree} trees at n={f.n} (testreebag + votes + cpu_varimp over "
+                                   f"{f.p} features + find_terminal_node + dense-branch pair counts), {t_total:.1f} s",
+                         "trees": done, "seconds": t_total, "pair_updates": U}
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from rfx_b200 import abi, synth
+
+    n, T = args.n, args.trees
+    X, y = synth.mixed_cover(n)
+    cat = synth.detect_categorical(X)
+    f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
+    per_step = []
+    U_tot, t_tot = 0, 0.0
+    for s in range(args.warmup + args.steps):
+        sub = f.subset([s % f.ntree])
+        v, info = cpu_baseline_run(X, y, sub, budget_s=0.0, min_trees=1)
+        if s >= args.warmup:
+            U_tot += info["pair_updates"]
+            t_tot += info["seconds"]
+            per_step.append(info["seconds"])
+    value = U_tot / t_tot
+    line = {"metric": "prox pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "n": n, "ntree": T, "parallelism": "host cores (OpenMP)"},
+            "cpu_baseline": {"value": value, "unit": "pair-updates/s", "cores": info["cores"], "kind": info["kind"],
+                             "sample": f"each step = 1 tree of the {T}-tree forest at n={n} (reference per-tree "
+                                       "sequence; pair counts by the dense-branch restatement)"},
+            "e2e": {"value": value, "unit": "pair-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_SAMPLES)
+    ap.add_argument("--trees", type=int, default=N_TREES)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    from rfx_b200 import abi
+
+    X, y, f, grow_s = make_forest(args.n, args.trees, rank, ws, barrier)
+    n, p, T = f.n, f.p, f.ntree
+    ctx = abi.Context(local)
+    ctx.load(f, X, y)
+    L = n * (n + 1) // 2
+    dev = torch.device("cuda", local)
+    S = torch.empty(L, dtype=torch.int32, device=dev)
+    avimp = torch.empty(p, dtype=torch.float32, device=dev)
+    sqsd = torch.empty(p, dtype=torch.float32, device=dev)
+    qimp = torch.empty(n, dtype=torch.float32, device=dev)
+    qimpm = torch.empty(n * p, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    def step():
+        ctx.proximity_upper(S)
+        ctx.varimp(True, avimp, sqsd, qimp, qimpm)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    U = ctx.pair_updates()
+    ctx.profile(True)
+    _, launches0 = ctx.profile_read()
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    stage_ms, launches1 = ctx.profile_read()
+    gpu_launches = launches1 - launches0
+    ctx.profile(False)
+    ms_max = ms
+    if pg is not None:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = ws * U / (ms_max / 1000.0)
+
+    # roofline of the dominant kernel
+    hbm, peak_src = peaks()
+    kernels = {k: v for k, v in stage_ms.items() if v > 0}
+    dom = max(kernels, key=kernels.get)
+    alg_bytes = {
+        # S written once + leaf keys read + bag flags read
+        "pair_counts": L * 4 + T * n * 4 + T * n * 1,
+        # per (tree, sample): bag flag + key written; X rows for OOB walks
+        "route": T * n * (1 + 4),
+        "leaf_lists": T * n * (4 + 4) * 2,
+        # OOB (tree, sample) units: flag byte + flip words written, joob, perm
+        "varimp_tree": T * n * (1 + 8 * ((p + 63) // 64)) + 2 * 4 * T * n,
+        "varimp_sample": T * n * (1 + 1 + 8 * ((p + 63) // 64)) + n * p * 4,
+        "varimp_feature": T * p * 4,
+    }
+    achieved = alg_bytes.get(dom, 0) / (kernels[dom] / 1000.0) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"{dom}_dram.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            d = json.load(fh)
+        traffic = d.get("dram_bytes_per_launch_fullsize")
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_src,
+                "alg_bytes_per_launch": alg_bytes.get(dom, 0), "kernel_ms": kernels[dom]}
+
+    line = {"metric": "prox pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded mixed-type cover-shaped generator; forest grown by the library's "
+                    "restatement of the reference grower)",
+            "config": {"workload": WORKLOAD, "n": n, "p": p, "ntree": T, "pair_updates_per_step": U,
+                       "l2": "inputs larger than L2 (S 5.0 GB written per step; nodes and leaf keys > 126 MB)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "forest_grow_s": round(grow_s, 2)},
+            "roofline": roofline, "gpu_launches": gpu_launches,
+            "breakdown_ms": {k: round(v, 4) for k, v in kernels.items()}}
+    if clk:
+        line["clocks"] = clk
+
+    # end to end through the public API with host buffers
+    if not args.no_e2e:
+        pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+        Sh = pin((L,), torch.int32)
+        av_h, sq_h = pin((p,), torch.float32), pin((p,), torch.float32)
+        qi_h, qm_h = pin((n,), torch.float32), pin((n * p,), torch.float32)
+        Xh = pin(X.shape, torch.float32)
+        Xh[...] = X
+        yh = pin(y.shape, torch.int32)
+        yh[...] = y
+        fh = f.subset(range(T))
+        for k in ("offs", "nodestatus", "bestvar", "xbestsplit", "treemap", "nodeclass", "nin", "cat"):
+            a = getattr(fh, k)
+            b = pin(a.shape, {np.dtype(np.int64): torch.int64, np.dtype(np.int32): torch.int32,
+                              np.dtype(np.float32): torch.float32}[a.dtype])
+            b[...] = a
+            setattr(fh, k, b)
+        h2d = X.nbytes + y.nbytes + sum(getattr(fh, k).nbytes for k in
+                                        ("offs", "nodestatus", "bestvar", "xbestsplit", "treemap", "nodeclass",
+                                         "nin", "cat"))
+        d2h = Sh.nbytes + av_h.nbytes + sq_h.nbytes + qi_h.nbytes + qm_h.nbytes
+        ctx2 = abi.Context(local)
+
+        def e2e_step():
+            ctx2.load(fh, Xh, yh)
+            ctx2.proximity_upper(Sh)
+            ctx2.varimp(True, av_h, sq_h, qi_h, qm_h)
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        ke = max(1, min(args.steps, 3))
+        for _ in range(ke):
+            e2e_step()
+        te = (time.perf_counter() - t0) / ke
+        ctx2.close()
+        if pg is not None:
+            t = torch.tensor([te], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            te = float(t.item())
+        line["e2e"] = {"value": ws * U / te, "unit": "pair-updates/s", "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h), "ms_per_step": te * 1000.0, "steps": ke}
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, info = cpu_baseline_run(X, y, f)
+        line["cpu_baseline"] = {"value": v, "unit": "pair-updates/s", "cores": info["cores"], "kind": info["kind"],
+                                "sample": info["sample"]}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

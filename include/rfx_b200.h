@@ -1,0 +1,179 @@
+/*
+ * rfx_b200 — C ABI of the B200 (sm_100a) post-growth random-forest analysis
+ * path: OOB / in-bag / test-set leaf routing, OOB votes, exact INT32 proximity
+ * pair counts, finishprox normalisation, permutation importance (overall and
+ * local), and the low-rank proximity + MDS forms.
+ *
+ * Every entry point returns an rfx_status (0 = success) and never throws.
+ * Pointers are plain host or device pointers (the library inspects each one
+ * with cudaPointerGetAttributes): outputs written to DEVICE memory are
+ * enqueued on the context's stream and the call returns without waiting;
+ * outputs written to HOST memory are complete when the call returns.
+ * All output buffers are caller-allocated.
+ *
+ * Reference interfaces replaced (chriskuchar/RFX):
+ *   the post-growth section of gpu_growtree_batch (cuda/rf_growtree.cu:2706-4130,
+ *   declared in src/rf_random_forest.cpp:35-51) and the per-tree CPU sequence of
+ *   RandomForest::grow_tree_single (src/rf_random_forest.cpp:1043-1309), plus the
+ *   low-rank handle API get_lowrank_factors_host / compute_mds_from_factors_host
+ *   (cuda/rf_lowrank_helpers.cu:13,55).
+ */
+#ifndef RFX_B200_H
+#define RFX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int rfx_status;
+
+enum {
+    RFX_OK = 0,
+    RFX_ERR_INVALID = 1,      /* bad argument or size */
+    RFX_ERR_CUDA = 2,         /* CUDA runtime error (message in rfx_last_error) */
+    RFX_ERR_OOM = 3,          /* device allocation failed */
+    RFX_ERR_STATE = 4,        /* call order (e.g. no forest loaded) */
+    RFX_ERR_UNSUPPORTED = 5,  /* feature outside the supported set (e.g. casewise) */
+    RFX_ERR_TIMEOUT = 6,      /* a bounded device wait gave up */
+    RFX_ERR_FOREST = 7,       /* forest failed validation */
+    RFX_ERR_NO_DEVICE = 8     /* no CUDA device / extension unusable */
+};
+
+typedef struct rfx_ctx rfx_ctx;
+
+/* Per-context settings, passed by value (the reference's mutable global
+ * rf::g_config, include/rf_config.hpp:17-114, has no counterpart here). */
+typedef struct rfx_config {
+    int32_t device;          /* CUDA device ordinal */
+    int32_t use_casewise;    /* must be 0: case-wise weighting is rejected */
+    int32_t n_threads_cpu;   /* host threads for rfx_grow_forest (0 = all) */
+    int32_t reserved[5];
+} rfx_config;
+
+/* A forest and the training data it was grown on, in the compact layout:
+ * tree t owns nodes [offs[t], offs[t+1]) of nodestatus/bestvar/xbestsplit/
+ * nodeclass, 2 entries per node of treemap (left, right), and maxcat entries
+ * per node of catgoleft (NULL = all zero, as the reference's CPU grower leaves
+ * it).  nin is ntree x n bootstrap multiplicities; X is n x p float32
+ * row-major; y holds labels 0..nclass-1; cat[p] is 1 for numeric features and
+ * the number of levels for categorical ones.  Replaces the padded
+ * ntree x maxnode arrays of rf::RandomForest (src/rf_random_forest.cpp:326-335). */
+typedef struct rfx_forest_view {
+    int32_t n, p, nclass, maxcat, ntree;
+    const int64_t* offs;        /* ntree + 1 */
+    const int32_t* nodestatus;  /* -1 terminal, 1 split, 2 unsplit */
+    const int32_t* bestvar;
+    const float* xbestsplit;
+    const int32_t* treemap;     /* 2 per node */
+    const int32_t* nodeclass;
+    const int32_t* catgoleft;   /* maxcat per node, or NULL */
+    const int32_t* nin;         /* ntree * n */
+    const float* X;             /* n * p */
+    const int32_t* y;           /* n */
+    const int32_t* cat;         /* p */
+} rfx_forest_view;
+
+/* Last error message of the calling thread ("" if none). */
+const char* rfx_last_error(void);
+
+rfx_status rfx_ctx_create(const rfx_config* cfg, rfx_ctx** out);
+rfx_status rfx_ctx_destroy(rfx_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t) for event timing by callers. */
+rfx_status rfx_ctx_stream(rfx_ctx* ctx, void** stream);
+rfx_status rfx_synchronize(rfx_ctx* ctx);
+
+/* Validate and upload a forest (replaces the per-tree H2D copies of
+ * cuda/rf_growtree.cu:2618-2657).  Rejects out-of-range children, bestvar or
+ * labels before any launch.  The library keeps its own device copies. */
+rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* view);
+
+/* OOB routing + votes: cpu_testreebag (src/rf_testreebag.cpp:13-125) and the
+ * vote loop of grow_tree_single (src/rf_random_forest.cpp:1107-1153) over all
+ * trees.  q[n*nclass] receives integer vote counts; nout[n] the reference's
+ * doubled OOB count (src/rf_bootstrap.cpp:61 and src/rf_random_forest.cpp:1110).
+ * leaf (optional, ntree*n) receives per-tree node ids: OOB samples from the
+ * testreebag walk, in-bag samples from find_terminal_node
+ * (src/rf_random_forest.cpp:2194-2244). */
+rfx_status rfx_route_oob(rfx_ctx* ctx, int32_t* q, int32_t* nout, int32_t* leaf);
+
+/* OOB error, predictions and probabilities from the votes of rfx_route_oob
+ * (compute_classification_error src/rf_random_forest.cpp:2413-2462,
+ * compute_oob_predictions :2246-2301).  Any output may be NULL. */
+rfx_status rfx_oob_summary(rfx_ctx* ctx, float* oob_error, int32_t* pred, float* proba);
+
+/* Exact pair counts: S[i,j] = C[i,j] + C[j,i] for i <= j, packed row-major
+ * upper triangle with the diagonal (len = n(n+1)/2, diagonal 0), where C[i,j]
+ * counts trees with i out-of-bag, j in-bag and both in the same terminal node:
+ * the dense branch of cpu_proximity (src/rf_proximity.cpp:99-231) accumulated
+ * over all trees.  Replaces cuda_proximity_upper_triangle_fp16_kernel
+ * (cuda/rf_proximity_upper_triangle.cu:149). */
+rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len);
+
+/* Total pair updates sum_t sum_leaf noob_leaf * nin_leaf of the last
+ * rfx_proximity_upper_i32 (the unit of the pair-update throughput). */
+rfx_status rfx_pair_updates(rfx_ctx* ctx, int64_t* count);
+
+/* cpu_finishprox (src/rf_finishprox.cpp:12-74) applied to S (device or host,
+ * packed as above) with the doubled nout:
+ *   P[i,j] = 0.5 * ((S/2)/nout_i + (S/2)/nout_j), P[i,i] = 1, rows with
+ * nout_i = 0 unscaled, in FP64, stored as float32 — full n x n (full = 1, the
+ * layout get_proximity_matrix returns, python/randomforest_py.cpp:1114-1177)
+ * or packed upper triangle (full = 0). */
+rfx_status rfx_finishprox(rfx_ctx* ctx, const int32_t* S, float* P, int full);
+
+/* Permutation importance over all trees and all features
+ * (cpu_varimp src/rf_varimp.cpp:106-302 with cpu_testreeimp :32-104 and
+ * cpu_permobmr :16-30, accumulated as src/rf_random_forest.cpp:1217-1230).
+ * avimp[p] = feature_importances_, sqsd[p], qimp[n], qimpm[n*p] (sample-major,
+ * before localimp); impn = 1 computes qimp/qimpm (local importance), which may
+ * then be NULL when impn = 0. */
+rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* qimp, float* qimpm);
+
+/* localimp (src/rf_utilities.cpp:28-43) as get_local_importance returns it:
+ * out[idx] = 100 * (qimp[idx % n] - qimpm[idx]) / ntree for idx < n*p. */
+rfx_status rfx_localimp(rfx_ctx* ctx, const float* qimp, const float* qimpm, float* out);
+
+/* Test-set votes (predict_classification / predict_proba,
+ * src/rf_random_forest.cpp:1925-2036, :2303-2411): votes[m*nclass]. */
+rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes);
+
+/* Per-stage device timing.  With profiling enabled, every stage launch is
+ * bracketed by CUDA events on the context stream; rfx_profile_read waits for
+ * the stream and returns, per stage, the mean duration of its launches since
+ * profiling was (re)enabled (the last 64 at most; ms, -1 if never run), and
+ * the number of kernels the library has launched since the context was
+ * created.  Stage order: route, leaf lists, pair counts,
+ * finishprox, varimp per-tree, varimp per-sample, varimp per-feature, predict,
+ * oob summary, localimp. */
+enum { RFX_NUM_STAGES = 10 };
+rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable);
+rfx_status rfx_profile_read(rfx_ctx* ctx, float* stage_ms, int64_t* kernel_launches);
+
+/* Forest producer (not on the analysis path): cpu_bootstrap + cpu_growtree
+ * (src/rf_bootstrap.cpp:14-82, src/rf_growtree.cpp:382-945) restated with a
+ * partition per node; trees grown in parallel host threads.  Arrays are
+ * allocated by the library and released with rfx_free_forest. */
+typedef struct rfx_grown_forest {
+    int32_t ntree;
+    int64_t* offs;
+    int32_t* nodestatus;
+    int32_t* bestvar;
+    float* xbestsplit;
+    int32_t* treemap;
+    int32_t* nodeclass;
+    int32_t* nin;
+} rfx_grown_forest;
+
+rfx_status rfx_grow_forest(const float* X, const int32_t* y, int32_t n, int32_t p, int32_t nclass,
+                           int32_t ntree, int32_t mtry, int32_t minndsize, int32_t maxnode, int32_t iseed,
+                           int32_t n_threads, rfx_grown_forest* out);
+rfx_status rfx_free_forest(rfx_grown_forest* f);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RFX_B200_H */

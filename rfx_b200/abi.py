@@ -1,0 +1,245 @@
+"""ctypes binding of the C ABI (include/rfx_b200.h) — the call path the parity
+tests and bench.py use.  It mirrors the ctypes stub a reference maintainer
+would add.
+
+Device outputs may be given as torch CUDA tensors (or raw device addresses);
+host outputs as numpy arrays.  There is no CPU fallback: if the library or a
+CUDA device is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+from .forest import Forest
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "librfx_b200.so")
+
+RFX_OK = 0
+STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ERR_OOM", 4: "RFX_ERR_STATE",
+                5: "RFX_ERR_UNSUPPORTED", 6: "RFX_ERR_TIMEOUT", 7: "RFX_ERR_FOREST", 8: "RFX_ERR_NO_DEVICE"}
+
+# Every symbol include/rfx_b200.h declares (checked by the CPU tests).
+EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
+           "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
+           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_profile_enable", "rfx_profile_read",
+           "rfx_grow_forest", "rfx_free_forest"]
+
+STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
+          "predict", "oob_summary", "localimp"]
+
+
+class RfxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("use_casewise", ctypes.c_int32), ("n_threads_cpu", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
+
+
+class _ForestView(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("p", ctypes.c_int32), ("nclass", ctypes.c_int32), ("maxcat", ctypes.c_int32),
+                ("ntree", ctypes.c_int32), ("offs", ctypes.c_void_p), ("nodestatus", ctypes.c_void_p),
+                ("bestvar", ctypes.c_void_p), ("xbestsplit", ctypes.c_void_p), ("treemap", ctypes.c_void_p),
+                ("nodeclass", ctypes.c_void_p), ("catgoleft", ctypes.c_void_p), ("nin", ctypes.c_void_p),
+                ("X", ctypes.c_void_p), ("y", ctypes.c_void_p), ("cat", ctypes.c_void_p)]
+
+
+class _Grown(ctypes.Structure):
+    _fields_ = [("ntree", ctypes.c_int32), ("offs", ctypes.POINTER(ctypes.c_int64)),
+                ("nodestatus", ctypes.POINTER(ctypes.c_int32)), ("bestvar", ctypes.POINTER(ctypes.c_int32)),
+                ("xbestsplit", ctypes.POINTER(ctypes.c_float)), ("treemap", ctypes.POINTER(ctypes.c_int32)),
+                ("nodeclass", ctypes.POINTER(ctypes.c_int32)), ("nin", ctypes.POINTER(ctypes.c_int32))]
+
+
+_LIB = None
+
+
+def lib():
+    """Load librfx_b200.so (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RfxError(8, f"native library missing: {LIB_PATH} (run python -m rfx_b200.build)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.rfx_last_error.restype = ctypes.c_char_p
+        _LIB = L
+    return _LIB
+
+
+def _check(st: int):
+    if st != RFX_OK:
+        raise RfxError(st, lib().rfx_last_error().decode())
+
+
+def _ptr(a) -> Optional[int]:
+    """Address of a numpy array, a torch tensor, or an int device address."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported buffer type {type(a)}")
+
+
+def _vp(a):
+    p = _ptr(a)
+    return None if p is None else ctypes.c_void_p(p)
+
+
+def grow_forest(X, y, ntree: int, mtry: int, minndsize: int = 1, maxnode: int = 0, iseed: int = 12345,
+                n_threads: int = 0, nclass: Optional[int] = None, cat=None, maxcat: int = 10) -> Forest:
+    """Grow a forest with the library's restatement of the reference grower."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.int32)
+    n, p = X.shape
+    c = int(nclass if nclass is not None else np.unique(y).size)
+    g = _Grown()
+    _check(lib().rfx_grow_forest(_vp(X), _vp(y), n, p, c, ntree, mtry, minndsize, maxnode, iseed, n_threads,
+                                 ctypes.byref(g)))
+    try:
+        offs = np.ctypeslib.as_array(g.offs, shape=(ntree + 1,)).copy()
+        N = int(offs[-1])
+        arr = lambda ptr, k: np.ctypeslib.as_array(ptr, shape=(k,)).copy()
+        f = Forest(n=n, p=p, nclass=c, maxcat=maxcat, nnode=np.diff(offs).astype(np.int32), offs=offs,
+                   nodestatus=arr(g.nodestatus, N), bestvar=arr(g.bestvar, N), xbestsplit=arr(g.xbestsplit, N),
+                   treemap=arr(g.treemap, 2 * N), nodeclass=arr(g.nodeclass, N),
+                   nin=arr(g.nin, ntree * n).reshape(ntree, n),
+                   cat=np.ascontiguousarray(cat if cat is not None else np.ones(p), dtype=np.int32))
+    finally:
+        lib().rfx_free_forest(ctypes.byref(g))
+    return f
+
+
+class Context:
+    """One rfx_ctx: a device, a stream, and (after load) a resident forest."""
+
+    def __init__(self, device: int = 0, use_casewise: bool = False):
+        cfg = _Config(device=device, use_casewise=int(use_casewise), n_threads_cpu=0)
+        h = ctypes.c_void_p()
+        _check(lib().rfx_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.forest: Optional[Forest] = None
+
+    def close(self):
+        if self._h:
+            lib().rfx_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(lib().rfx_ctx_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def synchronize(self):
+        _check(lib().rfx_synchronize(self._h))
+
+    def profile(self, enable: bool = True):
+        _check(lib().rfx_profile_enable(self._h, int(bool(enable))))
+
+    def profile_read(self):
+        """(dict stage -> ms of its last launch, kernel launches so far)."""
+        ms = np.zeros(len(STAGES), np.float32)
+        cnt = ctypes.c_int64(0)
+        _check(lib().rfx_profile_read(self._h, _vp(ms), ctypes.byref(cnt)))
+        return {s: float(v) for s, v in zip(STAGES, ms)}, int(cnt.value)
+
+    def load(self, forest: Forest, X, y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.int32)
+        f = forest
+        keep = [np.ascontiguousarray(a) for a in (f.offs, f.nodestatus, f.bestvar, f.xbestsplit, f.treemap,
+                                                  f.nodeclass, f.nin, f.cat)]
+        cg = None if f.catgoleft is None else np.ascontiguousarray(f.catgoleft, dtype=np.int32)
+        v = _ForestView(n=f.n, p=f.p, nclass=f.nclass, maxcat=f.maxcat, ntree=f.ntree,
+                        offs=_ptr(keep[0].astype(np.int64, copy=False)), nodestatus=_ptr(keep[1]),
+                        bestvar=_ptr(keep[2]), xbestsplit=_ptr(keep[3]), treemap=_ptr(keep[4]),
+                        nodeclass=_ptr(keep[5]), catgoleft=_ptr(cg), nin=_ptr(keep[6]), X=_ptr(X), y=_ptr(y),
+                        cat=_ptr(keep[7]))
+        _check(lib().rfx_forest_load(self._h, ctypes.byref(v)))
+        self.forest = f
+        self.n, self.p, self.nclass, self.ntree = f.n, f.p, f.nclass, f.ntree
+
+    # --- analysis ---------------------------------------------------------
+    def route_oob(self, q=None, nout=None, leaf=None):
+        """Integer OOB votes q (n, c), doubled nout (n,), optional leaf (T, n)."""
+        if q is None:
+            q = np.zeros((self.n, self.nclass), np.int32)
+        if nout is None:
+            nout = np.zeros(self.n, np.int32)
+        _check(lib().rfx_route_oob(self._h, _vp(q), _vp(nout), _vp(leaf)))
+        return q, nout, leaf
+
+    def oob_summary(self):
+        err = np.zeros(1, np.float32)
+        pred = np.zeros(self.n, np.int32)
+        proba = np.zeros((self.n, self.nclass), np.float32)
+        _check(lib().rfx_oob_summary(self._h, _vp(err), _vp(pred), _vp(proba)))
+        return float(err[0]), pred, proba
+
+    def proximity_upper(self, S=None):
+        """Packed upper-triangle INT32 pair counts (n(n+1)/2,)."""
+        L = self.n * (self.n + 1) // 2
+        if S is None:
+            S = np.zeros(L, np.int32)
+        _check(lib().rfx_proximity_upper_i32(self._h, _vp(S), ctypes.c_size_t(L)))
+        return S
+
+    def pair_updates(self) -> int:
+        c = ctypes.c_int64(0)
+        _check(lib().rfx_pair_updates(self._h, ctypes.byref(c)))
+        return int(c.value)
+
+    def finishprox(self, S, P=None, full=True):
+        if P is None:
+            P = np.zeros((self.n, self.n) if full else self.n * (self.n + 1) // 2, np.float32)
+        _check(lib().rfx_finishprox(self._h, _vp(S), _vp(P), int(bool(full))))
+        return P
+
+    def varimp(self, impn=True, avimp=None, sqsd=None, qimp=None, qimpm=None):
+        if avimp is None:
+            avimp = np.zeros(self.p, np.float32)
+        if sqsd is None:
+            sqsd = np.zeros(self.p, np.float32)
+        if impn and qimp is None:
+            qimp = np.zeros(self.n, np.float32)
+        if impn and qimpm is None:
+            qimpm = np.zeros(self.n * self.p, np.float32)
+        _check(lib().rfx_varimp(self._h, int(bool(impn)), _vp(avimp), _vp(sqsd), _vp(qimp), _vp(qimpm)))
+        return avimp, sqsd, qimp, qimpm
+
+    def localimp(self, qimp, qimpm, out=None):
+        if out is None:
+            out = np.zeros((self.n, self.p), np.float32)
+        _check(lib().rfx_localimp(self._h, _vp(qimp), _vp(qimpm), _vp(out)))
+        return out
+
+    def predict_votes(self, Xt, votes=None):
+        m = int(Xt.shape[0])
+        if isinstance(Xt, np.ndarray):
+            Xt = np.ascontiguousarray(Xt, dtype=np.float32)
+        if votes is None:
+            votes = np.zeros((m, self.nclass), np.int32)
+        _check(lib().rfx_predict(self._h, _vp(Xt), m, _vp(votes)))
+        return votes

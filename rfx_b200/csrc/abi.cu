@@ -1,0 +1,852 @@
+// C ABI of librfx_b200: context, forest validation/upload, and the analysis
+// entry points declared in include/rfx_b200.h.  No exception crosses the ABI.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "rfx_internal.cuh"
+
+namespace rfxhost {
+void bootstrap(int n, int tree, int32_t* nin);
+int grow_forest(const float* X, const int32_t* y, int n, int p, int nclass, int ntree, int mtry, int minndsize,
+                int maxnode, int iseed, int nthreads, std::vector<int64_t>& offs, std::vector<int32_t>& nodestatus,
+                std::vector<int32_t>& bestvar, std::vector<float>& xbestsplit, std::vector<int32_t>& treemap,
+                std::vector<int32_t>& nodeclass, int32_t* nin_all);
+}
+
+namespace rfx {
+
+rfx_status launch_route_leaf(Ctx* c, int32_t* d_leaf);
+
+namespace {
+thread_local std::string g_last_error;
+
+// MT19937 of include/rf_utils.hpp:74-141, for cpu_permobmr's permutations.
+struct MT {
+    uint32_t mt[624];
+    int mti;
+    void seed(uint32_t s) {
+        mt[0] = s;
+        for (mti = 1; mti < 624; ++mti) mt[mti] = 1812433253UL * (mt[mti - 1] ^ (mt[mti - 1] >> 30)) + (uint32_t)mti;
+    }
+    float randomu() {
+        static const uint32_t mag01[2] = {0x0UL, 0x9908b0dfUL};
+        uint32_t y;
+        if (mti >= 624) {
+            int kk;
+            for (kk = 0; kk < 624 - 397; ++kk) {
+                y = (mt[kk] & 0x80000000UL) | (mt[kk + 1] & 0x7fffffffUL);
+                mt[kk] = mt[kk + 397] ^ (y >> 1) ^ mag01[y & 1];
+            }
+            for (; kk < 623; ++kk) {
+                y = (mt[kk] & 0x80000000UL) | (mt[kk + 1] & 0x7fffffffUL);
+                mt[kk] = mt[kk + (397 - 624)] ^ (y >> 1) ^ mag01[y & 1];
+            }
+            y = (mt[623] & 0x80000000UL) | (mt[0] & 0x7fffffffUL);
+            mt[623] = mt[396] ^ (y >> 1) ^ mag01[y & 1];
+            mti = 0;
+        }
+        y = mt[mti++];
+        y ^= (y >> 11);
+        y ^= (y << 7) & 0x9d2c5680UL;
+        y ^= (y << 15) & 0xefc60000UL;
+        y ^= (y >> 18);
+        return (float)((double)y / (double)0xffffffffUL);
+    }
+};
+
+// cpu_permobmr (src/rf_varimp.cpp:16-30): positions permuted by swaps with
+// j = (int)(randomu() * noob).  A draw that rounds to 1.0f gives j == noob,
+// which the reference uses to index one past its vector; it is counted and
+// clamped here.
+int make_perm(int noob, int32_t* perm) {
+    MT rng;
+    rng.seed(42u);
+    int bad = 0;
+    for (int i = 0; i < noob; ++i) perm[i] = i;
+    for (int i = 0; i < noob; ++i) {
+        int j = (int)(rng.randomu() * (float)noob);
+        if (j >= noob) {
+            j = noob - 1;
+            ++bad;
+        }
+        std::swap(perm[i], perm[j]);
+    }
+    return bad;
+}
+
+template <typename T>
+void dfree(Ctx* c, T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+void free_forest(Ctx* c) {
+    dfree(c, c->d_X); dfree(c, c->d_y); dfree(c, c->d_cat); dfree(c, c->d_nodes); dfree(c, c->d_nodeclass);
+    dfree(c, c->d_leafidx); dfree(c, c->d_catgoleft); dfree(c, c->d_offs); dfree(c, c->d_nnode);
+    dfree(c, c->d_inbag); dfree(c, c->d_segbase); dfree(c, c->d_iv); dfree(c, c->d_noob); dfree(c, c->d_permoff);
+    dfree(c, c->d_perm); dfree(c, c->d_invnoob); dfree(c, c->d_key); dfree(c, c->d_segoff); dfree(c, c->d_memb);
+    dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_vflags); dfree(c, c->d_flips);
+    dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
+    dfree(c, c->d_sqsd);
+    c->loaded = c->routed = c->csr_built = false;
+    c->bytes = 0;
+}
+
+// Copy helper: device->(device|host) of `bytes` bytes on the context stream.
+rfx_status copy_out(Ctx* c, void* dst, const void* src, size_t bytes) {
+    if (!dst || bytes == 0) return RFX_OK;
+    RFX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));
+    return RFX_OK;
+}
+
+rfx_status finish_host(Ctx* c, bool any_host) {
+    if (!any_host) return RFX_OK;
+    RFX_CUDA(cudaStreamSynchronize(c->stream));
+    return check_device_errors(c);
+}
+
+}  // namespace
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+rfx_status cuda_fail(cudaError_t e, const char* what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return RFX_ERR_OOM;
+    }
+    return RFX_ERR_CUDA;
+}
+
+bool is_device_ptr(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+rfx_status check_device_errors(Ctx* c) {
+    uint32_t bits = 0;
+    RFX_CUDA(cudaMemcpy(&bits, c->d_err, sizeof(bits), cudaMemcpyDeviceToHost));
+    if (!bits) return RFX_OK;
+    RFX_CUDA(cudaMemset(c->d_err, 0, sizeof(uint32_t)));
+    std::string m = "device checks raised:";
+    if (bits & ERR_STALE_JVR)
+        m += " a cpu_testreeimp walk ended without a terminal node (the reference would keep a stale vote);";
+    if (bits & ERR_TRAVERSAL_LIMIT) m += " a walk hit its step limit;";
+    set_error(m);
+    return RFX_ERR_UNSUPPORTED;
+}
+
+}  // namespace rfx
+
+using namespace rfx;
+
+extern "C" {
+
+const char* rfx_last_error(void) { return g_last_error.c_str(); }
+
+rfx_status rfx_ctx_create(const rfx_config* cfg, rfx_ctx** out) {
+    if (!out) {
+        set_error("rfx_ctx_create: out is null");
+        return RFX_ERR_INVALID;
+    }
+    *out = nullptr;
+    rfx_config conf{};
+    if (cfg) conf = *cfg;
+    if (conf.use_casewise) {
+        set_error("use_casewise=True is not supported (case-wise weighting is out of scope)");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error(std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
+        return RFX_ERR_NO_DEVICE;
+    }
+    if (conf.device < 0 || conf.device >= ndev) {
+        set_error("device ordinal out of range");
+        return RFX_ERR_INVALID;
+    }
+    Ctx* c = new (std::nothrow) Ctx();
+    if (!c) return RFX_ERR_OOM;
+    c->cfg = conf;
+    c->device = conf.device;
+    e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_fail(e, "rfx_ctx_create");
+    }
+    rfx_status st = dalloc(c, &c->d_err, 1);
+    if (st == RFX_OK) st = dalloc(c, &c->d_pairs, 4);
+    if (st != RFX_OK) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return st;
+    }
+    cudaMemset(c->d_err, 0, sizeof(uint32_t));
+    *out = reinterpret_cast<rfx_ctx*>(c);
+    return RFX_OK;
+}
+
+rfx_status rfx_ctx_destroy(rfx_ctx* ctx) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return RFX_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_forest(c);
+    for (int s = 0; s < ST_COUNT; ++s) {
+        for (cudaEvent_t e : c->ev_start[s]) cudaEventDestroy(e);
+        for (cudaEvent_t e : c->ev_end[s]) cudaEventDestroy(e);
+    }
+    if (c->d_err) cudaFree(c->d_err);
+    if (c->d_pairs) cudaFree(c->d_pairs);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return RFX_OK;
+}
+
+rfx_status rfx_ctx_stream(rfx_ctx* ctx, void** stream) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !stream) return RFX_ERR_INVALID;
+    *stream = (void*)c->stream;
+    return RFX_OK;
+}
+
+rfx_status rfx_synchronize(rfx_ctx* ctx) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return RFX_ERR_INVALID;
+    cudaSetDevice(c->device);
+    RFX_CUDA(cudaStreamSynchronize(c->stream));
+    return check_device_errors(c);
+}
+
+rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !v) {
+        set_error("rfx_forest_load: null argument");
+        return RFX_ERR_INVALID;
+    }
+    try {
+        cudaSetDevice(c->device);
+        const int n = v->n, p = v->p, nclass = v->nclass, T = v->ntree;
+        const int maxcat = v->maxcat;
+        if (n < 1 || p < 1 || nclass < 1 || T < 1 || maxcat < 1) {
+            set_error("rfx_forest_load: n, p, nclass, ntree and maxcat must be >= 1");
+            return RFX_ERR_INVALID;
+        }
+        if (p > 65535) {
+            set_error("rfx_forest_load: at most 65535 features");
+            return RFX_ERR_UNSUPPORTED;
+        }
+        if (!v->offs || !v->nodestatus || !v->bestvar || !v->xbestsplit || !v->treemap || !v->nodeclass || !v->nin ||
+            !v->X || !v->y || !v->cat) {
+            set_error("rfx_forest_load: a required array is null");
+            return RFX_ERR_INVALID;
+        }
+        if (v->offs[0] != 0) {
+            set_error("rfx_forest_load: offs[0] must be 0");
+            return RFX_ERR_FOREST;
+        }
+        for (int i = 0; i < n; ++i)
+            if (v->y[i] < 0 || v->y[i] >= nclass) {
+                set_error("rfx_forest_load: label out of [0, nclass) at sample " + std::to_string(i));
+                return RFX_ERR_INVALID;
+            }
+        if (v->catgoleft)
+            for (int m = 0; m < p; ++m)
+                if (v->cat[m] != 1 && v->cat[m] > maxcat) {
+                    set_error("rfx_forest_load: cat[m] exceeds maxcat with a catgoleft table");
+                    return RFX_ERR_FOREST;
+                }
+        std::vector<int32_t> nnode(T), nleaf(T), noob(T);
+        std::vector<int64_t> segbase(T + 1, 0);
+        const int W = (p + 63) / 64;
+        std::vector<uint64_t> iv((size_t)T * W, 0);
+        for (int t = 0; t < T; ++t) {
+            const int64_t a = v->offs[t], b = v->offs[t + 1];
+            if (b <= a || b - a > (int64_t)2 * n + 1) {
+                set_error("rfx_forest_load: tree " + std::to_string(t) + " has an invalid node count");
+                return RFX_ERR_FOREST;
+            }
+            nnode[t] = (int)(b - a);
+        }
+        const int64_t N = v->offs[T];
+        std::vector<DNode> nodes((size_t)N);
+        std::vector<int32_t> leafidx((size_t)N);
+        for (int t = 0; t < T; ++t) {
+            const int64_t o = v->offs[t];
+            const int nn = nnode[t];
+            int L = 0;
+            for (int k = 0; k < nn; ++k) {
+                const int64_t g = o + k;
+                const int st = v->nodestatus[g];
+                if (st < -128 || st > 127) {
+                    set_error("rfx_forest_load: nodestatus out of range in tree " + std::to_string(t));
+                    return RFX_ERR_FOREST;
+                }
+                const int bv = v->bestvar[g];
+                const int l = v->treemap[2 * g], r = v->treemap[2 * g + 1];
+                if (st != -1) {
+                    if (bv < 0 || bv >= p) {
+                        set_error("rfx_forest_load: bestvar out of range at tree " + std::to_string(t) + " node " +
+                                  std::to_string(k));
+                        return RFX_ERR_FOREST;
+                    }
+                    if (l < 0 || l >= nn || r < 0 || r >= nn) {
+                        set_error("rfx_forest_load: child out of range at tree " + std::to_string(t) + " node " +
+                                  std::to_string(k));
+                        return RFX_ERR_FOREST;
+                    }
+                    iv[(size_t)t * W + (bv >> 6)] |= 1ull << (bv & 63);
+                }
+                DNode d;
+                d.split = v->xbestsplit[g];
+                d.left = l;
+                d.right = r;
+                const int var = (st != -1) ? bv : 0;
+                const int catf = (st != -1 && v->cat[var] != 1) ? 1 : 0;
+                d.meta = (var & 0xffff) | ((st & 0xff) << 16) | (catf << 24);
+                nodes[(size_t)g] = d;
+                leafidx[(size_t)g] = (st == -1) ? L++ : -1;
+            }
+            nleaf[t] = L;
+            segbase[t + 1] = segbase[t] + 2 * (int64_t)L + 1;
+            // varimp marks features of nodes [0, max(nnode, 1)); nnode >= 1 here
+        }
+        std::vector<uint8_t> inbag((size_t)T * n);
+        for (int t = 0; t < T; ++t) {
+            int cnt = 0;
+            for (int i = 0; i < n; ++i) {
+                const int32_t m = v->nin[(size_t)t * n + i];
+                if (m < 0) {
+                    set_error("rfx_forest_load: negative nin");
+                    return RFX_ERR_FOREST;
+                }
+                inbag[(size_t)t * n + i] = m > 0;
+                cnt += (m == 0);
+            }
+            noob[t] = cnt;
+        }
+        // permutations per distinct noob
+        std::map<int, int> perm_at;
+        for (int t = 0; t < T; ++t) perm_at[noob[t]] = 0;
+        std::vector<int> distinct;
+        int64_t total = 0;
+        for (auto& kv : perm_at) {
+            kv.second = (int)total;
+            distinct.push_back(kv.first);
+            total += std::max(kv.first, 1);
+        }
+        std::vector<int32_t> perm((size_t)total);
+        {
+            std::vector<std::thread> th;
+            const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), (int)distinct.size()));
+            std::atomic<int> next{0};
+            for (int q = 0; q < nth; ++q)
+                th.emplace_back([&]() {
+                    for (;;) {
+                        int d = next.fetch_add(1);
+                        if (d >= (int)distinct.size()) break;
+                        make_perm(distinct[d], perm.data() + perm_at[distinct[d]]);
+                    }
+                });
+            for (auto& x : th) x.join();
+        }
+        std::vector<int32_t> permoff(T);
+        std::vector<float> invnoob(T);
+        for (int t = 0; t < T; ++t) {
+            permoff[t] = perm_at[noob[t]];
+            volatile float f = (float)noob[t];
+            invnoob[t] = 1.0f / f;
+        }
+        if (total > INT32_MAX) {
+            set_error("rfx_forest_load: permutation tables too large");
+            return RFX_ERR_UNSUPPORTED;
+        }
+
+        free_forest(c);
+        c->n = n; c->p = p; c->nclass = nclass; c->maxcat = maxcat; c->T = T; c->N = N;
+        c->h_offs.assign(v->offs, v->offs + T + 1);
+        c->h_nnode = nnode;
+        c->h_nleaf = nleaf;
+        c->h_segbase = segbase;
+        c->h_noob = noob;
+        c->iv_words = W;
+        c->max_keys = 0;
+        c->max_nnode = 0;
+        for (int t = 0; t < T; ++t) {
+            c->max_keys = std::max(c->max_keys, 2 * nleaf[t]);
+            c->max_nnode = std::max(c->max_nnode, nnode[t]);
+        }
+        rfx_status st = RFX_OK;
+#define ALLOC(ptr, cnt) \
+    if (st == RFX_OK) st = dalloc(c, &c->ptr, (size_t)(cnt));
+        ALLOC(d_X, (size_t)n * p);
+        ALLOC(d_y, n);
+        ALLOC(d_cat, p);
+        ALLOC(d_nodes, N);
+        ALLOC(d_nodeclass, N);
+        ALLOC(d_leafidx, N);
+        if (v->catgoleft) ALLOC(d_catgoleft, (size_t)N * maxcat);
+        ALLOC(d_offs, T + 1);
+        ALLOC(d_nnode, T);
+        ALLOC(d_inbag, (size_t)T * n);
+        ALLOC(d_segbase, T + 1);
+        ALLOC(d_iv, (size_t)T * W);
+        ALLOC(d_noob, T);
+        ALLOC(d_permoff, T);
+        ALLOC(d_perm, total);
+        ALLOC(d_invnoob, T);
+        ALLOC(d_key, (size_t)T * n);
+        ALLOC(d_segoff, segbase[T]);
+        ALLOC(d_memb, (size_t)T * n);
+        ALLOC(d_votes, (size_t)n * nclass);
+        ALLOC(d_nout, n);
+#undef ALLOC
+        if (st != RFX_OK) {
+            free_forest(c);
+            return st;
+        }
+        auto up = [&](void* d, const void* h, size_t bytes) {
+            return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c->stream);
+        };
+        cudaError_t e = cudaSuccess;
+        if (e == cudaSuccess) e = up(c->d_X, v->X, sizeof(float) * (size_t)n * p);
+        if (e == cudaSuccess) e = up(c->d_y, v->y, sizeof(int32_t) * n);
+        if (e == cudaSuccess) e = up(c->d_cat, v->cat, sizeof(int32_t) * p);
+        if (e == cudaSuccess) e = up(c->d_nodes, nodes.data(), sizeof(DNode) * (size_t)N);
+        if (e == cudaSuccess) e = up(c->d_nodeclass, v->nodeclass, sizeof(int32_t) * (size_t)N);
+        if (e == cudaSuccess) e = up(c->d_leafidx, leafidx.data(), sizeof(int32_t) * (size_t)N);
+        if (e == cudaSuccess && v->catgoleft)
+            e = up(c->d_catgoleft, v->catgoleft, sizeof(int32_t) * (size_t)N * maxcat);
+        if (e == cudaSuccess) e = up(c->d_offs, v->offs, sizeof(int64_t) * (T + 1));
+        if (e == cudaSuccess) e = up(c->d_nnode, nnode.data(), sizeof(int32_t) * T);
+        if (e == cudaSuccess) e = up(c->d_inbag, inbag.data(), (size_t)T * n);
+        if (e == cudaSuccess) e = up(c->d_segbase, segbase.data(), sizeof(int64_t) * (T + 1));
+        if (e == cudaSuccess) e = up(c->d_iv, iv.data(), sizeof(uint64_t) * (size_t)T * W);
+        if (e == cudaSuccess) e = up(c->d_noob, noob.data(), sizeof(int32_t) * T);
+        if (e == cudaSuccess) e = up(c->d_permoff, permoff.data(), sizeof(int32_t) * T);
+        if (e == cudaSuccess) e = up(c->d_perm, perm.data(), sizeof(int32_t) * (size_t)total);
+        if (e == cudaSuccess) e = up(c->d_invnoob, invnoob.data(), sizeof(float) * T);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            free_forest(c);
+            return cuda_fail(e, "rfx_forest_load upload");
+        }
+        c->loaded = true;
+        return RFX_OK;
+    } catch (const std::bad_alloc&) {
+        set_error("rfx_forest_load: host allocation failed");
+        return RFX_ERR_OOM;
+    } catch (const std::exception& ex) {
+        set_error(std::string("rfx_forest_load: ") + ex.what());
+        return RFX_ERR_INVALID;
+    }
+}
+
+static rfx_status need_forest(Ctx* c) {
+    if (!c) {
+        set_error("null context");
+        return RFX_ERR_INVALID;
+    }
+    if (!c->loaded) {
+        set_error("no forest loaded");
+        return RFX_ERR_STATE;
+    }
+    cudaSetDevice(c->device);
+    return RFX_OK;
+}
+
+rfx_status rfx_route_oob(rfx_ctx* ctx, int32_t* q, int32_t* nout, int32_t* leaf) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    bool any_host = false;
+    if (leaf) {
+        int32_t* dleaf = leaf;
+        const bool dev = is_device_ptr(leaf);
+        if (!dev) {
+            if ((st = dalloc(c, &c->d_joob, (size_t)c->T * c->n))) return st;  // reuse as staging
+            dleaf = c->d_joob;
+        }
+        if ((st = launch_route_leaf(c, dleaf))) return st;
+        RFX_CUDA(cudaGetLastError());
+        if (!dev) {
+            if ((st = copy_out(c, leaf, dleaf, sizeof(int32_t) * (size_t)c->T * c->n))) return st;
+            any_host = true;
+        }
+        // nout is produced by launch_route; run it as well (cheap)
+    }
+    if ((st = launch_route(c))) return st;
+    c->routed = true;
+    c->csr_built = false;
+    if (q) {
+        any_host |= !is_device_ptr(q);
+        if ((st = copy_out(c, q, c->d_votes, sizeof(int32_t) * (size_t)c->n * c->nclass))) return st;
+    }
+    if (nout) {
+        any_host |= !is_device_ptr(nout);
+        if ((st = copy_out(c, nout, c->d_nout, sizeof(int32_t) * (size_t)c->n))) return st;
+    }
+    return finish_host(c, any_host);
+}
+
+rfx_status rfx_oob_summary(rfx_ctx* ctx, float* oob_error, int32_t* pred, float* proba) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!c->routed) {
+        if ((st = launch_route(c))) return st;
+        c->routed = true;
+    }
+    float* d_e = nullptr;
+    int32_t* d_p = nullptr;
+    float* d_pr = nullptr;
+    const bool he = oob_error && !is_device_ptr(oob_error);
+    const bool hp = pred && !is_device_ptr(pred);
+    const bool hpr = proba && !is_device_ptr(proba);
+    std::vector<void*> tmp;
+    auto tmpalloc = [&](size_t bytes) -> void* {
+        void* d = nullptr;
+        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        tmp.push_back(d);
+        return d;
+    };
+    d_e = he ? (float*)tmpalloc(sizeof(float)) : oob_error;
+    d_p = hp ? (int32_t*)tmpalloc(sizeof(int32_t) * c->n) : pred;
+    d_pr = hpr ? (float*)tmpalloc(sizeof(float) * (size_t)c->n * c->nclass) : proba;
+    if ((he && !d_e) || (hp && !d_p) || (hpr && !d_pr)) {
+        for (void* d : tmp) cudaFree(d);
+        set_error("rfx_oob_summary: staging allocation failed");
+        return RFX_ERR_OOM;
+    }
+    st = launch_oob_summary(c, d_e, d_p, d_pr);
+    if (st == RFX_OK && he) st = copy_out(c, oob_error, d_e, sizeof(float));
+    if (st == RFX_OK && hp) st = copy_out(c, pred, d_p, sizeof(int32_t) * c->n);
+    if (st == RFX_OK && hpr) st = copy_out(c, proba, d_pr, sizeof(float) * (size_t)c->n * c->nclass);
+    if (st == RFX_OK) st = finish_host(c, he || hp || hpr);
+    cudaStreamSynchronize(c->stream);
+    for (void* d : tmp) cudaFree(d);
+    return st;
+}
+
+rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!S || len != (size_t)upper_len(c->n)) {
+        set_error("rfx_proximity_upper_i32: S must hold n(n+1)/2 entries");
+        return RFX_ERR_INVALID;
+    }
+    const bool dev = is_device_ptr(S);
+    int32_t* dS = S;
+    if (!dev) {
+        cudaError_t e = cudaMalloc((void**)&dS, sizeof(int32_t) * len);
+        if (e != cudaSuccess) return cuda_fail(e, "rfx_proximity_upper_i32 staging");
+    }
+    // every call does the full pass: routing, per-tree leaf lists, pair counts
+    st = launch_route(c);
+    if (st == RFX_OK) st = launch_build_csr(c);
+    if (st == RFX_OK) st = launch_pairs_upper(c, dS);
+    if (st == RFX_OK) {
+        c->routed = true;
+        c->csr_built = true;
+    }
+    if (st == RFX_OK && !dev) {
+        st = copy_out(c, S, dS, sizeof(int32_t) * len);
+        if (st == RFX_OK) st = finish_host(c, true);
+    }
+    if (!dev) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(dS);
+    }
+    return st;
+}
+
+rfx_status rfx_pair_updates(rfx_ctx* ctx, int64_t* count) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!count) return RFX_ERR_INVALID;
+    unsigned long long v = 0;
+    RFX_CUDA(cudaStreamSynchronize(c->stream));
+    RFX_CUDA(cudaMemcpy(&v, c->d_pairs, sizeof(v), cudaMemcpyDeviceToHost));
+    *count = (int64_t)v;
+    return RFX_OK;
+}
+
+rfx_status rfx_finishprox(rfx_ctx* ctx, const int32_t* S, float* P, int full) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!S || !P) {
+        set_error("rfx_finishprox: null argument");
+        return RFX_ERR_INVALID;
+    }
+    if (!c->routed) {
+        if ((st = launch_route(c))) return st;
+        c->routed = true;
+    }
+    const size_t slen = (size_t)upper_len(c->n);
+    const size_t plen = full ? (size_t)c->n * c->n : slen;
+    const bool sdev = is_device_ptr(S), pdev = is_device_ptr(P);
+    const int32_t* dS = S;
+    float* dP = P;
+    int32_t* sS = nullptr;
+    if (!sdev) {
+        cudaError_t e = cudaMalloc((void**)&sS, sizeof(int32_t) * slen);
+        if (e != cudaSuccess) return cuda_fail(e, "rfx_finishprox staging");
+        e = cudaMemcpyAsync(sS, S, sizeof(int32_t) * slen, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) {
+            cudaFree(sS);
+            return cuda_fail(e, "rfx_finishprox H2D");
+        }
+        dS = sS;
+    }
+    if (!pdev) {
+        cudaError_t e = cudaMalloc((void**)&dP, sizeof(float) * plen);
+        if (e != cudaSuccess) {
+            if (sS) cudaFree(sS);
+            return cuda_fail(e, "rfx_finishprox staging");
+        }
+    }
+    st = launch_finishprox(c, dS, dP, full);
+    if (st == RFX_OK && !pdev) st = copy_out(c, P, dP, sizeof(float) * plen);
+    if (st == RFX_OK) st = finish_host(c, !sdev || !pdev);
+    if (!sdev || !pdev) cudaStreamSynchronize(c->stream);
+    if (sS) cudaFree(sS);
+    if (!pdev) cudaFree(dP);
+    return st;
+}
+
+rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* qimp, float* qimpm) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    const int T = c->T, n = c->n, p = c->p, W = c->iv_words;
+    if (W > 4) {
+        set_error("rfx_varimp supports at most 256 features");
+        return RFX_ERR_UNSUPPORTED;
+    }
+#define ALLOC(ptr, cnt) \
+    if (st == RFX_OK) st = dalloc(c, &c->ptr, (size_t)(cnt));
+    ALLOC(d_joob, (size_t)T * n);
+    ALLOC(d_vflags, (size_t)T * n);
+    ALLOC(d_flips, (size_t)T * n * W);
+    ALLOC(d_right, T);
+    ALLOC(d_rightimp, (size_t)T * p);
+    ALLOC(d_qimp, n);
+    ALLOC(d_qimpm, (size_t)n * p);
+    ALLOC(d_avimp, p);
+    ALLOC(d_sqsd, p);
+#undef ALLOC
+    if (st) return st;
+    if ((st = launch_varimp(c, impn ? 1 : 0))) return st;
+    bool any_host = false;
+    auto out = [&](float* dst, const float* src, size_t cnt) -> rfx_status {
+        if (!dst) return RFX_OK;
+        any_host |= !is_device_ptr(dst);
+        return copy_out(c, dst, src, sizeof(float) * cnt);
+    };
+    if ((st = out(avimp, c->d_avimp, p))) return st;
+    if ((st = out(sqsd, c->d_sqsd, p))) return st;
+    if (impn) {
+        if ((st = out(qimp, c->d_qimp, n))) return st;
+        if ((st = out(qimpm, c->d_qimpm, (size_t)n * p))) return st;
+    }
+    return finish_host(c, any_host);
+}
+
+rfx_status rfx_localimp(rfx_ctx* ctx, const float* qimp, const float* qimpm, float* outp) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!qimp || !qimpm || !outp) return RFX_ERR_INVALID;
+    const size_t np = (size_t)c->n * c->p;
+    std::vector<void*> tmp;
+    auto stage_in = [&](const float* h, size_t cnt) -> const float* {
+        if (is_device_ptr(h)) return h;
+        float* d = nullptr;
+        if (cudaMalloc((void**)&d, sizeof(float) * cnt) != cudaSuccess) return nullptr;
+        tmp.push_back(d);
+        cudaMemcpyAsync(d, h, sizeof(float) * cnt, cudaMemcpyHostToDevice, c->stream);
+        return d;
+    };
+    const float* dq = stage_in(qimp, c->n);
+    const float* dqm = stage_in(qimpm, np);
+    const bool odev = is_device_ptr(outp);
+    float* dout = outp;
+    if (!odev) {
+        if (cudaMalloc((void**)&dout, sizeof(float) * np) != cudaSuccess) dout = nullptr;
+        else tmp.push_back(dout);
+    }
+    if (!dq || !dqm || !dout) {
+        cudaGetLastError();
+        cudaStreamSynchronize(c->stream);
+        for (void* d : tmp) cudaFree(d);
+        set_error("rfx_localimp: staging allocation failed");
+        return RFX_ERR_OOM;
+    }
+    st = launch_localimp(c, dq, dqm, dout);
+    if (st == RFX_OK && !odev) st = copy_out(c, outp, dout, sizeof(float) * np);
+    if (st == RFX_OK) st = finish_host(c, !tmp.empty());
+    cudaStreamSynchronize(c->stream);
+    for (void* d : tmp) cudaFree(d);
+    return st;
+}
+
+rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (m < 0 || (!X && m > 0) || !votes) return RFX_ERR_INVALID;
+    const bool xdev = is_device_ptr(X), vdev = is_device_ptr(votes);
+    const float* dX = X;
+    int32_t* dv = votes;
+    std::vector<void*> tmp;
+    if (!xdev && m > 0) {
+        float* d = nullptr;
+        cudaError_t e = cudaMalloc((void**)&d, sizeof(float) * (size_t)m * c->p);
+        if (e != cudaSuccess) return cuda_fail(e, "rfx_predict staging");
+        tmp.push_back(d);
+        cudaMemcpyAsync(d, X, sizeof(float) * (size_t)m * c->p, cudaMemcpyHostToDevice, c->stream);
+        dX = d;
+    }
+    if (!vdev) {
+        int32_t* d = nullptr;
+        cudaError_t e = cudaMalloc((void**)&d, sizeof(int32_t) * std::max<size_t>(1, (size_t)m * c->nclass));
+        if (e != cudaSuccess) {
+            for (void* q : tmp) cudaFree(q);
+            return cuda_fail(e, "rfx_predict staging");
+        }
+        tmp.push_back(d);
+        dv = d;
+    }
+    st = launch_predict(c, dX, m, dv);
+    if (st == RFX_OK && !vdev) st = copy_out(c, votes, dv, sizeof(int32_t) * (size_t)m * c->nclass);
+    if (st == RFX_OK) st = finish_host(c, !tmp.empty());
+    cudaStreamSynchronize(c->stream);
+    for (void* q : tmp) cudaFree(q);
+    return st;
+}
+
+rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return RFX_ERR_INVALID;
+    cudaSetDevice(c->device);
+    RFX_CUDA(cudaStreamSynchronize(c->stream));
+    if (enable && c->ev_start[0].empty()) {
+        for (int s = 0; s < ST_COUNT; ++s) {
+            c->ev_start[s].resize(Ctx::EV_RING);
+            c->ev_end[s].resize(Ctx::EV_RING);
+            for (int k = 0; k < Ctx::EV_RING; ++k) {
+                RFX_CUDA(cudaEventCreate(&c->ev_start[s][k]));
+                RFX_CUDA(cudaEventCreate(&c->ev_end[s][k]));
+            }
+        }
+    }
+    for (int s = 0; s < ST_COUNT; ++s) c->ev_count[s] = 0;
+    c->profile = enable != 0;
+    return RFX_OK;
+}
+
+rfx_status rfx_profile_read(rfx_ctx* ctx, float* stage_ms, int64_t* kernel_launches) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c) return RFX_ERR_INVALID;
+    cudaSetDevice(c->device);
+    RFX_CUDA(cudaStreamSynchronize(c->stream));
+    if (stage_ms) {
+        for (int s = 0; s < ST_COUNT; ++s) {
+            stage_ms[s] = -1.0f;
+            const long long cnt = std::min<long long>(c->ev_count[s], Ctx::EV_RING);
+            if (cnt <= 0 || c->ev_start[s].empty()) continue;
+            double sum = 0.0;
+            int good = 0;
+            for (int k = 0; k < cnt; ++k) {
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, c->ev_start[s][k], c->ev_end[s][k]) == cudaSuccess) {
+                    sum += ms;
+                    ++good;
+                } else {
+                    cudaGetLastError();
+                }
+            }
+            if (good) stage_ms[s] = (float)(sum / good);
+        }
+    }
+    if (kernel_launches) *kernel_launches = c->launches;
+    return RFX_OK;
+}
+
+rfx_status rfx_grow_forest(const float* X, const int32_t* y, int32_t n, int32_t p, int32_t nclass, int32_t ntree,
+                           int32_t mtry, int32_t minndsize, int32_t maxnode, int32_t iseed, int32_t n_threads,
+                           rfx_grown_forest* out) {
+    if (!X || !y || !out || n < 1 || p < 1 || nclass < 1 || ntree < 1 || mtry < 1 || minndsize < 1) {
+        set_error("rfx_grow_forest: invalid argument");
+        return RFX_ERR_INVALID;
+    }
+    try {
+        std::memset(out, 0, sizeof(*out));
+        std::vector<int64_t> offs;
+        std::vector<int32_t> ns, bv, tm, nc;
+        std::vector<float> xs;
+        int32_t* nin = (int32_t*)std::malloc(sizeof(int32_t) * (size_t)ntree * n);
+        if (!nin) return RFX_ERR_OOM;
+        const int mx = maxnode > 0 ? maxnode : 2 * n + 1;
+        rfxhost::grow_forest(X, y, n, p, nclass, ntree, mtry, minndsize, mx, iseed, n_threads, offs, ns, bv, xs, tm,
+                             nc, nin);
+        auto dup = [](const auto& vec) {
+            using T = typename std::decay_t<decltype(vec)>::value_type;
+            T* d = (T*)std::malloc(sizeof(T) * std::max<size_t>(1, vec.size()));
+            if (d) std::copy(vec.begin(), vec.end(), d);
+            return d;
+        };
+        out->ntree = ntree;
+        out->offs = dup(offs);
+        out->nodestatus = dup(ns);
+        out->bestvar = dup(bv);
+        out->xbestsplit = dup(xs);
+        out->treemap = dup(tm);
+        out->nodeclass = dup(nc);
+        out->nin = nin;
+        if (!out->offs || !out->nodestatus || !out->bestvar || !out->xbestsplit || !out->treemap || !out->nodeclass) {
+            rfx_free_forest(out);
+            return RFX_ERR_OOM;
+        }
+        return RFX_OK;
+    } catch (const std::bad_alloc&) {
+        set_error("rfx_grow_forest: host allocation failed");
+        return RFX_ERR_OOM;
+    }
+}
+
+rfx_status rfx_free_forest(rfx_grown_forest* f) {
+    if (!f) return RFX_OK;
+    std::free(f->offs);
+    std::free(f->nodestatus);
+    std::free(f->bestvar);
+    std::free(f->xbestsplit);
+    std::free(f->treemap);
+    std::free(f->nodeclass);
+    std::free(f->nin);
+    std::memset(f, 0, sizeof(*f));
+    return RFX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,316 @@
+// Exact proximity pair counts.
+//
+// Per tree t, the samples of every terminal node ("leaf") are split into an
+// out-of-bag list and an in-bag list.  cpu_proximity's dense branch
+// (src/rf_proximity.cpp:173-230) adds 1 to C[i][j] for every OOB i and in-bag j
+// of the same leaf.  Here S = C + C^T is produced directly in its packed
+// upper-triangle form.
+//
+// Stage 1 (build_csr_kernel, one warp per tree): a stable counting sort of the
+//   tree's samples by key = 2*leaf + inbag.  seg[t][k] .. seg[t][k+1] is the
+//   member range of key k in memb[t*n ...], members ascending by sample id.
+//   A single warp walks the samples in order, so equal keys keep index order.
+// Stage 2 (pairs_row_kernel, row-owner): one CTA owns row i of S restricted to
+//   a column window; for every tree it binary-searches, in the member list of
+//   the opposite bag status of i's leaf, the members j in (i, window) and adds 1
+//   to a shared-memory accumulator per member; the accumulated row segment is
+//   then written once, coalesced.  Work is proportional to the pair updates,
+//   and S is written exactly once.
+#include "rfx_internal.cuh"
+
+#include <algorithm>
+
+namespace rfx {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Stage 1
+// ---------------------------------------------------------------------------
+constexpr int CSR_PREFETCH = 4;  // 32-sample groups loaded ahead per lane
+
+__global__ void __launch_bounds__(32)
+build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restrict__ segbase,
+                 int32_t* __restrict__ segoff, int32_t* __restrict__ memb, int smem_keys,
+                 uint32_t* __restrict__ err) {
+    extern __shared__ int32_t cnt[];
+    const int t = blockIdx.x;
+    const int lane = threadIdx.x;
+    const int64_t sb = segbase[t];
+    const int K = (int)(segbase[t + 1] - sb) - 1;  // number of keys of this tree
+    const int32_t* kt = key + (size_t)t * n;
+    int32_t* mt = memb + (size_t)t * n;
+    int32_t* so = segoff + sb;
+    // counters: shared memory when the key table fits, else the tree's own
+    // segment-offset table in global memory
+    const bool use_smem = K + 1 <= smem_keys;
+    int32_t* ctr = use_smem ? cnt : so;  // global-counter path: slower, still exact
+    for (int k = lane; k <= K; k += 32) ctr[k] = 0;
+    __syncwarp();
+    // histogram
+    for (int base = 0; base < n; base += 32 * CSR_PREFETCH) {
+        int kv[CSR_PREFETCH];
+#pragma unroll
+        for (int u = 0; u < CSR_PREFETCH; ++u) {
+            const int i = base + u * 32 + lane;
+            kv[u] = i < n ? __ldg(kt + i) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < CSR_PREFETCH; ++u)
+            if (kv[u] >= 0) atomicAdd(ctr + kv[u], 1);
+    }
+    __syncwarp();
+    // exclusive scan over K+1 counters (the last one is 0 and becomes the total)
+    int carry = 0;
+    for (int k0 = 0; k0 <= K; k0 += 32) {
+        const int k = k0 + lane;
+        int v = k <= K ? ctr[k] : 0;
+        int incl = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        const int excl = carry + incl - v;
+        if (k <= K) {
+            ctr[k] = excl;
+            if (use_smem) so[k] = excl;
+        }
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+    // stable scatter: one warp, samples in index order; equal keys inside a
+    // 32-sample group are ranked by lane (= index) order
+    for (int base = 0; base < n; base += 32 * CSR_PREFETCH) {
+        int kv[CSR_PREFETCH];
+#pragma unroll
+        for (int u = 0; u < CSR_PREFETCH; ++u) {
+            const int i = base + u * 32 + lane;
+            kv[u] = i < n ? __ldg(kt + i) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < CSR_PREFETCH; ++u) {
+            const int i = base + u * 32 + lane;
+            const int k = kv[u];
+            const unsigned grp = __match_any_sync(0xffffffffu, k);
+            const int leader = __ffs(grp) - 1;
+            const int rank = __popc(grp & ((1u << lane) - 1u));
+            int start = 0;
+            if (k >= 0 && lane == leader) {
+                start = ctr[k];
+                ctr[k] = start + __popc(grp);
+            }
+            start = __shfl_sync(0xffffffffu, start, leader);
+            if (k >= 0) mt[start + rank] = i;
+            __syncwarp();
+        }
+    }
+    // global-counter path: the counters now hold segment ends; a follow-up
+    // kernel (fix_global_segoff_kernel) turns them back into starts
+}
+
+// Fallback pass for trees whose key table did not fit in shared memory:
+// rebuild segment starts from the ends left by the scatter (start[k] = end[k-1]).
+__global__ void fix_global_segoff_kernel(const int64_t* __restrict__ segbase, int32_t* __restrict__ segoff,
+                                         int smem_keys) {
+    const int t = blockIdx.x;
+    const int64_t sb = segbase[t];
+    const int K = (int)(segbase[t + 1] - sb) - 1;
+    if (K + 1 <= smem_keys) return;
+    if (threadIdx.x != 0) return;
+    int32_t* so = segoff + sb;
+    for (int k = K; k >= 1; --k) so[k] = so[k - 1];
+    so[0] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2
+// ---------------------------------------------------------------------------
+constexpr int ROW_THREADS = 512;
+constexpr int ROW_WARPS = ROW_THREADS / 32;
+
+__device__ __forceinline__ int lower_bound_i32(const int32_t* __restrict__ a, int lo, int hi, int v) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(ROW_THREADS)
+pairs_row_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ segoff,
+                 const int64_t* __restrict__ segbase, const int32_t* __restrict__ memb, int n, int T,
+                 int win, int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+    extern __shared__ uint32_t acc[];
+    __shared__ int pref[ROW_WARPS][33];
+    __shared__ long long segb[ROW_WARPS][32];
+    const int i = blockIdx.x;
+    const int c0 = blockIdx.y * win;
+    if (c0 >= n) return;
+    const int c1 = min(n, c0 + win);
+    if (c1 <= i) return;  // window entirely left of the diagonal
+    const int lo_col = max(i + 1, c0);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int width = c1 - c0;
+    for (int k = tid; k < width; k += ROW_THREADS) acc[k] = 0u;
+    __syncthreads();
+    unsigned long long my_pairs = 0;
+    for (int t0 = w * 32; t0 < T; t0 += ROW_WARPS * 32) {
+        const int t = t0 + lane;
+        long long b = 0;
+        int len = 0;
+        if (t < T && lo_col < c1) {
+            const int k = __ldg(key + (size_t)t * n + i);
+            if (k >= 0) {
+                const int ok = k ^ 1;  // the opposite bag status in the same leaf
+                const int32_t* so = segoff + segbase[t];
+                const int s0 = __ldg(so + ok), s1 = __ldg(so + ok + 1);
+                const int32_t* mt = memb + (size_t)t * n;
+                int bb = s0, ee = s1;
+                if (s1 > s0) {
+                    bb = lower_bound_i32(mt, s0, s1, lo_col);
+                    ee = (c1 >= n) ? s1 : lower_bound_i32(mt, bb, s1, c1);
+                }
+                b = (long long)t * n + bb;  // absolute index into memb
+                len = ee - bb;
+            }
+        }
+        // warp-level load-balanced expansion of the 32 member ranges
+        int incl = len;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        pref[w][lane + 1] = incl;
+        if (lane == 0) pref[w][0] = 0;
+        segb[w][lane] = b;
+        __syncwarp();
+        for (int pos = lane; pos < total; pos += 32) {
+            // find the range s with pref[s] <= pos < pref[s+1]
+            int lo = 0, hi = 32;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (pref[w][mid] <= pos) lo = mid;
+                else hi = mid;
+            }
+            const int j = __ldg(memb + (size_t)segb[w][lo] + (pos - pref[w][lo]));
+            atomicAdd(acc + (j - c0), 1u);
+        }
+        my_pairs += (unsigned long long)len;
+        __syncwarp();
+    }
+    __syncthreads();
+    // write row i, columns [max(i, c0), c1) of the packed upper triangle
+    const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
+    for (int j = max(i, c0) + tid; j < c1; j += ROW_THREADS) S[rowoff + j] = (int32_t)acc[j - c0];
+    if (pairs) {
+        // block reduction of the pair-update count
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
+        if (lane == 0 && my_pairs) atomicAdd(pairs, my_pairs);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// finishprox
+// ---------------------------------------------------------------------------
+constexpr int FP_TILE = 32;
+
+__device__ __forceinline__ double fp_value(int32_t s, double inv_i, double inv_j, bool sc_i, bool sc_j) {
+    const double h = __ddiv_rn((double)s, 2.0);
+    const double a = sc_i ? __dmul_rn(h, inv_i) : h;
+    const double b = sc_j ? __dmul_rn(h, inv_j) : h;
+    return __dmul_rn(0.5, __dadd_rn(a, b));
+}
+
+// One CTA per (I, J) tile with I <= J; computes the 32x32 values from the
+// packed S rows of tile I and writes tile (I, J) and its mirror (J, I) of the
+// full matrix, or tile (I, J) of the packed triangle.
+__global__ void __launch_bounds__(FP_TILE * 8)
+finishprox_kernel(const int32_t* __restrict__ S, const int32_t* __restrict__ nout, int n, int full,
+                  float* __restrict__ P) {
+    __shared__ float tile[FP_TILE][FP_TILE + 1];
+    const int I = blockIdx.y, J = blockIdx.x;
+    if (J < I) return;
+    const int tx = threadIdx.x % FP_TILE, ty = threadIdx.x / FP_TILE;  // 32 x 8
+    const int j = J * FP_TILE + tx;
+    const bool jv = j < n;
+    const int nj = jv ? nout[j] : 0;
+    const double inv_j = nj > 0 ? __ddiv_rn(1.0, (double)nj) : 1.0;
+    for (int r = ty; r < FP_TILE; r += 8) {
+        const int i = I * FP_TILE + r;
+        float v = 0.0f;
+        if (i < n && jv && j >= i) {
+            const int ni = nout[i];
+            const double inv_i = ni > 0 ? __ddiv_rn(1.0, (double)ni) : 1.0;
+            const int64_t idx = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 + (j - i);
+            double d = (j == i) ? 1.0 : fp_value(S[idx], inv_i, inv_j, ni > 0, nj > 0);
+            v = __double2float_rn(d);
+            if (full) P[(size_t)i * n + j] = v;
+            else P[idx] = v;
+        }
+        tile[r][tx] = v;
+    }
+    if (!full) return;
+    __syncthreads();
+    // mirror: P[j][i] for j in tile J rows, i in tile I columns (strictly lower part)
+    for (int r = ty; r < FP_TILE; r += 8) {
+        const int jj = J * FP_TILE + r;
+        const int ii = I * FP_TILE + tx;
+        if (jj < n && ii < n && jj > ii) P[(size_t)jj * n + ii] = tile[tx][r];
+    }
+}
+
+}  // namespace
+
+rfx_status launch_build_csr(Ctx* c) {
+    int dev_smem = 0;
+    RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    // budget per tree-warp; several warps (trees) share an SM
+    int smem_keys = std::min(c->max_keys + 1, (dev_smem - 1024) / 4);
+    smem_keys = std::max(smem_keys, 32);
+    const size_t smem = (size_t)smem_keys * sizeof(int32_t);
+    StageTimer st(c, ST_CSR, c->max_keys + 1 > smem_keys ? 2 : 1);
+    RFX_CUDA(cudaFuncSetAttribute(build_csr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    build_csr_kernel<<<c->T, 32, smem, c->stream>>>(c->d_key, c->n, c->d_segbase, c->d_segoff, c->d_memb, smem_keys,
+                                                    c->d_err);
+    RFX_CUDA(cudaGetLastError());
+    if (c->max_keys + 1 > smem_keys) {
+        fix_global_segoff_kernel<<<c->T, 32, 0, c->stream>>>(c->d_segbase, c->d_segoff, smem_keys);
+        RFX_CUDA(cudaGetLastError());
+    }
+    return RFX_OK;
+}
+
+int pairs_window(const Ctx* c) {
+    // columns per CTA: 96 KB of u32 accumulators (two CTAs per SM)
+    const int win_max = 24 * 1024;
+    return std::min(c->n, win_max);
+}
+
+rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
+    const int win = pairs_window(c);
+    const size_t smem = (size_t)win * sizeof(uint32_t);
+    RFX_CUDA(cudaFuncSetAttribute(pairs_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
+    StageTimer st(c, ST_PAIRS, 1);
+    dim3 grid(c->n, (c->n + win - 1) / win);
+    pairs_row_kernel<<<grid, ROW_THREADS, smem, c->stream>>>(c->d_key, c->d_segoff, c->d_segbase, c->d_memb, c->n,
+                                                             c->T, win, dS, c->d_pairs);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full) {
+    StageTimer st(c, ST_FINISHPROX, 1);
+    const int nt = (c->n + FP_TILE - 1) / FP_TILE;
+    dim3 grid(nt, nt);
+    finishprox_kernel<<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+}  // namespace rfx

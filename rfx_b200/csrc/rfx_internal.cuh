@@ -1,0 +1,170 @@
+// Internal declarations shared by the CUDA translation units of librfx_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rfx_b200.h"
+
+namespace rfx {
+
+// Device node record (16 bytes, one int4 load per traversal step):
+//   x = split threshold (float bits), y = left child, z = right child,
+//   w = var (bits 0..15) | status as int8 (bits 16..23) | categorical (bit 24).
+// Node ids are local to their tree.
+struct __align__(16) DNode {
+    float split;
+    int32_t left;
+    int32_t right;
+    int32_t meta;
+};
+
+__host__ __device__ inline int node_var(int32_t meta) { return meta & 0xffff; }
+__host__ __device__ inline int node_status(int32_t meta) { return (int)(int8_t)((meta >> 16) & 0xff); }
+__host__ __device__ inline bool node_cat(int32_t meta) { return (meta >> 24) & 1; }
+
+// Error bits raised by kernels into ctx->d_err (checked by the host after sync).
+enum : uint32_t {
+    ERR_STALE_JVR = 1u,       // testreeimp broke without assigning (stale jvr in the reference)
+    ERR_TRAVERSAL_LIMIT = 2u, // a bounded walk hit its step limit
+    ERR_SMEM_KEYS = 4u,       // per-tree key table exceeded its shared-memory budget
+};
+
+enum Stage : int {
+    ST_ROUTE = 0, ST_CSR, ST_PAIRS, ST_FINISHPROX, ST_VARIMP_TREE, ST_VARIMP_SAMPLE, ST_VARIMP_FEATURE,
+    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_COUNT
+};
+
+struct Ctx {
+    int device = 0;
+    bool profile = false;
+    static constexpr int EV_RING = 64;  // launches remembered per stage
+    std::vector<cudaEvent_t> ev_start[ST_COUNT];
+    std::vector<cudaEvent_t> ev_end[ST_COUNT];
+    long long ev_count[ST_COUNT] = {};
+    long long launches = 0;
+    cudaStream_t stream = nullptr;
+    rfx_config cfg{};
+
+    // forest
+    bool loaded = false;
+    int n = 0, p = 0, nclass = 0, maxcat = 0, T = 0;
+    int64_t N = 0;                      // total nodes
+    std::vector<int64_t> h_offs;        // T+1
+    std::vector<int32_t> h_nnode;       // T
+    std::vector<int32_t> h_nleaf;       // T: terminal nodes per tree
+    std::vector<int64_t> h_segbase;     // T+1: start of each tree's key-offset table
+    std::vector<int32_t> h_noob;        // T
+    int max_keys = 0;                   // max_t 2*nleaf_t
+    int max_nnode = 0;
+    int iv_words = 0;                   // ceil(p / 64)
+
+    float* d_X = nullptr;               // n*p
+    int32_t* d_y = nullptr;             // n
+    int32_t* d_cat = nullptr;           // p
+    DNode* d_nodes = nullptr;           // N
+    int32_t* d_nodeclass = nullptr;     // N
+    int32_t* d_leafidx = nullptr;       // N: dense terminal index (node order) or -1
+    int32_t* d_catgoleft = nullptr;     // N*maxcat or null
+    int64_t* d_offs = nullptr;          // T+1
+    int32_t* d_nnode = nullptr;         // T
+    uint8_t* d_inbag = nullptr;         // T*n
+    int64_t* d_segbase = nullptr;       // T+1
+    uint64_t* d_iv = nullptr;           // T*iv_words: features used by non-terminal nodes
+    int32_t* d_noob = nullptr;          // T
+    int32_t* d_permoff = nullptr;       // T: offset of the tree's permutation in d_perm
+    int32_t* d_perm = nullptr;          // concatenated permutations per distinct noob
+    float* d_invnoob = nullptr;         // T: 1.0f / noob
+
+    // analysis scratch (allocated lazily)
+    int32_t* d_key = nullptr;           // T*n: 2*leafidx + inbag, or -1
+    int32_t* d_segoff = nullptr;        // segbase[T]: per-tree key offsets (+1 sentinel each)
+    int32_t* d_memb = nullptr;          // T*n: members grouped by key, ascending within a key
+    int32_t* d_votes = nullptr;         // n*nclass
+    int32_t* d_nout = nullptr;          // n
+    uint32_t* d_err = nullptr;          // error bits
+    unsigned long long* d_pairs = nullptr;  // pair-update counter
+    bool routed = false;
+    bool csr_built = false;
+    int64_t last_pairs = 0;
+
+    // varimp scratch
+    int32_t* d_joob = nullptr;          // T*n
+    uint8_t* d_vflags = nullptr;        // T*n: bit1 testreebag correct, bit2 testreeimp correct
+    uint64_t* d_flips = nullptr;        // T*n*iv_words
+    int32_t* d_right = nullptr;         // T
+    int32_t* d_rightimp = nullptr;      // T*p
+    float* d_qimp = nullptr;            // n (internal accumulators)
+    float* d_qimpm = nullptr;           // n*p
+    float* d_avimp = nullptr;           // p
+    float* d_sqsd = nullptr;            // p
+
+    size_t bytes = 0;                   // device bytes held
+};
+
+// RAII stage bracket: records events around a stage when profiling is on and
+// counts the kernels the stage launches.
+struct StageTimer {
+    Ctx* c;
+    int s;
+    int slot = -1;
+    StageTimer(Ctx* c_, int s_, int kernels) : c(c_), s(s_) {
+        c->launches += kernels;
+        if (c->profile && !c->ev_start[s].empty()) {
+            slot = (int)(c->ev_count[s] % Ctx::EV_RING);
+            cudaEventRecord(c->ev_start[s][slot], c->stream);
+        }
+    }
+    ~StageTimer() {
+        if (slot >= 0) {
+            cudaEventRecord(c->ev_end[s][slot], c->stream);
+            c->ev_count[s]++;
+        }
+    }
+};
+
+// error helpers (thread-local message)
+void set_error(const std::string& msg);
+rfx_status cuda_fail(cudaError_t e, const char* what);
+
+#define RFX_CUDA(call)                                         \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return ::rfx::cuda_fail(e_, #call); \
+    } while (0)
+
+// device allocation tracked in ctx->bytes
+template <typename T>
+rfx_status dalloc(Ctx* c, T** p, size_t count) {
+    if (*p) return RFX_OK;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        set_error(std::string("device allocation of ") + std::to_string(count * sizeof(T)) + " bytes failed: " +
+                  cudaGetErrorString(e));
+        return RFX_ERR_OOM;
+    }
+    c->bytes += count * sizeof(T);
+    return RFX_OK;
+}
+
+bool is_device_ptr(const void* p);
+
+// kernel launchers (each returns after enqueueing on ctx->stream)
+rfx_status launch_route(Ctx* c);
+rfx_status launch_build_csr(Ctx* c);
+rfx_status launch_pairs_upper(Ctx* c, int32_t* dS);
+rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full);
+rfx_status launch_oob_summary(Ctx* c, float* d_err_out, int32_t* d_pred, float* d_proba);
+rfx_status launch_varimp(Ctx* c, int impn);
+rfx_status launch_localimp(Ctx* c, const float* d_qimp, const float* d_qimpm, float* d_out);
+rfx_status launch_predict(Ctx* c, const float* dX, int m, int32_t* d_votes);
+rfx_status check_device_errors(Ctx* c);
+
+inline int64_t upper_len(int64_t n) { return n * (n + 1) / 2; }
+
+}  // namespace rfx

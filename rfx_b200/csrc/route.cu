@@ -1,0 +1,168 @@
+// Leaf routing of every (tree, sample): OOB samples with the testreebag walk
+// (their votes go to q), in-bag samples with find_terminal_node.  The output
+// key feeds the pair-count kernels:
+//   key = 2 * leafidx + (in-bag ? 1 : 0)   when the node is terminal,
+//   key = -1                               otherwise (excluded from proximity,
+//                                          as nod[] = -1 excludes it in
+//                                          cpu_proximity, src/rf_proximity.cpp:114-136).
+// Grid: x = sample chunk, y = tree, so CTAs resident at the same time work on
+// the same few trees and their node arrays stay in L2.
+#include "walks.cuh"
+
+namespace rfx {
+
+namespace {
+
+constexpr int ROUTE_THREADS = 256;
+
+__global__ void __launch_bounds__(ROUTE_THREADS)
+route_kernel(const float* __restrict__ X, int n, int p, int nclass, const DNode* __restrict__ nodes,
+             const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
+             const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+             const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
+             const int32_t* __restrict__ catgoleft, int maxcat, int32_t* __restrict__ key_out,
+             int32_t* __restrict__ leaf_out, int32_t* __restrict__ votes) {
+    const int t = blockIdx.y;
+    const int i = blockIdx.x * ROUTE_THREADS + threadIdx.x;
+    if (i >= n) return;
+    const int64_t o = offs[t];
+    const DNode* tn = nodes + o;
+    const int32_t* tc = nodeclass + o;
+    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+    const int nn = nnode_arr[t];
+    const float* xrow = X + (size_t)i * p;
+    const size_t ti = (size_t)t * n + i;
+    const bool ib = inbag[ti] != 0;
+    int node;
+    if (!ib) {
+        int cls;
+        node = walk_testreebag(xrow, p, tn, tc, nn, cat, cgl, maxcat, &cls);
+        if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
+    } else {
+        node = walk_terminal(xrow, p, tn, cat, cgl, maxcat, 2 * n + 1);
+    }
+    const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
+    key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
+    if (leaf_out) leaf_out[ti] = node;
+}
+
+// nout[i] = 2 * (number of trees with i out of bag): the reference increments
+// it in cpu_bootstrap and again in the vote loop.
+__global__ void nout_kernel(const uint8_t* __restrict__ inbag, int n, int T, int32_t* __restrict__ nout) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = 0;
+    for (int t = 0; t < T; ++t) c += inbag[(size_t)t * n + i] == 0;
+    nout[i] = 2 * c;
+}
+
+// OOB error / prediction / probability from integer votes, with the
+// reference's float arithmetic: argmax with >= (ties to the higher class),
+// total votes summed in float, probability = q / total (or 1/nclass).
+__global__ void oob_summary_kernel(const int32_t* __restrict__ votes, const int32_t* __restrict__ nout,
+                                   const int32_t* __restrict__ y, int n, int nclass, int32_t* __restrict__ pred,
+                                   float* __restrict__ proba, unsigned int* __restrict__ counts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t* q = votes + (size_t)i * nclass;
+    const float uni = __double2float_rn(1.0 / (double)nclass);
+    if (nout[i] > 0) {
+        int best = 0;
+        float mx = (float)q[0];
+        float tot = 0.0f;
+        for (int c = 0; c < nclass; ++c) {
+            const float v = (float)q[c];
+            tot = __fadd_rn(tot, v);
+            if (v >= mx) {
+                mx = v;
+                best = c;
+            }
+        }
+        if (pred) pred[i] = best;
+        if (proba)
+            for (int c = 0; c < nclass; ++c)
+                proba[(size_t)i * nclass + c] = tot > 0.0f ? __fdiv_rn((float)q[c], tot) : uni;
+        atomicAdd(counts + 0, 1u);
+        if (best == y[i]) atomicAdd(counts + 1, 1u);
+    } else {
+        if (pred) pred[i] = 0;
+        if (proba)
+            for (int c = 0; c < nclass; ++c) proba[(size_t)i * nclass + c] = uni;
+    }
+}
+
+__global__ void oob_error_kernel(const unsigned int* __restrict__ counts, float* __restrict__ err) {
+    const unsigned total = counts[0], correct = counts[1];
+    *err = total > 0 ? __fsub_rn(1.0f, __fdiv_rn((float)correct, (float)total)) : 0.0f;
+}
+
+constexpr int PRED_THREADS = 256;
+
+__global__ void __launch_bounds__(PRED_THREADS)
+predict_kernel(const float* __restrict__ X, int m, int p, int nclass, int maxnode, const DNode* __restrict__ nodes,
+               const int32_t* __restrict__ nodeclass, const int64_t* __restrict__ offs,
+               const int32_t* __restrict__ cat, const int32_t* __restrict__ catgoleft, int maxcat,
+               int32_t* __restrict__ votes) {
+    const int t = blockIdx.y;
+    const int s = blockIdx.x * PRED_THREADS + threadIdx.x;
+    if (s >= m) return;
+    const int64_t o = offs[t];
+    const int c = walk_predict(X + (size_t)s * p, p, nclass, nodes + o, nodeclass + o, cat,
+                               catgoleft ? catgoleft + o * maxcat : nullptr, maxcat, maxnode);
+    if (c >= 0) atomicAdd(votes + (size_t)s * nclass + c, 1);
+}
+
+}  // namespace
+
+rfx_status launch_route(Ctx* c) {
+    StageTimer st(c, ST_ROUTE, 2);
+    RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
+    dim3 grid((c->n + ROUTE_THREADS - 1) / ROUTE_THREADS, c->T);
+    route_kernel<<<grid, ROUTE_THREADS, 0, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
+                                                        c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+                                                        c->d_catgoleft, c->maxcat, c->d_key, nullptr, c->d_votes);
+    RFX_CUDA(cudaGetLastError());
+    nout_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_inbag, c->n, c->T, c->d_nout);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+rfx_status launch_route_leaf(Ctx* c, int32_t* d_leaf) {
+    StageTimer st(c, ST_ROUTE, 1);
+    dim3 grid((c->n + ROUTE_THREADS - 1) / ROUTE_THREADS, c->T);
+    // votes are recomputed identically; clear first so they stay exact
+    RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
+    route_kernel<<<grid, ROUTE_THREADS, 0, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
+                                                        c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+                                                        c->d_catgoleft, c->maxcat, c->d_key, d_leaf, c->d_votes);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+rfx_status launch_oob_summary(Ctx* c, float* d_errout, int32_t* d_pred, float* d_proba) {
+    StageTimer st(c, ST_OOB, d_errout ? 2 : 1);
+    unsigned int* counts = reinterpret_cast<unsigned int*>(c->d_pairs) + 2;  // scratch words after the pair counter
+    RFX_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), c->stream));
+    oob_summary_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_votes, c->d_nout, c->d_y, c->n, c->nclass,
+                                                                   d_pred, d_proba, counts);
+    RFX_CUDA(cudaGetLastError());
+    if (d_errout) {
+        oob_error_kernel<<<1, 1, 0, c->stream>>>(counts, d_errout);
+        RFX_CUDA(cudaGetLastError());
+    }
+    return RFX_OK;
+}
+
+rfx_status launch_predict(Ctx* c, const float* dX, int m, int32_t* d_votes) {
+    StageTimer st(c, ST_PREDICT, m > 0 ? 1 : 0);
+    RFX_CUDA(cudaMemsetAsync(d_votes, 0, sizeof(int32_t) * (size_t)m * c->nclass, c->stream));
+    if (m == 0) return RFX_OK;
+    dim3 grid((m + PRED_THREADS - 1) / PRED_THREADS, c->T);
+    predict_kernel<<<grid, PRED_THREADS, 0, c->stream>>>(dX, m, c->p, c->nclass, 2 * c->n + 1, c->d_nodes,
+                                                         c->d_nodeclass, c->d_offs, c->d_cat, c->d_catgoleft,
+                                                         c->maxcat, d_votes);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+}  // namespace rfx

@@ -1,0 +1,317 @@
+// Permutation importance for all trees and all features in three launches.
+//
+// cpu_varimp (src/rf_varimp.cpp:106-302) re-routes every OOB sample once per
+// used feature k, with x[pjoob[r]][k] in place of x[joob[r]][k], where pjoob is
+// cpu_permobmr's permutation (:16-30; it depends on noob only).  A permuted walk
+// can only leave the unpermuted path at a node that splits on k, so one walk
+// along the unpermuted cpu_testreeimp path (:45-103) decides every feature at
+// once: at each node on the path whose feature k has not yet diverged, the
+// permuted value is tried; where it goes the other way, a side walk from the
+// other child (with k permuted) gives that feature's class.  Features that
+// never diverge keep the unpermuted class.  Per (tree, sample) this yields
+//   bit "testreebag correct", bit "testreeimp correct", and a flip mask over
+//   features, from which
+//   rightimp[t][k] = #testreeimp-correct + sum of signed flips (exact integers).
+//
+// varimp_tree_kernel  - one CTA per tree: OOB list (joob), walks, flip masks,
+//                       per-tree integer counts.
+// varimp_sample_kernel- one thread per sample: qimp / qimpm float sums in tree
+//                       order, 1/noob per correct OOB tree (the reference adds
+//                       each tree's temporaries in tree order,
+//                       src/rf_random_forest.cpp:1217-1230).
+// varimp_feature_kernel - one thread per feature: avimp / sqsd sums of
+//                       rr = (right - rightimp) / noob in tree order.
+#include "walks.cuh"
+
+namespace rfx {
+
+namespace {
+
+constexpr int VT = 256;  // threads of the per-tree kernel
+
+enum { DIR_BREAK = -2 };
+
+// One decision of the cpu_testreeimp walk at node nd (local id kt) for value x.
+__device__ __forceinline__ int imp_decide(const DNode& nd, int kt, float x, const int32_t* __restrict__ cgl,
+                                          int maxcat) {
+    if (!node_cat(nd.meta)) return (x <= nd.split) ? nd.left : nd.right;
+    const int jcat = __float2int_rz(__fadd_rn(x, 0.5f));
+    if (jcat >= 0 && jcat < maxcat) return (cgl_at(cgl, maxcat, kt, jcat) == 1) ? nd.left : nd.right;
+    return DIR_BREAK;
+}
+
+// Side walk of the permuted traversal from node kt with feature mr taken from
+// xperm; budget = remaining loop iterations of the reference's k < nnode loop.
+// Returns the class, or -1 when the reference would break without assigning.
+__device__ __forceinline__ int imp_side_walk(const float* __restrict__ xrow, const float* __restrict__ xperm, int mr,
+                                             int p, int kt, int budget, const DNode* __restrict__ nodes,
+                                             const int32_t* __restrict__ nclass_of, const int32_t* __restrict__ cgl,
+                                             int maxcat) {
+    for (int s = 0; s < budget; ++s) {
+        const DNode nd = load_node(nodes, kt);
+        if (node_status(nd.meta) == -1) return __ldg(nclass_of + kt);
+        const int m = node_var(nd.meta);
+        if (m >= p) return -1;
+        const float x = __ldg((m == mr ? xperm : xrow) + m);
+        const int nx = imp_decide(nd, kt, x, cgl, maxcat);
+        if (nx == DIR_BREAK) return -1;
+        kt = nx;
+    }
+    return -1;
+}
+
+template <int W>
+__global__ void __launch_bounds__(VT)
+varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
+                   const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
+                   const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+                   const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
+                   const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ permoff,
+                   const int32_t* __restrict__ perm_all, int32_t* __restrict__ joob_all,
+                   uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips, int32_t* __restrict__ right_out,
+                   int32_t* __restrict__ rightimp_out, uint32_t* __restrict__ err) {
+    extern __shared__ int32_t delta[];  // p counters
+    __shared__ int wsum[VT / 32];
+    __shared__ int s_base;
+    __shared__ int s_red[2];
+    const int t = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int64_t o = offs[t];
+    const DNode* tn = nodes + o;
+    const int32_t* tc = nodeclass + o;
+    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+    const int nn = nnode_arr[t];
+    const int nnv = nn > 0 ? nn : 1;
+    const uint8_t* ib = inbag + (size_t)t * n;
+    int32_t* joob = joob_all + (size_t)t * n;
+    for (int k = tid; k < p; k += VT) delta[k] = 0;
+    if (tid == 0) {
+        s_base = 0;
+        s_red[0] = 0;
+        s_red[1] = 0;
+    }
+    __syncthreads();
+    // 1. joob: OOB samples in ascending order (block-wide stream compaction)
+    for (int base = 0; base < n; base += VT) {
+        const int i = base + tid;
+        const int f = (i < n && ib[i] == 0) ? 1 : 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wsum[wid] = __popc(bal);
+        __syncthreads();
+        int woff = 0, tot = 0;
+        for (int q = 0; q < VT / 32; ++q) {
+            if (q < wid) woff += wsum[q];
+            tot += wsum[q];
+        }
+        if (f) joob[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = i;
+        __syncthreads();
+        if (tid == 0) s_base += tot;
+        __syncthreads();
+    }
+    const int noob = s_base;
+    const int32_t* perm = perm_all + permoff[t];
+    int my_right = 0, my_imp = 0;
+    uint32_t my_err = 0;
+    for (int r = tid; r < noob; r += VT) {
+        const int i = joob[r];
+        const int ip = joob[perm[r]];
+        const float* xi = X + (size_t)i * p;
+        const float* xp = X + (size_t)ip * p;
+        const int yi = y[i];
+        int cls_tb;
+        walk_testreebag(xi, p, tn, tc, nn, cat, cgl, maxcat, &cls_tb);
+        const int base_tb = (cls_tb == yi);
+        uint64_t done[W], pcorr[W];
+#pragma unroll
+        for (int q = 0; q < W; ++q) done[q] = pcorr[q] = 0ull;
+        int kt = 0, jvr0 = -1;
+        bool ok = false;
+        for (int step = 0; step < nnv; ++step) {
+            const DNode nd = load_node(tn, kt);
+            if (node_status(nd.meta) == -1) {
+                jvr0 = __ldg(tc + kt);
+                ok = true;
+                break;
+            }
+            const int m = node_var(nd.meta);
+            if (m >= p) break;
+            const int dir_o = imp_decide(nd, kt, __ldg(xi + m), cgl, maxcat);
+            if (dir_o == DIR_BREAK) break;
+            const int wq = m >> 6;
+            const uint64_t bit = 1ull << (m & 63);
+            uint64_t dword = 0;
+#pragma unroll
+            for (int q = 0; q < W; ++q)
+                if (q == wq) dword = done[q];
+            if (!(dword & bit)) {
+                const int dir_p = imp_decide(nd, kt, __ldg(xp + m), cgl, maxcat);
+                if (dir_p != dir_o) {
+                    int cls_m = -1;
+                    if (dir_p != DIR_BREAK)
+                        cls_m = imp_side_walk(xi, xp, m, p, dir_p, nnv - step - 1, tn, tc, cgl, maxcat);
+                    if (cls_m < 0) my_err |= ERR_STALE_JVR;
+#pragma unroll
+                    for (int q = 0; q < W; ++q)
+                        if (q == wq) {
+                            done[q] |= bit;
+                            if (cls_m == yi) pcorr[q] |= bit;
+                        }
+                }
+            }
+            kt = dir_o;
+        }
+        if (!ok) my_err |= ERR_STALE_JVR;
+        const int base_imp = (ok && jvr0 == yi);
+        const uint64_t bmask = base_imp ? ~0ull : 0ull;
+        const size_t ti = (size_t)t * n + i;
+        vflags[ti] = (uint8_t)(1 | (base_tb << 1) | (base_imp << 2));
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            const uint64_t fl = done[q] & (pcorr[q] ^ bmask);
+            flips[ti * W + q] = fl;
+            uint64_t f = fl;
+            while (f) {
+                const int b = __ffsll((long long)f) - 1;
+                f &= f - 1;
+                atomicAdd(delta + q * 64 + b, base_imp ? -1 : 1);
+            }
+        }
+        my_right += base_tb;
+        my_imp += base_imp;
+    }
+    // block reductions
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        my_right += __shfl_down_sync(0xffffffffu, my_right, d);
+        my_imp += __shfl_down_sync(0xffffffffu, my_imp, d);
+    }
+    if (lane == 0) {
+        atomicAdd(&s_red[0], my_right);
+        atomicAdd(&s_red[1], my_imp);
+    }
+    if (my_err) atomicOr(err, my_err);
+    __syncthreads();
+    if (tid == 0) right_out[t] = s_red[0];
+    for (int k = tid; k < p; k += VT) rightimp_out[(size_t)t * p + k] = s_red[1] + delta[k];
+}
+
+// qimp / qimpm: per sample, trees in order.  acc is [p][blockDim] in shared
+// memory so consecutive threads hit consecutive banks.
+template <int W>
+__global__ void varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restrict__ vflags,
+                                     const uint64_t* __restrict__ flips, const uint64_t* __restrict__ iv,
+                                     const float* __restrict__ invnoob, int n, int p, int T, int impn,
+                                     float* __restrict__ qimp, float* __restrict__ qimpm) {
+    extern __shared__ float acc[];
+    const int tid = threadIdx.x, B = blockDim.x;
+    const int i = blockIdx.x * B + tid;
+    const bool valid = i < n;
+    for (int k = 0; k < p; ++k) acc[k * B + tid] = 0.0f;
+    float q = 0.0f;
+    if (valid && impn) {
+        for (int t = 0; t < T; ++t) {
+            const size_t ti = (size_t)t * n + i;
+            if (inbag[ti] != 0) continue;
+            const uint8_t fl = vflags[ti];
+            const float inv = invnoob[t];
+            const bool btb = (fl >> 1) & 1, bimp = (fl >> 2) & 1;
+            if (btb) q = __fadd_rn(q, inv);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                const uint64_t fw = flips[ti * W + w];
+                const uint64_t ivw = iv[(size_t)t * W + w];
+                // correct_k = iv_k ? (bimp ^ flip_k) : btb
+                const uint64_t corr = (ivw & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivw & (btb ? ~0ull : 0ull));
+                const int kend = min(64, p - w * 64);
+                for (int kk = 0; kk < kend; ++kk)
+                    if ((corr >> kk) & 1ull) {
+                        float* a = acc + (w * 64 + kk) * B + tid;
+                        *a = __fadd_rn(*a, inv);
+                    }
+            }
+        }
+    }
+    if (!valid) return;
+    if (impn) {
+        qimp[i] = q;
+        for (int k = 0; k < p; ++k) qimpm[(size_t)i * p + k] = acc[k * B + tid];
+    }
+}
+
+__global__ void varimp_feature_kernel(const int32_t* __restrict__ right, const int32_t* __restrict__ rightimp,
+                                      const int32_t* __restrict__ noob, const uint64_t* __restrict__ iv, int W,
+                                      int p, int T, float* __restrict__ avimp, float* __restrict__ sqsd) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= p) return;
+    float a = 0.0f, s = 0.0f;
+    for (int t = 0; t < T; ++t) {
+        if (!((iv[(size_t)t * W + (k >> 6)] >> (k & 63)) & 1ull)) continue;
+        const float rr = __fdiv_rn(__fsub_rn((float)right[t], (float)rightimp[(size_t)t * p + k]), (float)noob[t]);
+        a = __fadd_rn(a, rr);
+        s = __fadd_rn(s, __fmul_rn(rr, rr));
+    }
+    avimp[k] = a;
+    sqsd[k] = s;
+}
+
+__global__ void localimp_kernel(const float* __restrict__ qimp, const float* __restrict__ qimpm, int n, int p, int T,
+                                float* __restrict__ out) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)n * p) return;
+    const int nn = (int)(idx % (size_t)n);
+    out[idx] = __fdiv_rn(__fmul_rn(100.0f, __fsub_rn(qimp[nn], qimpm[idx])), (float)T);
+}
+
+template <int W>
+rfx_status launch_varimp_w(Ctx* c, int impn) {
+    const size_t smem = (size_t)c->p * sizeof(int32_t);
+    {
+    StageTimer st(c, ST_VARIMP_TREE, 1);
+    varimp_tree_kernel<W><<<c->T, VT, smem, c->stream>>>(
+        c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+        c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, c->d_vflags, c->d_flips, c->d_right,
+        c->d_rightimp, c->d_err);
+    RFX_CUDA(cudaGetLastError());
+    }
+    if (impn) {
+        StageTimer st(c, ST_VARIMP_SAMPLE, 1);
+        int B = 128;
+        while (B > 32 && (size_t)B * c->p * sizeof(float) > 96 * 1024) B >>= 1;
+        const size_t smem2 = (size_t)B * c->p * sizeof(float);
+        RFX_CUDA(cudaFuncSetAttribute(varimp_sample_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)std::max<size_t>(smem2, 1)));
+        varimp_sample_kernel<W><<<(c->n + B - 1) / B, B, smem2, c->stream>>>(
+            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, impn, c->d_qimp,
+            c->d_qimpm);
+        RFX_CUDA(cudaGetLastError());
+    }
+    StageTimer st(c, ST_VARIMP_FEATURE, 1);
+    varimp_feature_kernel<<<(c->p + 127) / 128, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,
+                                                                      W, c->p, c->T, c->d_avimp, c->d_sqsd);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+}  // namespace
+
+rfx_status launch_varimp(Ctx* c, int impn) {
+    switch (c->iv_words) {
+        case 1: return launch_varimp_w<1>(c, impn);
+        case 2: return launch_varimp_w<2>(c, impn);
+        case 3: return launch_varimp_w<3>(c, impn);
+        case 4: return launch_varimp_w<4>(c, impn);
+        default:
+            set_error("rfx_varimp supports at most 256 features");
+            return RFX_ERR_UNSUPPORTED;
+    }
+}
+
+rfx_status launch_localimp(Ctx* c, const float* d_qimp, const float* d_qimpm, float* d_out) {
+    StageTimer st(c, ST_LOCALIMP, 1);
+    const size_t total = (size_t)c->n * c->p;
+    localimp_kernel<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(d_qimp, d_qimpm, c->n, c->p, c->T, d_out);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+}  // namespace rfx

@@ -1,0 +1,127 @@
+// Device tree walks, one per routing rule of the reference.  They differ in
+// their stopping rule and categorical handling, and each is restated exactly:
+//   walk_testreebag  - cpu_testreebag        (src/rf_testreebag.cpp:39-123)
+//   walk_terminal    - find_terminal_node    (src/rf_random_forest.cpp:2194-2244)
+//   walk_predict     - predict_classification (src/rf_random_forest.cpp:1959-2013)
+//   (the testreeimp walk lives in varimp.cu: it also tracks permutations)
+// Float conversions and roundings are spelled with explicit intrinsics so that
+// no compiler contraction changes a result.
+#pragma once
+#include "rfx_internal.cuh"
+
+namespace rfx {
+
+__device__ __forceinline__ DNode load_node(const DNode* __restrict__ nodes, int k) {
+    int4 v = __ldg(reinterpret_cast<const int4*>(nodes) + k);
+    DNode d;
+    d.split = __int_as_float(v.x);
+    d.left = v.y;
+    d.right = v.z;
+    d.meta = v.w;
+    return d;
+}
+
+__device__ __forceinline__ int cgl_at(const int32_t* __restrict__ cgl, int maxcat, int node, int idx) {
+    return cgl ? __ldg(cgl + (size_t)node * maxcat + idx) : 0;
+}
+
+// Returns the node id; *cls receives the class (nodeclass of the final node,
+// or of the root on the fallback path).
+__device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
+                                               const int32_t* __restrict__ nclass_of, int nnode,
+                                               const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                               int maxcat, int* cls) {
+    int kt = 0;
+    int steps = 0;
+    DNode nd = load_node(nodes, 0);
+    while (node_status(nd.meta) == 1 && steps < 1000) {
+        steps++;
+        if (steps >= 1000) break;
+        const int m = node_var(nd.meta);
+        if (m >= p) break;
+        const float v = __ldg(xrow + m);
+        if (!node_cat(nd.meta)) {
+            kt = (v <= nd.split) ? nd.left : nd.right;
+        } else {
+            const int iv = __float2int_rz(v);
+            if (iv >= 0 && iv < __ldg(cat + m)) {
+                kt = (cgl_at(cgl, maxcat, kt, iv) == 1) ? nd.left : nd.right;
+            } else {
+                kt = nd.right;
+            }
+        }
+        if (kt < 0 || kt >= nnode) {
+            kt = 0;
+            nd = load_node(nodes, 0);
+            break;
+        }
+        nd = load_node(nodes, kt);
+        if (node_status(nd.meta) != 1) break;
+    }
+    const int st = node_status(nd.meta);
+    if (st == -1 || st == 2) {
+        *cls = __ldg(nclass_of + kt);
+        return kt;
+    }
+    *cls = __ldg(nclass_of + 0);
+    return 0;
+}
+
+// find_terminal_node: stops only at status -1; invalid category or variable
+// returns the root.  maxnode is the reference's loop bound (2n+1).
+__device__ __forceinline__ int walk_terminal(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
+                                             const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                             int maxcat, int maxnode) {
+    int cur = 0;
+    for (int k = 0; k < maxnode; ++k) {
+        const DNode nd = load_node(nodes, cur);
+        if (node_status(nd.meta) == -1) return cur;
+        const int m = node_var(nd.meta);
+        if (m >= p) return 0;
+        const float v = __ldg(xrow + m);
+        if (!node_cat(nd.meta)) {
+            cur = (v <= nd.split) ? nd.left : nd.right;
+        } else {
+            const int j = __double2int_rz(__dadd_rn((double)v, 0.5));
+            if (j >= 1 && j <= __ldg(cat + m)) {
+                cur = (cgl_at(cgl, maxcat, cur, j - 1) == 1) ? nd.left : nd.right;
+            } else {
+                return 0;
+            }
+        }
+    }
+    return 0;
+}
+
+// predict_classification's walk: returns the voted class, or -1 for no vote
+// (loop bound reached).  Invalid paths vote for class 0.
+__device__ __forceinline__ int walk_predict(const float* __restrict__ xrow, int p, int nclass,
+                                            const DNode* __restrict__ nodes, const int32_t* __restrict__ nclass_of,
+                                            const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                            int maxcat, int maxnode) {
+    int kt = 0;
+    for (int k = 0; k < maxnode; ++k) {
+        if (kt >= maxnode) return 0;
+        const DNode nd = load_node(nodes, kt);
+        if (node_status(nd.meta) == -1) {
+            const int c = __ldg(nclass_of + kt);
+            return (c >= 0 && c < nclass) ? c : 0;
+        }
+        const int m = node_var(nd.meta);
+        if (m >= p) return 0;
+        const float v = __ldg(xrow + m);
+        if (!node_cat(nd.meta)) {
+            kt = (v <= nd.split) ? nd.left : nd.right;
+        } else {
+            const int j = __double2int_rz(__dadd_rn((double)v, 0.5));
+            if (j >= 1 && j <= __ldg(cat + m)) {
+                kt = (cgl_at(cgl, maxcat, kt, j - 1) == 1) ? nd.left : nd.right;
+            } else {
+                return 0;
+            }
+        }
+    }
+    return -1;
+}
+
+}  // namespace rfx

@@ -1,0 +1,29 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def built():
+    """Native libraries built in-tree (cheap when up to date)."""
+    from rfx_b200 import build
+    from oracle import oracle
+
+    build.build()
+    oracle.build()
+    return True
+
+
+def has_reference():
+    from oracle import reference
+
+    return reference.available()

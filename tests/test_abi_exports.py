@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports every symbol include/rfx_b200.h declares
+(no compute calls: this runs without a GPU)."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+
+def test_header_symbols_exported(built):
+    from rfx_b200 import abi
+
+    hdr = open(os.path.join(ROOT, "include", "rfx_b200.h")).read()
+    declared = sorted(set(re.findall(r"^\s*(?:rfx_status|const char\*)\s+(rfx_\w+)\s*\(", hdr, re.M)))
+    assert declared, "no declarations found"
+    lib = ctypes.CDLL(abi.LIB_PATH)
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    assert sorted(abi.EXPORTS) == declared
+
+
+def test_no_device_is_an_error_not_a_fallback(built):
+    """Without a CUDA device the context refuses to open (no CPU fallback)."""
+    import torch
+
+    from rfx_b200 import abi
+
+    if torch.cuda.is_available():
+        return
+    try:
+        abi.Context(0)
+    except abi.RfxError as e:
+        assert e.status in (2, 8)
+    else:
+        raise AssertionError("context opened without a device")
+
+
+def test_casewise_rejected(built):
+    from rfx_b200 import abi
+
+    try:
+        abi.Context(0, use_casewise=True)
+    except abi.RfxError as e:
+        assert e.status == 5
+    else:
+        raise AssertionError("use_casewise accepted")
