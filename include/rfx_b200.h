@@ -147,8 +147,8 @@ rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes);
  * the number of kernels the library has launched since the context was
  * created.  Stage order: route, leaf lists, pair counts,
  * finishprox, varimp per-tree, varimp per-sample, varimp per-feature, predict,
- * oob summary, localimp. */
-enum { RFX_NUM_STAGES = 10 };
+ * oob summary, localimp, pair-range table. */
+enum { RFX_NUM_STAGES = 11 };
 rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable);
 rfx_status rfx_profile_read(rfx_ctx* ctx, float* stage_ms, int64_t* kernel_launches);
 

@@ -30,7 +30,7 @@ EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_strea
            "rfx_grow_forest", "rfx_free_forest"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
-          "predict", "oob_summary", "localimp"]
+          "predict", "oob_summary", "localimp", "pair_ranges"]
 
 
 class RfxError(RuntimeError):

@@ -94,7 +94,7 @@ void free_forest(Ctx* c) {
     dfree(c, c->d_perm); dfree(c, c->d_invnoob); dfree(c, c->d_key); dfree(c, c->d_segoff); dfree(c, c->d_memb);
     dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_vflags); dfree(c, c->d_flips);
     dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
-    dfree(c, c->d_sqsd);
+    dfree(c, c->d_sqsd); dfree(c, c->d_opp); dfree(c, c->d_order);
     c->loaded = c->routed = c->csr_built = false;
     c->bytes = 0;
 }
@@ -649,7 +649,7 @@ rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* 
     ALLOC(d_joob, (size_t)T * n);
     ALLOC(d_vflags, (size_t)T * n);
     ALLOC(d_flips, (size_t)T * n * W);
-    ALLOC(d_right, T);
+    ALLOC(d_right, 2 * (size_t)T);
     ALLOC(d_rightimp, (size_t)T * p);
     ALLOC(d_qimp, n);
     ALLOC(d_qimpm, (size_t)n * p);

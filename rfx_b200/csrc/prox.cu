@@ -19,6 +19,8 @@
 #include "rfx_internal.cuh"
 
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 
 namespace rfx {
 
@@ -27,66 +29,78 @@ namespace {
 // ---------------------------------------------------------------------------
 // Stage 1
 // ---------------------------------------------------------------------------
-constexpr int CSR_PREFETCH = 4;  // 32-sample groups loaded ahead per lane
+constexpr int CSR_THREADS = 128;
+constexpr int CSR_PREFETCH = 16;  // 32-sample groups loaded ahead by the scattering warp
 
-__global__ void __launch_bounds__(32)
+// One CTA per tree.  All warps build the key histogram; the exclusive scan
+// runs over four quarters in parallel; warp 0 alone then scatters the samples
+// in index order (equal keys inside a 32-sample group are ranked by lane), so
+// every key's member list is ascending by sample id.
+__global__ void __launch_bounds__(CSR_THREADS)
 build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restrict__ segbase,
                  int32_t* __restrict__ segoff, int32_t* __restrict__ memb, int smem_keys,
                  uint32_t* __restrict__ err) {
     extern __shared__ int32_t cnt[];
+    __shared__ int qtot[CSR_THREADS / 32];
     const int t = blockIdx.x;
-    const int lane = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int64_t sb = segbase[t];
     const int K = (int)(segbase[t + 1] - sb) - 1;  // number of keys of this tree
     const int32_t* kt = key + (size_t)t * n;
     int32_t* mt = memb + (size_t)t * n;
     int32_t* so = segoff + sb;
     // counters: shared memory when the key table fits, else the tree's own
-    // segment-offset table in global memory
+    // segment-offset table in global memory (slower, still exact)
     const bool use_smem = K + 1 <= smem_keys;
-    int32_t* ctr = use_smem ? cnt : so;  // global-counter path: slower, still exact
-    for (int k = lane; k <= K; k += 32) ctr[k] = 0;
-    __syncwarp();
-    // histogram
-    for (int base = 0; base < n; base += 32 * CSR_PREFETCH) {
-        int kv[CSR_PREFETCH];
-#pragma unroll
-        for (int u = 0; u < CSR_PREFETCH; ++u) {
-            const int i = base + u * 32 + lane;
-            kv[u] = i < n ? __ldg(kt + i) : -1;
-        }
-#pragma unroll
-        for (int u = 0; u < CSR_PREFETCH; ++u)
-            if (kv[u] >= 0) atomicAdd(ctr + kv[u], 1);
+    int32_t* ctr = use_smem ? cnt : so;
+    for (int k = tid; k <= K; k += CSR_THREADS) ctr[k] = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += CSR_THREADS) {
+        const int k = __ldg(kt + i);
+        if (k >= 0) atomicAdd(ctr + k, 1);
     }
-    __syncwarp();
-    // exclusive scan over K+1 counters (the last one is 0 and becomes the total)
+    __syncthreads();
+    // exclusive scan of K+1 counters: quarter q = [q*Q, min((q+1)*Q, K+1))
+    const int Q = (K + 1 + 3) / 4;
+    const int q0 = w * Q, q1 = min(K + 1, q0 + Q);
     int carry = 0;
-    for (int k0 = 0; k0 <= K; k0 += 32) {
+    for (int k0 = q0; k0 < q1; k0 += 32) {
         const int k = k0 + lane;
-        int v = k <= K ? ctr[k] : 0;
+        const int v = k < q1 ? ctr[k] : 0;
         int incl = v;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-            int u = __shfl_up_sync(0xffffffffu, incl, d);
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
             if (lane >= d) incl += u;
         }
-        const int excl = carry + incl - v;
-        if (k <= K) {
-            ctr[k] = excl;
-            if (use_smem) so[k] = excl;
-        }
+        if (k < q1) ctr[k] = carry + incl - v;
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
-    __syncwarp();
-    // stable scatter: one warp, samples in index order; equal keys inside a
-    // 32-sample group are ranked by lane (= index) order
+    if (lane == 0) qtot[w] = carry;
+    __syncthreads();
+    int qoff = 0;
+    for (int q = 0; q < w; ++q) qoff += qtot[q];
+    for (int k = q0 + lane; k < q1; k += 32) {
+        const int v = ctr[k] + qoff;
+        ctr[k] = v;
+        if (use_smem) so[k] = v;
+    }
+    __syncthreads();
+    if (w != 0) return;
+    // stable scatter by one warp, samples in index order; the next batch of
+    // keys is loaded while the current one is placed
+    int kv[CSR_PREFETCH], kn[CSR_PREFETCH];
+#pragma unroll
+    for (int u = 0; u < CSR_PREFETCH; ++u) {
+        const int i = u * 32 + lane;
+        kv[u] = i < n ? __ldg(kt + i) : -1;
+    }
     for (int base = 0; base < n; base += 32 * CSR_PREFETCH) {
-        int kv[CSR_PREFETCH];
+        const int nb = base + 32 * CSR_PREFETCH;
 #pragma unroll
         for (int u = 0; u < CSR_PREFETCH; ++u) {
-            const int i = base + u * 32 + lane;
-            kv[u] = i < n ? __ldg(kt + i) : -1;
+            const int i = nb + u * 32 + lane;
+            kn[u] = i < n ? __ldg(kt + i) : -1;
         }
 #pragma unroll
         for (int u = 0; u < CSR_PREFETCH; ++u) {
@@ -104,6 +118,8 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
             if (k >= 0) mt[start + rank] = i;
             __syncwarp();
         }
+#pragma unroll
+        for (int u = 0; u < CSR_PREFETCH; ++u) kv[u] = kn[u];
     }
     // global-counter path: the counters now hold segment ends; a follow-up
     // kernel (fix_global_segoff_kernel) turns them back into starts
@@ -215,6 +231,207 @@ pairs_row_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ se
 }
 
 // ---------------------------------------------------------------------------
+// Stage 2, full-row form (used when a whole row of u16 counters fits in shared
+// memory and ntree < 65536).
+//   opp_kernel: per (tree, sample), the member range of the opposite bag status
+//     in the sample's leaf, already cut to members > sample (binary search
+//     done once here, with full memory-level parallelism), stored sample-major
+//     opp[i][t] = {start within the tree's member list, length}.
+//   row_order_kernel: rows are processed in tree 0's leaf order (then the
+//     samples tree 0 excludes), so CTAs running at the same time own rows that
+//     share leaves and read the same member lists from L2.
+//   pairs_row16_kernel: one CTA per row; u16 counters packed two per 32-bit
+//     word; every (row, tree) range expanded across a warp with several member
+//     loads in flight per lane.
+// ---------------------------------------------------------------------------
+constexpr int OPP_TILE = 32;
+
+__global__ void __launch_bounds__(OPP_TILE * 8)
+opp_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase,
+           const int32_t* __restrict__ memb, int n, int T, int2* __restrict__ opp) {
+    __shared__ int2 tile[OPP_TILE][OPP_TILE + 1];
+    const int i0 = blockIdx.x * OPP_TILE, t0 = blockIdx.y * OPP_TILE;
+    const int tx = threadIdx.x % OPP_TILE, ty = threadIdx.x / OPP_TILE;
+    for (int r = ty; r < OPP_TILE; r += 8) {
+        const int t = t0 + r, i = i0 + tx;
+        int2 v = make_int2(0, 0);
+        if (t < T && i < n) {
+            const int k = __ldg(key + (size_t)t * n + i);
+            if (k >= 0) {
+                const int32_t* so = segoff + segbase[t];
+                int lo = __ldg(so + (k ^ 1)), hi = __ldg(so + (k ^ 1) + 1);
+                const int s1 = hi;
+                const int32_t* mt = memb + (size_t)t * n;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (__ldg(mt + mid) <= i) lo = mid + 1;
+                    else hi = mid;
+                }
+                v = make_int2(lo, s1 - lo);
+            }
+        }
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < OPP_TILE; r += 8) {
+        const int i = i0 + r, t = t0 + tx;
+        if (i < n && t < T) opp[(size_t)i * T + t] = tile[tx][r];
+    }
+}
+
+__global__ void __launch_bounds__(1024)
+row_order_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ segoff,
+                 const int64_t* __restrict__ segbase, const int32_t* __restrict__ memb, int n,
+                 int32_t* __restrict__ order) {
+    __shared__ int wsum[32];
+    __shared__ int s_base;
+    const int K0 = (int)(segbase[1] - segbase[0]) - 1;
+    const int cnt0 = segoff[segbase[0] + K0];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int q = tid; q < cnt0; q += 1024) order[q] = memb[q];
+    if (tid == 0) s_base = cnt0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + tid;
+        const int f = (i < n && key[i] < 0) ? 1 : 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wsum[wid] = __popc(bal);
+        __syncthreads();
+        int woff = 0, tot = 0;
+        for (int q = 0; q < 32; ++q) {
+            if (q < wid) woff += wsum[q];
+            tot += wsum[q];
+        }
+        if (f) order[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = i;
+        __syncthreads();
+        if (tid == 0) s_base += tot;
+        __syncthreads();
+    }
+}
+
+constexpr int R16_THREADS = 512;
+constexpr int R16_WARPS = R16_THREADS / 32;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, int w, int* total) {
+    int incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += u;
+    }
+    if (lane == 31) wtot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        static_assert(R16_WARPS <= 32, "one warp scans the per-warp totals");
+        const int x0 = lane < R16_WARPS ? wtot[lane] : 0;
+        int x = x0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += u;
+        }
+        if (lane < R16_WARPS) wtot[lane] = x - x0;
+        if (lane == R16_WARPS - 1) wtot[R16_WARPS] = x;
+    }
+    __syncthreads();
+    *total = wtot[R16_WARPS];
+    const int r = wtot[w] + incl - v;
+    __syncthreads();  // wtot is reused by the next scan
+    return r;
+}
+
+// One CTA per row.  Each round takes 1024 trees' member ranges of this row,
+// drops the empty ones, and cuts the rest into 32-member pieces; every warp
+// owns a contiguous run of pieces (so warps finish together whatever the range
+// lengths) and processes a piece with its 32 lanes on 32 consecutive members:
+// coalesced loads and one shared-memory atomic per member.
+__global__ void __launch_bounds__(R16_THREADS)
+pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
+                   int n, int T, int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+    extern __shared__ uint32_t acc[];  // ceil(n/2) words, two u16 counters each
+    __shared__ long long cb[R16_THREADS];      // absolute start of each non-empty range
+    __shared__ int clen[R16_THREADS];          // its length
+    __shared__ int cp0[R16_THREADS + 1];       // its first piece index (+ sentinel)
+    __shared__ int wtot[R16_WARPS + 1];
+    const int i = order[blockIdx.x];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int words = (n + 1) >> 1;
+    {
+        uint4* a4 = reinterpret_cast<uint4*>(acc);
+        const int w4 = words >> 2;
+        for (int k = tid; k < w4; k += R16_THREADS) a4[k] = make_uint4(0u, 0u, 0u, 0u);
+        for (int k = (w4 << 2) + tid; k < words; k += R16_THREADS) acc[k] = 0u;
+    }
+    unsigned long long my_pairs = 0;
+    const int2* orow = opp + (size_t)i * T;
+    for (int t0 = 0; t0 < T; t0 += R16_THREADS) {
+        const int t = t0 + tid;
+        long long b = 0;
+        int len = 0;
+        if (t < T) {
+            const int2 v = __ldg(orow + t);
+            b = (long long)t * n + v.x;
+            len = v.y;
+        }
+        my_pairs += (unsigned long long)len;
+        const int np = (len + 31) >> 5;
+        int nseg, P;
+        const int cidx = block_exclusive_scan(np > 0 ? 1 : 0, wtot, lane, w, &nseg);
+        const int pfx = block_exclusive_scan(np, wtot, lane, w, &P);
+        if (np > 0) {
+            cb[cidx] = b;
+            clen[cidx] = len;
+            cp0[cidx] = pfx;
+        }
+        if (tid == 0) cp0[nseg] = P;
+        __syncthreads();  // also orders the accumulator zeroing before any update
+        // warp w owns pieces [q0, q1); walk the ranges they cover, 32 lanes on
+        // consecutive members, four loads in flight per lane
+        const int per = (P + R16_WARPS - 1) / R16_WARPS;
+        const int q0 = w * per;
+        const int q1 = min(P, q0 + per);
+        if (q0 < q1) {
+            int lo = 0, hi = nseg;  // cp0[lo] <= q0 < cp0[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (cp0[mid] <= q0) lo = mid;
+                else hi = mid;
+            }
+            uint32_t* accw = acc;
+            for (int c = lo; c < nseg; ++c) {
+                const int pc = cp0[c];
+                if (pc >= q1) break;
+                const int a = (max(pc, q0) - pc) << 5;
+                const int e = min((q1 - pc) << 5, clen[c]);
+                const int32_t* mp = memb + cb[c];
+                int off = a + lane;
+                for (; off + 96 < e; off += 128) {
+                    const int j0 = __ldg(mp + off), j1 = __ldg(mp + off + 32);
+                    const int j2 = __ldg(mp + off + 64), j3 = __ldg(mp + off + 96);
+                    atomicAdd(accw + (j0 >> 1), 1u << ((j0 & 1) << 4));
+                    atomicAdd(accw + (j1 >> 1), 1u << ((j1 & 1) << 4));
+                    atomicAdd(accw + (j2 >> 1), 1u << ((j2 & 1) << 4));
+                    atomicAdd(accw + (j3 >> 1), 1u << ((j3 & 1) << 4));
+                }
+                for (; off < e; off += 32) {
+                    const int j = __ldg(mp + off);
+                    atomicAdd(accw + (j >> 1), 1u << ((j & 1) << 4));
+                }
+            }
+        }
+        __syncthreads();  // the range tables are rewritten by the next round
+    }
+    const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
+    const uint16_t* a16 = reinterpret_cast<const uint16_t*>(acc);
+    for (int j = i + tid; j < n; j += R16_THREADS) S[rowoff + j] = (int32_t)a16[j];
+    if (pairs) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
+        if (lane == 0 && my_pairs) atomicAdd(pairs, my_pairs);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // finishprox
 // ---------------------------------------------------------------------------
 constexpr int FP_TILE = 32;
@@ -275,7 +492,7 @@ rfx_status launch_build_csr(Ctx* c) {
     const size_t smem = (size_t)smem_keys * sizeof(int32_t);
     StageTimer st(c, ST_CSR, c->max_keys + 1 > smem_keys ? 2 : 1);
     RFX_CUDA(cudaFuncSetAttribute(build_csr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    build_csr_kernel<<<c->T, 32, smem, c->stream>>>(c->d_key, c->n, c->d_segbase, c->d_segoff, c->d_memb, smem_keys,
+    build_csr_kernel<<<c->T, CSR_THREADS, smem, c->stream>>>(c->d_key, c->n, c->d_segbase, c->d_segoff, c->d_memb, smem_keys,
                                                     c->d_err);
     RFX_CUDA(cudaGetLastError());
     if (c->max_keys + 1 > smem_keys) {
@@ -291,7 +508,41 @@ int pairs_window(const Ctx* c) {
     return std::min(c->n, win_max);
 }
 
+bool use_row16(const Ctx* c, int dev_smem) {
+    // RFX_PAIRS_KERNEL=windowed selects the windowed u32 kernel (used for
+    // large n or ntree >= 65536) so that it can be tested at small sizes.
+    const char* force = getenv("RFX_PAIRS_KERNEL");
+    if (force && std::string(force) == "windowed") return false;
+    const size_t words = ((size_t)c->n + 1) / 2;
+    return c->T < 65536 && words * 4 + 20 * 1024 <= (size_t)dev_smem;
+}
+
 rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
+    int dev_smem = 0;
+    RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    if (use_row16(c, dev_smem)) {
+        rfx_status st0 = dalloc(c, &c->d_opp, (size_t)c->T * c->n);
+        if (st0 == RFX_OK) st0 = dalloc(c, &c->d_order, (size_t)c->n);
+        if (st0 != RFX_OK) return st0;
+        RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
+        {
+            StageTimer st(c, ST_OPP, 2);
+            dim3 g((c->n + OPP_TILE - 1) / OPP_TILE, (c->T + OPP_TILE - 1) / OPP_TILE);
+            opp_kernel<<<g, OPP_TILE * 8, 0, c->stream>>>(c->d_key, c->d_segoff, c->d_segbase, c->d_memb, c->n,
+                                                           c->T, c->d_opp);
+            RFX_CUDA(cudaGetLastError());
+            row_order_kernel<<<1, 1024, 0, c->stream>>>(c->d_key, c->d_segoff, c->d_segbase, c->d_memb, c->n,
+                                                        c->d_order);
+            RFX_CUDA(cudaGetLastError());
+        }
+        const size_t smem = ((size_t)c->n + 1) / 2 * sizeof(uint32_t);
+        RFX_CUDA(cudaFuncSetAttribute(pairs_row16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        StageTimer st(c, ST_PAIRS, 1);
+        pairs_row16_kernel<<<c->n, R16_THREADS, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, dS,
+                                                                   c->d_pairs);
+        RFX_CUDA(cudaGetLastError());
+        return RFX_OK;
+    }
     const int win = pairs_window(c);
     const size_t smem = (size_t)win * sizeof(uint32_t);
     RFX_CUDA(cudaFuncSetAttribute(pairs_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -34,7 +34,7 @@ enum : uint32_t {
 
 enum Stage : int {
     ST_ROUTE = 0, ST_CSR, ST_PAIRS, ST_FINISHPROX, ST_VARIMP_TREE, ST_VARIMP_SAMPLE, ST_VARIMP_FEATURE,
-    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_COUNT
+    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_OPP, ST_COUNT
 };
 
 struct Ctx {
@@ -82,6 +82,8 @@ struct Ctx {
     int32_t* d_key = nullptr;           // T*n: 2*leafidx + inbag, or -1
     int32_t* d_segoff = nullptr;        // segbase[T]: per-tree key offsets (+1 sentinel each)
     int32_t* d_memb = nullptr;          // T*n: members grouped by key, ascending within a key
+    int2* d_opp = nullptr;              // n*T: opposite-status member range cut to members > i
+    int32_t* d_order = nullptr;         // n: row processing order
     int32_t* d_votes = nullptr;         // n*nclass
     int32_t* d_nout = nullptr;          // n
     uint32_t* d_err = nullptr;          // error bits
@@ -94,8 +96,8 @@ struct Ctx {
     int32_t* d_joob = nullptr;          // T*n
     uint8_t* d_vflags = nullptr;        // T*n: bit1 testreebag correct, bit2 testreeimp correct
     uint64_t* d_flips = nullptr;        // T*n*iv_words
-    int32_t* d_right = nullptr;         // T
-    int32_t* d_rightimp = nullptr;      // T*p
+    int32_t* d_right = nullptr;         // 2T: per tree #correct (testreebag), #correct (testreeimp)
+    int32_t* d_rightimp = nullptr;      // T*p: signed flip counts per tree and feature
     float* d_qimp = nullptr;            // n (internal accumulators)
     float* d_qimpm = nullptr;           // n*p
     float* d_avimp = nullptr;           // p

@@ -13,8 +13,9 @@
 //   features, from which
 //   rightimp[t][k] = #testreeimp-correct + sum of signed flips (exact integers).
 //
-// varimp_tree_kernel  - one CTA per tree: OOB list (joob), walks, flip masks,
-//                       per-tree integer counts.
+// joob_kernel        - one CTA per tree: OOB list (joob, ascending).
+// varimp_walk_kernel - one thread per (tree, OOB sample) over the whole grid:
+//                       walks, flip masks, per-tree integer counts.
 // varimp_sample_kernel- one thread per sample: qimp / qimpm float sums in tree
 //                       order, 1/noob per correct OOB tree (the reference adds
 //                       each tree's temporaries in tree order,
@@ -23,11 +24,13 @@
 //                       rr = (right - rightimp) / noob in tree order.
 #include "walks.cuh"
 
+#include <algorithm>
+
 namespace rfx {
 
 namespace {
 
-constexpr int VT = 256;  // threads of the per-tree kernel
+constexpr int VT = 256;  // threads of the per-tree OOB-list kernel
 
 enum { DIR_BREAK = -2 };
 
@@ -43,12 +46,13 @@ __device__ __forceinline__ int imp_decide(const DNode& nd, int kt, float x, cons
 // Side walk of the permuted traversal from node kt with feature mr taken from
 // xperm; budget = remaining loop iterations of the reference's k < nnode loop.
 // Returns the class, or -1 when the reference would break without assigning.
+template <typename Src>
 __device__ __forceinline__ int imp_side_walk(const float* __restrict__ xrow, const float* __restrict__ xperm, int mr,
-                                             int p, int kt, int budget, const DNode* __restrict__ nodes,
+                                             int p, int kt, int budget, const Src& nodes,
                                              const int32_t* __restrict__ nclass_of, const int32_t* __restrict__ cgl,
                                              int maxcat) {
     for (int s = 0; s < budget; ++s) {
-        const DNode nd = load_node(nodes, kt);
+        const DNode nd = nodes(kt);
         if (node_status(nd.meta) == -1) return __ldg(nclass_of + kt);
         const int m = node_var(nd.meta);
         if (m >= p) return -1;
@@ -60,38 +64,17 @@ __device__ __forceinline__ int imp_side_walk(const float* __restrict__ xrow, con
     return -1;
 }
 
-template <int W>
+// OOB samples of every tree in ascending order (joob of cpu_varimp).
 __global__ void __launch_bounds__(VT)
-varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
-                   const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
-                   const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
-                   const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
-                   const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ permoff,
-                   const int32_t* __restrict__ perm_all, int32_t* __restrict__ joob_all,
-                   uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips, int32_t* __restrict__ right_out,
-                   int32_t* __restrict__ rightimp_out, uint32_t* __restrict__ err) {
-    extern __shared__ int32_t delta[];  // p counters
+joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all) {
     __shared__ int wsum[VT / 32];
     __shared__ int s_base;
-    __shared__ int s_red[2];
     const int t = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int64_t o = offs[t];
-    const DNode* tn = nodes + o;
-    const int32_t* tc = nodeclass + o;
-    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
-    const int nn = nnode_arr[t];
-    const int nnv = nn > 0 ? nn : 1;
     const uint8_t* ib = inbag + (size_t)t * n;
     int32_t* joob = joob_all + (size_t)t * n;
-    for (int k = tid; k < p; k += VT) delta[k] = 0;
-    if (tid == 0) {
-        s_base = 0;
-        s_red[0] = 0;
-        s_red[1] = 0;
-    }
+    if (tid == 0) s_base = 0;
     __syncthreads();
-    // 1. joob: OOB samples in ascending order (block-wide stream compaction)
     for (int base = 0; base < n; base += VT) {
         const int i = base + tid;
         const int f = (i < n && ib[i] == 0) ? 1 : 0;
@@ -108,18 +91,53 @@ varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         if (tid == 0) s_base += tot;
         __syncthreads();
     }
-    const int noob = s_base;
-    const int32_t* perm = perm_all + permoff[t];
+}
+
+constexpr int VW = 128;  // threads per CTA of the walk kernel
+
+// One thread per (tree, OOB position r): grid = (ceil(max noob / VW), T).
+template <int W>
+__global__ void __launch_bounds__(VW, 12)
+varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
+                   const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
+                   const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+                   const int32_t* __restrict__ noob_arr, const int32_t* __restrict__ cat,
+                   const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ permoff,
+                   const int32_t* __restrict__ perm_all, const int32_t* __restrict__ joob_all,
+                   uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips, int32_t* __restrict__ counts,
+                   int32_t* __restrict__ delta_out, uint32_t* __restrict__ err) {
+    extern __shared__ int32_t delta[];  // p counters
+    __shared__ int s_red[2];
+    const int t = blockIdx.y;
+    const int noob = noob_arr[t];
+    const int r0 = blockIdx.x * VW;
+    if (r0 >= noob) return;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (int k = tid; k < p; k += VW) delta[k] = 0;
+    if (tid == 0) {
+        s_red[0] = 0;
+        s_red[1] = 0;
+    }
+    __syncthreads();
+    const int64_t o = offs[t];
+    const DNode* tn = nodes + o;
+    const int32_t* tc = nodeclass + o;
+    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+    const int nn = nnode_arr[t];
+    const int nnv = nn > 0 ? nn : 1;
+    const int32_t* joob = joob_all + (size_t)t * n;
+    const GlobalNodes src{tn};
     int my_right = 0, my_imp = 0;
     uint32_t my_err = 0;
-    for (int r = tid; r < noob; r += VT) {
+    const int r = r0 + tid;
+    if (r < noob) {
         const int i = joob[r];
-        const int ip = joob[perm[r]];
+        const int ip = joob[__ldg(perm_all + permoff[t] + r)];
         const float* xi = X + (size_t)i * p;
         const float* xp = X + (size_t)ip * p;
         const int yi = y[i];
         int cls_tb;
-        walk_testreebag(xi, p, tn, tc, nn, cat, cgl, maxcat, &cls_tb);
+        walk_testreebag_src(xi, p, src, tc, nn, cat, cgl, maxcat, &cls_tb);
         const int base_tb = (cls_tb == yi);
         uint64_t done[W], pcorr[W];
 #pragma unroll
@@ -127,7 +145,7 @@ varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         int kt = 0, jvr0 = -1;
         bool ok = false;
         for (int step = 0; step < nnv; ++step) {
-            const DNode nd = load_node(tn, kt);
+            const DNode nd = src(kt);
             if (node_status(nd.meta) == -1) {
                 jvr0 = __ldg(tc + kt);
                 ok = true;
@@ -148,7 +166,7 @@ varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                 if (dir_p != dir_o) {
                     int cls_m = -1;
                     if (dir_p != DIR_BREAK)
-                        cls_m = imp_side_walk(xi, xp, m, p, dir_p, nnv - step - 1, tn, tc, cgl, maxcat);
+                        cls_m = imp_side_walk(xi, xp, m, p, dir_p, nnv - step - 1, src, tc, cgl, maxcat);
                     if (cls_m < 0) my_err |= ERR_STALE_JVR;
 #pragma unroll
                     for (int q = 0; q < W; ++q)
@@ -176,10 +194,9 @@ varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                 atomicAdd(delta + q * 64 + b, base_imp ? -1 : 1);
             }
         }
-        my_right += base_tb;
-        my_imp += base_imp;
+        my_right = base_tb;
+        my_imp = base_imp;
     }
-    // block reductions
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         my_right += __shfl_down_sync(0xffffffffu, my_right, d);
@@ -191,54 +208,62 @@ varimp_tree_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     }
     if (my_err) atomicOr(err, my_err);
     __syncthreads();
-    if (tid == 0) right_out[t] = s_red[0];
-    for (int k = tid; k < p; k += VT) rightimp_out[(size_t)t * p + k] = s_red[1] + delta[k];
+    if (tid == 0) {
+        if (s_red[0]) atomicAdd(counts + 2 * t, s_red[0]);
+        if (s_red[1]) atomicAdd(counts + 2 * t + 1, s_red[1]);
+    }
+    for (int k = tid; k < p; k += VW)
+        if (delta[k]) atomicAdd(delta_out + (size_t)t * p + k, delta[k]);
 }
 
-// qimp / qimpm: per sample, trees in order.  acc is [p][blockDim] in shared
-// memory so consecutive threads hit consecutive banks.
+// qimp / qimpm: one thread per (sample, group of 8 features); each thread
+// keeps its 8 running sums in registers and walks the trees in order, adding
+// 1/noob for every OOB tree where the feature's permuted vote is correct
+// (group 0 also sums qimp from the testreebag votes).  The float sums follow
+// the reference's tree order exactly.
+constexpr int VS_FEAT = 8;
+
 template <int W>
-__global__ void varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restrict__ vflags,
-                                     const uint64_t* __restrict__ flips, const uint64_t* __restrict__ iv,
-                                     const float* __restrict__ invnoob, int n, int p, int T, int impn,
-                                     float* __restrict__ qimp, float* __restrict__ qimpm) {
-    extern __shared__ float acc[];
-    const int tid = threadIdx.x, B = blockDim.x;
-    const int i = blockIdx.x * B + tid;
-    const bool valid = i < n;
-    for (int k = 0; k < p; ++k) acc[k * B + tid] = 0.0f;
-    float q = 0.0f;
-    if (valid && impn) {
-        for (int t = 0; t < T; ++t) {
-            const size_t ti = (size_t)t * n + i;
-            if (inbag[ti] != 0) continue;
-            const uint8_t fl = vflags[ti];
-            const float inv = invnoob[t];
-            const bool btb = (fl >> 1) & 1, bimp = (fl >> 2) & 1;
-            if (btb) q = __fadd_rn(q, inv);
+__global__ void __launch_bounds__(256)
+varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restrict__ vflags,
+                     const uint64_t* __restrict__ flips, const uint64_t* __restrict__ iv,
+                     const float* __restrict__ invnoob, int n, int p, int T, float* __restrict__ qimp,
+                     float* __restrict__ qimpm) {
+    const int G = (p + VS_FEAT - 1) / VS_FEAT;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * G) return;
+    const int i = (int)(idx / G);
+    const int g = (int)(idx % G);
+    const int k0 = g * VS_FEAT;
+    const int wq = k0 >> 6, sh = k0 & 63;  // 8-feature groups never straddle a 64-bit word
+    float acc[VS_FEAT];
 #pragma unroll
-            for (int w = 0; w < W; ++w) {
-                const uint64_t fw = flips[ti * W + w];
-                const uint64_t ivw = iv[(size_t)t * W + w];
-                // correct_k = iv_k ? (bimp ^ flip_k) : btb
-                const uint64_t corr = (ivw & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivw & (btb ? ~0ull : 0ull));
-                const int kend = min(64, p - w * 64);
-                for (int kk = 0; kk < kend; ++kk)
-                    if ((corr >> kk) & 1ull) {
-                        float* a = acc + (w * 64 + kk) * B + tid;
-                        *a = __fadd_rn(*a, inv);
-                    }
-            }
-        }
+    for (int u = 0; u < VS_FEAT; ++u) acc[u] = 0.0f;
+    float q = 0.0f;
+    for (int t = 0; t < T; ++t) {
+        const size_t ti = (size_t)t * n + i;
+        if (__ldg(inbag + ti) != 0) continue;
+        const uint8_t fl = __ldg(vflags + ti);
+        const float inv = __ldg(invnoob + t);
+        const bool btb = (fl >> 1) & 1, bimp = (fl >> 2) & 1;
+        if (btb) q = __fadd_rn(q, inv);
+        const uint64_t fw = __ldg(flips + ti * W + wq);
+        const uint64_t ivw = __ldg(iv + (size_t)t * W + wq);
+        const uint64_t corr = (ivw & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivw & (btb ? ~0ull : 0ull));
+        const uint32_t cb = (uint32_t)(corr >> sh) & 0xffu;
+#pragma unroll
+        for (int u = 0; u < VS_FEAT; ++u)
+            if ((cb >> u) & 1u) acc[u] = __fadd_rn(acc[u], inv);
     }
-    if (!valid) return;
-    if (impn) {
-        qimp[i] = q;
-        for (int k = 0; k < p; ++k) qimpm[(size_t)i * p + k] = acc[k * B + tid];
-    }
+    if (g == 0) qimp[i] = q;
+#pragma unroll
+    for (int u = 0; u < VS_FEAT; ++u)
+        if (k0 + u < p) qimpm[(size_t)i * p + k0 + u] = acc[u];
 }
 
-__global__ void varimp_feature_kernel(const int32_t* __restrict__ right, const int32_t* __restrict__ rightimp,
+// counts[2t] = #OOB correct by testreebag (right), counts[2t+1] = #OOB correct
+// by the unpermuted testreeimp walk; rightimp[t][k] = counts[2t+1] + delta[t][k].
+__global__ void varimp_feature_kernel(const int32_t* __restrict__ counts, const int32_t* __restrict__ delta,
                                       const int32_t* __restrict__ noob, const uint64_t* __restrict__ iv, int W,
                                       int p, int T, float* __restrict__ avimp, float* __restrict__ sqsd) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -246,7 +271,8 @@ __global__ void varimp_feature_kernel(const int32_t* __restrict__ right, const i
     float a = 0.0f, s = 0.0f;
     for (int t = 0; t < T; ++t) {
         if (!((iv[(size_t)t * W + (k >> 6)] >> (k & 63)) & 1ull)) continue;
-        const float rr = __fdiv_rn(__fsub_rn((float)right[t], (float)rightimp[(size_t)t * p + k]), (float)noob[t]);
+        const int rightimp = counts[2 * t + 1] + delta[(size_t)t * p + k];
+        const float rr = __fdiv_rn(__fsub_rn((float)counts[2 * t], (float)rightimp), (float)noob[t]);
         a = __fadd_rn(a, rr);
         s = __fadd_rn(s, __fmul_rn(rr, rr));
     }
@@ -266,23 +292,26 @@ template <int W>
 rfx_status launch_varimp_w(Ctx* c, int impn) {
     const size_t smem = (size_t)c->p * sizeof(int32_t);
     {
-    StageTimer st(c, ST_VARIMP_TREE, 1);
-    varimp_tree_kernel<W><<<c->T, VT, smem, c->stream>>>(
-        c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
-        c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, c->d_vflags, c->d_flips, c->d_right,
-        c->d_rightimp, c->d_err);
-    RFX_CUDA(cudaGetLastError());
+        StageTimer st(c, ST_VARIMP_TREE, 2);
+        RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
+        RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
+        joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob);
+        RFX_CUDA(cudaGetLastError());
+        int max_noob = 1;
+        for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
+        dim3 grid((max_noob + VW - 1) / VW, c->T);
+        varimp_walk_kernel<W><<<grid, VW, smem, c->stream>>>(
+            c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs, c->d_nnode, c->d_noob, c->d_cat,
+            c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, c->d_vflags, c->d_flips, c->d_right,
+            c->d_rightimp, c->d_err);
+        RFX_CUDA(cudaGetLastError());
     }
     if (impn) {
         StageTimer st(c, ST_VARIMP_SAMPLE, 1);
-        int B = 128;
-        while (B > 32 && (size_t)B * c->p * sizeof(float) > 96 * 1024) B >>= 1;
-        const size_t smem2 = (size_t)B * c->p * sizeof(float);
-        RFX_CUDA(cudaFuncSetAttribute(varimp_sample_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)std::max<size_t>(smem2, 1)));
-        varimp_sample_kernel<W><<<(c->n + B - 1) / B, B, smem2, c->stream>>>(
-            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, impn, c->d_qimp,
-            c->d_qimpm);
+        const long long G = (c->p + VS_FEAT - 1) / VS_FEAT;
+        const long long threads = (long long)c->n * G;
+        varimp_sample_kernel<W><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp, c->d_qimpm);
         RFX_CUDA(cudaGetLastError());
     }
     StageTimer st(c, ST_VARIMP_FEATURE, 1);

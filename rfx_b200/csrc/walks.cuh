@@ -11,8 +11,7 @@
 
 namespace rfx {
 
-__device__ __forceinline__ DNode load_node(const DNode* __restrict__ nodes, int k) {
-    int4 v = __ldg(reinterpret_cast<const int4*>(nodes) + k);
+__device__ __forceinline__ DNode as_node(int4 v) {
     DNode d;
     d.split = __int_as_float(v.x);
     d.left = v.y;
@@ -21,19 +20,40 @@ __device__ __forceinline__ DNode load_node(const DNode* __restrict__ nodes, int 
     return d;
 }
 
+__device__ __forceinline__ DNode load_node(const DNode* __restrict__ nodes, int k) {
+    return as_node(__ldg(reinterpret_cast<const int4*>(nodes) + k));
+}
+
+// Node source with the first `ntop` nodes of the tree staged in shared memory
+// (nodes are numbered in creation order, so these are the top levels).
+struct TopCachedNodes {
+    const int4* top;
+    int ntop;
+    const DNode* g;
+    __device__ __forceinline__ DNode operator()(int k) const {
+        return k < ntop ? as_node(top[k]) : as_node(__ldg(reinterpret_cast<const int4*>(g) + k));
+    }
+};
+
+struct GlobalNodes {
+    const DNode* g;
+    __device__ __forceinline__ DNode operator()(int k) const { return load_node(g, k); }
+};
+
 __device__ __forceinline__ int cgl_at(const int32_t* __restrict__ cgl, int maxcat, int node, int idx) {
     return cgl ? __ldg(cgl + (size_t)node * maxcat + idx) : 0;
 }
 
 // Returns the node id; *cls receives the class (nodeclass of the final node,
 // or of the root on the fallback path).
-__device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
-                                               const int32_t* __restrict__ nclass_of, int nnode,
-                                               const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
-                                               int maxcat, int* cls) {
+template <typename Src>
+__device__ __forceinline__ int walk_testreebag_src(const float* __restrict__ xrow, int p, const Src& nodes,
+                                                   const int32_t* __restrict__ nclass_of, int nnode,
+                                                   const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                   int maxcat, int* cls) {
     int kt = 0;
     int steps = 0;
-    DNode nd = load_node(nodes, 0);
+    DNode nd = nodes(0);
     while (node_status(nd.meta) == 1 && steps < 1000) {
         steps++;
         if (steps >= 1000) break;
@@ -52,10 +72,10 @@ __device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, i
         }
         if (kt < 0 || kt >= nnode) {
             kt = 0;
-            nd = load_node(nodes, 0);
+            nd = nodes(0);
             break;
         }
-        nd = load_node(nodes, kt);
+        nd = nodes(kt);
         if (node_status(nd.meta) != 1) break;
     }
     const int st = node_status(nd.meta);
@@ -67,14 +87,22 @@ __device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, i
     return 0;
 }
 
+__device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
+                                               const int32_t* __restrict__ nclass_of, int nnode,
+                                               const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                               int maxcat, int* cls) {
+    return walk_testreebag_src(xrow, p, GlobalNodes{nodes}, nclass_of, nnode, cat, cgl, maxcat, cls);
+}
+
 // find_terminal_node: stops only at status -1; invalid category or variable
 // returns the root.  maxnode is the reference's loop bound (2n+1).
-__device__ __forceinline__ int walk_terminal(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
-                                             const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
-                                             int maxcat, int maxnode) {
+template <typename Src>
+__device__ __forceinline__ int walk_terminal_src(const float* __restrict__ xrow, int p, const Src& nodes,
+                                                 const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                 int maxcat, int maxnode) {
     int cur = 0;
     for (int k = 0; k < maxnode; ++k) {
-        const DNode nd = load_node(nodes, cur);
+        const DNode nd = nodes(cur);
         if (node_status(nd.meta) == -1) return cur;
         const int m = node_var(nd.meta);
         if (m >= p) return 0;
@@ -91,6 +119,12 @@ __device__ __forceinline__ int walk_terminal(const float* __restrict__ xrow, int
         }
     }
     return 0;
+}
+
+__device__ __forceinline__ int walk_terminal(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
+                                             const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                             int maxcat, int maxnode) {
+    return walk_terminal_src(xrow, p, GlobalNodes{nodes}, cat, cgl, maxcat, maxnode);
 }
 
 // predict_classification's walk: returns the voted class, or -1 for no vote

@@ -204,11 +204,13 @@ def test_forest_validation_rejects_bad_children(built):
     ctx.close()
 
 
-def test_window_crossing_rows(built):
-    """n above one column window (24,576 columns): rows span two windows."""
+def test_window_crossing_rows(built, monkeypatch):
+    """Windowed kernel with n above one column window (24,576 columns): rows
+    span two windows."""
     from oracle import oracle as orc
     from rfx_b200 import abi
 
+    monkeypatch.setenv("RFX_PAIRS_KERNEL", "windowed")
     X, y = synth.mixed_cover(26000, seed=17)
     X, y, f = _grow(X, y, 6, 7)
     O = orc.analyse(X, y, f, do_imp=False)
@@ -217,6 +219,36 @@ def test_window_crossing_rows(built):
     S = ctx.proximity_upper()
     assert np.array_equal(S, O["S"])
     ctx.close()
+
+
+def test_many_trees_two_rounds(built):
+    """More trees than one expansion round of the row kernel (1024)."""
+    from oracle import oracle as orc
+    from rfx_b200 import abi
+
+    X, y, f = _grow(*synth.gaussian_classes(700, 6, 3, seed=4, mean_scale=0.7), 1100, 2)
+    O = orc.analyse(X, y, f, do_imp=True)
+    ctx = abi.Context(0)
+    ctx.load(f, X, y)
+    assert np.array_equal(ctx.proximity_upper(), O["S"])
+    avimp, sqsd, qimp, qimpm = ctx.varimp(True)
+    assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"])
+    ctx.close()
+
+
+def test_windowed_pair_kernel(built, monkeypatch):
+    """The windowed u32 pair kernel (large n or >= 65536 trees) on small cases."""
+    from oracle import oracle as orc
+    from rfx_b200 import abi
+
+    monkeypatch.setenv("RFX_PAIRS_KERNEL", "windowed")
+    for X, y, f in (_grow(*synth.mixed_cover(1800, seed=9), 20, 7), _grow(*synth.gaussian_classes(400, 5, 3), 30, 2)):
+        O = orc.analyse(X, y, f, do_imp=False)
+        ctx = abi.Context(0)
+        ctx.load(f, X, y)
+        assert np.array_equal(ctx.proximity_upper(), O["S"])
+        assert ctx.pair_updates() == int(O["S"].astype(np.int64).sum())
+        ctx.close()
 
 
 def test_full_size_properties(built):
