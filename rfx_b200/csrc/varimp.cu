@@ -263,21 +263,43 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
 
 // counts[2t] = #OOB correct by testreebag (right), counts[2t+1] = #OOB correct
 // by the unpermuted testreeimp walk; rightimp[t][k] = counts[2t+1] + delta[t][k].
+// One warp per feature: the lanes compute rr for 32 trees at once, then the
+// sums are added in tree order through shuffles (the float order of the
+// reference's per-tree accumulation).
 __global__ void varimp_feature_kernel(const int32_t* __restrict__ counts, const int32_t* __restrict__ delta,
                                       const int32_t* __restrict__ noob, const uint64_t* __restrict__ iv, int W,
                                       int p, int T, float* __restrict__ avimp, float* __restrict__ sqsd) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (k >= p) return;
     float a = 0.0f, s = 0.0f;
-    for (int t = 0; t < T; ++t) {
-        if (!((iv[(size_t)t * W + (k >> 6)] >> (k & 63)) & 1ull)) continue;
-        const int rightimp = counts[2 * t + 1] + delta[(size_t)t * p + k];
-        const float rr = __fdiv_rn(__fsub_rn((float)counts[2 * t], (float)rightimp), (float)noob[t]);
-        a = __fadd_rn(a, rr);
-        s = __fadd_rn(s, __fmul_rn(rr, rr));
+    for (int t0 = 0; t0 < T; t0 += 32) {
+        const int t = t0 + lane;
+        bool used = false;
+        float rr = 0.0f, r2 = 0.0f;
+        if (t < T) {
+            used = (iv[(size_t)t * W + (k >> 6)] >> (k & 63)) & 1ull;
+            if (used) {
+                const int rightimp = counts[2 * t + 1] + delta[(size_t)t * p + k];
+                rr = __fdiv_rn(__fsub_rn((float)counts[2 * t], (float)rightimp), (float)noob[t]);
+                r2 = __fmul_rn(rr, rr);
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, used);
+#pragma unroll 8
+        for (int l = 0; l < 32; ++l) {
+            const float x = __shfl_sync(0xffffffffu, rr, l);
+            const float x2 = __shfl_sync(0xffffffffu, r2, l);
+            if ((m >> l) & 1u) {
+                a = __fadd_rn(a, x);
+                s = __fadd_rn(s, x2);
+            }
+        }
     }
-    avimp[k] = a;
-    sqsd[k] = s;
+    if (lane == 0) {
+        avimp[k] = a;
+        sqsd[k] = s;
+    }
 }
 
 __global__ void localimp_kernel(const float* __restrict__ qimp, const float* __restrict__ qimpm, int n, int p, int T,
@@ -315,7 +337,7 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         RFX_CUDA(cudaGetLastError());
     }
     StageTimer st(c, ST_VARIMP_FEATURE, 1);
-    varimp_feature_kernel<<<(c->p + 127) / 128, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,
+    varimp_feature_kernel<<<(c->p + 3) / 4, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,
                                                                       W, c->p, c->T, c->d_avimp, c->d_sqsd);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
