@@ -140,6 +140,30 @@ rfx_status rfx_localimp(rfx_ctx* ctx, const float* qimp, const float* qimpm, flo
  * src/rf_random_forest.cpp:1925-2036, :2303-2411): votes[m*nclass]. */
 rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes);
 
+/* Allocation-free pair counts.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory while they run (a process
+ * that reserves the GPU's memory for its own arena up front and bans
+ * cudaMalloc/cudaFree afterwards, or a framework that lends the library only
+ * buffers it owns).  Computes the packed upper-triangle pair counts of
+ * rfx_proximity_upper_i32 from leaf indices the caller already holds:
+ *   leaf[t*n + i]  dense terminal-node index of sample i in tree t (terminal
+ *                  nodes numbered 0.. in node order), or -1 to leave it out;
+ *   inbag[t*n + i] nonzero when sample i is in-bag in tree t;
+ *   S[len]         output, len = n(n+1)/2.
+ * All three must be device memory; the work runs on `stream` (a cudaStream_t,
+ * NULL = default stream) and the call returns when it has finished.  It calls
+ * no cudaMalloc, cudaFree or allocating library routine: its temporaries live
+ * in one fixed array of about 26 MB inside the library, which every GPU that
+ * loads the library holds until the process exits.  Limits: n <= 32768,
+ * ntree <= 65535, ntree * n <= 1048576, 1 <= max_leaves <= n; larger inputs are
+ * rejected with RFX_ERR_INVALID.  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Every call uses the same array, so calls whose work
+ * overlaps on a GPU race with each other: serialise them. */
+rfx_status rfx_pair_counts_noalloc(const int32_t* leaf, const uint8_t* inbag, int32_t n, int32_t ntree,
+                                   int32_t max_leaves, int32_t* S, size_t len, void* stream);
+
 /* Per-stage device timing.  With profiling enabled, every stage launch is
  * bracketed by CUDA events on the context stream; rfx_profile_read waits for
  * the stream and returns, per stage, the mean duration of its launches since

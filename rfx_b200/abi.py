@@ -26,8 +26,8 @@ STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ER
 # Every symbol include/rfx_b200.h declares (checked by the CPU tests).
 EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
            "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
-           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_profile_enable", "rfx_profile_read",
-           "rfx_grow_forest", "rfx_free_forest"]
+           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_pair_counts_noalloc",
+           "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
           "predict", "oob_summary", "localimp", "pair_ranges"]
@@ -123,6 +123,12 @@ def grow_forest(X, y, ntree: int, mtry: int, minndsize: int = 1, maxnode: int = 
     finally:
         lib().rfx_free_forest(ctypes.byref(g))
     return f
+
+
+def pair_counts_noalloc(leaf, inbag, n: int, ntree: int, max_leaves: int, S, stream: int = 0) -> None:
+    """Allocation-free pair counts into the device buffer S (see include/rfx_b200.h)."""
+    _check(lib().rfx_pair_counts_noalloc(_vp(leaf), _vp(inbag), int(n), int(ntree), int(max_leaves), _vp(S),
+                                         ctypes.c_size_t(n * (n + 1) // 2), ctypes.c_void_p(stream)))
 
 
 class Context:

@@ -555,6 +555,37 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
     return RFX_OK;
 }
 
+// Pair-count pipeline on caller-provided device buffers (no context, no
+// allocation): leaf lists, opposite ranges, row order, then the full-row
+// kernel.  Used by the allocation-free entry point in noalloc.cu.
+rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream) {
+    int dev = 0, dev_smem = 0;
+    RFX_CUDA(cudaGetDevice(&dev));
+    RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const int max_keys = 2 * a.max_leaves;
+    int smem_keys = std::min(max_keys + 1, (dev_smem - 1024) / 4);
+    smem_keys = std::max(smem_keys, 32);
+    const size_t smem = (size_t)smem_keys * sizeof(int32_t);
+    RFX_CUDA(cudaFuncSetAttribute(build_csr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    build_csr_kernel<<<a.T, CSR_THREADS, smem, stream>>>(a.key, a.n, a.segbase, a.segoff, a.memb, smem_keys,
+                                                         a.err);
+    RFX_CUDA(cudaGetLastError());
+    if (max_keys + 1 > smem_keys) {
+        fix_global_segoff_kernel<<<a.T, 32, 0, stream>>>(a.segbase, a.segoff, smem_keys);
+        RFX_CUDA(cudaGetLastError());
+    }
+    dim3 g((a.n + OPP_TILE - 1) / OPP_TILE, (a.T + OPP_TILE - 1) / OPP_TILE);
+    opp_kernel<<<g, OPP_TILE * 8, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.T, a.opp);
+    RFX_CUDA(cudaGetLastError());
+    row_order_kernel<<<1, 1024, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.order);
+    RFX_CUDA(cudaGetLastError());
+    const size_t smem2 = ((size_t)a.n + 1) / 2 * sizeof(uint32_t);
+    RFX_CUDA(cudaFuncSetAttribute(pairs_row16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    pairs_row16_kernel<<<a.n, R16_THREADS, smem2, stream>>>(a.opp, a.memb, a.order, a.n, a.T, a.S, nullptr);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
 rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full) {
     StageTimer st(c, ST_FINISHPROX, 1);
     const int nt = (c->n + FP_TILE - 1) / FP_TILE;

@@ -169,4 +169,19 @@ rfx_status check_device_errors(Ctx* c);
 
 inline int64_t upper_len(int64_t n) { return n * (n + 1) / 2; }
 
+// Device buffers of the pair-count pipeline when they are not owned by a
+// context (see noalloc.cu).
+struct PairsRawArgs {
+    int n, T, max_leaves;
+    const int32_t* key;      // T*n
+    const int64_t* segbase;  // T+1
+    int32_t* segoff;         // segbase[T]
+    int32_t* memb;           // T*n
+    int2* opp;               // n*T
+    int32_t* order;          // n
+    uint32_t* err;
+    int32_t* S;              // n(n+1)/2
+};
+rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream);
+
 }  // namespace rfx
