@@ -367,6 +367,16 @@ extern "C" int rh_analyse_trees(const float* X, const int* y, const int* cat, in
     }
 }
 
+// cpu_permobmr (src/rf_varimp.cpp:16-30) on joob = 0..noob-1: the permuted
+// OOB positions.  Only call it for noob values whose MT19937(42) stream has no
+// draw that rounds to 1.0f (the reference then indexes past its vector).
+extern "C" int rh_permobmr(int noob, int* out) {
+    std::vector<integer_t> joob(noob);
+    for (int i = 0; i < noob; ++i) joob[i] = i;
+    rf::cpu_permobmr(joob.data(), out, noob);
+    return 0;
+}
+
 extern "C" int rh_finishprox(int n, const int* nout, double* prox, double* proxsym) {
     rf::cpu_finishprox(n, nout, prox, proxsym);
     return 0;

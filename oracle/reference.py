@@ -129,6 +129,13 @@ def analyse_trees(X, y, forest, t0=0, t1=None, do_imp=True, impn=True, do_prox=F
     return state
 
 
+def permobmr(noob: int) -> np.ndarray:
+    """The reference's cpu_permobmr permutation of OOB positions 0..noob-1."""
+    out = np.zeros(max(noob, 1), np.int32)
+    lib().rh_permobmr(int(noob), _p(out))
+    return out[:noob]
+
+
 def finishprox(prox_rowmajor, nout):
     """cpu_finishprox on a square [row][col] matrix; returns [row][col]."""
     n = nout.size
