@@ -140,6 +140,15 @@ rfx_status rfx_localimp(rfx_ctx* ctx, const float* qimp, const float* qimpm, flo
  * src/rf_random_forest.cpp:1925-2036, :2303-2411): votes[m*nclass]. */
 rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes);
 
+/* Classical 3-D MDS of the full proximity matrix, as compute_mds_3d_cpu
+ * (src/rf_mds_cpu.cpp:88-341) computes it when called by the binding
+ * (python/randomforest_py.cpp:1221-1243): P is the n x n float32 matrix of
+ * rfx_finishprox(full = 1) (host or device); rows are divided by nout again,
+ * D = max - P, double centring of D^2, the 3 largest eigenpairs (eigenvalues
+ * > 1e-10, descending) in FP64; coords = n x 3 row-major float64, each column
+ * defined up to sign.  evals (optional, host) receives the 3 eigenvalues. */
+rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* evals);
+
 /* Allocation-free pair counts.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run (a process

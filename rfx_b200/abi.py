@@ -26,7 +26,7 @@ STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ER
 # Every symbol include/rfx_b200.h declares (checked by the CPU tests).
 EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
            "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
-           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_pair_counts_noalloc",
+           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
@@ -240,6 +240,14 @@ class Context:
             out = np.zeros((self.n, self.p), np.float32)
         _check(lib().rfx_localimp(self._h, _vp(qimp), _vp(qimpm), _vp(out)))
         return out
+
+    def mds3d_full(self, P, coords=None):
+        """compute_mds_3d_cpu on the full float32 proximity matrix: (coords n x 3, eigenvalues)."""
+        if coords is None:
+            coords = np.zeros((self.n, 3), np.float64)
+        ev = np.zeros(3, np.float64)
+        _check(lib().rfx_mds3d_full(self._h, _vp(P), _vp(coords), _vp(ev)))
+        return coords, ev
 
     def predict_votes(self, Xt, votes=None):
         m = int(Xt.shape[0])

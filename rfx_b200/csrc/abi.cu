@@ -746,6 +746,51 @@ rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes) 
     return st;
 }
 
+rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* evals) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!P || !coords) {
+        set_error("rfx_mds3d_full: null argument");
+        return RFX_ERR_INVALID;
+    }
+    if (!c->routed) {
+        if ((st = launch_route(c))) return st;
+        c->routed = true;
+    }
+    const size_t nn = (size_t)c->n * c->n;
+    const float* dP = P;
+    float* sP = nullptr;
+    if (!is_device_ptr(P)) {
+        cudaError_t e = cudaMalloc((void**)&sP, sizeof(float) * nn);
+        if (e != cudaSuccess) return cuda_fail(e, "rfx_mds3d_full staging");
+        e = cudaMemcpyAsync(sP, P, sizeof(float) * nn, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) {
+            cudaFree(sP);
+            return cuda_fail(e, "rfx_mds3d_full H2D");
+        }
+        dP = sP;
+    }
+    const bool cdev = is_device_ptr(coords);
+    double* dC = coords;
+    if (!cdev) {
+        cudaError_t e = cudaMalloc((void**)&dC, sizeof(double) * (size_t)c->n * 3);
+        if (e != cudaSuccess) {
+            if (sP) cudaFree(sP);
+            return cuda_fail(e, "rfx_mds3d_full staging");
+        }
+    }
+    double ev[3] = {0, 0, 0};
+    st = launch_mds3d_full(c, dP, dC, ev);
+    if (st == RFX_OK && !cdev) st = copy_out(c, coords, dC, sizeof(double) * (size_t)c->n * 3);
+    if (st == RFX_OK) st = finish_host(c, true);
+    cudaStreamSynchronize(c->stream);
+    if (sP) cudaFree(sP);
+    if (!cdev) cudaFree(dC);
+    if (st == RFX_OK && evals) std::copy(ev, ev + 3, evals);
+    return st;
+}
+
 rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (!c) return RFX_ERR_INVALID;

@@ -166,6 +166,7 @@ rfx_status launch_varimp(Ctx* c, int impn);
 rfx_status launch_localimp(Ctx* c, const float* d_qimp, const float* d_qimpm, float* d_out);
 rfx_status launch_predict(Ctx* c, const float* dX, int m, int32_t* d_votes);
 rfx_status check_device_errors(Ctx* c);
+rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* evals);
 
 inline int64_t upper_len(int64_t n) { return n * (n + 1) / 2; }
 
