@@ -149,6 +149,43 @@ rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes);
  * defined up to sign.  evals (optional, host) receives the 3 eigenvalues. */
 rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* evals);
 
+/* Low-rank proximity (replaces the rank-1-per-tree QLORA accumulation of
+ * LowRankProximityMatrix, cuda/rf_proximity_lowrank.cu:863-1071, and the
+ * handle API get_lowrank_factors_host, cuda/rf_lowrank_helpers.cu:13):
+ * P ~= I + A A^T with A (n x rank, float32 row-major) from a randomised range
+ * finder over the leaf indicators of the loaded forest (rank + oversample
+ * columns, power_iters power iterations, CholeskyQR2 in FP64, FP64
+ * Rayleigh-Ritz).  precision 0 = FP32 throughout; 1 = BF16 storage of the
+ * sketch inputs and leaf sums with FP32 accumulation, final product in FP32.
+ * The context keeps the factors for the calls below; A and evals (host, the
+ * rank eigenvalues) may be NULL. */
+typedef struct rfx_lowrank_opts {
+    int32_t rank;
+    int32_t oversample;
+    int32_t power_iters;
+    int32_t precision;
+    uint64_t seed;
+} rfx_lowrank_opts;
+rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* opts, float* A, float* evals);
+
+/* Quantised factors with one scale per column (format 1: INT8, q = round(A/s),
+ * s = max|A[:,c]|/127; format 2: FP8 e4m3, s = max|A[:,c]|/448).  q is n x rank
+ * bytes, scales rank floats (either may be NULL).  The reference quantises with
+ * one per-tensor scale (cuda/rf_quantization_kernels.cu:107-120). */
+rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales);
+
+/* k-dimensional classical MDS from the factors (compute_mds_from_factors,
+ * cuda/rf_proximity_lowrank.cu:1935-2531): D = 1 - P off the diagonal with
+ * P = I + A A^T, double centring applied in factor space, the k largest
+ * eigenpairs; coords n x k row-major float64.  use_quantized = 1 uses the
+ * dequantised factors of rfx_lowrank_quantize. */
+rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, double* coords, double* evals);
+
+/* Outlier scores from the factors (compute_outlier_scores,
+ * src/rf_random_forest.cpp:2489-2520): 1 / sum_j P_ij^2, divided by the
+ * median element sorted[n/2]. */
+rfx_status rfx_outlier_scores(rfx_ctx* ctx, int use_quantized, float* scores);
+
 /* Allocation-free pair counts.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run (a process

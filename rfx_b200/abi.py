@@ -26,7 +26,8 @@ STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ER
 # Every symbol include/rfx_b200.h declares (checked by the CPU tests).
 EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
            "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
-           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_pair_counts_noalloc",
+           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
+           "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
@@ -50,6 +51,11 @@ class _ForestView(ctypes.Structure):
                 ("bestvar", ctypes.c_void_p), ("xbestsplit", ctypes.c_void_p), ("treemap", ctypes.c_void_p),
                 ("nodeclass", ctypes.c_void_p), ("catgoleft", ctypes.c_void_p), ("nin", ctypes.c_void_p),
                 ("X", ctypes.c_void_p), ("y", ctypes.c_void_p), ("cat", ctypes.c_void_p)]
+
+
+class _LowrankOpts(ctypes.Structure):
+    _fields_ = [("rank", ctypes.c_int32), ("oversample", ctypes.c_int32), ("power_iters", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("seed", ctypes.c_uint64)]
 
 
 class _Grown(ctypes.Structure):
@@ -248,6 +254,35 @@ class Context:
         ev = np.zeros(3, np.float64)
         _check(lib().rfx_mds3d_full(self._h, _vp(P), _vp(coords), _vp(ev)))
         return coords, ev
+
+    def lowrank(self, rank, oversample=16, power_iters=1, precision=0, seed=12345, A=None):
+        """Factors A (n x rank float32, P ~= I + A A^T) and the rank eigenvalues."""
+        self._rank_guess = rank
+        if A is None:
+            A = np.zeros((self.n, rank), np.float32)
+        ev = np.zeros(rank, np.float32)
+        o = _LowrankOpts(rank=rank, oversample=oversample, power_iters=power_iters, precision=precision, seed=seed)
+        _check(lib().rfx_lowrank(self._h, ctypes.byref(o), _vp(A), _vp(ev)))
+        return A, ev
+
+    def lowrank_quantize(self, fmt):
+        """fmt 1 = INT8, 2 = FP8 e4m3: (q as uint8 bytes n x rank, scales)."""
+        r = self._rank_guess
+        q = np.zeros((self.n, r), np.uint8)
+        sc = np.zeros(r, np.float32)
+        _check(lib().rfx_lowrank_quantize(self._h, int(fmt), _vp(q), _vp(sc)))
+        return q, sc
+
+    def mds_from_factors(self, k=3, use_quantized=False):
+        coords = np.zeros((self.n, k), np.float64)
+        ev = np.zeros(k, np.float64)
+        _check(lib().rfx_mds_from_factors(self._h, int(k), int(bool(use_quantized)), _vp(coords), _vp(ev)))
+        return coords, ev
+
+    def outlier_scores(self, use_quantized=False):
+        out = np.zeros(self.n, np.float32)
+        _check(lib().rfx_outlier_scores(self._h, int(bool(use_quantized)), _vp(out)))
+        return out
 
     def predict_votes(self, Xt, votes=None):
         m = int(Xt.shape[0])

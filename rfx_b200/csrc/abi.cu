@@ -95,6 +95,11 @@ void free_forest(Ctx* c) {
     dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_vflags); dfree(c, c->d_flips);
     dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
     dfree(c, c->d_sqsd); dfree(c, c->d_opp); dfree(c, c->d_order);
+    dfree(c, c->d_lrA); dfree(c, c->d_lrAq); dfree(c, c->d_lrScale);
+    if (c->d_lrQ) cudaFree(c->d_lrQ);
+    c->d_lrQ = nullptr;
+    c->lr_rank = 0;
+    c->lr_qformat = 0;
     c->loaded = c->routed = c->csr_built = false;
     c->bytes = 0;
 }
@@ -789,6 +794,135 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
     if (!cdev) cudaFree(dC);
     if (st == RFX_OK && evals) std::copy(ev, ev + 3, evals);
     return st;
+}
+
+rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* o, float* A, float* evals) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!o) return RFX_ERR_INVALID;
+    const int k = o->rank;
+    if (k < 1 || o->oversample < 0 || o->power_iters < 0 || o->power_iters > 8) {
+        set_error("rfx_lowrank: invalid options");
+        return RFX_ERR_INVALID;
+    }
+    dfree(c, c->d_lrA);
+    dfree(c, c->d_lrAq);
+    dfree(c, c->d_lrScale);
+    if (c->d_lrQ) cudaFree(c->d_lrQ);
+    c->d_lrQ = nullptr;
+    c->lr_rank = 0;
+    c->lr_qformat = 0;
+    if ((st = dalloc(c, &c->d_lrA, (size_t)c->n * k))) return st;
+    std::vector<float> ev(k);
+    st = lowrank_compute(c, k, o->oversample, o->power_iters, o->precision, o->seed ? o->seed : 12345ull, c->d_lrA,
+                         ev.data());
+    if (st) return st;
+    c->lr_rank = k;
+    if (evals) std::copy(ev.begin(), ev.end(), evals);
+    if (A) {
+        if ((st = copy_out(c, A, c->d_lrA, sizeof(float) * (size_t)c->n * k))) return st;
+        RFX_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return check_device_errors(c);
+}
+
+rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!c->lr_rank) {
+        set_error("rfx_lowrank_quantize: no factors (call rfx_lowrank first)");
+        return RFX_ERR_STATE;
+    }
+    if (format != 1 && format != 2) {
+        set_error("rfx_lowrank_quantize: format must be 1 (INT8) or 2 (FP8 e4m3)");
+        return RFX_ERR_INVALID;
+    }
+    const int k = c->lr_rank;
+    const size_t nk = (size_t)c->n * k;
+    if (c->d_lrQ) cudaFree(c->d_lrQ);
+    c->d_lrQ = nullptr;
+    if (cudaMalloc(&c->d_lrQ, nk) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("rfx_lowrank_quantize: allocation failed");
+        return RFX_ERR_OOM;
+    }
+    if ((st = dalloc(c, &c->d_lrScale, k))) return st;
+    if ((st = dalloc(c, &c->d_lrAq, nk))) return st;
+    if ((st = lowrank_quantize(c, c->d_lrA, k, format, c->d_lrQ, c->d_lrScale))) return st;
+    if ((st = lowrank_dequantize(c, c->d_lrQ, c->d_lrScale, k, format, c->d_lrAq))) return st;
+    c->lr_qformat = format;
+    if (q && (st = copy_out(c, q, c->d_lrQ, nk))) return st;
+    if (scales && (st = copy_out(c, scales, c->d_lrScale, sizeof(float) * k))) return st;
+    RFX_CUDA(cudaStreamSynchronize(c->stream));
+    return RFX_OK;
+}
+
+static const float* factors_for(Ctx* c, int use_quantized) {
+    if (use_quantized) return c->lr_qformat ? c->d_lrAq : nullptr;
+    return c->d_lrA;
+}
+
+rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, double* coords, double* evals) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    const float* dA = c->lr_rank ? factors_for(c, use_quantized) : nullptr;
+    if (!dA) {
+        set_error("Low-rank factors not available (call rfx_lowrank, and rfx_lowrank_quantize for quantized factors)");
+        return RFX_ERR_STATE;
+    }
+    if (!coords || k < 1) return RFX_ERR_INVALID;
+    const bool cdev = is_device_ptr(coords);
+    double* dC = coords;
+    if (!cdev) {
+        cudaError_t e = cudaMalloc((void**)&dC, sizeof(double) * (size_t)c->n * k);
+        if (e != cudaSuccess) return cuda_fail(e, "rfx_mds_from_factors staging");
+    }
+    std::vector<double> ev(8, 0.0);
+    int iters = 0;
+    st = launch_mds_factors(c, dA, c->lr_rank, k, 600, 1e-10, dC, ev.data(), &iters);
+    if (st == RFX_OK && !cdev) st = copy_out(c, coords, dC, sizeof(double) * (size_t)c->n * k);
+    if (st == RFX_OK) st = finish_host(c, true);
+    cudaStreamSynchronize(c->stream);
+    if (!cdev) cudaFree(dC);
+    if (st == RFX_OK && evals) std::copy(ev.begin(), ev.begin() + k, evals);
+    return st;
+}
+
+rfx_status rfx_outlier_scores(rfx_ctx* ctx, int use_quantized, float* scores) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    const float* dA = c->lr_rank ? factors_for(c, use_quantized) : nullptr;
+    if (!dA || !scores) {
+        set_error("rfx_outlier_scores: factors not available");
+        return RFX_ERR_STATE;
+    }
+    float* d = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(float) * c->n);
+    if (e != cudaSuccess) return cuda_fail(e, "rfx_outlier_scores");
+    st = launch_outlier_scores(c, dA, c->lr_rank, d);
+    std::vector<float> h(c->n);
+    if (st == RFX_OK) {
+        e = cudaMemcpy(h.data(), d, sizeof(float) * c->n, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "rfx_outlier_scores D2H");
+    }
+    cudaFree(d);
+    if (st) return st;
+    // normalise by the median element sorted[n/2], as compute_outlier_scores does
+    std::vector<float> srt = h;
+    std::nth_element(srt.begin(), srt.begin() + c->n / 2, srt.end());
+    const float med = srt[c->n / 2];
+    if (med > 0)
+        for (auto& x : h) x /= med;
+    if (is_device_ptr(scores)) {
+        RFX_CUDA(cudaMemcpy(scores, h.data(), sizeof(float) * c->n, cudaMemcpyHostToDevice));
+    } else {
+        std::copy(h.begin(), h.end(), scores);
+    }
+    return RFX_OK;
 }
 
 rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable) {

@@ -1,0 +1,489 @@
+// Low-rank proximity: a randomised range finder over the leaf indicators.
+//
+// The normalised proximity of cpu_finishprox (src/rf_finishprox.cpp:12-74) is
+//   P = I + M,  M = 1/4 (D S + S D),  D = diag(1/nout_i) (1 where nout_i = 0),
+// with S = C + C^T the pair counts of cpu_proximity's dense branch.  S is never
+// formed: S X = sum_t (Z_oob,t Z_in,t^T + Z_in,t Z_oob,t^T) X is applied tree by
+// tree through the leaf member lists (per leaf key, the sum of the members'
+// rows of X, then every sample adds the sum of the opposite bag status of its
+// own leaf).  The factors replace the reference's rank-1-per-tree QLORA
+// accumulation (cuda/rf_proximity_lowrank.cu:863-1071) and satisfy
+// P ~= I + A A^T with A = Q U_k Lambda_k^(1/2) from the top-k eigenpairs of
+// M restricted to the range Q of the sketch M^(q+1) Omega.
+//
+// Forms:
+//   FP32  - X, leaf sums and products in FP32;
+//   mixed - X and leaf sums stored in BF16 (the Gaussian test matrix is
+//           exact in BF16), FP32 accumulation; the final product M Q that
+//           builds the Rayleigh-Ritz projection runs in FP32 (one refinement).
+// FP64 is used for the k' x k' Gram (CholeskyQR2) and the eigensolve only.
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "dense.cuh"
+#include "rfx_internal.cuh"
+
+namespace rfx {
+namespace {
+
+__device__ __forceinline__ float ld_val(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_val(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void st_val(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st_val(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+
+// Gaussian from a counter hash (splitmix64) and Box-Muller.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+template <typename T>
+__global__ void gauss_kernel(T* __restrict__ out, int64_t count, uint64_t seed) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const uint64_t h = mix64(seed ^ mix64((uint64_t)idx));
+    const double u1 = ((h >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+    const double u2 = (double)(mix64(h) >> 11) * (1.0 / 9007199254740992.0);
+    const double g = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+    st_val(out + idx, (float)g);
+}
+
+// X = [V | D V] in the storage type (n x 2w), from V (n x w, FP32).
+template <typename TX>
+__global__ void pack_x_kernel(const float* __restrict__ V, const float* __restrict__ dinv, int n, int w,
+                              TX* __restrict__ X) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * w) return;
+    const int i = (int)(idx / w), c = (int)(idx % w);
+    const float v = V[idx];
+    st_val(X + (size_t)i * 2 * w + c, v);
+    st_val(X + (size_t)i * 2 * w + w + c, __fmul_rn(v, dinv[i]));
+}
+
+// Leaf-key sums of X rows for trees [t0, t1): G[gofs[t-t0] + key][c] =
+// sum over members j of key of X[j][c].  One warp per key.
+template <typename TX, typename TG>
+__global__ void segsum_kernel(const TX* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
+                              const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
+                              int t1, const int64_t* __restrict__ gofs, TG* __restrict__ G) {
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    // locate (tree, key): gofs holds the key prefix of the batch (in keys)
+    const int64_t total = gofs[t1 - t0];
+    if (warp >= total) return;
+    int lo = 0, hi = t1 - t0;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (gofs[mid] <= warp) lo = mid;
+        else hi = mid;
+    }
+    const int t = t0 + lo;
+    const int key = (int)(warp - gofs[lo]);
+    const int32_t* so = segoff + segbase[t];
+    const int s0 = so[key], s1 = so[key + 1];
+    const int32_t* mt = memb + (size_t)t * n;
+    TG* g = G + (size_t)warp * W;
+    for (int c0 = 0; c0 < W; c0 += 32) {
+        const int c = c0 + lane;
+        float acc = 0.0f;
+        if (c < W)
+            for (int q = s0; q < s1; ++q) acc += ld_val(X + (size_t)__ldg(mt + q) * W + c);
+        if (c < W) st_val(g + c, acc);
+    }
+}
+
+// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample.
+template <typename TG>
+__global__ void pull_kernel(const TG* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
+                            const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate) {
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int i = (int)warp;
+    float acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = 0.0f;
+    for (int t = t0; t < t1; ++t) {
+        const int k = __ldg(key + (size_t)t * n + i);
+        if (k < 0) continue;
+        const TG* g = G + (size_t)(gofs[t - t0] + (k ^ 1)) * W;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int c = lane + 32 * q;
+            if (c < W) acc[q] += ld_val(g + c);
+        }
+    }
+    float* y = Y + (size_t)i * W;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int c = lane + 32 * q;
+        if (c < W) y[c] = accumulate ? y[c] + acc[q] : acc[q];
+    }
+}
+
+// MV = 1/4 (D Y[:, :w] + Y[:, w:])
+__global__ void combine_kernel(const float* __restrict__ Y, const float* __restrict__ dinv, int n, int w,
+                               float* __restrict__ out) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * w) return;
+    const int i = (int)(idx / w), c = (int)(idx % w);
+    const float a = Y[(size_t)i * 2 * w + c], b = Y[(size_t)i * 2 * w + w + c];
+    out[idx] = 0.25f * (dinv[i] * a + b);
+}
+
+__global__ void dinv_kernel(const int32_t* __restrict__ nout, int n, float* __restrict__ dinv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dinv[i] = nout[i] > 0 ? (float)(1.0 / (double)nout[i]) : 1.0f;
+}
+
+// G[w x w] (FP64) += X^T Y over rows; X, Y n x w FP32.  Block: 256 threads,
+// 64-row chunks, each thread accumulates (w*w)/256 entries.
+constexpr int GW = 128;  // maximum width
+__global__ void __launch_bounds__(256) gram_f32_kernel(const float* __restrict__ X, const float* __restrict__ Y,
+                                                       int n, int w, double* __restrict__ G) {
+    __shared__ float Xs[32][GW], Ys[32][GW];
+    const int tid = threadIdx.x;
+    const int ww = w * w;
+    double acc[64];
+#pragma unroll
+    for (int q = 0; q < 64; ++q) acc[q] = 0.0;
+    for (int r0 = blockIdx.x * 32; r0 < n; r0 += gridDim.x * 32) {
+        for (int e = tid; e < 32 * w; e += 256) {
+            const int r = e / w, c = e % w;
+            Xs[r][c] = (r0 + r < n) ? X[(size_t)(r0 + r) * w + c] : 0.0f;
+            Ys[r][c] = (r0 + r < n) ? Y[(size_t)(r0 + r) * w + c] : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int q = 0; q < 64; ++q) {
+            const int e = tid + q * 256;
+            if (e >= ww) break;
+            const int a = e / w, b = e % w;
+            double s = 0.0;
+            for (int r = 0; r < 32; ++r) s += (double)Xs[r][a] * (double)Ys[r][b];
+            acc[q] += s;
+        }
+        __syncthreads();
+    }
+    for (int q = 0; q < 64; ++q) {
+        const int e = tid + q * 256;
+        if (e >= ww) break;
+        atomicAdd(G + e, acc[q]);
+    }
+}
+
+// One CTA: T = L^{-T} for G = L L^T (w x w), in shared memory (dynamic).
+__global__ void chol_inv_w_kernel(const double* __restrict__ G, int w, double* __restrict__ Tm, int* __restrict__ bad) {
+    extern __shared__ double sm[];
+    double* L = sm;
+    double* Li = sm + w * w;
+    __shared__ double flag;
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) L[e] = G[e];
+    __syncthreads();
+    if (!cta_cholesky(L, w, w, &flag) && threadIdx.x == 0) *bad = 1;
+    cta_tri_inverse(L, Li, w, w);
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        const int i = e / w, j = e % w;
+        Tm[i * w + j] = Li[j * w + i];
+    }
+}
+
+// out[n x m] = X[n x w] T[w x m] (FP32 X, FP64 T)
+__global__ void right_mul_kernel(const float* __restrict__ X, const double* __restrict__ Tm, int n, int w, int m,
+                                 float* __restrict__ out) {
+    extern __shared__ double Ts[];
+    for (int e = threadIdx.x; e < w * m; e += blockDim.x) Ts[e] = Tm[e];
+    __syncthreads();
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * m) return;
+    const int i = (int)(idx / m), c = (int)(idx % m);
+    double v = 0.0;
+    for (int k = 0; k < w; ++k) v += (double)X[(size_t)i * w + k] * Ts[k * m + c];
+    out[idx] = (float)v;
+}
+
+// One CTA: eigen-decomposition of the symmetrised w x w H.
+__global__ void eig_w_kernel(const double* __restrict__ H, int w, double* __restrict__ evals,
+                             double* __restrict__ evecs) {
+    extern __shared__ double sm[];
+    double* A = sm;
+    double* U = sm + w * w;
+    __shared__ int pairs[2 * 64];
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
+        const int i = e / w, j = e % w;
+        A[e] = 0.5 * (H[i * w + j] + H[j * w + i]);
+    }
+    __syncthreads();
+    cta_jacobi(A, U, w, w, 14, pairs);
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) evecs[e] = U[e];
+    for (int i = threadIdx.x; i < w; i += blockDim.x) evals[i] = A[i * w + i];
+}
+
+__global__ void colmax_kernel(const float* __restrict__ A, int n, int k, unsigned int* __restrict__ mx) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * k) return;
+    atomicMax(mx + (idx % k), __float_as_uint(fabsf(A[idx])));
+}
+
+__global__ void quant_i8_kernel(const float* __restrict__ A, int n, int k, const unsigned int* __restrict__ mx,
+                                int8_t* __restrict__ q, float* __restrict__ scale) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < k) scale[idx] = __uint_as_float(mx[idx]) / 127.0f;
+    if (idx >= (int64_t)n * k) return;
+    const float s = __uint_as_float(mx[idx % k]) / 127.0f;
+    const float v = s > 0.0f ? rintf(A[idx] / s) : 0.0f;
+    q[idx] = (int8_t)fmaxf(-127.0f, fminf(127.0f, v));
+}
+
+__global__ void quant_fp8_kernel(const float* __restrict__ A, int n, int k, const unsigned int* __restrict__ mx,
+                                 __nv_fp8_e4m3* __restrict__ q, float* __restrict__ scale) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < k) scale[idx] = __uint_as_float(mx[idx]) / 448.0f;
+    if (idx >= (int64_t)n * k) return;
+    const float s = __uint_as_float(mx[idx % k]) / 448.0f;
+    q[idx] = __nv_fp8_e4m3(s > 0.0f ? A[idx] / s : 0.0f);
+}
+
+template <typename TQ>
+__global__ void dequant_kernel(const TQ* __restrict__ q, const float* __restrict__ scale, int n, int k,
+                               float* __restrict__ A) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * k) return;
+    A[idx] = (float)q[idx] * scale[idx % k];
+}
+
+struct DevBufs {
+    std::vector<void*> p;
+    ~DevBufs() {
+        for (void* x : p) cudaFree(x);
+    }
+    template <typename T>
+    T* get(size_t count) {
+        void* x = nullptr;
+        if (cudaMalloc(&x, sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        p.push_back(x);
+        return static_cast<T*>(x);
+    }
+};
+
+inline unsigned nblk(int64_t count, int b = 256) { return (unsigned)((count + b - 1) / b); }
+
+}  // namespace
+
+// Apply M to V (n x w FP32) into MV (n x w FP32).  TX/TG: storage types of the
+// packed inputs and the leaf sums.
+template <typename TX, typename TG>
+rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, TX* X, TG* G, float* Y,
+                   const std::vector<int64_t>& batch_start, int64_t* d_gofs, const std::vector<int64_t>& h_gofs_all) {
+    cudaStream_t s = c->stream;
+    const int n = c->n, W = 2 * w;
+    pack_x_kernel<TX><<<nblk((int64_t)n * w), 256, 0, s>>>(V, dinv, n, w, X);
+    RFX_CUDA(cudaGetLastError());
+    c->launches += 1;
+    for (size_t b = 0; b + 1 < batch_start.size(); ++b) {
+        const int t0 = (int)batch_start[b], t1 = (int)batch_start[b + 1];
+        // key prefix of this batch (device copy prepared by the caller)
+        const int64_t* gofs = d_gofs + (h_gofs_all[b]);
+        const int64_t keys = h_gofs_all[b + 1] - h_gofs_all[b] - 1;  // stored with one sentinel per batch
+        (void)keys;
+        const int64_t total_keys = c->h_segbase[t1] - c->h_segbase[t0] - (t1 - t0);
+        segsum_kernel<TX, TG><<<nblk(total_keys * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0,
+                                                                   t1, gofs, G);
+        pull_kernel<TG><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0);
+        c->launches += 2;
+        RFX_CUDA(cudaGetLastError());
+    }
+    combine_kernel<<<nblk((int64_t)n * w), 256, 0, s>>>(Y, dinv, n, w, MV);
+    c->launches += 1;
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int precision, uint64_t seed,
+                           float* d_A_out, float* h_evals) {
+    cudaStream_t s = c->stream;
+    const int n = c->n, T = c->T;
+    const int w = k + oversample;
+    if (k < 1 || w > GW || w > n) {
+        set_error("rfx_lowrank: need 1 <= rank and rank + oversample <= min(128, n)");
+        return RFX_ERR_INVALID;
+    }
+    rfx_status st = launch_route(c);
+    if (st == RFX_OK) st = launch_build_csr(c);
+    if (st != RFX_OK) return st;
+    c->routed = true;
+    c->csr_built = true;
+    const int W = 2 * w;
+    // tree batches: leaf-sum storage per batch bounded to ~512 MB
+    const size_t gbytes_row = (size_t)W * (precision ? 2 : 4);
+    std::vector<int64_t> batch_start{0};
+    std::vector<int64_t> h_gofs;  // per batch: key prefix (batch-local), with a sentinel
+    std::vector<int64_t> gofs_index;  // offset of each batch's prefix inside h_gofs
+    int64_t max_batch_keys = 0;
+    {
+        int t = 0;
+        while (t < T) {
+            int64_t keys = 0;
+            int t1 = t;
+            while (t1 < T) {
+                const int64_t kt = c->h_segbase[t1 + 1] - c->h_segbase[t1] - 1;
+                if (t1 > t && (size_t)(keys + kt) * gbytes_row > ((size_t)512 << 20)) break;
+                keys += kt;
+                ++t1;
+            }
+            gofs_index.push_back((int64_t)h_gofs.size());
+            int64_t acc = 0;
+            for (int q = t; q < t1; ++q) {
+                h_gofs.push_back(acc);
+                acc += c->h_segbase[q + 1] - c->h_segbase[q] - 1;
+            }
+            h_gofs.push_back(acc);
+            max_batch_keys = std::max(max_batch_keys, acc);
+            batch_start.push_back(t1);
+            t = t1;
+        }
+        gofs_index.push_back((int64_t)h_gofs.size());
+    }
+    DevBufs d;
+    float* dinv = d.get<float>(n);
+    float* Om = d.get<float>((size_t)n * w);
+    float* Yw = d.get<float>((size_t)n * w);
+    float* Q = d.get<float>((size_t)n * w);
+    float* Z = d.get<float>((size_t)n * w);
+    float* Ybig = d.get<float>((size_t)n * W);
+    int64_t* d_gofs = d.get<int64_t>(h_gofs.size());
+    double* Gm = d.get<double>((size_t)w * w);
+    double* Tm = d.get<double>((size_t)w * w);
+    double* ev = d.get<double>(w);
+    double* U = d.get<double>((size_t)w * w);
+    int* bad = d.get<int>(1);
+    void* X = precision ? (void*)d.get<__nv_bfloat16>((size_t)n * W) : (void*)d.get<float>((size_t)n * W);
+    void* G = precision ? (void*)d.get<__nv_bfloat16>((size_t)max_batch_keys * W)
+                        : (void*)d.get<float>((size_t)max_batch_keys * W);
+    void* X32 = precision ? (void*)d.get<float>((size_t)n * W) : X;
+    void* G32 = precision ? (void*)d.get<float>((size_t)max_batch_keys * W) : G;
+    if (!dinv || !Om || !Yw || !Q || !Z || !Ybig || !d_gofs || !Gm || !Tm || !ev || !U || !bad || !X || !G || !X32 ||
+        !G32) {
+        set_error("rfx_lowrank: device allocation failed");
+        return RFX_ERR_OOM;
+    }
+    RFX_CUDA(cudaMemcpyAsync(d_gofs, h_gofs.data(), sizeof(int64_t) * h_gofs.size(), cudaMemcpyHostToDevice, s));
+    RFX_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+    dinv_kernel<<<nblk(n), 256, 0, s>>>(c->d_nout, n, dinv);
+    gauss_kernel<float><<<nblk((int64_t)n * w), 256, 0, s>>>(Om, (int64_t)n * w, seed);
+    c->launches += 2;
+    // per-batch prefix pointers: apply_m takes the whole table and indexes it
+    std::vector<int64_t> pref_at(gofs_index.begin(), gofs_index.end());
+    auto apply = [&](const float* V, float* MV, bool fp32) -> rfx_status {
+        if (fp32)
+            return apply_m<float, float>(c, V, w, MV, dinv, (float*)X32, (float*)G32, Ybig, batch_start, d_gofs,
+                                         pref_at);
+        return apply_m<__nv_bfloat16, __nv_bfloat16>(c, V, w, MV, dinv, (__nv_bfloat16*)X, (__nv_bfloat16*)G, Ybig,
+                                                     batch_start, d_gofs, pref_at);
+    };
+    const size_t sm2 = 2 * (size_t)w * w * sizeof(double);
+    RFX_CUDA(cudaFuncSetAttribute(chol_inv_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    RFX_CUDA(cudaFuncSetAttribute(eig_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    RFX_CUDA(cudaFuncSetAttribute(right_mul_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * w * w)));
+    auto orth = [&](const float* src, float* out) -> rfx_status {
+        // CholeskyQR2 with FP64 Gram and FP64 triangular factors
+        const float* cur = src;
+        float* tmp = Z;
+        for (int pass = 0; pass < 2; ++pass) {
+            RFX_CUDA(cudaMemsetAsync(Gm, 0, sizeof(double) * w * w, s));
+            gram_f32_kernel<<<std::min(1024, (n + 31) / 32), 256, 0, s>>>(cur, cur, n, w, Gm);
+            chol_inv_w_kernel<<<1, 256, sm2, s>>>(Gm, w, Tm, bad);
+            float* dst = pass == 0 ? tmp : out;
+            right_mul_kernel<<<nblk((int64_t)n * w), 256, sizeof(double) * w * w, s>>>(cur, Tm, n, w, w, dst);
+            c->launches += 3;
+            RFX_CUDA(cudaGetLastError());
+            cur = dst;
+        }
+        return RFX_OK;
+    };
+    const bool mixed = precision != 0;
+    // sketch: Yw = M Om, then power iterations
+    if ((st = apply(Om, Yw, !mixed)) != RFX_OK) return st;
+    for (int q = 0; q < power_iters; ++q) {
+        if ((st = orth(Yw, Q)) != RFX_OK) return st;
+        if ((st = apply(Q, Yw, !mixed)) != RFX_OK) return st;
+    }
+    if ((st = orth(Yw, Q)) != RFX_OK) return st;
+    // Rayleigh-Ritz with an FP32 product (the refinement step of the mixed form)
+    if ((st = apply(Q, Yw, true)) != RFX_OK) return st;
+    RFX_CUDA(cudaMemsetAsync(Gm, 0, sizeof(double) * w * w, s));
+    gram_f32_kernel<<<std::min(1024, (n + 31) / 32), 256, 0, s>>>(Q, Yw, n, w, Gm);
+    eig_w_kernel<<<1, 256, sm2, s>>>(Gm, w, ev, U);
+    c->launches += 2;
+    RFX_CUDA(cudaGetLastError());
+    std::vector<double> hev(w), hU((size_t)w * w);
+    RFX_CUDA(cudaMemcpyAsync(hev.data(), ev, sizeof(double) * w, cudaMemcpyDeviceToHost, s));
+    RFX_CUDA(cudaMemcpyAsync(hU.data(), U, sizeof(double) * w * w, cudaMemcpyDeviceToHost, s));
+    RFX_CUDA(cudaStreamSynchronize(s));
+    int hbad = 0;
+    RFX_CUDA(cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hbad) {
+        set_error("rfx_lowrank: the sketch lost rank (Cholesky pivot <= 0)");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    // top-k eigenpairs (largest first); A = Q U_k sqrt(max(lambda, 0))
+    std::vector<int> idx(w);
+    for (int q = 0; q < w; ++q) idx[q] = q;
+    std::sort(idx.begin(), idx.end(), [&](int a, int b) { return hev[a] > hev[b]; });
+    std::vector<double> Tk((size_t)w * k);
+    for (int col = 0; col < k; ++col) {
+        const double lam = hev[idx[col]];
+        const double sc = lam > 0 ? std::sqrt(lam) : 0.0;
+        if (h_evals) h_evals[col] = (float)lam;
+        for (int r = 0; r < w; ++r) Tk[(size_t)r * k + col] = hU[(size_t)r * w + idx[col]] * sc;
+    }
+    RFX_CUDA(cudaMemcpyAsync(Tm, Tk.data(), sizeof(double) * w * k, cudaMemcpyHostToDevice, s));
+    right_mul_kernel<<<nblk((int64_t)n * k), 256, sizeof(double) * w * k, s>>>(Q, Tm, n, w, k, d_A_out);
+    c->launches += 1;
+    RFX_CUDA(cudaGetLastError());
+    RFX_CUDA(cudaStreamSynchronize(s));
+    return RFX_OK;
+}
+
+rfx_status lowrank_quantize(Ctx* c, const float* dA, int k, int format, void* dq, float* dscale) {
+    cudaStream_t s = c->stream;
+    const int n = c->n;
+    DevBufs d;
+    unsigned int* mx = d.get<unsigned int>(k);
+    if (!mx) return RFX_ERR_OOM;
+    RFX_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned int) * k, s));
+    colmax_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, mx);
+    if (format == 1)
+        quant_i8_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, mx, (int8_t*)dq, dscale);
+    else
+        quant_fp8_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, mx, (__nv_fp8_e4m3*)dq, dscale);
+    c->launches += 2;
+    RFX_CUDA(cudaGetLastError());
+    RFX_CUDA(cudaStreamSynchronize(s));
+    return RFX_OK;
+}
+
+rfx_status lowrank_dequantize(Ctx* c, const void* dq, const float* dscale, int k, int format, float* dA) {
+    cudaStream_t s = c->stream;
+    const int n = c->n;
+    if (format == 1)
+        dequant_kernel<int8_t><<<nblk((int64_t)n * k), 256, 0, s>>>((const int8_t*)dq, dscale, n, k, dA);
+    else
+        dequant_kernel<__nv_fp8_e4m3><<<nblk((int64_t)n * k), 256, 0, s>>>((const __nv_fp8_e4m3*)dq, dscale, n, k,
+                                                                           dA);
+    c->launches += 1;
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+}  // namespace rfx

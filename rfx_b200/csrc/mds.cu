@@ -230,7 +230,8 @@ struct Dev {
 // and the factor MDS.
 template <typename Apply>
 rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double* d_out, double* evals_out,
-                         uint64_t seed) {
+                         uint64_t seed, double tol = 1e-14, const double* warm_in = nullptr, double* keep_out = nullptr,
+                         int* iters_out = nullptr) {
     cudaStream_t s = c->stream;
     Dev d;
     double* V = d.get<double>((size_t)n * S_BLK);
@@ -246,9 +247,12 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
         set_error("MDS: device allocation failed");
         return RFX_ERR_OOM;
     }
-    // start block: seeded Gaussian (srand(12345 + 1000*eig) seeds the reference's
-    // factor MDS; any start converges to the same subspace)
-    {
+    // start block: a warm start (a previous basis) or a seeded Gaussian
+    // (srand(12345 + 1000*eig) seeds the reference's factor MDS; any start
+    // converges to the same subspace)
+    if (warm_in) {
+        RFX_CUDA(cudaMemcpyAsync(V, warm_in, sizeof(double) * (size_t)n * S_BLK, cudaMemcpyDeviceToDevice, s));
+    } else {
         std::vector<double> h((size_t)n * S_BLK);
         std::mt19937_64 rng(seed);
         std::normal_distribution<double> nd(0.0, 1.0);
@@ -299,7 +303,8 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
             double delta = 0.0;
             for (int q = 0; q < k; ++q) delta = std::max(delta, std::fabs(a[q] - b[q]) / std::max(std::fabs(a[q]), 1e-300));
             prev = cur;
-            if (delta < 1e-14 || it == max_iter) break;
+            if (iters_out) *iters_out = it;
+            if (delta < tol || it == max_iter) break;
         }
         if ((st = orth(W, V)) != RFX_OK) return st;
     }
@@ -327,7 +332,239 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
     RFX_CUDA(cudaMemcpyAsync(sel, hs.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
     RFX_CUDA(cudaMemcpyAsync(scale, hsc.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
     coords_kernel<<<(unsigned)(((size_t)n * k + 255) / 256), 256, 0, s>>>(V, U, sel, scale, n, k, d_out);
+    if (keep_out) RFX_CUDA(cudaMemcpyAsync(keep_out, V, sizeof(double) * (size_t)n * S_BLK, cudaMemcpyDeviceToDevice, s));
     c->launches += 1;
+    RFX_CUDA(cudaGetLastError());
+    RFX_CUDA(cudaStreamSynchronize(s));
+    return RFX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MDS from low-rank factors.
+//
+// With P ~= I + A A^T (A: n x k) and D_ij = 1 - P_ij off the diagonal, 0 on it
+// (the reference's compute_mds_from_factors distance D = 1 - P / max(diag P),
+// cuda/rf_proximity_lowrank.cu:1966-2003, with the unit diagonal of P),
+//   D^2 = 11^T - 2 A A^T + (A.A)(A.A)^T - diag(c),  c_i = (1 - |a_i|^2)^2,
+// where (A.A) is the row-wise Kronecker square, and the double-centred
+//   B = J A A^T J - 1/2 J (A.A)(A.A)^T J + 1/2 J diag(c) J.
+// B V is applied without forming n x n objects:
+//   u = J V;  T1 = A (A^T u);  M_j = A^T diag(u_j) A (k x k);
+//   T2_ij = a_i^T M_j a_i;  B V = J (T1 - T2/2 + c.u/2).
+// The two k^2-wide reductions (M_j and the quadratic forms) carry the work.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void colmean_kernel(const double* __restrict__ V, int n, double* __restrict__ mean) {
+    // one block per column
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += V[(size_t)i * S_BLK + j];
+    __shared__ double red[32];
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+        if (threadIdx.x == 0) mean[j] = v / (double)n;
+    }
+}
+
+// u = V - mean (FP64), also as FP32
+__global__ void center_kernel(const double* __restrict__ V, const double* __restrict__ mean, int n,
+                              double* __restrict__ u, float* __restrict__ u32) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * S_BLK) return;
+    const double v = V[idx] - mean[idx % S_BLK];
+    u[idx] = v;
+    u32[idx] = (float)v;
+}
+
+// AtU[a][j] += sum_i A[i][a] u[i][j]  (FP64 accumulation)
+__global__ void atu_kernel(const float* __restrict__ A, const float* __restrict__ u, int n, int k,
+                           double* __restrict__ AtU) {
+    const int a = threadIdx.x % 64, j = threadIdx.x / 64;  // 64 x 4 per pass
+    for (int jj = j; jj < S_BLK; jj += 4) {
+        if (a >= k) continue;
+        double s = 0.0;
+        for (int i = blockIdx.x; i < n; i += gridDim.x) s += (double)A[(size_t)i * k + a] * (double)u[(size_t)i * S_BLK + jj];
+        atomicAdd(AtU + a * S_BLK + jj, s);
+    }
+}
+
+// M[j][a][b] += sum over a row chunk of u[i][j] A[i][a] A[i][b]; one CTA per
+// (row chunk, j); each thread a 4 x 4 block of (a, b).  k <= 64.
+constexpr int MS_ROWS = 128;
+__global__ void __launch_bounds__(256) mstack_f32_kernel(const float* __restrict__ A, const float* __restrict__ u,
+                                                         int n, int k, float* __restrict__ M) {
+    __shared__ float As[MS_ROWS][65];
+    __shared__ float us[MS_ROWS];
+    const int j = blockIdx.y;
+    const int tid = threadIdx.x;
+    const int ab = tid;  // 16 x 16 blocks of 4 x 4
+    const int a0 = (ab / 16) * 4, b0 = (ab % 16) * 4;
+    float acc[4][4] = {};
+    for (int r0 = blockIdx.x * MS_ROWS; r0 < n; r0 += gridDim.x * MS_ROWS) {
+        for (int e = tid; e < MS_ROWS * 64; e += 256) {
+            const int r = e / 64, c = e % 64;
+            As[r][c] = (r0 + r < n && c < k) ? A[(size_t)(r0 + r) * k + c] : 0.0f;
+        }
+        for (int r = tid; r < MS_ROWS; r += 256) us[r] = (r0 + r < n) ? u[(size_t)(r0 + r) * S_BLK + j] : 0.0f;
+        __syncthreads();
+        for (int r = 0; r < MS_ROWS; ++r) {
+            const float w = us[r];
+            float x[4], y[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                x[q] = As[r][a0 + q] * w;
+                y[q] = As[r][b0 + q];
+            }
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(x[p], y[q], acc[p][q]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (a0 + p < k && b0 + q < k) atomicAdd(M + ((size_t)j * k + a0 + p) * k + b0 + q, acc[p][q]);
+}
+
+// T2[i][j] = a_i^T M_j a_i for 4 consecutive j per CTA (M slices in shared memory)
+__global__ void __launch_bounds__(256) quadform_f32_kernel(const float* __restrict__ A, const float* __restrict__ M,
+                                                           int n, int k, float* __restrict__ T2) {
+    extern __shared__ float Ms[];  // 4 * k * k
+    const int j0 = blockIdx.y * 4;
+    for (int e = threadIdx.x; e < 4 * k * k; e += blockDim.x) Ms[e] = M[(size_t)j0 * k * k + e];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float a[64];
+#pragma unroll
+    for (int q = 0; q < 64; ++q) a[q] = q < k ? A[(size_t)i * k + q] : 0.0f;
+    for (int jj = 0; jj < 4; ++jj) {
+        const float* Mj = Ms + jj * k * k;
+        float t = 0.0f;
+#pragma unroll 4
+        for (int r = 0; r < k; ++r) {
+            float v = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 64; ++q)
+                if (q < k) v = fmaf(Mj[r * k + q], a[q], v);
+            t = fmaf(a[r], v, t);
+        }
+        T2[(size_t)i * S_BLK + j0 + jj] = t;
+    }
+}
+
+// W = T1 - T2/2 + c.u/2 with T1 = A (A^T u) (FP64 accumulation), before centring
+__global__ void factor_combine_kernel(const float* __restrict__ A, const double* __restrict__ AtU,
+                                      const float* __restrict__ T2, const double* __restrict__ u, int n, int k,
+                                      double* __restrict__ W) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * S_BLK) return;
+    const int i = (int)(idx / S_BLK), j = (int)(idx % S_BLK);
+    double t1 = 0.0, nrm = 0.0;
+    for (int a = 0; a < k; ++a) {
+        const double x = A[(size_t)i * k + a];
+        t1 += x * AtU[a * S_BLK + j];
+        nrm += x * x;
+    }
+    const double cc = (1.0 - nrm) * (1.0 - nrm);
+    W[idx] = t1 - 0.5 * (double)T2[idx] + 0.5 * cc * u[idx];
+}
+
+__global__ void subtract_mean_kernel(double* __restrict__ W, const double* __restrict__ mean, int n) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * S_BLK) return;
+    W[idx] -= mean[idx % S_BLK];
+}
+
+// o_i = 1 / sum_j P_ij^2 with P = I + A A^T off the diagonal plus the unit
+// diagonal: sum_j P_ij^2 = 1 + (a_i^T (A^T A) a_i - |a_i|^4)  (exact algebra of
+// the factor form; compute_outlier_scores, src/rf_random_forest.cpp:2489-2520,
+// on the full matrix).
+__global__ void outlier_raw_kernel(const float* __restrict__ A, const double* __restrict__ AtA, int n, int k,
+                                   float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double q = 0.0, nrm = 0.0;
+    for (int a = 0; a < k; ++a) {
+        const double x = A[(size_t)i * k + a];
+        nrm += x * x;
+        double v = 0.0;
+        for (int b = 0; b < k; ++b) v += AtA[a * k + b] * (double)A[(size_t)i * k + b];
+        q += x * v;
+    }
+    const double ss = 1.0 + (q - nrm * nrm);
+    out[i] = (float)(1.0 / ss);
+}
+
+__global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __restrict__ AtA) {
+    const int e = blockIdx.y * blockDim.x + threadIdx.x;  // output index
+    if (e >= k * k) return;
+    const int a = e / k, b = e % k;
+    double s = 0.0;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) s += (double)A[(size_t)i * k + a] * (double)A[(size_t)i * k + b];
+    atomicAdd(AtA + e, s);
+}
+
+}  // namespace
+
+rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_iter, double tol, double* d_coords,
+                              double* evals, int* iters) {
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    if (k < 1 || k > 64 || ndim < 1 || ndim > 8 || n < S_BLK) {
+        set_error("compute_mds_from_factors: need rank <= 64, 1 <= k <= 8 and n >= 16");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    Dev d;
+    double* mean = d.get<double>(S_BLK);
+    double* u = d.get<double>((size_t)n * S_BLK);
+    float* u32 = d.get<float>((size_t)n * S_BLK);
+    double* AtU = d.get<double>((size_t)k * S_BLK);
+    float* M = d.get<float>((size_t)S_BLK * k * k);
+    float* T2 = d.get<float>((size_t)n * S_BLK);
+    if (!mean || !u || !u32 || !AtU || !M || !T2) {
+        set_error("compute_mds_from_factors: device allocation failed");
+        return RFX_ERR_OOM;
+    }
+    const size_t qsm = 4 * (size_t)k * k * sizeof(float);
+    RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));
+    auto apply = [&](const double* V, double* W) -> rfx_status {
+        const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
+        colmean_kernel<<<S_BLK, 256, 0, s>>>(V, n, mean);
+        center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
+        RFX_CUDA(cudaMemsetAsync(AtU, 0, sizeof(double) * k * S_BLK, s));
+        atu_kernel<<<512, 256, 0, s>>>(dA, u32, n, k, AtU);
+        RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
+        mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
+        quadform_f32_kernel<<<dim3((n + 255) / 256, S_BLK / 4), 256, qsm, s>>>(dA, M, n, k, T2);
+        factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
+        colmean_kernel<<<S_BLK, 256, 0, s>>>(W, n, mean);
+        subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
+        c->launches += 8;
+        RFX_CUDA(cudaGetLastError());
+        return RFX_OK;
+    };
+    return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters);
+}
+
+rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out) {
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    Dev d;
+    double* AtA = d.get<double>((size_t)k * k);
+    if (!AtA) return RFX_ERR_OOM;
+    RFX_CUDA(cudaMemsetAsync(AtA, 0, sizeof(double) * k * k, s));
+    ata_kernel<<<dim3(256, (k * k + 255) / 256), 256, 0, s>>>(dA, n, k, AtA);
+    outlier_raw_kernel<<<(n + 255) / 256, 256, 0, s>>>(dA, AtA, n, k, d_out);
+    c->launches += 2;
     RFX_CUDA(cudaGetLastError());
     RFX_CUDA(cudaStreamSynchronize(s));
     return RFX_OK;

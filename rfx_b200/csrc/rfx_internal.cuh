@@ -103,6 +103,14 @@ struct Ctx {
     float* d_avimp = nullptr;           // p
     float* d_sqsd = nullptr;            // p
 
+    // low-rank factors (P ~= I + A A^T)
+    float* d_lrA = nullptr;             // n*lr_rank FP32
+    float* d_lrAq = nullptr;            // n*lr_rank dequantised copy
+    void* d_lrQ = nullptr;              // n*lr_rank quantised (int8 or fp8)
+    float* d_lrScale = nullptr;         // lr_rank per-column scales
+    int lr_rank = 0;
+    int lr_qformat = 0;                 // 0 none, 1 INT8, 2 FP8 e4m3
+
     size_t bytes = 0;                   // device bytes held
 };
 
@@ -167,6 +175,13 @@ rfx_status launch_localimp(Ctx* c, const float* d_qimp, const float* d_qimpm, fl
 rfx_status launch_predict(Ctx* c, const float* dX, int m, int32_t* d_votes);
 rfx_status check_device_errors(Ctx* c);
 rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* evals);
+rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_iter, double tol, double* d_coords,
+                              double* evals, int* iters);
+rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out);
+rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int precision, uint64_t seed,
+                           float* d_A_out, float* h_evals);
+rfx_status lowrank_quantize(Ctx* c, const float* dA, int k, int format, void* dq, float* dscale);
+rfx_status lowrank_dequantize(Ctx* c, const void* dq, const float* dscale, int k, int format, float* dA);
 
 inline int64_t upper_len(int64_t n) { return n * (n + 1) / 2; }
 

@@ -1,0 +1,111 @@
+"""Low-rank proximity (rfx_lowrank) and the calls built on its factors,
+against dense FP64 computations in numpy on the same forest.
+
+* factors: P ~= I + A A^T.  The relative Frobenius error of the off-diagonal
+  part M = P - I is compared with the best possible rank-k positive
+  semidefinite error (top-k eigenvalues of the exact M, FP64): the randomised
+  range finder must be within 25% of it, and the mixed (BF16-storage) form
+  within 2% of the FP32 form.
+* factor MDS: classical MDS of D = 1 - (I + A A^T) off the diagonal, dense in
+  FP64 (numpy.linalg.eigh), Procrustes RMS <= 1e-6 x scale.
+* outlier scores: 1 / sum_j P_ij^2 normalised by sorted[n/2], rtol 1e-4.
+* quantisation: INT8 error <= half a step per column; FP8 e4m3 <= 1/16 relative.
+"""
+import numpy as np
+import pytest
+
+from rfx_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup(built):
+    from oracle import oracle as orc
+    from rfx_b200 import abi
+
+    X, y = synth.gaussian_classes(1600, 10, 4, seed=12, mean_scale=1.2)
+    f = abi.grow_forest(X, y, 120, 3, 1, nclass=4, cat=synth.detect_categorical(X))
+    ctx = abi.Context(0)
+    ctx.load(f, X, y)
+    _, nout, _ = ctx.route_oob()
+    S = ctx.proximity_upper()
+    P = orc.finishprox(S, nout, full=True, double=True)
+    M = P - np.eye(f.n)
+    yield ctx, f, P, M
+    ctx.close()
+
+
+def rel_err(M, A):
+    R = M - A @ A.T
+    np.fill_diagonal(R, 0.0)
+    M0 = M.copy()
+    np.fill_diagonal(M0, 0.0)
+    return np.linalg.norm(R) / np.linalg.norm(M0)
+
+
+def best_err(M, k):
+    w, V = np.linalg.eigh(M)
+    idx = np.argsort(w)[::-1][:k]
+    lam = np.clip(w[idx], 0, None)
+    A = V[:, idx] * np.sqrt(lam)
+    return rel_err(M, A)
+
+
+@pytest.mark.parametrize("k", [8, 24])
+def test_factor_error_near_optimal(setup, k):
+    ctx, f, P, M = setup
+    A, ev = ctx.lowrank(k, oversample=16, power_iters=2, precision=0)
+    e = rel_err(M, A.astype(np.float64))
+    b = best_err(M, k)
+    assert e <= 1.25 * b + 1e-6, (e, b)
+    Am, _ = ctx.lowrank(k, oversample=16, power_iters=2, precision=1)
+    em = rel_err(M, Am.astype(np.float64))
+    assert em <= 1.02 * e + 1e-6, (em, e)
+
+
+def test_factor_mds_matches_dense(setup):
+    ctx, f, P, M = setup
+    A, _ = ctx.lowrank(16, oversample=16, power_iters=2, precision=0)
+    C, ev = ctx.mds_from_factors(3)
+    A64 = A.astype(np.float64)
+    Pl = np.eye(f.n) + A64 @ A64.T
+    D = 1.0 - Pl
+    np.fill_diagonal(D, 0.0)
+    D2 = D * D
+    n = f.n
+    J = np.eye(n) - 1.0 / n
+    B = -0.5 * J @ D2 @ J
+    w, V = np.linalg.eigh(B)
+    idx = np.argsort(w)[::-1][:3]
+    R = V[:, idx] * np.sqrt(w[idx])
+    U, _, Vt = np.linalg.svd(C.T @ R)
+    rms = np.sqrt(np.mean((C @ (U @ Vt) - R) ** 2))
+    assert rms <= 1e-6 * np.sqrt(np.mean(R ** 2)), rms
+    assert np.allclose(ev, w[idx], rtol=1e-8)
+
+
+def test_outlier_scores(setup):
+    ctx, f, P, M = setup
+    A, _ = ctx.lowrank(16, oversample=16, power_iters=2, precision=0)
+    o = ctx.outlier_scores()
+    A64 = A.astype(np.float64)
+    G = A64 @ A64.T
+    np.fill_diagonal(G, 0.0)
+    raw = 1.0 / (1.0 + (G ** 2).sum(1))
+    med = np.sort(raw)[f.n // 2]
+    assert np.allclose(o, raw / med, rtol=1e-4)
+
+
+def test_quantized_factors(setup):
+    ctx, f, P, M = setup
+    A, _ = ctx.lowrank(16, oversample=16, power_iters=2, precision=0)
+    q, sc = ctx.lowrank_quantize(1)
+    deq = q.view(np.int8).astype(np.float32) * sc
+    assert np.all(np.abs(deq - A) <= 0.5 * sc + 1e-7)
+    q8, sc8 = ctx.lowrank_quantize(2)
+    import torch
+    d8 = torch.from_numpy(q8).view(torch.float8_e4m3fn).float().numpy() * sc8
+    assert np.all(np.abs(d8 - A) <= np.abs(A) / 16 + sc8 * 2 ** -6)
+    C8, _ = ctx.mds_from_factors(3, use_quantized=True)
+    assert np.all(np.isfinite(C8))
