@@ -156,7 +156,8 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
  * finder over the leaf indicators of the loaded forest (rank + oversample
  * columns, power_iters power iterations, CholeskyQR2 in FP64, FP64
  * Rayleigh-Ritz).  precision 0 = FP32 throughout; 1 = BF16 storage of the
- * sketch inputs and leaf sums with FP32 accumulation, final product in FP32.
+ * sketch inputs and leaf sums with FP32 accumulation; 2 = as 1 with the last
+ * product (the Rayleigh-Ritz projection) in FP32.
  * The context keeps the factors for the calls below; A and evals (host, the
  * rank eigenvalues) may be NULL. */
 typedef struct rfx_lowrank_opts {
@@ -178,8 +179,17 @@ rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales
  * cuda/rf_proximity_lowrank.cu:1935-2531): D = 1 - P off the diagonal with
  * P = I + A A^T, double centring applied in factor space, the k largest
  * eigenpairs; coords n x k row-major float64.  use_quantized = 1 uses the
- * dequantised factors of rfx_lowrank_quantize. */
-rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, double* coords, double* evals);
+ * dequantised factors of rfx_lowrank_quantize.  precision 0 applies the
+ * operator in FP32; precision 1 (rank 32 or 64) runs tcgen05 BF16 GEMMs with
+ * FP32 accumulation until the iteration stalls at the BF16 rounding level, then
+ * refines that basis with FP32 iterations. */
+rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int precision, double* coords,
+                                double* evals);
+
+/* One application W = B V of the double-centred factor-space MDS operator of
+ * rfx_mds_from_factors to an n x 16 FP64 block V (row-major; host or device);
+ * precision 0 = FP32 products, 1 = tcgen05 BF16 products (rank 32 or 64). */
+rfx_status rfx_factor_mds_operator(rfx_ctx* ctx, int use_quantized, int precision, const double* V, double* W);
 
 /* Outlier scores from the factors (compute_outlier_scores,
  * src/rf_random_forest.cpp:2489-2520): 1 / sum_j P_ij^2, divided by the
@@ -217,8 +227,9 @@ rfx_status rfx_pair_counts_noalloc(const int32_t* leaf, const uint8_t* inbag, in
  * the number of kernels the library has launched since the context was
  * created.  Stage order: route, leaf lists, pair counts,
  * finishprox, varimp per-tree, varimp per-sample, varimp per-feature, predict,
- * oob summary, localimp, pair-range table. */
-enum { RFX_NUM_STAGES = 11 };
+ * oob summary, localimp, pair-range table, low-rank operator product,
+ * low-rank orthonormalisation, MDS from factors, full-matrix MDS. */
+enum { RFX_NUM_STAGES = 15 };
 rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable);
 rfx_status rfx_profile_read(rfx_ctx* ctx, float* stage_ms, int64_t* kernel_launches);
 

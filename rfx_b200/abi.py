@@ -27,11 +27,12 @@ STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ER
 EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
            "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
            "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
-           "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
+           "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_factor_mds_operator", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
-          "predict", "oob_summary", "localimp", "pair_ranges"]
+          "predict", "oob_summary", "localimp", "pair_ranges", "lowrank_product", "lowrank_orth", "mds_factors",
+          "mds_full"]
 
 
 class RfxError(RuntimeError):
@@ -273,11 +274,19 @@ class Context:
         _check(lib().rfx_lowrank_quantize(self._h, int(fmt), _vp(q), _vp(sc)))
         return q, sc
 
-    def mds_from_factors(self, k=3, use_quantized=False):
+    def mds_from_factors(self, k=3, use_quantized=False, precision=0):
         coords = np.zeros((self.n, k), np.float64)
         ev = np.zeros(k, np.float64)
-        _check(lib().rfx_mds_from_factors(self._h, int(k), int(bool(use_quantized)), _vp(coords), _vp(ev)))
+        _check(lib().rfx_mds_from_factors(self._h, int(k), int(bool(use_quantized)), int(precision), _vp(coords),
+                                          _vp(ev)))
         return coords, ev
+
+    def factor_operator(self, V, use_quantized=False, precision=0):
+        """W = B V for an n x 16 FP64 block (the factor MDS operator)."""
+        V = np.ascontiguousarray(V, np.float64)
+        W = np.zeros_like(V)
+        _check(lib().rfx_factor_mds_operator(self._h, int(bool(use_quantized)), int(precision), _vp(V), _vp(W)))
+        return W
 
     def outlier_scores(self, use_quantized=False):
         out = np.zeros(self.n, np.float32)

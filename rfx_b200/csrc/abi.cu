@@ -864,7 +864,8 @@ static const float* factors_for(Ctx* c, int use_quantized) {
     return c->d_lrA;
 }
 
-rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, double* coords, double* evals) {
+rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int precision, double* coords,
+                                double* evals) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     rfx_status st = need_forest(c);
     if (st) return st;
@@ -882,12 +883,43 @@ rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, double* 
     }
     std::vector<double> ev(8, 0.0);
     int iters = 0;
-    st = launch_mds_factors(c, dA, c->lr_rank, k, 600, 1e-10, dC, ev.data(), &iters);
+    c->last_mds_tc_iters = c->last_mds_f32_iters = 0;
+    st = launch_mds_factors(c, dA, c->lr_rank, k, 600, 1e-10, dC, ev.data(), &iters, precision);
+    if (precision == 0) c->last_mds_f32_iters = iters;
     if (st == RFX_OK && !cdev) st = copy_out(c, coords, dC, sizeof(double) * (size_t)c->n * k);
     if (st == RFX_OK) st = finish_host(c, true);
     cudaStreamSynchronize(c->stream);
     if (!cdev) cudaFree(dC);
     if (st == RFX_OK && evals) std::copy(ev.begin(), ev.begin() + k, evals);
+    return st;
+}
+
+rfx_status rfx_factor_mds_operator(rfx_ctx* ctx, int use_quantized, int precision, const double* V, double* W) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    const float* dA = c->lr_rank ? factors_for(c, use_quantized) : nullptr;
+    if (!dA || !V || !W) {
+        set_error("rfx_factor_mds_operator: factors not available or null block");
+        return RFX_ERR_STATE;
+    }
+    const size_t cnt = (size_t)c->n * 16;
+    double *dV = nullptr, *dW = nullptr;
+    RFX_CUDA(cudaMalloc((void**)&dV, sizeof(double) * cnt));
+    cudaError_t e = cudaMalloc((void**)&dW, sizeof(double) * cnt);
+    if (e != cudaSuccess) {
+        cudaFree(dV);
+        return cuda_fail(e, "rfx_factor_mds_operator");
+    }
+    e = cudaMemcpy(dV, V, sizeof(double) * cnt, cudaMemcpyDefault);
+    st = e == cudaSuccess ? launch_factor_operator(c, dA, c->lr_rank, dV, dW, precision) : cuda_fail(e, "copy");
+    if (st == RFX_OK) {
+        e = cudaMemcpy(W, dW, sizeof(double) * cnt, cudaMemcpyDefault);
+        if (e != cudaSuccess) st = cuda_fail(e, "copy");
+    }
+    cudaFree(dV);
+    cudaFree(dW);
+    if (st == RFX_OK) st = check_device_errors(c);
     return st;
 }
 

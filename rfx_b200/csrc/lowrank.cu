@@ -13,9 +13,9 @@
 //
 // Forms:
 //   FP32  - X, leaf sums and products in FP32;
-//   mixed - X and leaf sums stored in BF16 (the Gaussian test matrix is
-//           exact in BF16), FP32 accumulation; the final product M Q that
-//           builds the Rayleigh-Ritz projection runs in FP32 (one refinement).
+//   mixed - X and leaf sums stored in BF16, FP32 accumulation (precision 1);
+//           precision 2 also recomputes the last product M Q, which builds the
+//           Rayleigh-Ritz projection, in FP32.
 // FP64 is used for the k' x k' Gram (CholeskyQR2) and the eigensolve only.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -286,6 +286,7 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
                    const std::vector<int64_t>& batch_start, int64_t* d_gofs, const std::vector<int64_t>& h_gofs_all) {
     cudaStream_t s = c->stream;
     const int n = c->n, W = 2 * w;
+    StageTimer stt(c, ST_LR_PRODUCT, 0);
     pack_x_kernel<TX><<<nblk((int64_t)n * w), 256, 0, s>>>(V, dinv, n, w, X);
     RFX_CUDA(cudaGetLastError());
     c->launches += 1;
@@ -369,8 +370,8 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     void* X = precision ? (void*)d.get<__nv_bfloat16>((size_t)n * W) : (void*)d.get<float>((size_t)n * W);
     void* G = precision ? (void*)d.get<__nv_bfloat16>((size_t)max_batch_keys * W)
                         : (void*)d.get<float>((size_t)max_batch_keys * W);
-    void* X32 = precision ? (void*)d.get<float>((size_t)n * W) : X;
-    void* G32 = precision ? (void*)d.get<float>((size_t)max_batch_keys * W) : G;
+    void* X32 = precision == 2 ? (void*)d.get<float>((size_t)n * W) : X;
+    void* G32 = precision == 2 ? (void*)d.get<float>((size_t)max_batch_keys * W) : G;
     if (!dinv || !Om || !Yw || !Q || !Z || !Ybig || !d_gofs || !Gm || !Tm || !ev || !U || !bad || !X || !G || !X32 ||
         !G32) {
         set_error("rfx_lowrank: device allocation failed");
@@ -397,6 +398,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
                                   (int)(sizeof(double) * w * w)));
     auto orth = [&](const float* src, float* out) -> rfx_status {
         // CholeskyQR2 with FP64 Gram and FP64 triangular factors
+        StageTimer stt(c, ST_LR_ORTH, 0);
         const float* cur = src;
         float* tmp = Z;
         for (int pass = 0; pass < 2; ++pass) {
@@ -419,8 +421,8 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
         if ((st = apply(Q, Yw, !mixed)) != RFX_OK) return st;
     }
     if ((st = orth(Yw, Q)) != RFX_OK) return st;
-    // Rayleigh-Ritz with an FP32 product (the refinement step of the mixed form)
-    if ((st = apply(Q, Yw, true)) != RFX_OK) return st;
+    // Rayleigh-Ritz projection; precision 2 recomputes this last product in FP32
+    if ((st = apply(Q, Yw, !mixed || precision == 2)) != RFX_OK) return st;
     RFX_CUDA(cudaMemsetAsync(Gm, 0, sizeof(double) * w * w, s));
     gram_f32_kernel<<<std::min(1024, (n + 31) / 32), 256, 0, s>>>(Q, Yw, n, w, Gm);
     eig_w_kernel<<<1, 256, sm2, s>>>(Gm, w, ev, U);

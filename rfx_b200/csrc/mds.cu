@@ -284,7 +284,7 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
     };
     rfx_status st;
     if ((st = orth(V, V)) != RFX_OK) return st;  // src and Out may alias: Xt sits between
-    std::vector<double> prev(S_BLK, 0.0), cur(S_BLK, 0.0);
+    std::vector<double> prev(S_BLK, 0.0), cur(S_BLK, 0.0), hist;
     std::vector<double> hU(S_BLK * S_BLK);
     for (int it = 1; it <= max_iter; ++it) {
         if ((st = apply(V, W)) != RFX_OK) return st;
@@ -304,7 +304,12 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
             for (int q = 0; q < k; ++q) delta = std::max(delta, std::fabs(a[q] - b[q]) / std::max(std::fabs(a[q]), 1e-300));
             prev = cur;
             if (iters_out) *iters_out = it;
-            if (delta < tol || it == max_iter) break;
+            // stop at the tolerance, or when the change no longer shrinks (the
+            // operator's rounding floor has been reached)
+            hist.push_back(delta);
+            const size_t hn = hist.size();
+            const bool stalled = it >= 40 && hn >= 4 && hist[hn - 1] > 0.5 * hist[hn - 4];
+            if (delta < tol || stalled || it == max_iter) break;
         }
         if ((st = orth(W, V)) != RFX_OK) return st;
     }
@@ -515,8 +520,10 @@ __global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __
 
 }  // namespace
 
+rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32, float* M, float* T2);
+
 rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_iter, double tol, double* d_coords,
-                              double* evals, int* iters) {
+                              double* evals, int* iters, int precision) {
     const int n = c->n;
     cudaStream_t s = c->stream;
     if (k < 1 || k > 64 || ndim < 1 || ndim > 8 || n < S_BLK) {
@@ -534,25 +541,92 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
         set_error("compute_mds_from_factors: device allocation failed");
         return RFX_ERR_OOM;
     }
+    StageTimer stt(c, ST_MDS_FACTORS, 0);
     const size_t qsm = 4 * (size_t)k * k * sizeof(float);
     RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));
+    bool tensor = false;
     auto apply = [&](const double* V, double* W) -> rfx_status {
         const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
         colmean_kernel<<<S_BLK, 256, 0, s>>>(V, n, mean);
         center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
         RFX_CUDA(cudaMemsetAsync(AtU, 0, sizeof(double) * k * S_BLK, s));
         atu_kernel<<<512, 256, 0, s>>>(dA, u32, n, k, AtU);
-        RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
-        mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
-        quadform_f32_kernel<<<dim3((n + 255) / 256, S_BLK / 4), 256, qsm, s>>>(dA, M, n, k, T2);
+        if (tensor) {
+            rfx_status st = launch_factor_ops_tc(c, dA, k, u32, M, T2);
+            if (st != RFX_OK) return st;
+        } else {
+            RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
+            mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
+            quadform_f32_kernel<<<dim3((n + 255) / 256, S_BLK / 4), 256, qsm, s>>>(dA, M, n, k, T2);
+            c->launches += 2;
+        }
         factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
         colmean_kernel<<<S_BLK, 256, 0, s>>>(W, n, mean);
         subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
-        c->launches += 8;
+        c->launches += 6;
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
-    return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters);
+    if (precision == 0 || (k != 32 && k != 64))
+        return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters);
+    // mixed: BF16 tensor-core iterations to the BF16 rounding floor, then FP32
+    // iterations from that basis (the FP32 residual refinement)
+    double* basis = d.get<double>((size_t)n * S_BLK);
+    if (!basis) return RFX_ERR_OOM;
+    tensor = true;
+    int it1 = 0, it2 = 0;
+    rfx_status st = subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, 1e-7, nullptr, basis, &it1);
+    if (st != RFX_OK) return st;
+    tensor = false;
+    st = subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, basis, nullptr, &it2);
+    if (iters) *iters = it1 + it2;
+    c->last_mds_tc_iters = it1;
+    c->last_mds_f32_iters = it2;
+    return st;
+}
+
+// One application W = B V of the factor-space MDS operator (n x 16 blocks, FP64).
+rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* V, double* W, int precision) {
+    const int n = c->n;
+    cudaStream_t s = c->stream;
+    if (k < 1 || k > 64) {
+        set_error("factor operator: rank must be 1..64");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    if (precision && k != 32 && k != 64) {
+        set_error("factor operator: the tensor-core form needs rank 32 or 64");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    Dev d;
+    double* mean = d.get<double>(S_BLK);
+    double* u = d.get<double>((size_t)n * S_BLK);
+    float* u32 = d.get<float>((size_t)n * S_BLK);
+    double* AtU = d.get<double>((size_t)k * S_BLK);
+    float* M = d.get<float>((size_t)S_BLK * k * k);
+    float* T2 = d.get<float>((size_t)n * S_BLK);
+    if (!mean || !u || !u32 || !AtU || !M || !T2) return RFX_ERR_OOM;
+    const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
+    colmean_kernel<<<S_BLK, 256, 0, s>>>(V, n, mean);
+    center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
+    RFX_CUDA(cudaMemsetAsync(AtU, 0, sizeof(double) * k * S_BLK, s));
+    atu_kernel<<<512, 256, 0, s>>>(dA, u32, n, k, AtU);
+    rfx_status st = RFX_OK;
+    if (precision) {
+        st = launch_factor_ops_tc(c, dA, k, u32, M, T2);
+    } else {
+        const size_t qsm = 4 * (size_t)k * k * sizeof(float);
+        RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));
+        RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
+        mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
+        quadform_f32_kernel<<<dim3((n + 255) / 256, S_BLK / 4), 256, qsm, s>>>(dA, M, n, k, T2);
+    }
+    if (st != RFX_OK) return st;
+    factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
+    colmean_kernel<<<S_BLK, 256, 0, s>>>(W, n, mean);
+    subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
+    RFX_CUDA(cudaGetLastError());
+    RFX_CUDA(cudaStreamSynchronize(s));
+    return RFX_OK;
 }
 
 rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out) {
@@ -573,6 +647,7 @@ rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out) {
 rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* evals) {
     const int n = c->n;
     cudaStream_t s = c->stream;
+    StageTimer stt(c, ST_MDS_FULL, 0);
     if (n < 2) {
         set_error("MDS requires at least 2 samples");
         return RFX_ERR_INVALID;

@@ -34,7 +34,7 @@ enum : uint32_t {
 
 enum Stage : int {
     ST_ROUTE = 0, ST_CSR, ST_PAIRS, ST_FINISHPROX, ST_VARIMP_TREE, ST_VARIMP_SAMPLE, ST_VARIMP_FEATURE,
-    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_OPP, ST_COUNT
+    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_OPP, ST_LR_PRODUCT, ST_LR_ORTH, ST_MDS_FACTORS, ST_MDS_FULL, ST_COUNT
 };
 
 struct Ctx {
@@ -110,6 +110,8 @@ struct Ctx {
     float* d_lrScale = nullptr;         // lr_rank per-column scales
     int lr_rank = 0;
     int lr_qformat = 0;                 // 0 none, 1 INT8, 2 FP8 e4m3
+    int last_mds_tc_iters = 0;          // iterations of the last factor MDS (tensor-core phase)
+    int last_mds_f32_iters = 0;         // and its FP32 phase
 
     size_t bytes = 0;                   // device bytes held
 };
@@ -176,8 +178,9 @@ rfx_status launch_predict(Ctx* c, const float* dX, int m, int32_t* d_votes);
 rfx_status check_device_errors(Ctx* c);
 rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* evals);
 rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_iter, double tol, double* d_coords,
-                              double* evals, int* iters);
+                              double* evals, int* iters, int precision);
 rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out);
+rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* V, double* W, int precision);
 rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int precision, uint64_t seed,
                            float* d_A_out, float* h_evals);
 rfx_status lowrank_quantize(Ctx* c, const float* dA, int k, int format, void* dq, float* dscale);

@@ -109,3 +109,41 @@ def test_quantized_factors(setup):
     assert np.all(np.abs(d8 - A) <= np.abs(A) / 16 + sc8 * 2 ** -6)
     C8, _ = ctx.mds_from_factors(3, use_quantized=True)
     assert np.all(np.isfinite(C8))
+
+
+@pytest.mark.parametrize("rank", [32, 64])
+def test_tensor_core_operator_matches_fp32(setup, rank):
+    """The tcgen05 BF16 form of the factor MDS operator against its FP32 form
+    on a random block: relative difference at the BF16 level (<= 2e-2)."""
+    ctx, f, P, M = setup
+    ctx.lowrank(rank, oversample=16, power_iters=1, precision=0)
+    rng = np.random.default_rng(3)
+    V = rng.normal(size=(f.n, 16))
+    W32 = ctx.factor_operator(V, precision=0)
+    Wtc = ctx.factor_operator(V, precision=1)
+    rel = np.linalg.norm(Wtc - W32) / np.linalg.norm(W32)
+    assert rel <= 2e-2, rel
+    # the FP32 form against dense FP64 algebra
+    A, _ = ctx.lowrank(rank, oversample=16, power_iters=1, precision=0)
+    A64 = A.astype(np.float64)
+    n = f.n
+    u = V - V.mean(0)
+    G = A64 @ A64.T
+    D = -G
+    np.fill_diagonal(D, 0.0)
+    D2 = (1.0 + D) ** 2
+    np.fill_diagonal(D2, 0.0)
+    J = np.eye(n) - 1.0 / n
+    Bm = -0.5 * J @ D2 @ J
+    Wd = Bm @ V
+    assert np.linalg.norm(W32 - Wd) / np.linalg.norm(Wd) <= 1e-5
+
+
+def test_mixed_factor_mds_matches_fp32(setup):
+    ctx, f, P, M = setup
+    ctx.lowrank(32, oversample=16, power_iters=1, precision=0)
+    C32, e32 = ctx.mds_from_factors(3, precision=0)
+    Cm, em = ctx.mds_from_factors(3, precision=1)
+    U, _, Vt = np.linalg.svd(Cm.T @ C32)
+    rms = np.sqrt(np.mean((Cm @ (U @ Vt) - C32) ** 2))
+    assert rms <= 1e-5 * np.sqrt(np.mean(C32 ** 2)), rms
