@@ -154,7 +154,8 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
  * handle API get_lowrank_factors_host, cuda/rf_lowrank_helpers.cu:13):
  * P ~= I + A A^T with A (n x rank, float32 row-major) from a randomised range
  * finder over the leaf indicators of the loaded forest (rank + oversample
- * columns, power_iters power iterations, CholeskyQR2 in FP64, FP64
+ * columns rounded up to a multiple of 8, at most 128 and at most n;
+ * power_iters power iterations, CholeskyQR2 in FP64, FP64
  * Rayleigh-Ritz).  precision 0 = FP32 throughout; 1 = BF16 storage of the
  * sketch inputs and leaf sums with FP32 accumulation; 2 = as 1 with the last
  * product (the Rayleigh-Ritz projection) in FP32.
@@ -182,7 +183,8 @@ rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales
  * dequantised factors of rfx_lowrank_quantize.  precision 0 applies the
  * operator in FP32; precision 1 (rank 32 or 64) runs tcgen05 BF16 GEMMs with
  * FP32 accumulation until the iteration stalls at the BF16 rounding level, then
- * refines that basis with FP32 iterations. */
+ * takes one FP32 step (an FP32 operator product and Rayleigh-Ritz) from that
+ * basis. */
 rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int precision, double* coords,
                                 double* evals);
 

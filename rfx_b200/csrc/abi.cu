@@ -282,7 +282,9 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
         std::vector<uint64_t> iv((size_t)T * W, 0);
         for (int t = 0; t < T; ++t) {
             const int64_t a = v->offs[t], b = v->offs[t + 1];
-            if (b <= a || b - a > (int64_t)2 * n + 1) {
+            // trees may come from a larger training set than the rows loaded
+            // here (a row subsample), so only positivity and int32 range are checked
+            if (b <= a || b - a > (int64_t)INT32_MAX / 2) {
                 set_error("rfx_forest_load: tree " + std::to_string(t) + " has an invalid node count");
                 return RFX_ERR_FOREST;
             }

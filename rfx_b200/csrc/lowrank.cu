@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "dense.cuh"
@@ -66,15 +67,53 @@ __global__ void pack_x_kernel(const float* __restrict__ V, const float* __restri
     st_val(X + (size_t)i * 2 * w + w + c, __fmul_rn(v, dinv[i]));
 }
 
-// Leaf-key sums of X rows for trees [t0, t1): G[gofs[t-t0] + key][c] =
-// sum over members j of key of X[j][c].  One warp per key.
-template <typename TX, typename TG>
-__global__ void segsum_kernel(const TX* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
+// 16-byte chunks of a row: E values of type T per chunk.
+template <typename T>
+struct Chunk;
+template <>
+struct Chunk<float> {
+    static constexpr int E = 4;
+    __device__ static void load(const float* p, float* v) {
+        const float4 x = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    }
+    __device__ static void store(float* p, const float* v) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+};
+template <>
+struct Chunk<__nv_bfloat16> {
+    static constexpr int E = 8;
+    __device__ static void load(const __nv_bfloat16* p, float* v) {
+        const uint4 x = __ldg(reinterpret_cast<const uint4*>(p));
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float2 f = __bfloat1622float2(h[q]);
+            v[2 * q] = f.x;
+            v[2 * q + 1] = f.y;
+        }
+    }
+    __device__ static void store(__nv_bfloat16* p, const float* v) {
+        uint4 x;
+        __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&x);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+        *reinterpret_cast<uint4*>(p) = x;
+    }
+};
+
+// Leaf-key sums of X rows for trees [t0, t1): G[gofs[t-t0] + key][:] = sum
+// over members j of key of X[j][:].  One warp per key; rows move as 16-byte
+// chunks (lane l owns chunks l and l + 32), the lanes fetch 32 member ids at
+// once, and successive members' rows are independent loads.
+template <typename T>
+__global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
                               const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
-                              int t1, const int64_t* __restrict__ gofs, TG* __restrict__ G) {
+                              int t1, const int64_t* __restrict__ gofs, T* __restrict__ G) {
+    constexpr int E = Chunk<T>::E;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    // locate (tree, key): gofs holds the key prefix of the batch (in keys)
     const int64_t total = gofs[t1 - t0];
     if (warp >= total) return;
     int lo = 0, hi = t1 - t0;
@@ -87,44 +126,92 @@ __global__ void segsum_kernel(const TX* __restrict__ X, int n, int W, const int3
     const int key = (int)(warp - gofs[lo]);
     const int32_t* so = segoff + segbase[t];
     const int s0 = so[key], s1 = so[key + 1];
-    const int32_t* mt = memb + (size_t)t * n;
-    TG* g = G + (size_t)warp * W;
-    for (int c0 = 0; c0 < W; c0 += 32) {
-        const int c = c0 + lane;
-        float acc = 0.0f;
-        if (c < W)
-            for (int q = s0; q < s1; ++q) acc += ld_val(X + (size_t)__ldg(mt + q) * W + c);
-        if (c < W) st_val(g + c, acc);
+    const int32_t* mt = memb + (size_t)t * n + s0;
+    const int m = s1 - s0;
+    const int CH = W / E;
+    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
+    float a0[E], a1[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
+    for (int base = 0; base < m; base += 32) {
+        const int myj = base + lane < m ? __ldg(mt + base + lane) : 0;
+        const int cnt = min(32, m - base);
+#pragma unroll 4
+        for (int q = 0; q < cnt; ++q) {
+            const int j = __shfl_sync(0xffffffffu, myj, q);
+            const T* xr = X + (size_t)j * W;
+            float v[E];
+            if (c0ok) {
+                Chunk<T>::load(xr + lane * E, v);
+#pragma unroll
+                for (int e = 0; e < E; ++e) a0[e] += v[e];
+            }
+            if (c1ok) {
+                Chunk<T>::load(xr + (lane + 32) * E, v);
+#pragma unroll
+                for (int e = 0; e < E; ++e) a1[e] += v[e];
+            }
+        }
     }
+    T* gout = G + (size_t)warp * W;
+    if (c0ok) Chunk<T>::store(gout + lane * E, a0);
+    if (c1ok) Chunk<T>::store(gout + (lane + 32) * E, a1);
 }
 
-// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample.
-template <typename TG>
-__global__ void pull_kernel(const TG* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
+// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample,
+// 16-byte chunks per lane, 32 trees' keys fetched at once.
+template <typename T>
+__global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
                             const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate) {
+    constexpr int E = Chunk<T>::E;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
     const int i = (int)warp;
-    float acc[8];
+    const int CH = W / E;
+    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
+    float a0[E], a1[E];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) acc[q] = 0.0f;
-    for (int t = t0; t < t1; ++t) {
-        const int k = __ldg(key + (size_t)t * n + i);
-        if (k < 0) continue;
-        const TG* g = G + (size_t)(gofs[t - t0] + (k ^ 1)) * W;
+    for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
+    for (int tb = t0; tb < t1; tb += 32) {
+        const int t = tb + lane;
+        long long gi = -1;
+        if (t < t1) {
+            const int k = __ldg(key + (size_t)t * n + i);
+            if (k >= 0) gi = gofs[t - t0] + (k ^ 1);
+        }
+        const int cnt = min(32, t1 - tb);
+#pragma unroll 4
+        for (int q = 0; q < cnt; ++q) {
+            const long long r = __shfl_sync(0xffffffffu, gi, q);
+            if (r < 0) continue;
+            const T* gr = G + (size_t)r * W;
+            float v[E];
+            if (c0ok) {
+                Chunk<T>::load(gr + lane * E, v);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int c = lane + 32 * q;
-            if (c < W) acc[q] += ld_val(g + c);
+                for (int e = 0; e < E; ++e) a0[e] += v[e];
+            }
+            if (c1ok) {
+                Chunk<T>::load(gr + (lane + 32) * E, v);
+#pragma unroll
+                for (int e = 0; e < E; ++e) a1[e] += v[e];
+            }
         }
     }
     float* y = Y + (size_t)i * W;
+    if (c0ok)
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        const int c = lane + 32 * q;
-        if (c < W) y[c] = accumulate ? y[c] + acc[q] : acc[q];
-    }
+        for (int e = 0; e < E; ++e) {
+            const int c = lane * E + e;
+            y[c] = accumulate ? y[c] + a0[e] : a0[e];
+        }
+    if (c1ok)
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int c = (lane + 32) * E + e;
+            y[c] = accumulate ? y[c] + a1[e] : a1[e];
+        }
 }
 
 // MV = 1/4 (D Y[:, :w] + Y[:, w:])
@@ -297,8 +384,9 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
         const int64_t keys = h_gofs_all[b + 1] - h_gofs_all[b] - 1;  // stored with one sentinel per batch
         (void)keys;
         const int64_t total_keys = c->h_segbase[t1] - c->h_segbase[t0] - (t1 - t0);
-        segsum_kernel<TX, TG><<<nblk(total_keys * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0,
-                                                                   t1, gofs, G);
+        static_assert(std::is_same<TX, TG>::value, "X and the leaf sums share one storage type");
+        segsum_kernel<TX><<<nblk(total_keys * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0, t1,
+                                                                gofs, G);
         pull_kernel<TG><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0);
         c->launches += 2;
         RFX_CUDA(cudaGetLastError());
@@ -313,9 +401,9 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
                            float* d_A_out, float* h_evals) {
     cudaStream_t s = c->stream;
     const int n = c->n, T = c->T;
-    const int w = k + oversample;
+    const int w = (k + oversample + 7) / 8 * 8;  // rows of whole 16-byte chunks
     if (k < 1 || w > GW || w > n) {
-        set_error("rfx_lowrank: need 1 <= rank and rank + oversample <= min(128, n)");
+        set_error("rfx_lowrank: need 1 <= rank and rank + oversample (rounded up to a multiple of 8) <= min(128, n)");
         return RFX_ERR_INVALID;
     }
     rfx_status st = launch_route(c);
@@ -324,7 +412,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     c->routed = true;
     c->csr_built = true;
     const int W = 2 * w;
-    // tree batches: leaf-sum storage per batch bounded to ~512 MB
+    // tree batches: leaf-sum storage per batch bounded to ~4 GB
     const size_t gbytes_row = (size_t)W * (precision ? 2 : 4);
     std::vector<int64_t> batch_start{0};
     std::vector<int64_t> h_gofs;  // per batch: key prefix (batch-local), with a sentinel
@@ -337,7 +425,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
             int t1 = t;
             while (t1 < T) {
                 const int64_t kt = c->h_segbase[t1 + 1] - c->h_segbase[t1] - 1;
-                if (t1 > t && (size_t)(keys + kt) * gbytes_row > ((size_t)512 << 20)) break;
+                if (t1 > t && (size_t)(keys + kt) * gbytes_row > ((size_t)4 << 30)) break;
                 keys += kt;
                 ++t1;
             }

@@ -569,16 +569,17 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     };
     if (precision == 0 || (k != 32 && k != 64))
         return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters);
-    // mixed: BF16 tensor-core iterations to the BF16 rounding floor, then FP32
-    // iterations from that basis (the FP32 residual refinement)
+    // mixed: BF16 tensor-core iterations to the BF16 rounding floor, then one
+    // FP32 refinement step from that basis
     double* basis = d.get<double>((size_t)n * S_BLK);
     if (!basis) return RFX_ERR_OOM;
     tensor = true;
     int it1 = 0, it2 = 0;
     rfx_status st = subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, 1e-7, nullptr, basis, &it1);
     if (st != RFX_OK) return st;
+    // one FP32 step from that basis: an FP32 product and its Rayleigh-Ritz
     tensor = false;
-    st = subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, basis, nullptr, &it2);
+    st = subspace_topk(c, n, ndim, apply, 1, d_coords, evals, 12345, tol, basis, nullptr, &it2);
     if (iters) *iters = it1 + it2;
     c->last_mds_tc_iters = it1;
     c->last_mds_f32_iters = it2;

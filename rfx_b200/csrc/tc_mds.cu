@@ -284,7 +284,7 @@ rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32
     const int n = c->n;
     constexpr int S = 16;
     RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S * k * k, s));
-    const int ksplit = 148;
+    const int ksplit = 37;  // 296 CTAs for rank 64: two per SM, few partial-tile atomics
     auto run = [&](auto mk, auto qk, int K) -> rfx_status {
         const int sm_m = 2 * (128 * KCH * 2 + K * KCH * 2);
         const int sm_q = 128 * K * 2 + 256 * K * 2;

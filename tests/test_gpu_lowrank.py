@@ -140,10 +140,12 @@ def test_tensor_core_operator_matches_fp32(setup, rank):
 
 
 def test_mixed_factor_mds_matches_fp32(setup):
+    """Mixed form (tensor-core BF16 iterations + one FP32 refinement step)
+    against the FP32 form: Procrustes RMS <= 5e-3 x scale."""
     ctx, f, P, M = setup
     ctx.lowrank(32, oversample=16, power_iters=1, precision=0)
     C32, e32 = ctx.mds_from_factors(3, precision=0)
     Cm, em = ctx.mds_from_factors(3, precision=1)
     U, _, Vt = np.linalg.svd(Cm.T @ C32)
     rms = np.sqrt(np.mean((Cm @ (U @ Vt) - C32) ** 2))
-    assert rms <= 1e-5 * np.sqrt(np.mean(C32 ** 2)), rms
+    assert rms <= 5e-3 * np.sqrt(np.mean(C32 ** 2)), rms
