@@ -37,8 +37,8 @@ sys.path.insert(0, ROOT)
 N_SAMPLES = 50_000
 N_TREES = 1000
 MTRY = 7
-WORKLOAD = ("exact pair counts + varimp: n=50000 p=54 (10 continuous + one-hot 4 + one-hot 40) c=7, "
-            "ntree=1000 mtry=7 nodesize=1, INT32 upper-triangle S (n(n+1)/2) + all 54 feature permutations")
+WORKLOAD = ("exact pair counts + varimp: n={n} p=54 (10 continuous + one-hot 4 + one-hot 40) c=7, "
+            "ntree={T} mtry=7 nodesize=1, INT32 upper-triangle S (n(n+1)/2) + all 54 feature permutations")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -197,7 +197,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "n": n, "ntree": T, "parallelism": "host cores (OpenMP)"},
+            "config": {"workload": WORKLOAD.format(n=n, T=T), "n": n, "ntree": T, "parallelism": "host cores (OpenMP)"},
             "cpu_baseline": {"value": value, "unit": "pair-updates/s", "cores": info["cores"], "kind": info["kind"],
                              "sample": f"each step = 1 tree of the {T}-tree forest at n={n} (reference per-tree "
                                        "sequence; pair counts by the dense-branch restatement)"},
@@ -217,8 +217,8 @@ def run_lowrank(args):
 
     from rfx_b200 import abi, synth
 
-    n = args.n if args.n != N_SAMPLES else 200_000
-    T = args.trees if args.trees != N_TREES else 2000
+    n = args.n if args.n is not None else 200_000
+    T = args.trees if args.trees is not None else 2000
     k = 64
     X, y = synth.mixed_cover(n, seed=synth.SEED_BASE + 3)
     cat = synth.detect_categorical(X)
@@ -306,14 +306,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N_SAMPLES)
-    ap.add_argument("--trees", type=int, default=N_TREES)
+    ap.add_argument("--n", type=int, default=None, help="samples (default 50000; 200000 for --workload lowrank)")
+    ap.add_argument("--trees", type=int, default=None, help="trees (default 1000; 2000 for --workload lowrank)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="exact", choices=["exact", "lowrank"])
     args = ap.parse_args()
     if args.workload == "lowrank":
         return run_lowrank(args)
+    args.n = N_SAMPLES if args.n is None else args.n
+    args.trees = N_TREES if args.trees is None else args.trees
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
@@ -418,7 +420,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded mixed-type cover-shaped generator; forest grown by the library's "
                     "restatement of the reference grower)",
-            "config": {"workload": WORKLOAD, "n": n, "p": p, "ntree": T, "pair_updates_per_step": U,
+            "config": {"workload": WORKLOAD.format(n=n, T=T), "n": n, "p": p, "ntree": T, "pair_updates_per_step": U,
                        "l2": "inputs larger than L2 (S 5.0 GB written per step; nodes and leaf keys > 126 MB)",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "forest_grow_s": round(grow_s, 2)},
