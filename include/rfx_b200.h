@@ -154,7 +154,7 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
  * handle API get_lowrank_factors_host, cuda/rf_lowrank_helpers.cu:13):
  * P ~= I + A A^T with A (n x rank, float32 row-major) from a randomised range
  * finder over the leaf indicators of the loaded forest (rank + oversample
- * columns rounded up to a multiple of 8, at most 128 and at most n;
+ * columns rounded up to a multiple of 8, at most 120 and at most n;
  * power_iters power iterations, CholeskyQR2 in FP64, FP64
  * Rayleigh-Ritz).  precision 0 = FP32 throughout; 1 = BF16 storage of the
  * sketch inputs and leaf sums with FP32 accumulation; 2 = as 1 with the last

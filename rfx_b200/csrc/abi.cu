@@ -87,6 +87,19 @@ void dfree(Ctx* c, T*& p) {
     p = nullptr;
 }
 
+// cudaMalloc that, when device memory is short, first hands the context's
+// kept scratch blocks back to the driver and tries once more.
+cudaError_t ctx_malloc(Ctx* c, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation && !c->scratch_free.empty()) {
+        cudaGetLastError();
+        cudaStreamSynchronize(c->stream);
+        c->scratch_release();
+        e = cudaMalloc(p, bytes);
+    }
+    return e;
+}
+
 void free_forest(Ctx* c) {
     dfree(c, c->d_X); dfree(c, c->d_y); dfree(c, c->d_cat); dfree(c, c->d_nodes); dfree(c, c->d_nodeclass);
     dfree(c, c->d_leafidx); dfree(c, c->d_catgoleft); dfree(c, c->d_offs); dfree(c, c->d_nnode);
@@ -102,6 +115,7 @@ void free_forest(Ctx* c) {
     c->lr_qformat = 0;
     c->loaded = c->routed = c->csr_built = false;
     c->bytes = 0;
+    c->scratch_release();
 }
 
 // Copy helper: device->(device|host) of `bytes` bytes on the context stream.
@@ -528,7 +542,7 @@ rfx_status rfx_oob_summary(rfx_ctx* ctx, float* oob_error, int32_t* pred, float*
     std::vector<void*> tmp;
     auto tmpalloc = [&](size_t bytes) -> void* {
         void* d = nullptr;
-        if (cudaMalloc(&d, bytes) != cudaSuccess) {
+        if (ctx_malloc(c, (void**)&d, bytes) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
@@ -564,7 +578,7 @@ rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len) {
     const bool dev = is_device_ptr(S);
     int32_t* dS = S;
     if (!dev) {
-        cudaError_t e = cudaMalloc((void**)&dS, sizeof(int32_t) * len);
+        cudaError_t e = ctx_malloc(c, (void**)&dS, sizeof(int32_t) * len);
         if (e != cudaSuccess) return cuda_fail(e, "rfx_proximity_upper_i32 staging");
     }
     // every call does the full pass: routing, per-tree leaf lists, pair counts
@@ -617,7 +631,7 @@ rfx_status rfx_finishprox(rfx_ctx* ctx, const int32_t* S, float* P, int full) {
     float* dP = P;
     int32_t* sS = nullptr;
     if (!sdev) {
-        cudaError_t e = cudaMalloc((void**)&sS, sizeof(int32_t) * slen);
+        cudaError_t e = ctx_malloc(c, (void**)&sS, sizeof(int32_t) * slen);
         if (e != cudaSuccess) return cuda_fail(e, "rfx_finishprox staging");
         e = cudaMemcpyAsync(sS, S, sizeof(int32_t) * slen, cudaMemcpyHostToDevice, c->stream);
         if (e != cudaSuccess) {
@@ -627,7 +641,7 @@ rfx_status rfx_finishprox(rfx_ctx* ctx, const int32_t* S, float* P, int full) {
         dS = sS;
     }
     if (!pdev) {
-        cudaError_t e = cudaMalloc((void**)&dP, sizeof(float) * plen);
+        cudaError_t e = ctx_malloc(c, (void**)&dP, sizeof(float) * plen);
         if (e != cudaSuccess) {
             if (sS) cudaFree(sS);
             return cuda_fail(e, "rfx_finishprox staging");
@@ -690,7 +704,7 @@ rfx_status rfx_localimp(rfx_ctx* ctx, const float* qimp, const float* qimpm, flo
     auto stage_in = [&](const float* h, size_t cnt) -> const float* {
         if (is_device_ptr(h)) return h;
         float* d = nullptr;
-        if (cudaMalloc((void**)&d, sizeof(float) * cnt) != cudaSuccess) return nullptr;
+        if (ctx_malloc(c, (void**)&d, sizeof(float) * cnt) != cudaSuccess) return nullptr;
         tmp.push_back(d);
         cudaMemcpyAsync(d, h, sizeof(float) * cnt, cudaMemcpyHostToDevice, c->stream);
         return d;
@@ -700,7 +714,7 @@ rfx_status rfx_localimp(rfx_ctx* ctx, const float* qimp, const float* qimpm, flo
     const bool odev = is_device_ptr(outp);
     float* dout = outp;
     if (!odev) {
-        if (cudaMalloc((void**)&dout, sizeof(float) * np) != cudaSuccess) dout = nullptr;
+        if (ctx_malloc(c, (void**)&dout, sizeof(float) * np) != cudaSuccess) dout = nullptr;
         else tmp.push_back(dout);
     }
     if (!dq || !dqm || !dout) {
@@ -729,7 +743,7 @@ rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes) 
     std::vector<void*> tmp;
     if (!xdev && m > 0) {
         float* d = nullptr;
-        cudaError_t e = cudaMalloc((void**)&d, sizeof(float) * (size_t)m * c->p);
+        cudaError_t e = ctx_malloc(c, (void**)&d, sizeof(float) * (size_t)m * c->p);
         if (e != cudaSuccess) return cuda_fail(e, "rfx_predict staging");
         tmp.push_back(d);
         cudaMemcpyAsync(d, X, sizeof(float) * (size_t)m * c->p, cudaMemcpyHostToDevice, c->stream);
@@ -737,7 +751,7 @@ rfx_status rfx_predict(rfx_ctx* ctx, const float* X, int32_t m, int32_t* votes) 
     }
     if (!vdev) {
         int32_t* d = nullptr;
-        cudaError_t e = cudaMalloc((void**)&d, sizeof(int32_t) * std::max<size_t>(1, (size_t)m * c->nclass));
+        cudaError_t e = ctx_malloc(c, (void**)&d, sizeof(int32_t) * std::max<size_t>(1, (size_t)m * c->nclass));
         if (e != cudaSuccess) {
             for (void* q : tmp) cudaFree(q);
             return cuda_fail(e, "rfx_predict staging");
@@ -769,7 +783,7 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
     const float* dP = P;
     float* sP = nullptr;
     if (!is_device_ptr(P)) {
-        cudaError_t e = cudaMalloc((void**)&sP, sizeof(float) * nn);
+        cudaError_t e = ctx_malloc(c, (void**)&sP, sizeof(float) * nn);
         if (e != cudaSuccess) return cuda_fail(e, "rfx_mds3d_full staging");
         e = cudaMemcpyAsync(sP, P, sizeof(float) * nn, cudaMemcpyHostToDevice, c->stream);
         if (e != cudaSuccess) {
@@ -781,7 +795,7 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
     const bool cdev = is_device_ptr(coords);
     double* dC = coords;
     if (!cdev) {
-        cudaError_t e = cudaMalloc((void**)&dC, sizeof(double) * (size_t)c->n * 3);
+        cudaError_t e = ctx_malloc(c, (void**)&dC, sizeof(double) * (size_t)c->n * 3);
         if (e != cudaSuccess) {
             if (sP) cudaFree(sP);
             return cuda_fail(e, "rfx_mds3d_full staging");
@@ -845,7 +859,7 @@ rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales
     const size_t nk = (size_t)c->n * k;
     if (c->d_lrQ) cudaFree(c->d_lrQ);
     c->d_lrQ = nullptr;
-    if (cudaMalloc(&c->d_lrQ, nk) != cudaSuccess) {
+    if (ctx_malloc(c, (void**)&c->d_lrQ, nk) != cudaSuccess) {
         cudaGetLastError();
         set_error("rfx_lowrank_quantize: allocation failed");
         return RFX_ERR_OOM;
@@ -880,7 +894,7 @@ rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int prec
     const bool cdev = is_device_ptr(coords);
     double* dC = coords;
     if (!cdev) {
-        cudaError_t e = cudaMalloc((void**)&dC, sizeof(double) * (size_t)c->n * k);
+        cudaError_t e = ctx_malloc(c, (void**)&dC, sizeof(double) * (size_t)c->n * k);
         if (e != cudaSuccess) return cuda_fail(e, "rfx_mds_from_factors staging");
     }
     std::vector<double> ev(8, 0.0);
@@ -907,8 +921,8 @@ rfx_status rfx_factor_mds_operator(rfx_ctx* ctx, int use_quantized, int precisio
     }
     const size_t cnt = (size_t)c->n * 16;
     double *dV = nullptr, *dW = nullptr;
-    RFX_CUDA(cudaMalloc((void**)&dV, sizeof(double) * cnt));
-    cudaError_t e = cudaMalloc((void**)&dW, sizeof(double) * cnt);
+    RFX_CUDA(ctx_malloc(c, (void**)&dV, sizeof(double) * cnt));
+    cudaError_t e = ctx_malloc(c, (void**)&dW, sizeof(double) * cnt);
     if (e != cudaSuccess) {
         cudaFree(dV);
         return cuda_fail(e, "rfx_factor_mds_operator");
@@ -935,7 +949,7 @@ rfx_status rfx_outlier_scores(rfx_ctx* ctx, int use_quantized, float* scores) {
         return RFX_ERR_STATE;
     }
     float* d = nullptr;
-    cudaError_t e = cudaMalloc((void**)&d, sizeof(float) * c->n);
+    cudaError_t e = ctx_malloc(c, (void**)&d, sizeof(float) * c->n);
     if (e != cudaSuccess) return cuda_fail(e, "rfx_outlier_scores");
     st = launch_outlier_scores(c, dA, c->lr_rank, d);
     std::vector<float> h(c->n);

@@ -57,7 +57,9 @@ __device__ inline void cta_tri_inverse(const double* L, double* Linv, int s, int
 // Cyclic Jacobi eigendecomposition of the symmetric s x s matrix A (destroyed):
 // eigenvalues on the diagonal of A, eigenvectors in the columns of V.
 // Rotations of disjoint index pairs are applied in parallel (round-robin
-// ordering); `sweeps` full sweeps.
+// ordering); at most `sweeps` full sweeps, fewer once every off-diagonal entry
+// is at FP64 rounding relative to its diagonal pair.  A leading dimension
+// ld = s + 1 keeps the column passes free of shared-memory bank conflicts.
 __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweeps, int* pairs) {
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = tid; e < s * s; e += nt) V[(e / s) * ld + (e % s)] = ((e / s) == (e % s)) ? 1.0 : 0.0;
@@ -65,6 +67,18 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
     const int m = (s % 2) ? s + 1 : s;  // round-robin needs an even count (index s = dummy)
     __shared__ double cs[64][2];
     for (int sw = 0; sw < sweeps; ++sw) {
+        // converged when every off-diagonal entry is negligible against its
+        // diagonal pair, |a_pq| <= 1e-16 sqrt(|a_pp a_qq|) (the relative
+        // criterion, which keeps small eigenvalues accurate)
+        int active = 0;
+        for (int e = tid; e < s * s; e += nt) {
+            const int r = e / s, q = e % s;
+            if (r < q) {
+                const double v = A[r * ld + q];
+                if (v * v > 1e-32 * fabs(A[r * ld + r] * A[q * ld + q])) active = 1;
+            }
+        }
+        if (!__syncthreads_or(active)) break;
         for (int round = 0; round < m - 1; ++round) {
             // round-robin tournament: index 0 stays, indices 1..m-1 rotate;
             // pair k joins positions k and m-1-k

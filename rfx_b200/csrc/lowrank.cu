@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
+#include <cstdlib>
 #include <vector>
 
 #include "dense.cuh"
@@ -104,58 +105,162 @@ struct Chunk<__nv_bfloat16> {
 };
 
 // Leaf-key sums of X rows for trees [t0, t1): G[gofs[t-t0] + key][:] = sum
-// over members j of key of X[j][:].  One warp per key; rows move as 16-byte
-// chunks (lane l owns chunks l and l + 32), the lanes fetch 32 member ids at
-// once, and successive members' rows are independent loads.
+// over members j of key of X[j][:].  The member list of each tree (keys in
+// order, members of a key contiguous) is cut into chunks of SEG_CH positions,
+// one warp per chunk, so a leaf with thousands of members is spread over many
+// warps.  A key that lies inside one chunk is written to G directly; a key that
+// crosses a chunk boundary leaves FP32 partial sums (Pf: the chunk's first key,
+// Pl: its last key) that segsum_fix_kernel adds up in chunk order.  Rows move
+// as 16-byte chunks (lane l owns chunks l and l + 32).  G rows of empty keys
+// must be zero beforehand.
+constexpr int SEG_CH = 64;
+
+template <typename T>
+__device__ __forceinline__ void add_row(const T* xr, int lane, bool c0ok, bool c1ok, float* a0, float* a1) {
+    constexpr int E = Chunk<T>::E;
+    float v[E];
+    if (c0ok) {
+        Chunk<T>::load(xr + lane * E, v);
+#pragma unroll
+        for (int e = 0; e < E; ++e) a0[e] += v[e];
+    }
+    if (c1ok) {
+        Chunk<T>::load(xr + (lane + 32) * E, v);
+#pragma unroll
+        for (int e = 0; e < E; ++e) a1[e] += v[e];
+    }
+}
+
+template <typename TO>
+__device__ __forceinline__ void store_row(TO* out, int lane, bool c0ok, bool c1ok, const float* a0, const float* a1) {
+    constexpr int E = Chunk<TO>::E;
+    static_assert(E == 4 || E == 8, "16-byte chunks");
+    if (c0ok) Chunk<TO>::store(out + lane * E, a0);
+    if (c1ok) Chunk<TO>::store(out + (lane + 32) * E, a1);
+}
+
+// FP32 partial rows use 4-float chunks; with BF16 rows (8 values per chunk) a
+// partial row is stored as two float chunks per lane chunk.
+template <typename T>
+__device__ __forceinline__ void store_partial(float* out, int lane, bool c0ok, bool c1ok, const float* a0,
+                                              const float* a1) {
+    constexpr int E = Chunk<T>::E;
+#pragma unroll
+    for (int h = 0; h < E / 4; ++h) {
+        if (c0ok) Chunk<float>::store(out + lane * E + 4 * h, a0 + 4 * h);
+        if (c1ok) Chunk<float>::store(out + (lane + 32) * E + 4 * h, a1 + 4 * h);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void add_partial(const float* in, int lane, bool c0ok, bool c1ok, float* a0, float* a1) {
+    constexpr int E = Chunk<T>::E;
+    float v[4];
+#pragma unroll
+    for (int h = 0; h < E / 4; ++h) {
+        if (c0ok) {
+            Chunk<float>::load(in + lane * E + 4 * h, v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) a0[4 * h + e] += v[e];
+        }
+        if (c1ok) {
+            Chunk<float>::load(in + (lane + 32) * E + 4 * h, v);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) a1[4 * h + e] += v[e];
+        }
+    }
+}
+
 template <typename T>
 __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
                               const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
-                              int t1, const int64_t* __restrict__ gofs, T* __restrict__ G) {
+                              int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
+                              float* __restrict__ Pf, float* __restrict__ Pl, int32_t* __restrict__ fk) {
     constexpr int E = Chunk<T>::E;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const int64_t total = gofs[t1 - t0];
-    if (warp >= total) return;
-    int lo = 0, hi = t1 - t0;
+    if (warp >= (int64_t)(t1 - t0) * cpt) return;
+    const int tb = (int)(warp / cpt), ch = (int)(warp % cpt);
+    const int t = t0 + tb;
+    const int32_t* so = segoff + segbase[t];
+    const int K = (int)(segbase[t + 1] - segbase[t]) - 1;
+    const int ntot = __ldg(so + K);
+    const int cs = ch * SEG_CH;
+    if (cs >= ntot) {
+        if (lane == 0) fk[warp] = -1;
+        return;
+    }
+    const int ce = min(cs + SEG_CH, ntot);
+    // key holding position cs: the largest k with so[k] <= cs (so[0] = 0)
+    int lo = 0, hi = K;
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (gofs[mid] <= warp) lo = mid;
+        if (__ldg(so + mid) <= cs) lo = mid;
         else hi = mid;
     }
-    const int t = t0 + lo;
-    const int key = (int)(warp - gofs[lo]);
-    const int32_t* so = segoff + segbase[t];
-    const int s0 = so[key], s1 = so[key + 1];
-    const int32_t* mt = memb + (size_t)t * n + s0;
-    const int m = s1 - s0;
+    int key = lo;
+    if (lane == 0) fk[warp] = key;
+    const int32_t* mt = memb + (size_t)t * n;
+    const int m0 = cs + lane < ce ? __ldg(mt + cs + lane) : 0;
+    const int m1 = cs + 32 + lane < ce ? __ldg(mt + cs + 32 + lane) : 0;
+    const int CH = W / E;
+    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
+    int pos = cs;
+    while (pos < ce) {
+        const int kbeg = __ldg(so + key), kend = __ldg(so + key + 1);
+        const int e = min(kend, ce);
+        float a0[E], a1[E];
+#pragma unroll
+        for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
+#pragma unroll 4
+        for (int q = pos; q < e; ++q) {
+            const int r = q - cs;  // warp-uniform
+            const int j = __shfl_sync(0xffffffffu, r < 32 ? m0 : m1, r & 31);
+            add_row<T>(X + (size_t)j * W, lane, c0ok, c1ok, a0, a1);
+        }
+        if (kbeg >= cs && kend <= ce) {
+            store_row<T>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
+        } else if (pos == cs) {
+            store_partial<T>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+        } else {
+            store_partial<T>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+        }
+        pos = e;
+        if (pos < ce) {
+            ++key;
+            while (__ldg(so + key + 1) <= pos) ++key;  // skip empty keys; pos < ntot = so[K] bounds key < K
+        }
+    }
+}
+
+// Keys that cross chunk boundaries: the chunk after the one a key starts in
+// sums the key's partial rows in chunk order and writes its G row.
+template <typename T>
+__global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase,
+                                  int t0, int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
+                                  const float* __restrict__ Pf, const float* __restrict__ Pl,
+                                  const int32_t* __restrict__ fk) {
+    constexpr int E = Chunk<T>::E;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= (int64_t)(t1 - t0) * cpt) return;
+    const int tb = (int)(warp / cpt), ch = (int)(warp % cpt);
+    if (ch == 0) return;
+    const int key = fk[warp];
+    if (key < 0) return;
+    const int32_t* so = segoff + segbase[t0 + tb];
+    const int kbeg = __ldg(so + key), kend = __ldg(so + key + 1);
+    const int cs = ch * SEG_CH;
+    if (!(kbeg < cs && kbeg >= cs - SEG_CH)) return;  // owned by this chunk iff the key starts in the previous one
     const int CH = W / E;
     const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
     float a0[E], a1[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
-    for (int base = 0; base < m; base += 32) {
-        const int myj = base + lane < m ? __ldg(mt + base + lane) : 0;
-        const int cnt = min(32, m - base);
-#pragma unroll 4
-        for (int q = 0; q < cnt; ++q) {
-            const int j = __shfl_sync(0xffffffffu, myj, q);
-            const T* xr = X + (size_t)j * W;
-            float v[E];
-            if (c0ok) {
-                Chunk<T>::load(xr + lane * E, v);
-#pragma unroll
-                for (int e = 0; e < E; ++e) a0[e] += v[e];
-            }
-            if (c1ok) {
-                Chunk<T>::load(xr + (lane + 32) * E, v);
-#pragma unroll
-                for (int e = 0; e < E; ++e) a1[e] += v[e];
-            }
-        }
-    }
-    T* gout = G + (size_t)warp * W;
-    if (c0ok) Chunk<T>::store(gout + lane * E, a0);
-    if (c1ok) Chunk<T>::store(gout + (lane + 32) * E, a1);
+    for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
+    add_partial<T>((kbeg == cs - SEG_CH ? Pf : Pl) + (size_t)(warp - 1) * W, lane, c0ok, c1ok, a0, a1);
+    for (int c2 = ch; c2 * SEG_CH < kend; ++c2)
+        add_partial<T>(Pf + (size_t)(warp - ch + c2) * W, lane, c0ok, c1ok, a0, a1);
+    store_row<T>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
 }
 
 // Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample,
@@ -298,18 +403,19 @@ __global__ void right_mul_kernel(const float* __restrict__ X, const double* __re
 // One CTA: eigen-decomposition of the symmetrised w x w H.
 __global__ void eig_w_kernel(const double* __restrict__ H, int w, double* __restrict__ evals,
                              double* __restrict__ evecs) {
-    extern __shared__ double sm[];
+    extern __shared__ double sm[];  // two w x (w + 1) arrays
+    const int ld = w + 1;
     double* A = sm;
-    double* U = sm + w * w;
+    double* U = sm + w * ld;
     __shared__ int pairs[2 * 64];
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) {
         const int i = e / w, j = e % w;
-        A[e] = 0.5 * (H[i * w + j] + H[j * w + i]);
+        A[i * ld + j] = 0.5 * (H[i * w + j] + H[j * w + i]);
     }
     __syncthreads();
-    cta_jacobi(A, U, w, w, 14, pairs);
-    for (int e = threadIdx.x; e < w * w; e += blockDim.x) evecs[e] = U[e];
-    for (int i = threadIdx.x; i < w; i += blockDim.x) evals[i] = A[i * w + i];
+    cta_jacobi(A, U, w, ld, 30, pairs);
+    for (int e = threadIdx.x; e < w * w; e += blockDim.x) evecs[e] = U[(e / w) * ld + (e % w)];
+    for (int i = threadIdx.x; i < w; i += blockDim.x) evals[i] = A[i * ld + i];
 }
 
 __global__ void colmax_kernel(const float* __restrict__ A, int n, int k, unsigned int* __restrict__ mx) {
@@ -345,22 +451,6 @@ __global__ void dequant_kernel(const TQ* __restrict__ q, const float* __restrict
     A[idx] = (float)q[idx] * scale[idx % k];
 }
 
-struct DevBufs {
-    std::vector<void*> p;
-    ~DevBufs() {
-        for (void* x : p) cudaFree(x);
-    }
-    template <typename T>
-    T* get(size_t count) {
-        void* x = nullptr;
-        if (cudaMalloc(&x, sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        p.push_back(x);
-        return static_cast<T*>(x);
-    }
-};
 
 inline unsigned nblk(int64_t count, int b = 256) { return (unsigned)((count + b - 1) / b); }
 
@@ -370,7 +460,8 @@ inline unsigned nblk(int64_t count, int b = 256) { return (unsigned)((count + b 
 // packed inputs and the leaf sums.
 template <typename TX, typename TG>
 rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, TX* X, TG* G, float* Y,
-                   const std::vector<int64_t>& batch_start, int64_t* d_gofs, const std::vector<int64_t>& h_gofs_all) {
+                   const std::vector<int64_t>& batch_start, int64_t* d_gofs, const std::vector<int64_t>& h_gofs_all,
+                   float* Pf, float* Pl, int32_t* fk) {
     cudaStream_t s = c->stream;
     const int n = c->n, W = 2 * w;
     StageTimer stt(c, ST_LR_PRODUCT, 0);
@@ -385,10 +476,15 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
         (void)keys;
         const int64_t total_keys = c->h_segbase[t1] - c->h_segbase[t0] - (t1 - t0);
         static_assert(std::is_same<TX, TG>::value, "X and the leaf sums share one storage type");
-        segsum_kernel<TX><<<nblk(total_keys * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0, t1,
-                                                                gofs, G);
+        const int cpt = (n + SEG_CH - 1) / SEG_CH;
+        const int64_t chunks = (int64_t)(t1 - t0) * cpt;
+        RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(TG) * (size_t)total_keys * W, s));
+        segsum_kernel<TX><<<nblk(chunks * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0, t1,
+                                                            cpt, gofs, G, Pf, Pl, fk);
+        segsum_fix_kernel<TG><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt, gofs, G,
+                                                                Pf, Pl, fk);
         pull_kernel<TG><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0);
-        c->launches += 2;
+        c->launches += 3;
         RFX_CUDA(cudaGetLastError());
     }
     combine_kernel<<<nblk((int64_t)n * w), 256, 0, s>>>(Y, dinv, n, w, MV);
@@ -402,22 +498,33 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     cudaStream_t s = c->stream;
     const int n = c->n, T = c->T;
     const int w = (k + oversample + 7) / 8 * 8;  // rows of whole 16-byte chunks
-    if (k < 1 || w > GW || w > n) {
-        set_error("rfx_lowrank: need 1 <= rank and rank + oversample (rounded up to a multiple of 8) <= min(128, n)");
+    if (k < 1 || w > 120 || w > n) {  // 120: two w x (w + 1) FP64 arrays in one CTA's shared memory
+        set_error("rfx_lowrank: need 1 <= rank and rank + oversample (rounded up to a multiple of 8) <= min(120, n)");
         return RFX_ERR_INVALID;
     }
-    rfx_status st = launch_route(c);
-    if (st == RFX_OK) st = launch_build_csr(c);
-    if (st != RFX_OK) return st;
-    c->routed = true;
-    c->csr_built = true;
+    // leaf keys and member lists: reused when this forest's are already built
+    rfx_status st = RFX_OK;
+    if (!c->csr_built) {
+        st = launch_route(c);
+        if (st == RFX_OK) st = launch_build_csr(c);
+        if (st != RFX_OK) return st;
+        c->routed = true;
+        c->csr_built = true;
+    }
     const int W = 2 * w;
-    // tree batches: leaf-sum storage per batch bounded to ~4 GB
+    // tree batches: leaf sums of up to 4 GB per batch (fewer passes over the
+    // n x 2w accumulator beat L2-sized batches; RFX_LR_BATCH_MB overrides)
     const size_t gbytes_row = (size_t)W * (precision ? 2 : 4);
+    size_t batch_budget = (size_t)4 << 30;
+    if (const char* e = std::getenv("RFX_LR_BATCH_MB")) {
+        const long v = std::atol(e);
+        if (v > 0) batch_budget = (size_t)v << 20;
+    }
     std::vector<int64_t> batch_start{0};
     std::vector<int64_t> h_gofs;  // per batch: key prefix (batch-local), with a sentinel
     std::vector<int64_t> gofs_index;  // offset of each batch's prefix inside h_gofs
     int64_t max_batch_keys = 0;
+    int max_batch_trees = 0;
     {
         int t = 0;
         while (t < T) {
@@ -425,7 +532,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
             int t1 = t;
             while (t1 < T) {
                 const int64_t kt = c->h_segbase[t1 + 1] - c->h_segbase[t1] - 1;
-                if (t1 > t && (size_t)(keys + kt) * gbytes_row > ((size_t)4 << 30)) break;
+                if (t1 > t && (size_t)(keys + kt) * gbytes_row > batch_budget) break;
                 keys += kt;
                 ++t1;
             }
@@ -437,12 +544,13 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
             }
             h_gofs.push_back(acc);
             max_batch_keys = std::max(max_batch_keys, acc);
+            max_batch_trees = std::max(max_batch_trees, t1 - t);
             batch_start.push_back(t1);
             t = t1;
         }
         gofs_index.push_back((int64_t)h_gofs.size());
     }
-    DevBufs d;
+    Scratch d(c);
     float* dinv = d.get<float>(n);
     float* Om = d.get<float>((size_t)n * w);
     float* Yw = d.get<float>((size_t)n * w);
@@ -460,8 +568,12 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
                         : (void*)d.get<float>((size_t)max_batch_keys * W);
     void* X32 = precision == 2 ? (void*)d.get<float>((size_t)n * W) : X;
     void* G32 = precision == 2 ? (void*)d.get<float>((size_t)max_batch_keys * W) : G;
+    const size_t nchunks = (size_t)max_batch_trees * ((n + SEG_CH - 1) / SEG_CH);
+    float* Pf = d.get<float>(nchunks * W);
+    float* Pl = d.get<float>(nchunks * W);
+    int32_t* fk = d.get<int32_t>(nchunks);
     if (!dinv || !Om || !Yw || !Q || !Z || !Ybig || !d_gofs || !Gm || !Tm || !ev || !U || !bad || !X || !G || !X32 ||
-        !G32) {
+        !G32 || !Pf || !Pl || !fk) {
         set_error("rfx_lowrank: device allocation failed");
         return RFX_ERR_OOM;
     }
@@ -475,13 +587,14 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     auto apply = [&](const float* V, float* MV, bool fp32) -> rfx_status {
         if (fp32)
             return apply_m<float, float>(c, V, w, MV, dinv, (float*)X32, (float*)G32, Ybig, batch_start, d_gofs,
-                                         pref_at);
+                                         pref_at, Pf, Pl, fk);
         return apply_m<__nv_bfloat16, __nv_bfloat16>(c, V, w, MV, dinv, (__nv_bfloat16*)X, (__nv_bfloat16*)G, Ybig,
-                                                     batch_start, d_gofs, pref_at);
+                                                     batch_start, d_gofs, pref_at, Pf, Pl, fk);
     };
     const size_t sm2 = 2 * (size_t)w * w * sizeof(double);
     RFX_CUDA(cudaFuncSetAttribute(chol_inv_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-    RFX_CUDA(cudaFuncSetAttribute(eig_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+    const size_t sm_eig = 2 * (size_t)w * (w + 1) * sizeof(double);
+    RFX_CUDA(cudaFuncSetAttribute(eig_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_eig));
     RFX_CUDA(cudaFuncSetAttribute(right_mul_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * w * w)));
     auto orth = [&](const float* src, float* out) -> rfx_status {
@@ -513,7 +626,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     if ((st = apply(Q, Yw, !mixed || precision == 2)) != RFX_OK) return st;
     RFX_CUDA(cudaMemsetAsync(Gm, 0, sizeof(double) * w * w, s));
     gram_f32_kernel<<<std::min(1024, (n + 31) / 32), 256, 0, s>>>(Q, Yw, n, w, Gm);
-    eig_w_kernel<<<1, 256, sm2, s>>>(Gm, w, ev, U);
+    eig_w_kernel<<<1, 256, sm_eig, s>>>(Gm, w, ev, U);
     c->launches += 2;
     RFX_CUDA(cudaGetLastError());
     std::vector<double> hev(w), hU((size_t)w * w);
@@ -548,7 +661,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
 rfx_status lowrank_quantize(Ctx* c, const float* dA, int k, int format, void* dq, float* dscale) {
     cudaStream_t s = c->stream;
     const int n = c->n;
-    DevBufs d;
+    Scratch d(c);
     unsigned int* mx = d.get<unsigned int>(k);
     if (!mx) return RFX_ERR_OOM;
     RFX_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned int) * k, s));

@@ -182,16 +182,17 @@ __global__ void dright_kernel(const double* __restrict__ W, const double* __rest
 
 // One CTA: eigen-decomposition of the S x S projection H (symmetrised).
 __global__ void rr_kernel(const double* __restrict__ H, double* __restrict__ evals, double* __restrict__ evecs) {
-    __shared__ double A[S_BLK * S_BLK], U[S_BLK * S_BLK];
+    constexpr int LD = S_BLK + 1;
+    __shared__ double A[S_BLK * LD], U[S_BLK * LD];
     __shared__ int pairs[2 * 64];
     for (int e = threadIdx.x; e < S_BLK * S_BLK; e += blockDim.x) {
         const int i = e / S_BLK, j = e % S_BLK;
-        A[e] = 0.5 * (H[i * S_BLK + j] + H[j * S_BLK + i]);
+        A[i * LD + j] = 0.5 * (H[i * S_BLK + j] + H[j * S_BLK + i]);
     }
     __syncthreads();
-    cta_jacobi(A, U, S_BLK, S_BLK, 12, pairs);
-    for (int e = threadIdx.x; e < S_BLK * S_BLK; e += blockDim.x) evecs[e] = U[e];
-    for (int i = threadIdx.x; i < S_BLK; i += blockDim.x) evals[i] = A[i * S_BLK + i];
+    cta_jacobi(A, U, S_BLK, LD, 30, pairs);
+    for (int e = threadIdx.x; e < S_BLK * S_BLK; e += blockDim.x) evecs[e] = U[(e / S_BLK) * LD + (e % S_BLK)];
+    for (int i = threadIdx.x; i < S_BLK; i += blockDim.x) evals[i] = A[i * LD + i];
 }
 
 // coords[i][c] = (V U)[i][sel[c]] * scale[c]
@@ -205,22 +206,6 @@ __global__ void coords_kernel(const double* __restrict__ V, const double* __rest
     out[idx] = v * scale[c];
 }
 
-struct Dev {
-    std::vector<void*> ptrs;
-    ~Dev() {
-        for (void* p : ptrs) cudaFree(p);
-    }
-    template <typename T>
-    T* get(size_t count) {
-        void* p = nullptr;
-        if (cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        ptrs.push_back(p);
-        return static_cast<T*>(p);
-    }
-};
 
 }  // namespace
 
@@ -231,9 +216,9 @@ struct Dev {
 template <typename Apply>
 rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double* d_out, double* evals_out,
                          uint64_t seed, double tol = 1e-14, const double* warm_in = nullptr, double* keep_out = nullptr,
-                         int* iters_out = nullptr) {
+                         int* iters_out = nullptr, bool floor_stop = false) {
     cudaStream_t s = c->stream;
-    Dev d;
+    Scratch d(c);
     double* V = d.get<double>((size_t)n * S_BLK);
     double* W = d.get<double>((size_t)n * S_BLK);
     double* G = d.get<double>(S_BLK * S_BLK);
@@ -308,7 +293,13 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
             // operator's rounding floor has been reached)
             hist.push_back(delta);
             const size_t hn = hist.size();
-            const bool stalled = it >= 40 && hn >= 4 && hist[hn - 1] > 0.5 * hist[hn - 4];
+            // (no new minimum over the last three checks: the change only
+            // fluctuates; with floor_stop, for operators applied in FP32 or
+            // BF16, already when it has not halved over the last three checks)
+            const bool stalled =
+                it >= 40 && hn >= 4 &&
+                (floor_stop ? hist[hn - 1] > 0.5 * hist[hn - 4]
+                            : std::min(hist[hn - 1], std::min(hist[hn - 2], hist[hn - 3])) >= hist[hn - 4]);
             if (delta < tol || stalled || it == max_iter) break;
         }
         if ((st = orth(W, V)) != RFX_OK) return st;
@@ -360,20 +351,32 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
 // ---------------------------------------------------------------------------
 namespace {
 
-__global__ void colmean_kernel(const double* __restrict__ V, int n, double* __restrict__ mean) {
-    // one block per column
-    const int j = blockIdx.x;
+// Column means of an n x 16 FP64 block in a fixed summation order: per-CTA
+// partial sums over a strided row set, then one CTA adds the partials in CTA
+// order (reproducible run to run).
+constexpr int RED_CTAS = 296;
+
+__global__ void __launch_bounds__(256) colsum_part_kernel(const double* __restrict__ V, int n,
+                                                          double* __restrict__ part) {
+    const int r = threadIdx.x / S_BLK, j = threadIdx.x % S_BLK;  // 16 rows x 16 columns per pass
     double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += V[(size_t)i * S_BLK + j];
-    __shared__ double red[32];
-    for (int d = 16; d > 0; d >>= 1) s += __shfl_down_sync(0xffffffffu, s, d);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    for (int i = blockIdx.x * 16 + r; i < n; i += gridDim.x * 16) s += V[(size_t)i * S_BLK + j];
+    __shared__ double red[16][S_BLK];
+    red[r][j] = s;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-        for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
-        if (threadIdx.x == 0) mean[j] = v / (double)n;
+    if (threadIdx.x < S_BLK) {
+        double t = 0.0;
+        for (int q = 0; q < 16; ++q) t += red[q][threadIdx.x];
+        part[(size_t)blockIdx.x * S_BLK + threadIdx.x] = t;
     }
+}
+
+__global__ void colmean_final_kernel(const double* __restrict__ part, int nparts, int n, double* __restrict__ mean) {
+    const int j = threadIdx.x;
+    if (j >= S_BLK) return;
+    double s = 0.0;
+    for (int q = 0; q < nparts; ++q) s += part[(size_t)q * S_BLK + j];
+    mean[j] = s / (double)n;
 }
 
 // u = V - mean (FP64), also as FP32
@@ -386,16 +389,44 @@ __global__ void center_kernel(const double* __restrict__ V, const double* __rest
     u32[idx] = (float)v;
 }
 
-// AtU[a][j] += sum_i A[i][a] u[i][j]  (FP64 accumulation)
-__global__ void atu_kernel(const float* __restrict__ A, const float* __restrict__ u, int n, int k,
-                           double* __restrict__ AtU) {
-    const int a = threadIdx.x % 64, j = threadIdx.x / 64;  // 64 x 4 per pass
-    for (int jj = j; jj < S_BLK; jj += 4) {
-        if (a >= k) continue;
-        double s = 0.0;
-        for (int i = blockIdx.x; i < n; i += gridDim.x) s += (double)A[(size_t)i * k + a] * (double)u[(size_t)i * S_BLK + jj];
-        atomicAdd(AtU + a * S_BLK + jj, s);
+// AtU[a][j] = sum_i A[i][a] u[i][j] in FP64: per-CTA partials (64 columns x
+// 4 row groups per CTA, all 16 j per thread), then a fixed-order sum over CTAs.
+__global__ void __launch_bounds__(256) atu_part_kernel(const float* __restrict__ A, const float* __restrict__ u, int n,
+                                                       int k, double* __restrict__ part) {
+    const int a = threadIdx.x % 64, rg = threadIdx.x / 64;
+    double acc[S_BLK];
+#pragma unroll
+    for (int j = 0; j < S_BLK; ++j) acc[j] = 0.0;
+    if (a < k) {
+        for (int i = blockIdx.x * 4 + rg; i < n; i += gridDim.x * 4) {
+            const double x = (double)A[(size_t)i * k + a];
+            const float4* ur = reinterpret_cast<const float4*>(u + (size_t)i * S_BLK);
+#pragma unroll
+            for (int q = 0; q < S_BLK / 4; ++q) {
+                const float4 v = __ldg(ur + q);
+                acc[4 * q] = fma(x, (double)v.x, acc[4 * q]);
+                acc[4 * q + 1] = fma(x, (double)v.y, acc[4 * q + 1]);
+                acc[4 * q + 2] = fma(x, (double)v.z, acc[4 * q + 2]);
+                acc[4 * q + 3] = fma(x, (double)v.w, acc[4 * q + 3]);
+            }
+        }
     }
+    __shared__ double red[4][64][S_BLK + 1];
+#pragma unroll
+    for (int j = 0; j < S_BLK; ++j) red[rg][a][j] = acc[j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < k * S_BLK; e += blockDim.x) {
+        const int aa = e / S_BLK, j = e % S_BLK;
+        part[(size_t)blockIdx.x * k * S_BLK + e] = ((red[0][aa][j] + red[1][aa][j]) + red[2][aa][j]) + red[3][aa][j];
+    }
+}
+
+__global__ void atu_final_kernel(const double* __restrict__ part, int nparts, int k, double* __restrict__ AtU) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= k * S_BLK) return;
+    double s = 0.0;
+    for (int q = 0; q < nparts; ++q) s += part[(size_t)q * k * S_BLK + e];
+    AtU[e] = s;
 }
 
 // M[j][a][b] += sum over a row chunk of u[i][j] A[i][a] A[i][b]; one CTA per
@@ -522,6 +553,17 @@ __global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __
 
 rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32, float* M, float* T2);
 
+namespace {
+void col_mean(const double* V, int n, double* part, double* mean, cudaStream_t s) {
+    colsum_part_kernel<<<RED_CTAS, 256, 0, s>>>(V, n, part);
+    colmean_final_kernel<<<1, 32, 0, s>>>(part, RED_CTAS, n, mean);
+}
+void at_u(const float* A, const float* u, int n, int k, double* part, double* AtU, cudaStream_t s) {
+    atu_part_kernel<<<RED_CTAS, 256, 0, s>>>(A, u, n, k, part);
+    atu_final_kernel<<<(k * S_BLK + 255) / 256, 256, 0, s>>>(part, RED_CTAS, k, AtU);
+}
+}  // namespace
+
 rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_iter, double tol, double* d_coords,
                               double* evals, int* iters, int precision) {
     const int n = c->n;
@@ -530,14 +572,15 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
         set_error("compute_mds_from_factors: need rank <= 64, 1 <= k <= 8 and n >= 16");
         return RFX_ERR_UNSUPPORTED;
     }
-    Dev d;
+    Scratch d(c);
     double* mean = d.get<double>(S_BLK);
     double* u = d.get<double>((size_t)n * S_BLK);
     float* u32 = d.get<float>((size_t)n * S_BLK);
     double* AtU = d.get<double>((size_t)k * S_BLK);
     float* M = d.get<float>((size_t)S_BLK * k * k);
     float* T2 = d.get<float>((size_t)n * S_BLK);
-    if (!mean || !u || !u32 || !AtU || !M || !T2) {
+    double* part = d.get<double>((size_t)RED_CTAS * k * S_BLK);
+    if (!mean || !u || !u32 || !AtU || !M || !T2 || !part) {
         set_error("compute_mds_from_factors: device allocation failed");
         return RFX_ERR_OOM;
     }
@@ -547,10 +590,9 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     bool tensor = false;
     auto apply = [&](const double* V, double* W) -> rfx_status {
         const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
-        colmean_kernel<<<S_BLK, 256, 0, s>>>(V, n, mean);
+        col_mean(V, n, part, mean, s);
         center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
-        RFX_CUDA(cudaMemsetAsync(AtU, 0, sizeof(double) * k * S_BLK, s));
-        atu_kernel<<<512, 256, 0, s>>>(dA, u32, n, k, AtU);
+        at_u(dA, u32, n, k, part, AtU, s);
         if (tensor) {
             rfx_status st = launch_factor_ops_tc(c, dA, k, u32, M, T2);
             if (st != RFX_OK) return st;
@@ -561,25 +603,26 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
             c->launches += 2;
         }
         factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
-        colmean_kernel<<<S_BLK, 256, 0, s>>>(W, n, mean);
+        col_mean(W, n, part, mean, s);
         subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
-        c->launches += 6;
+        c->launches += 9;
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
     if (precision == 0 || (k != 32 && k != 64))
-        return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters);
+        return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters, true);
     // mixed: BF16 tensor-core iterations to the BF16 rounding floor, then one
     // FP32 refinement step from that basis
     double* basis = d.get<double>((size_t)n * S_BLK);
     if (!basis) return RFX_ERR_OOM;
     tensor = true;
     int it1 = 0, it2 = 0;
-    rfx_status st = subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, 1e-7, nullptr, basis, &it1);
+    rfx_status st =
+        subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, 1e-7, nullptr, basis, &it1, true);
     if (st != RFX_OK) return st;
     // one FP32 step from that basis: an FP32 product and its Rayleigh-Ritz
     tensor = false;
-    st = subspace_topk(c, n, ndim, apply, 1, d_coords, evals, 12345, tol, basis, nullptr, &it2);
+    st = subspace_topk(c, n, ndim, apply, 1, d_coords, evals, 12345, tol, basis, nullptr, &it2, true);
     if (iters) *iters = it1 + it2;
     c->last_mds_tc_iters = it1;
     c->last_mds_f32_iters = it2;
@@ -598,19 +641,19 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
         set_error("factor operator: the tensor-core form needs rank 32 or 64");
         return RFX_ERR_UNSUPPORTED;
     }
-    Dev d;
+    Scratch d(c);
     double* mean = d.get<double>(S_BLK);
     double* u = d.get<double>((size_t)n * S_BLK);
     float* u32 = d.get<float>((size_t)n * S_BLK);
     double* AtU = d.get<double>((size_t)k * S_BLK);
     float* M = d.get<float>((size_t)S_BLK * k * k);
     float* T2 = d.get<float>((size_t)n * S_BLK);
-    if (!mean || !u || !u32 || !AtU || !M || !T2) return RFX_ERR_OOM;
+    double* part = d.get<double>((size_t)RED_CTAS * k * S_BLK);
+    if (!mean || !u || !u32 || !AtU || !M || !T2 || !part) return RFX_ERR_OOM;
     const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
-    colmean_kernel<<<S_BLK, 256, 0, s>>>(V, n, mean);
+    col_mean(V, n, part, mean, s);
     center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
-    RFX_CUDA(cudaMemsetAsync(AtU, 0, sizeof(double) * k * S_BLK, s));
-    atu_kernel<<<512, 256, 0, s>>>(dA, u32, n, k, AtU);
+    at_u(dA, u32, n, k, part, AtU, s);
     rfx_status st = RFX_OK;
     if (precision) {
         st = launch_factor_ops_tc(c, dA, k, u32, M, T2);
@@ -623,7 +666,7 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
     }
     if (st != RFX_OK) return st;
     factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
-    colmean_kernel<<<S_BLK, 256, 0, s>>>(W, n, mean);
+    col_mean(W, n, part, mean, s);
     subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
     RFX_CUDA(cudaGetLastError());
     RFX_CUDA(cudaStreamSynchronize(s));
@@ -633,7 +676,7 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
 rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out) {
     const int n = c->n;
     cudaStream_t s = c->stream;
-    Dev d;
+    Scratch d(c);
     double* AtA = d.get<double>((size_t)k * k);
     if (!AtA) return RFX_ERR_OOM;
     RFX_CUDA(cudaMemsetAsync(AtA, 0, sizeof(double) * k * k, s));
@@ -657,7 +700,7 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
         set_error("rfx_mds3d_full: n must be at least 16");
         return RFX_ERR_UNSUPPORTED;
     }
-    Dev d;
+    Scratch d(c);
     double* B = d.get<double>((size_t)n * n);
     double* rowmean = d.get<double>(n);
     double* grand = d.get<double>(1);

@@ -3,7 +3,9 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "rfx_b200.h"
@@ -114,6 +116,49 @@ struct Ctx {
     int last_mds_f32_iters = 0;         // and its FP32 phase
 
     size_t bytes = 0;                   // device bytes held
+
+    // Scratch blocks of finished calls, kept by size for the next call with
+    // the same shapes.  All work of a context runs on its one stream, so a
+    // block handed back while its kernels are still queued is only reused by
+    // later work on that stream.
+    std::multimap<size_t, void*> scratch_free;
+    void scratch_release() {
+        for (auto& kv : scratch_free) cudaFree(kv.second);
+        scratch_free.clear();
+    }
+};
+
+// Per-call scratch drawn from the context's pool: get() reuses a kept block of
+// the same size or allocates one (after releasing the pool if memory is
+// short); the destructor returns every block to the pool.
+struct Scratch {
+    Ctx* c;
+    std::vector<std::pair<size_t, void*>> held;
+    explicit Scratch(Ctx* c_) : c(c_) {}
+    Scratch(const Scratch&) = delete;
+    Scratch& operator=(const Scratch&) = delete;
+    ~Scratch() {
+        for (auto& b : held) c->scratch_free.emplace(b.first, b.second);
+    }
+    template <typename T>
+    T* get(size_t count) {
+        const size_t bytes = ((sizeof(T) * (count ? count : 1)) + 255) & ~(size_t)255;
+        auto it = c->scratch_free.find(bytes);
+        void* x = nullptr;
+        if (it != c->scratch_free.end()) {
+            x = it->second;
+            c->scratch_free.erase(it);
+        } else if (cudaMalloc(&x, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            c->scratch_release();
+            if (cudaMalloc(&x, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+        }
+        held.emplace_back(bytes, x);
+        return static_cast<T*>(x);
+    }
 };
 
 // RAII stage bracket: records events around a stage when profiling is on and
@@ -153,6 +198,12 @@ rfx_status dalloc(Ctx* c, T** p, size_t count) {
     if (*p) return RFX_OK;
     if (count == 0) count = 1;
     cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e == cudaErrorMemoryAllocation && !c->scratch_free.empty()) {
+        cudaGetLastError();
+        cudaStreamSynchronize(c->stream);
+        c->scratch_release();
+        e = cudaMalloc((void**)p, count * sizeof(T));
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
