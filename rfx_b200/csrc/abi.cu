@@ -62,16 +62,16 @@ struct MT {
 };
 
 // cpu_permobmr (src/rf_varimp.cpp:16-30): positions permuted by swaps with
-// j = (int)(randomu() * noob).  A draw that rounds to 1.0f gives j == noob,
-// which the reference uses to index one past its vector; it is counted and
-// clamped here.
-int make_perm(int noob, int32_t* perm) {
-    MT rng;
-    rng.seed(42u);
+// j = (int)(randomu() * noob), the generator reseeded with 42 for every call,
+// so every noob uses the same draws u_0, u_1, ... (computed once, `u`).  A
+// draw that rounds to 1.0f gives j == noob, which the reference uses to index
+// one past its vector; it is counted and clamped here.
+int make_perm(int noob, const float* u, int32_t* perm) {
     int bad = 0;
     for (int i = 0; i < noob; ++i) perm[i] = i;
+    const float fn = (float)noob;
     for (int i = 0; i < noob; ++i) {
-        int j = (int)(rng.randomu() * (float)noob);
+        int j = (int)(u[i] * fn);
         if (j >= noob) {
             j = noob - 1;
             ++bad;
@@ -81,9 +81,19 @@ int make_perm(int noob, int32_t* perm) {
     return bad;
 }
 
+std::vector<float> mt_draws(int count) {
+    MT rng;
+    rng.seed(42u);
+    std::vector<float> u((size_t)std::max(count, 1));
+    for (int i = 0; i < count; ++i) u[i] = rng.randomu();
+    return u;
+}
+
+// Forest buffers go back to the context's pool, so reloading a forest of the
+// same shape allocates nothing.
 template <typename T>
 void dfree(Ctx* c, T*& p) {
-    if (p) cudaFree(p);
+    if (p) c->pool_put(p);
     p = nullptr;
 }
 
@@ -104,7 +114,7 @@ void free_forest(Ctx* c) {
     dfree(c, c->d_X); dfree(c, c->d_y); dfree(c, c->d_cat); dfree(c, c->d_nodes); dfree(c, c->d_nodeclass);
     dfree(c, c->d_leafidx); dfree(c, c->d_catgoleft); dfree(c, c->d_offs); dfree(c, c->d_nnode);
     dfree(c, c->d_inbag); dfree(c, c->d_segbase); dfree(c, c->d_iv); dfree(c, c->d_noob); dfree(c, c->d_permoff);
-    dfree(c, c->d_perm); dfree(c, c->d_invnoob); dfree(c, c->d_key); dfree(c, c->d_segoff); dfree(c, c->d_memb);
+    dfree(c, c->d_invnoob); dfree(c, c->d_key); dfree(c, c->d_segoff); dfree(c, c->d_memb);
     dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_vflags); dfree(c, c->d_flips);
     dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
     dfree(c, c->d_sqsd); dfree(c, c->d_opp); dfree(c, c->d_order);
@@ -115,7 +125,6 @@ void free_forest(Ctx* c) {
     c->lr_qformat = 0;
     c->loaded = c->routed = c->csr_built = false;
     c->bytes = 0;
-    c->scratch_release();
 }
 
 // Copy helper: device->(device|host) of `bytes` bytes on the context stream.
@@ -230,6 +239,8 @@ rfx_status rfx_ctx_destroy(rfx_ctx* ctx) {
         for (cudaEvent_t e : c->ev_start[s]) cudaEventDestroy(e);
         for (cudaEvent_t e : c->ev_end[s]) cudaEventDestroy(e);
     }
+    dfree(c, c->d_perm);
+    c->scratch_release();
     if (c->d_err) cudaFree(c->d_err);
     if (c->d_pairs) cudaFree(c->d_pairs);
     cudaStreamDestroy(c->stream);
@@ -291,9 +302,6 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
                     return RFX_ERR_FOREST;
                 }
         std::vector<int32_t> nnode(T), nleaf(T), noob(T);
-        std::vector<int64_t> segbase(T + 1, 0);
-        const int W = (p + 63) / 64;
-        std::vector<uint64_t> iv((size_t)T * W, 0);
         for (int t = 0; t < T; ++t) {
             const int64_t a = v->offs[t], b = v->offs[t + 1];
             // trees may come from a larger training set than the rows loaded
@@ -305,113 +313,12 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
             nnode[t] = (int)(b - a);
         }
         const int64_t N = v->offs[T];
-        std::vector<DNode> nodes((size_t)N);
-        std::vector<int32_t> leafidx((size_t)N);
-        for (int t = 0; t < T; ++t) {
-            const int64_t o = v->offs[t];
-            const int nn = nnode[t];
-            int L = 0;
-            for (int k = 0; k < nn; ++k) {
-                const int64_t g = o + k;
-                const int st = v->nodestatus[g];
-                if (st < -128 || st > 127) {
-                    set_error("rfx_forest_load: nodestatus out of range in tree " + std::to_string(t));
-                    return RFX_ERR_FOREST;
-                }
-                const int bv = v->bestvar[g];
-                const int l = v->treemap[2 * g], r = v->treemap[2 * g + 1];
-                if (st != -1) {
-                    if (bv < 0 || bv >= p) {
-                        set_error("rfx_forest_load: bestvar out of range at tree " + std::to_string(t) + " node " +
-                                  std::to_string(k));
-                        return RFX_ERR_FOREST;
-                    }
-                    if (l < 0 || l >= nn || r < 0 || r >= nn) {
-                        set_error("rfx_forest_load: child out of range at tree " + std::to_string(t) + " node " +
-                                  std::to_string(k));
-                        return RFX_ERR_FOREST;
-                    }
-                    iv[(size_t)t * W + (bv >> 6)] |= 1ull << (bv & 63);
-                }
-                DNode d;
-                d.split = v->xbestsplit[g];
-                d.left = l;
-                d.right = r;
-                const int var = (st != -1) ? bv : 0;
-                const int catf = (st != -1 && v->cat[var] != 1) ? 1 : 0;
-                d.meta = (var & 0xffff) | ((st & 0xff) << 16) | (catf << 24);
-                nodes[(size_t)g] = d;
-                leafidx[(size_t)g] = (st == -1) ? L++ : -1;
-            }
-            nleaf[t] = L;
-            segbase[t + 1] = segbase[t] + 2 * (int64_t)L + 1;
-            // varimp marks features of nodes [0, max(nnode, 1)); nnode >= 1 here
-        }
-        std::vector<uint8_t> inbag((size_t)T * n);
-        for (int t = 0; t < T; ++t) {
-            int cnt = 0;
-            for (int i = 0; i < n; ++i) {
-                const int32_t m = v->nin[(size_t)t * n + i];
-                if (m < 0) {
-                    set_error("rfx_forest_load: negative nin");
-                    return RFX_ERR_FOREST;
-                }
-                inbag[(size_t)t * n + i] = m > 0;
-                cnt += (m == 0);
-            }
-            noob[t] = cnt;
-        }
-        // permutations per distinct noob
-        std::map<int, int> perm_at;
-        for (int t = 0; t < T; ++t) perm_at[noob[t]] = 0;
-        std::vector<int> distinct;
-        int64_t total = 0;
-        for (auto& kv : perm_at) {
-            kv.second = (int)total;
-            distinct.push_back(kv.first);
-            total += std::max(kv.first, 1);
-        }
-        std::vector<int32_t> perm((size_t)total);
-        {
-            std::vector<std::thread> th;
-            const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), (int)distinct.size()));
-            std::atomic<int> next{0};
-            for (int q = 0; q < nth; ++q)
-                th.emplace_back([&]() {
-                    for (;;) {
-                        int d = next.fetch_add(1);
-                        if (d >= (int)distinct.size()) break;
-                        make_perm(distinct[d], perm.data() + perm_at[distinct[d]]);
-                    }
-                });
-            for (auto& x : th) x.join();
-        }
-        std::vector<int32_t> permoff(T);
-        std::vector<float> invnoob(T);
-        for (int t = 0; t < T; ++t) {
-            permoff[t] = perm_at[noob[t]];
-            volatile float f = (float)noob[t];
-            invnoob[t] = 1.0f / f;
-        }
-        if (total > INT32_MAX) {
-            set_error("rfx_forest_load: permutation tables too large");
-            return RFX_ERR_UNSUPPORTED;
-        }
+        const int W = (p + 63) / 64;
 
+        // device buffers (from the pool when a forest of this shape was loaded
+        // before); a load that fails leaves no forest loaded
         free_forest(c);
         c->n = n; c->p = p; c->nclass = nclass; c->maxcat = maxcat; c->T = T; c->N = N;
-        c->h_offs.assign(v->offs, v->offs + T + 1);
-        c->h_nnode = nnode;
-        c->h_nleaf = nleaf;
-        c->h_segbase = segbase;
-        c->h_noob = noob;
-        c->iv_words = W;
-        c->max_keys = 0;
-        c->max_nnode = 0;
-        for (int t = 0; t < T; ++t) {
-            c->max_keys = std::max(c->max_keys, 2 * nleaf[t]);
-            c->max_nnode = std::max(c->max_nnode, nnode[t]);
-        }
         rfx_status st = RFX_OK;
 #define ALLOC(ptr, cnt) \
     if (st == RFX_OK) st = dalloc(c, &c->ptr, (size_t)(cnt));
@@ -429,40 +336,154 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
         ALLOC(d_iv, (size_t)T * W);
         ALLOC(d_noob, T);
         ALLOC(d_permoff, T);
-        ALLOC(d_perm, total);
         ALLOC(d_invnoob, T);
         ALLOC(d_key, (size_t)T * n);
-        ALLOC(d_segoff, segbase[T]);
         ALLOC(d_memb, (size_t)T * n);
         ALLOC(d_votes, (size_t)n * nclass);
         ALLOC(d_nout, n);
+        if (st != RFX_OK) {
+            free_forest(c);
+            return st;
+        }
+        Scratch raw(c);
+        int32_t* r_status = raw.get<int32_t>(N);
+        int32_t* r_bestvar = raw.get<int32_t>(N);
+        float* r_split = raw.get<float>(N);
+        int32_t* r_treemap = raw.get<int32_t>(2 * (size_t)N);
+        int32_t* r_nin = raw.get<int32_t>((size_t)T * n);
+        int32_t* r_nleaf = raw.get<int32_t>(T);
+        LoadError* r_err = raw.get<LoadError>(1);
+        if (!r_status || !r_bestvar || !r_split || !r_treemap || !r_nin || !r_nleaf || !r_err) {
+            free_forest(c);
+            set_error("rfx_forest_load: device allocation failed");
+            return RFX_ERR_OOM;
+        }
+        cudaStream_t s = c->stream;
+        auto up = [&](void* d, const void* h, size_t bytes) {
+            return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
+        };
+        cudaError_t e = cudaMemsetAsync(r_err, 0, sizeof(LoadError), s);
+        if (e == cudaSuccess) e = up(c->d_X, v->X, sizeof(float) * (size_t)n * p);
+        if (e == cudaSuccess) e = up(c->d_y, v->y, sizeof(int32_t) * n);
+        if (e == cudaSuccess) e = up(c->d_cat, v->cat, sizeof(int32_t) * p);
+        if (e == cudaSuccess) e = up(c->d_offs, v->offs, sizeof(int64_t) * (T + 1));
+        if (e == cudaSuccess) e = up(c->d_nnode, nnode.data(), sizeof(int32_t) * T);
+        if (e == cudaSuccess) e = up(r_status, v->nodestatus, sizeof(int32_t) * (size_t)N);
+        if (e == cudaSuccess) e = up(r_bestvar, v->bestvar, sizeof(int32_t) * (size_t)N);
+        if (e == cudaSuccess) e = up(r_split, v->xbestsplit, sizeof(float) * (size_t)N);
+        if (e == cudaSuccess) e = up(r_treemap, v->treemap, sizeof(int32_t) * 2 * (size_t)N);
+        if (e == cudaSuccess) e = up(c->d_nodeclass, v->nodeclass, sizeof(int32_t) * (size_t)N);
+        if (e == cudaSuccess && v->catgoleft)
+            e = up(c->d_catgoleft, v->catgoleft, sizeof(int32_t) * (size_t)N * maxcat);
+        if (e == cudaSuccess) e = up(r_nin, v->nin, sizeof(int32_t) * (size_t)T * n);
+        if (e != cudaSuccess) {
+            free_forest(c);
+            return cuda_fail(e, "rfx_forest_load upload");
+        }
+        st = launch_pack_forest(s, T, n, p, c->d_offs, r_status, r_bestvar, r_split, r_treemap, c->d_cat, r_nin,
+                                c->d_nodes, c->d_leafidx, c->d_iv, r_nleaf, c->d_inbag, c->d_noob, r_err);
+        c->launches += 2;
+        LoadError herr{};
+        if (st == RFX_OK) {
+            e = cudaMemcpyAsync(nleaf.data(), r_nleaf, sizeof(int32_t) * T, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(noob.data(), c->d_noob, sizeof(int32_t) * T, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, r_err, sizeof(LoadError), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) st = cuda_fail(e, "rfx_forest_load pack");
+        }
+        if (st == RFX_OK && herr.code) {
+            const std::string where = " at tree " + std::to_string(herr.tree) + " node " + std::to_string(herr.node);
+            switch (herr.code) {
+                case 1: set_error("rfx_forest_load: nodestatus out of range" + where); break;
+                case 2: set_error("rfx_forest_load: bestvar out of range" + where); break;
+                case 3: set_error("rfx_forest_load: child out of range" + where); break;
+                default:
+                    set_error("rfx_forest_load: negative nin at tree " + std::to_string(herr.tree) + " sample " +
+                              std::to_string(herr.node));
+            }
+            st = RFX_ERR_FOREST;
+        }
+        if (st != RFX_OK) {
+            free_forest(c);
+            return st;
+        }
+        std::vector<int64_t> segbase(T + 1, 0);
+        for (int t = 0; t < T; ++t) segbase[t + 1] = segbase[t] + 2 * (int64_t)nleaf[t] + 1;
+
+        // permutation tables per distinct noob (kept while the set of noob values repeats)
+        std::vector<int> distinct(noob.begin(), noob.end());
+        std::sort(distinct.begin(), distinct.end());
+        distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+        std::vector<int64_t> at(distinct.size());
+        int64_t total = 0;
+        for (size_t d = 0; d < distinct.size(); ++d) {
+            at[d] = total;
+            total += std::max(distinct[d], 1);
+        }
+        if (total > INT32_MAX) {
+            free_forest(c);
+            set_error("rfx_forest_load: permutation tables too large");
+            return RFX_ERR_UNSUPPORTED;
+        }
+        if (!c->d_perm || distinct != c->perm_noobs) {
+            dfree(c, c->d_perm);
+            c->perm_noobs.clear();
+            std::vector<int32_t> perm((size_t)total);
+            const std::vector<float> u = mt_draws(distinct.empty() ? 1 : distinct.back());
+            std::vector<std::thread> th;
+            const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), (int)distinct.size()));
+            std::atomic<int> next{0};
+            for (int q = 0; q < nth; ++q)
+                th.emplace_back([&]() {
+                    for (;;) {
+                        const int d = next.fetch_add(1);
+                        if (d >= (int)distinct.size()) break;
+                        make_perm(distinct[d], u.data(), perm.data() + at[d]);
+                    }
+                });
+            for (auto& x : th) x.join();
+            if ((st = dalloc(c, &c->d_perm, (size_t)total)) != RFX_OK) {
+                free_forest(c);
+                return st;
+            }
+            e = up(c->d_perm, perm.data(), sizeof(int32_t) * (size_t)total);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) {
+                free_forest(c);
+                return cuda_fail(e, "rfx_forest_load permutation upload");
+            }
+            c->perm_noobs = distinct;
+        }
+        std::vector<int32_t> permoff(T);
+        std::vector<float> invnoob(T);
+        for (int t = 0; t < T; ++t) {
+            permoff[t] = (int32_t)at[std::lower_bound(distinct.begin(), distinct.end(), noob[t]) - distinct.begin()];
+            volatile float f = (float)noob[t];
+            invnoob[t] = 1.0f / f;
+        }
+        c->h_offs.assign(v->offs, v->offs + T + 1);
+        c->h_nnode = nnode;
+        c->h_nleaf = nleaf;
+        c->h_segbase = segbase;
+        c->h_noob = noob;
+        c->iv_words = W;
+        c->max_keys = 0;
+        c->max_nnode = 0;
+        for (int t = 0; t < T; ++t) {
+            c->max_keys = std::max(c->max_keys, 2 * nleaf[t]);
+            c->max_nnode = std::max(c->max_nnode, nnode[t]);
+        }
+        ALLOC(d_segoff, segbase[T]);
 #undef ALLOC
         if (st != RFX_OK) {
             free_forest(c);
             return st;
         }
-        auto up = [&](void* d, const void* h, size_t bytes) {
-            return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, c->stream);
-        };
-        cudaError_t e = cudaSuccess;
-        if (e == cudaSuccess) e = up(c->d_X, v->X, sizeof(float) * (size_t)n * p);
-        if (e == cudaSuccess) e = up(c->d_y, v->y, sizeof(int32_t) * n);
-        if (e == cudaSuccess) e = up(c->d_cat, v->cat, sizeof(int32_t) * p);
-        if (e == cudaSuccess) e = up(c->d_nodes, nodes.data(), sizeof(DNode) * (size_t)N);
-        if (e == cudaSuccess) e = up(c->d_nodeclass, v->nodeclass, sizeof(int32_t) * (size_t)N);
-        if (e == cudaSuccess) e = up(c->d_leafidx, leafidx.data(), sizeof(int32_t) * (size_t)N);
-        if (e == cudaSuccess && v->catgoleft)
-            e = up(c->d_catgoleft, v->catgoleft, sizeof(int32_t) * (size_t)N * maxcat);
-        if (e == cudaSuccess) e = up(c->d_offs, v->offs, sizeof(int64_t) * (T + 1));
-        if (e == cudaSuccess) e = up(c->d_nnode, nnode.data(), sizeof(int32_t) * T);
-        if (e == cudaSuccess) e = up(c->d_inbag, inbag.data(), (size_t)T * n);
-        if (e == cudaSuccess) e = up(c->d_segbase, segbase.data(), sizeof(int64_t) * (T + 1));
-        if (e == cudaSuccess) e = up(c->d_iv, iv.data(), sizeof(uint64_t) * (size_t)T * W);
-        if (e == cudaSuccess) e = up(c->d_noob, noob.data(), sizeof(int32_t) * T);
+        e = up(c->d_segbase, segbase.data(), sizeof(int64_t) * (T + 1));
         if (e == cudaSuccess) e = up(c->d_permoff, permoff.data(), sizeof(int32_t) * T);
-        if (e == cudaSuccess) e = up(c->d_perm, perm.data(), sizeof(int32_t) * (size_t)total);
         if (e == cudaSuccess) e = up(c->d_invnoob, invnoob.data(), sizeof(float) * T);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) {
             free_forest(c);
             return cuda_fail(e, "rfx_forest_load upload");
@@ -577,9 +598,13 @@ rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len) {
     }
     const bool dev = is_device_ptr(S);
     int32_t* dS = S;
+    Scratch staging(c);  // device staging for a host S, kept in the context's pool between calls
     if (!dev) {
-        cudaError_t e = ctx_malloc(c, (void**)&dS, sizeof(int32_t) * len);
-        if (e != cudaSuccess) return cuda_fail(e, "rfx_proximity_upper_i32 staging");
+        dS = staging.get<int32_t>(len);
+        if (!dS) {
+            set_error("rfx_proximity_upper_i32: device staging allocation failed");
+            return RFX_ERR_OOM;
+        }
     }
     // every call does the full pass: routing, per-tree leaf lists, pair counts
     st = launch_route(c);
@@ -593,10 +618,7 @@ rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len) {
         st = copy_out(c, S, dS, sizeof(int32_t) * len);
         if (st == RFX_OK) st = finish_host(c, true);
     }
-    if (!dev) {
-        cudaStreamSynchronize(c->stream);
-        cudaFree(dS);
-    }
+    if (!dev) cudaStreamSynchronize(c->stream);
     return st;
 }
 

@@ -122,10 +122,30 @@ struct Ctx {
     // block handed back while its kernels are still queued is only reused by
     // later work on that stream.
     std::multimap<size_t, void*> scratch_free;
+    std::map<void*, size_t> dsize;  // sizes of the buffers dalloc handed out
     void scratch_release() {
         for (auto& kv : scratch_free) cudaFree(kv.second);
         scratch_free.clear();
     }
+    void pool_put(void* p) {
+        auto it = dsize.find(p);
+        if (it == dsize.end()) {
+            cudaFree(p);
+            return;
+        }
+        scratch_free.emplace(it->second, p);
+        bytes -= it->second;
+        dsize.erase(it);
+    }
+    std::vector<int> perm_noobs;  // distinct noob values whose tables d_perm holds
+};
+
+// First failure found by the forest-packing kernels (code 0 = none).
+struct LoadError {
+    int code;  // 1 nodestatus, 2 bestvar, 3 child, 4 negative nin
+    int tree;
+    int node;  // node within the tree, or sample for code 4
+    int pad;
 };
 
 // Per-call scratch drawn from the context's pool: get() reuses a kept block of
@@ -197,21 +217,31 @@ template <typename T>
 rfx_status dalloc(Ctx* c, T** p, size_t count) {
     if (*p) return RFX_OK;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    const size_t bytes = (count * sizeof(T) + 255) & ~(size_t)255;
+    auto it = c->scratch_free.find(bytes);
+    if (it != c->scratch_free.end()) {
+        *p = static_cast<T*>(it->second);
+        c->scratch_free.erase(it);
+        c->dsize[(void*)*p] = bytes;
+        c->bytes += bytes;
+        return RFX_OK;
+    }
+    cudaError_t e = cudaMalloc((void**)p, bytes);
     if (e == cudaErrorMemoryAllocation && !c->scratch_free.empty()) {
         cudaGetLastError();
         cudaStreamSynchronize(c->stream);
         c->scratch_release();
-        e = cudaMalloc((void**)p, count * sizeof(T));
+        e = cudaMalloc((void**)p, bytes);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
-        set_error(std::string("device allocation of ") + std::to_string(count * sizeof(T)) + " bytes failed: " +
+        set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
                   cudaGetErrorString(e));
         return RFX_ERR_OOM;
     }
-    c->bytes += count * sizeof(T);
+    c->dsize[(void*)*p] = bytes;
+    c->bytes += bytes;
     return RFX_OK;
 }
 
@@ -220,6 +250,10 @@ bool is_device_ptr(const void* p);
 // kernel launchers (each returns after enqueueing on ctx->stream)
 rfx_status launch_route(Ctx* c);
 rfx_status launch_build_csr(Ctx* c);
+rfx_status launch_pack_forest(cudaStream_t s, int T, int n, int p, const int64_t* d_offs, const int32_t* status,
+                              const int32_t* bestvar, const float* split, const int32_t* treemap,
+                              const int32_t* d_cat, const int32_t* nin, DNode* nodes, int32_t* leafidx,
+                              uint64_t* iv, int32_t* nleaf, uint8_t* inbag, int32_t* noob, LoadError* err);
 rfx_status launch_pairs_upper(Ctx* c, int32_t* dS);
 rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full);
 rfx_status launch_oob_summary(Ctx* c, float* d_err_out, int32_t* d_pred, float* d_proba);
