@@ -198,6 +198,40 @@ rfx_status rfx_factor_mds_operator(rfx_ctx* ctx, int use_quantized, int precisio
  * median element sorted[n/2]. */
 rfx_status rfx_outlier_scores(rfx_ctx* ctx, int use_quantized, float* scores);
 
+/* Batched analysis of many independent forests in one CUDA graph (the
+ * reference analyses one forest per fit, so a batch of forests is a loop of
+ * separate fits, src/rf_random_forest.cpp:485-830).  Each item is a context
+ * with a loaded forest (its own stream) and DEVICE output buffers; NULL
+ * outputs skip that part: votes (n*nclass) and nout (n) as rfx_route_oob,
+ * oob_error / oob_pred as rfx_oob_summary, S (n(n+1)/2) as
+ * rfx_proximity_upper_i32, avimp/sqsd (and with impn, qimp/qimpm) as
+ * rfx_varimp.  Capture runs every item once eagerly (allocating what the
+ * chains need and checking the device flags), then records all items into
+ * one graph whose per-forest chains run concurrently; kernel_nodes (may be
+ * NULL) receives the graph's kernel count.  rfx_graph_launch replays the
+ * whole batch with one launch on `stream` (a cudaStream_t) and returns after
+ * enqueueing; it refuses a graph whose contexts were reloaded or released
+ * since capture.  Contexts must outlive the graph. */
+typedef struct rfx_batch_item {
+    rfx_ctx* ctx;
+    int32_t* votes;
+    int32_t* nout;
+    float* oob_error;
+    int32_t* oob_pred;
+    int32_t* S;
+    float* avimp;
+    float* sqsd;
+    float* qimp;
+    float* qimpm;
+    int32_t impn;
+    int32_t reserved;
+} rfx_batch_item;
+typedef struct rfx_graph rfx_graph;
+rfx_status rfx_graph_capture_batch(const rfx_batch_item* items, int32_t count, rfx_graph** out,
+                                   int64_t* kernel_nodes);
+rfx_status rfx_graph_launch(rfx_graph* g, void* stream);
+rfx_status rfx_graph_destroy(rfx_graph* g);
+
 /* Allocation-free pair counts.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run (a process

@@ -28,7 +28,8 @@ EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_strea
            "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
            "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
            "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_factor_mds_operator", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
-           "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest"]
+           "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest", "rfx_graph_capture_batch",
+           "rfx_graph_launch", "rfx_graph_destroy"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
           "predict", "oob_summary", "localimp", "pair_ranges", "lowrank_product", "lowrank_orth", "mds_factors",
@@ -57,6 +58,13 @@ class _ForestView(ctypes.Structure):
 class _LowrankOpts(ctypes.Structure):
     _fields_ = [("rank", ctypes.c_int32), ("oversample", ctypes.c_int32), ("power_iters", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+
+
+class _BatchItem(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("votes", ctypes.c_void_p), ("nout", ctypes.c_void_p),
+                ("oob_error", ctypes.c_void_p), ("oob_pred", ctypes.c_void_p), ("S", ctypes.c_void_p),
+                ("avimp", ctypes.c_void_p), ("sqsd", ctypes.c_void_p), ("qimp", ctypes.c_void_p),
+                ("qimpm", ctypes.c_void_p), ("impn", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class _Grown(ctypes.Structure):
@@ -132,6 +140,45 @@ def grow_forest(X, y, ntree: int, mtry: int, minndsize: int = 1, maxnode: int = 
     return f
 
 
+class BatchGraph:
+    """Many loaded contexts analysed by one CUDA graph (rfx_graph_capture_batch).
+
+    ``items`` is a list of dicts with key ``ctx`` (a :class:`Context` with a
+    loaded forest) and any of the device buffers ``votes``, ``nout``,
+    ``oob_error``, ``oob_pred``, ``S``, ``avimp``, ``sqsd``, ``qimp``,
+    ``qimpm`` (torch CUDA tensors or device addresses) plus ``impn``."""
+
+    KEYS = ("votes", "nout", "oob_error", "oob_pred", "S", "avimp", "sqsd", "qimp", "qimpm")
+
+    def __init__(self, items):
+        arr = (_BatchItem * len(items))()
+        self._keep = items
+        for k, it in enumerate(items):
+            arr[k].ctx = it["ctx"]._h.value
+            for key in self.KEYS:
+                setattr(arr[k], key, _ptr(it.get(key)))
+            arr[k].impn = int(bool(it.get("impn", False)))
+        h = ctypes.c_void_p()
+        kn = ctypes.c_int64(0)
+        _check(lib().rfx_graph_capture_batch(arr, len(items), ctypes.byref(h), ctypes.byref(kn)))
+        self._h = h
+        self.kernel_nodes = int(kn.value)
+
+    def launch(self, stream: int = 0):
+        _check(lib().rfx_graph_launch(self._h, ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().rfx_graph_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def pair_counts_noalloc(leaf, inbag, n: int, ntree: int, max_leaves: int, S, stream: int = 0) -> None:
     """Allocation-free pair counts into the device buffer S (see include/rfx_b200.h)."""
     _check(lib().rfx_pair_counts_noalloc(_vp(leaf), _vp(inbag), int(n), int(ntree), int(max_leaves), _vp(S),
@@ -204,12 +251,17 @@ class Context:
         _check(lib().rfx_route_oob(self._h, _vp(q), _vp(nout), _vp(leaf)))
         return q, nout, leaf
 
-    def oob_summary(self):
-        err = np.zeros(1, np.float32)
-        pred = np.zeros(self.n, np.int32)
-        proba = np.zeros((self.n, self.nclass), np.float32)
+    def oob_summary(self, err=None, pred=None, proba=None):
+        """OOB error, predictions and probabilities; with any output given
+        (host or device buffers) only the given ones are written and returned."""
+        if err is None and pred is None and proba is None:
+            err = np.zeros(1, np.float32)
+            pred = np.zeros(self.n, np.int32)
+            proba = np.zeros((self.n, self.nclass), np.float32)
+            _check(lib().rfx_oob_summary(self._h, _vp(err), _vp(pred), _vp(proba)))
+            return float(err[0]), pred, proba
         _check(lib().rfx_oob_summary(self._h, _vp(err), _vp(pred), _vp(proba)))
-        return float(err[0]), pred, proba
+        return err, pred, proba
 
     def proximity_upper(self, S=None):
         """Packed upper-triangle INT32 pair counts (n(n+1)/2,)."""

@@ -125,6 +125,7 @@ void free_forest(Ctx* c) {
     c->lr_qformat = 0;
     c->loaded = c->routed = c->csr_built = false;
     c->bytes = 0;
+    c->generation++;
 }
 
 // Copy helper: device->(device|host) of `bytes` bytes on the context stream.

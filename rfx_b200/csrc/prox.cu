@@ -491,7 +491,7 @@ rfx_status launch_build_csr(Ctx* c) {
     smem_keys = std::max(smem_keys, 32);
     const size_t smem = (size_t)smem_keys * sizeof(int32_t);
     StageTimer st(c, ST_CSR, c->max_keys + 1 > smem_keys ? 2 : 1);
-    RFX_CUDA(cudaFuncSetAttribute(build_csr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel, dev_smem)) return s0;
     build_csr_kernel<<<c->T, CSR_THREADS, smem, c->stream>>>(c->d_key, c->n, c->d_segbase, c->d_segoff, c->d_memb, smem_keys,
                                                     c->d_err);
     RFX_CUDA(cudaGetLastError());
@@ -536,7 +536,7 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
             RFX_CUDA(cudaGetLastError());
         }
         const size_t smem = ((size_t)c->n + 1) / 2 * sizeof(uint32_t);
-        RFX_CUDA(cudaFuncSetAttribute(pairs_row16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel, dev_smem)) return s0;
         StageTimer st(c, ST_PAIRS, 1);
         pairs_row16_kernel<<<c->n, R16_THREADS, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, dS,
                                                                    c->d_pairs);
@@ -545,7 +545,7 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
     }
     const int win = pairs_window(c);
     const size_t smem = (size_t)win * sizeof(uint32_t);
-    RFX_CUDA(cudaFuncSetAttribute(pairs_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (rfx_status s0 = allow_dyn_smem(pairs_row_kernel, dev_smem)) return s0;
     RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
     StageTimer st(c, ST_PAIRS, 1);
     dim3 grid(c->n, (c->n + win - 1) / win);
@@ -566,7 +566,7 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
     int smem_keys = std::min(max_keys + 1, (dev_smem - 1024) / 4);
     smem_keys = std::max(smem_keys, 32);
     const size_t smem = (size_t)smem_keys * sizeof(int32_t);
-    RFX_CUDA(cudaFuncSetAttribute(build_csr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel, dev_smem)) return s0;
     build_csr_kernel<<<a.T, CSR_THREADS, smem, stream>>>(a.key, a.n, a.segbase, a.segoff, a.memb, smem_keys,
                                                          a.err);
     RFX_CUDA(cudaGetLastError());
@@ -580,7 +580,7 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
     row_order_kernel<<<1, 1024, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.order);
     RFX_CUDA(cudaGetLastError());
     const size_t smem2 = ((size_t)a.n + 1) / 2 * sizeof(uint32_t);
-    RFX_CUDA(cudaFuncSetAttribute(pairs_row16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel, dev_smem)) return s0;
     pairs_row16_kernel<<<a.n, R16_THREADS, smem2, stream>>>(a.opp, a.memb, a.order, a.n, a.T, a.S, nullptr);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;

@@ -92,6 +92,7 @@ struct Ctx {
     unsigned long long* d_pairs = nullptr;  // pair-update counter
     bool routed = false;
     bool csr_built = false;
+    uint64_t generation = 0;            // bumped whenever the forest buffers are released
     int64_t last_pairs = 0;
 
     // varimp scratch
@@ -246,6 +247,19 @@ rfx_status dalloc(Ctx* c, T** p, size_t count) {
 }
 
 bool is_device_ptr(const void* p);
+
+// Raise a kernel's dynamic shared-memory limit to everything the device allows
+// beside its static shared memory.  Setting the limit (not the launch's own
+// size) keeps launches of other sizes, e.g. ones captured in a graph for other
+// forests, valid.
+template <typename K>
+rfx_status allow_dyn_smem(K* kernel, int dev_smem) {
+    cudaFuncAttributes a;
+    RFX_CUDA(cudaFuncGetAttributes(&a, kernel));
+    RFX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  dev_smem - (int)a.sharedSizeBytes));
+    return RFX_OK;
+}
 
 // kernel launchers (each returns after enqueueing on ctx->stream)
 rfx_status launch_route(Ctx* c);
