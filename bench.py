@@ -530,7 +530,8 @@ def main():
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "forest_grow_s": round(grow_s, 2)},
             "roofline": roofline, "gpu_launches": gpu_launches,
-            "breakdown_ms": {k: round(v, 4) for k, v in kernels.items()}}
+            "breakdown_ms": {k: round(v, 4) for k, v in kernels.items()},
+            "tuned_shapes": abi.tuned_shapes()}
     if clk:
         line["clocks"] = clk
 

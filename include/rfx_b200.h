@@ -232,6 +232,17 @@ rfx_status rfx_graph_capture_batch(const rfx_batch_item* items, int32_t count, r
 rfx_status rfx_graph_launch(rfx_graph* g, void* stream);
 rfx_status rfx_graph_destroy(rfx_graph* g);
 
+/* Launch-shape autotuner (no counterpart in the reference).  The routing,
+ * pair-count and varimp-walk stages each offer a few launch shapes with
+ * identical results; the first run for a problem shape (device and
+ * power-of-two buckets of n, ntree, p) times each once on the context stream
+ * and keeps the fastest for the process.  Setting RFX_AUTOTUNE=0 keeps the
+ * default shapes; nothing is tuned while a stream is being captured.
+ * rfx_tuned_shapes copies up to `cap` records of 6 int32 {stage (0 routing,
+ * 1 pair counts, 2 varimp walk), device, log2 n, log2 ntree, log2 p, shape}
+ * and sets *count to the number of records. */
+rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count);
+
 /* Allocation-free pair counts.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run (a process

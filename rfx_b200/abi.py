@@ -29,7 +29,7 @@ EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_strea
            "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
            "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_factor_mds_operator", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest", "rfx_graph_capture_batch",
-           "rfx_graph_launch", "rfx_graph_destroy"]
+           "rfx_graph_launch", "rfx_graph_destroy", "rfx_tuned_shapes"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
           "predict", "oob_summary", "localimp", "pair_ranges", "lowrank_product", "lowrank_orth", "mds_factors",
@@ -177,6 +177,26 @@ class BatchGraph:
             self.close()
         except Exception:
             pass
+
+
+TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk"}
+# launch shapes per stage, in the library's shape order
+TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees"], 1: ["256", "512", "1024"],
+                2: ["64", "128", "256"]}
+
+
+def tuned_shapes():
+    """Launch shapes the autotuner has picked in this process, as dicts."""
+    cnt = ctypes.c_int32(0)
+    _check(lib().rfx_tuned_shapes(None, 0, ctypes.byref(cnt)))
+    buf = np.zeros(6 * max(cnt.value, 1), np.int32)
+    _check(lib().rfx_tuned_shapes(_vp(buf), cnt.value, ctypes.byref(cnt)))
+    out = []
+    for r in buf[: 6 * cnt.value].reshape(-1, 6):
+        st = int(r[0])
+        out.append({"stage": TUNED_STAGES.get(st, str(st)), "device": int(r[1]), "log2_n": int(r[2]),
+                    "log2_ntree": int(r[3]), "log2_p": int(r[4]), "shape": TUNED_SHAPES[st][int(r[5])]})
+    return out
 
 
 def pair_counts_noalloc(leaf, inbag, n: int, ntree: int, max_leaves: int, S, stream: int = 0) -> None:

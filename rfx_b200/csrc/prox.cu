@@ -309,9 +309,11 @@ row_order_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ se
     }
 }
 
+// Launch shapes of the row kernel the autotuner chooses from (threads per
+// CTA); 512 is the default.
 constexpr int R16_THREADS = 512;
-constexpr int R16_WARPS = R16_THREADS / 32;
 
+template <int NW>
 __device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, int w, int* total) {
     int incl = v;
 #pragma unroll
@@ -322,49 +324,51 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, 
     if (lane == 31) wtot[w] = incl;
     __syncthreads();
     if (w == 0) {
-        static_assert(R16_WARPS <= 32, "one warp scans the per-warp totals");
-        const int x0 = lane < R16_WARPS ? wtot[lane] : 0;
+        static_assert(NW <= 32, "one warp scans the per-warp totals");
+        const int x0 = lane < NW ? wtot[lane] : 0;
         int x = x0;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const int u = __shfl_up_sync(0xffffffffu, x, d);
             if (lane >= d) x += u;
         }
-        if (lane < R16_WARPS) wtot[lane] = x - x0;
-        if (lane == R16_WARPS - 1) wtot[R16_WARPS] = x;
+        if (lane < NW) wtot[lane] = x - x0;
+        if (lane == NW - 1) wtot[NW] = x;
     }
     __syncthreads();
-    *total = wtot[R16_WARPS];
+    *total = wtot[NW];
     const int r = wtot[w] + incl - v;
     __syncthreads();  // wtot is reused by the next scan
     return r;
 }
 
-// One CTA per row.  Each round takes 1024 trees' member ranges of this row,
+// One CTA of NT threads per row.  Each round takes NT trees' member ranges of this row,
 // drops the empty ones, and cuts the rest into 32-member pieces; every warp
 // owns a contiguous run of pieces (so warps finish together whatever the range
 // lengths) and processes a piece with its 32 lanes on 32 consecutive members:
 // coalesced loads and one shared-memory atomic per member.
-__global__ void __launch_bounds__(R16_THREADS)
+template <int NT>
+__global__ void __launch_bounds__(NT)
 pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                    int n, int T, int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+    constexpr int NW = NT / 32;
     extern __shared__ uint32_t acc[];  // ceil(n/2) words, two u16 counters each
-    __shared__ long long cb[R16_THREADS];      // absolute start of each non-empty range
-    __shared__ int clen[R16_THREADS];          // its length
-    __shared__ int cp0[R16_THREADS + 1];       // its first piece index (+ sentinel)
-    __shared__ int wtot[R16_WARPS + 1];
+    __shared__ long long cb[NT];      // absolute start of each non-empty range
+    __shared__ int clen[NT];          // its length
+    __shared__ int cp0[NT + 1];       // its first piece index (+ sentinel)
+    __shared__ int wtot[NW + 1];
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int words = (n + 1) >> 1;
     {
         uint4* a4 = reinterpret_cast<uint4*>(acc);
         const int w4 = words >> 2;
-        for (int k = tid; k < w4; k += R16_THREADS) a4[k] = make_uint4(0u, 0u, 0u, 0u);
-        for (int k = (w4 << 2) + tid; k < words; k += R16_THREADS) acc[k] = 0u;
+        for (int k = tid; k < w4; k += NT) a4[k] = make_uint4(0u, 0u, 0u, 0u);
+        for (int k = (w4 << 2) + tid; k < words; k += NT) acc[k] = 0u;
     }
     unsigned long long my_pairs = 0;
     const int2* orow = opp + (size_t)i * T;
-    for (int t0 = 0; t0 < T; t0 += R16_THREADS) {
+    for (int t0 = 0; t0 < T; t0 += NT) {
         const int t = t0 + tid;
         long long b = 0;
         int len = 0;
@@ -376,8 +380,8 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
         my_pairs += (unsigned long long)len;
         const int np = (len + 31) >> 5;
         int nseg, P;
-        const int cidx = block_exclusive_scan(np > 0 ? 1 : 0, wtot, lane, w, &nseg);
-        const int pfx = block_exclusive_scan(np, wtot, lane, w, &P);
+        const int cidx = block_exclusive_scan<NW>(np > 0 ? 1 : 0, wtot, lane, w, &nseg);
+        const int pfx = block_exclusive_scan<NW>(np, wtot, lane, w, &P);
         if (np > 0) {
             cb[cidx] = b;
             clen[cidx] = len;
@@ -387,7 +391,7 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
         __syncthreads();  // also orders the accumulator zeroing before any update
         // warp w owns pieces [q0, q1); walk the ranges they cover, 32 lanes on
         // consecutive members, four loads in flight per lane
-        const int per = (P + R16_WARPS - 1) / R16_WARPS;
+        const int per = (P + NW - 1) / NW;
         const int q0 = w * per;
         const int q1 = min(P, q0 + per);
         if (q0 < q1) {
@@ -423,7 +427,7 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
     }
     const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
     const uint16_t* a16 = reinterpret_cast<const uint16_t*>(acc);
-    for (int j = i + tid; j < n; j += R16_THREADS) S[rowoff + j] = (int32_t)a16[j];
+    for (int j = i + tid; j < n; j += NT) S[rowoff + j] = (int32_t)a16[j];
     if (pairs) {
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
@@ -536,12 +540,24 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
             RFX_CUDA(cudaGetLastError());
         }
         const size_t smem = ((size_t)c->n + 1) / 2 * sizeof(uint32_t);
-        if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<256>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<512>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<1024>, dev_smem)) return s0;
         StageTimer st(c, ST_PAIRS, 1);
-        pairs_row16_kernel<<<c->n, R16_THREADS, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, dS,
-                                                                   c->d_pairs);
-        RFX_CUDA(cudaGetLastError());
-        return RFX_OK;
+        return autotune(c, TK_PAIRS16, 3, 1, [&](int shape) -> rfx_status {
+            RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
+            if (shape == 0)
+                pairs_row16_kernel<256><<<c->n, 256, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T,
+                                                                       dS, c->d_pairs);
+            else if (shape == 2)
+                pairs_row16_kernel<1024><<<c->n, 1024, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n,
+                                                                         c->T, dS, c->d_pairs);
+            else
+                pairs_row16_kernel<512><<<c->n, 512, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T,
+                                                                       dS, c->d_pairs);
+            RFX_CUDA(cudaGetLastError());
+            return RFX_OK;
+        });
     }
     const int win = pairs_window(c);
     const size_t smem = (size_t)win * sizeof(uint32_t);
@@ -580,8 +596,9 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
     row_order_kernel<<<1, 1024, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.order);
     RFX_CUDA(cudaGetLastError());
     const size_t smem2 = ((size_t)a.n + 1) / 2 * sizeof(uint32_t);
-    if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel, dev_smem)) return s0;
-    pairs_row16_kernel<<<a.n, R16_THREADS, smem2, stream>>>(a.opp, a.memb, a.order, a.n, a.T, a.S, nullptr);
+    if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<R16_THREADS>, dev_smem)) return s0;
+    pairs_row16_kernel<R16_THREADS><<<a.n, R16_THREADS, smem2, stream>>>(a.opp, a.memb, a.order, a.n, a.T, a.S,
+                                                                         nullptr);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
 }

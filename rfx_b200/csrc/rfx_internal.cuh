@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <string>
 #include <utility>
@@ -264,6 +265,10 @@ rfx_status allow_dyn_smem(K* kernel, int dev_smem) {
 // kernel launchers (each returns after enqueueing on ctx->stream)
 rfx_status launch_route(Ctx* c);
 rfx_status launch_build_csr(Ctx* c);
+
+// Autotuned stages: kernel ids and the launch shapes each offers.
+enum TuneKernel : int { TK_ROUTE = 0, TK_PAIRS16 = 1, TK_VWALK = 2 };
+rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<rfx_status(int)>& run);
 rfx_status launch_pack_forest(cudaStream_t s, int T, int n, int p, const int64_t* d_offs, const int32_t* status,
                               const int32_t* bestvar, const float* split, const int32_t* treemap,
                               const int32_t* d_cat, const int32_t* nin, DNode* nodes, int32_t* leafidx,

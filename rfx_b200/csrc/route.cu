@@ -13,37 +13,62 @@ namespace rfx {
 
 namespace {
 
-constexpr int ROUTE_THREADS = 256;
-
-__global__ void __launch_bounds__(ROUTE_THREADS)
-route_kernel(const float* __restrict__ X, int n, int p, int nclass, const DNode* __restrict__ nodes,
+// Launch shapes the autotuner chooses from: threads per CTA x trees per
+// thread (a thread walks TPC consecutive trees for its sample, reusing the
+// sample's feature row from L1).
+template <int RT, int TPC>
+__global__ void __launch_bounds__(RT)
+route_kernel(const float* __restrict__ X, int n, int p, int T, int nclass, const DNode* __restrict__ nodes,
              const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
              const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
              const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
              const int32_t* __restrict__ catgoleft, int maxcat, int32_t* __restrict__ key_out,
              int32_t* __restrict__ leaf_out, int32_t* __restrict__ votes) {
-    const int t = blockIdx.y;
-    const int i = blockIdx.x * ROUTE_THREADS + threadIdx.x;
+    const int i = blockIdx.x * RT + threadIdx.x;
     if (i >= n) return;
-    const int64_t o = offs[t];
-    const DNode* tn = nodes + o;
-    const int32_t* tc = nodeclass + o;
-    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
-    const int nn = nnode_arr[t];
     const float* xrow = X + (size_t)i * p;
-    const size_t ti = (size_t)t * n + i;
-    const bool ib = inbag[ti] != 0;
-    int node;
-    if (!ib) {
-        int cls;
-        node = walk_testreebag(xrow, p, tn, tc, nn, cat, cgl, maxcat, &cls);
-        if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
-    } else {
-        node = walk_terminal(xrow, p, tn, cat, cgl, maxcat, 2 * n + 1);
+#pragma unroll 1
+    for (int q = 0; q < TPC; ++q) {
+        const int t = blockIdx.y * TPC + q;
+        if (t >= T) return;
+        const int64_t o = offs[t];
+        const DNode* tn = nodes + o;
+        const int32_t* tc = nodeclass + o;
+        const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+        const int nn = nnode_arr[t];
+        const size_t ti = (size_t)t * n + i;
+        const bool ib = inbag[ti] != 0;
+        int node;
+        if (!ib) {
+            int cls;
+            node = walk_testreebag(xrow, p, tn, tc, nn, cat, cgl, maxcat, &cls);
+            if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
+        } else {
+            node = walk_terminal(xrow, p, tn, cat, cgl, maxcat, 2 * n + 1);
+        }
+        const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
+        key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
+        if (leaf_out) leaf_out[ti] = node;
     }
-    const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
-    key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
-    if (leaf_out) leaf_out[ti] = node;
+}
+
+constexpr int ROUTE_SHAPES = 5;
+
+// votes must be zero beforehand (the kernel adds to them)
+void route_launch(Ctx* c, int shape, int32_t* d_leaf) {
+    auto go = [&](auto kernel, int rt, int tpc) {
+        dim3 grid((c->n + rt - 1) / rt, (c->T + tpc - 1) / tpc);
+        kernel<<<grid, rt, 0, c->stream>>>(c->d_X, c->n, c->p, c->T, c->nclass, c->d_nodes, c->d_nodeclass,
+                                           c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+                                           c->d_catgoleft, c->maxcat, c->d_key, d_leaf, c->d_votes);
+    };
+    switch (shape) {
+        case 1: go(route_kernel<128, 1>, 128, 1); break;
+        case 2: go(route_kernel<512, 1>, 512, 1); break;
+        case 3: go(route_kernel<256, 2>, 256, 2); break;
+        case 4: go(route_kernel<256, 4>, 256, 4); break;
+        default: go(route_kernel<256, 1>, 256, 1); break;
+    }
 }
 
 // nout[i] = 2 * (number of trees with i out of bag): the reference increments
@@ -116,12 +141,13 @@ predict_kernel(const float* __restrict__ X, int m, int p, int nclass, int maxnod
 
 rfx_status launch_route(Ctx* c) {
     StageTimer st(c, ST_ROUTE, 2);
-    RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
-    dim3 grid((c->n + ROUTE_THREADS - 1) / ROUTE_THREADS, c->T);
-    route_kernel<<<grid, ROUTE_THREADS, 0, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
-                                                        c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
-                                                        c->d_catgoleft, c->maxcat, c->d_key, nullptr, c->d_votes);
-    RFX_CUDA(cudaGetLastError());
+    rfx_status r = autotune(c, TK_ROUTE, ROUTE_SHAPES, 0, [&](int shape) -> rfx_status {
+        RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
+        route_launch(c, shape, nullptr);
+        RFX_CUDA(cudaGetLastError());
+        return RFX_OK;
+    });
+    if (r != RFX_OK) return r;
     nout_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_inbag, c->n, c->T, c->d_nout);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
@@ -129,12 +155,9 @@ rfx_status launch_route(Ctx* c) {
 
 rfx_status launch_route_leaf(Ctx* c, int32_t* d_leaf) {
     StageTimer st(c, ST_ROUTE, 1);
-    dim3 grid((c->n + ROUTE_THREADS - 1) / ROUTE_THREADS, c->T);
     // votes are recomputed identically; clear first so they stay exact
     RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
-    route_kernel<<<grid, ROUTE_THREADS, 0, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
-                                                        c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
-                                                        c->d_catgoleft, c->maxcat, c->d_key, d_leaf, c->d_votes);
+    route_launch(c, 0, d_leaf);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
 }

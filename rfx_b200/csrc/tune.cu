@@ -1,0 +1,102 @@
+// Launch-shape autotuner.  A tunable stage offers a few launch shapes that
+// all compute the same result; the first time a stage runs for a given
+// problem shape (device, kernel, and power-of-two buckets of n, ntree and p)
+// each shape is run once and timed with CUDA events on the context stream,
+// the fastest is remembered for the rest of the process, and the stage's
+// result is the one the last timed run left behind (every shape writes the
+// complete result).  Tuning is skipped, and the default shape used, while the
+// stream is being captured into a graph or when RFX_AUTOTUNE=0.
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
+#include "rfx_internal.cuh"
+
+namespace rfx {
+namespace {
+
+int ilog2(long long v) {
+    int r = 0;
+    while (v > 1) {
+        v >>= 1;
+        ++r;
+    }
+    return r;
+}
+
+std::mutex g_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_choice;
+
+bool tuning_enabled() {
+    const char* e = std::getenv("RFX_AUTOTUNE");
+    return !(e && std::string(e) == "0");
+}
+
+}  // namespace
+
+rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<rfx_status(int)>& run) {
+    const auto key = std::make_tuple(kernel, c->device, ilog2(c->n), ilog2(c->T), ilog2(c->p));
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_choice.find(key);
+        if (it != g_choice.end()) return run(it->second);
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    RFX_CUDA(cudaStreamIsCapturing(c->stream, &cap));
+    if (!tuning_enabled() || cap != cudaStreamCaptureStatusNone || nvar < 2) return run(def);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RFX_CUDA(cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(e, "autotune");
+    }
+    rfx_status st = run(def);  // warm-up (caches, first-launch costs)
+    int best = def;
+    float best_ms = 3.0e38f;
+    for (int v = 0; v < nvar && st == RFX_OK; ++v) {
+        e = cudaEventRecord(e0, c->stream);
+        if (e == cudaSuccess) st = run(v);
+        if (e == cudaSuccess && st == RFX_OK) e = cudaEventRecord(e1, c->stream);
+        if (e == cudaSuccess && st == RFX_OK) e = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        if (e == cudaSuccess && st == RFX_OK) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) break;
+        if (st == RFX_OK && ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != RFX_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "autotune");
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_choice[key] = best;
+    return RFX_OK;
+}
+
+}  // namespace rfx
+
+extern "C" rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count) {
+    std::lock_guard<std::mutex> lk(rfx::g_mu);
+    int k = 0;
+    for (const auto& kv : rfx::g_choice) {
+        if (out && k < cap) {
+            int32_t* r = out + 6 * (size_t)k;
+            r[0] = std::get<0>(kv.first);
+            r[1] = std::get<1>(kv.first);
+            r[2] = std::get<2>(kv.first);
+            r[3] = std::get<3>(kv.first);
+            r[4] = std::get<4>(kv.first);
+            r[5] = kv.second;
+        }
+        ++k;
+    }
+    if (count) *count = k;
+    return RFX_OK;
+}

@@ -93,11 +93,10 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
     }
 }
 
-constexpr int VW = 128;  // threads per CTA of the walk kernel
-
-// One thread per (tree, OOB position r): grid = (ceil(max noob / VW), T).
-template <int W>
-__global__ void __launch_bounds__(VW, 12)
+// One thread per (tree, OOB position r): grid = (ceil(max noob / VW), T),
+// VW threads per CTA (a launch shape the autotuner picks: 64, 128 or 256).
+template <int W, int VW>
+__global__ void __launch_bounds__(VW, 1536 / VW)
 varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
                    const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
                    const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
@@ -315,18 +314,28 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
     const size_t smem = (size_t)c->p * sizeof(int32_t);
     {
         StageTimer st(c, ST_VARIMP_TREE, 2);
-        RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
-        RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
         joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob);
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
-        dim3 grid((max_noob + VW - 1) / VW, c->T);
-        varimp_walk_kernel<W><<<grid, VW, smem, c->stream>>>(
-            c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs, c->d_nnode, c->d_noob, c->d_cat,
-            c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, c->d_vflags, c->d_flips, c->d_right,
-            c->d_rightimp, c->d_err);
-        RFX_CUDA(cudaGetLastError());
+        auto go = [&](auto kernel, int vw) {
+            dim3 grid((max_noob + vw - 1) / vw, c->T);
+            kernel<<<grid, vw, smem, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
+                                                 c->d_nnode, c->d_noob, c->d_cat, c->d_catgoleft, c->maxcat,
+                                                 c->d_permoff, c->d_perm, c->d_joob, c->d_vflags, c->d_flips,
+                                                 c->d_right, c->d_rightimp, c->d_err);
+        };
+        rfx_status r = autotune(c, TK_VWALK, 3, 1, [&](int shape) -> rfx_status {
+            // the walk adds to the per-tree counts: clear them for every run
+            RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
+            RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
+            if (shape == 0) go(varimp_walk_kernel<W, 64>, 64);
+            else if (shape == 2) go(varimp_walk_kernel<W, 256>, 256);
+            else go(varimp_walk_kernel<W, 128>, 128);
+            RFX_CUDA(cudaGetLastError());
+            return RFX_OK;
+        });
+        if (r != RFX_OK) return r;
     }
     if (impn) {
         StageTimer st(c, ST_VARIMP_SAMPLE, 1);
