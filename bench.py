@@ -207,27 +207,42 @@ def run_reference(args):
 
 
 def run_lowrank(args):
-    """Low-rank proximity + 3-D MDS at n=200,000, 2,000 trees, rank 64:
-    the mixed form (BF16 storage, FP32 accumulate, FP32 final product) against
-    the plain FP32 form, both timed end to end on the device (factors, INT8
-    per-column quantisation, MDS from the quantised factors), with the relative
-    Frobenius error of each against the exact FP64 proximity on a seeded
-    20,000-row subsample."""
+    """Low-rank proximity + MDS, the mixed form against the plain FP32 form,
+    both timed end to end on the device, with the relative Frobenius error of
+    each against the exact FP64 proximity on a seeded 20,000-row subsample.
+
+    lowrank: n=200,000 cover-shaped rows, 2,000 trees, rank 64, factors INT8
+             with per-column scales, 3-D MDS from the quantised factors.
+    large:   n=1,000,000 Gaussian-mixture rows with 1% injected outliers, 500
+             trees (mtry 5, nodesize 5), rank 32, factors FP8 e4m3 with
+             per-column scales, 3-D MDS and outlier scores from the factors.
+    mixed = BF16 sketch storage with FP32 accumulation, tcgen05 BF16 MDS
+    products with one FP32 refinement step; FP32 = the same algorithm in FP32."""
     import torch
 
     from rfx_b200 import abi, synth
 
-    n = args.n if args.n is not None else 200_000
-    T = args.trees if args.trees is not None else 2000
-    k = 64
-    X, y = synth.mixed_cover(n, seed=synth.SEED_BASE + 3)
-    cat = synth.detect_categorical(X)
+    large = args.workload == "large"
+    if large:
+        n = args.n if args.n is not None else 1_000_000
+        T = args.trees if args.trees is not None else 500
+        k, fmt, mtry, minnd, nclass = 32, 2, 5, 5, 4
+        X, y, outl = synth.large_gmm(n, return_outliers=True)
+        cat = np.ones(X.shape[1], np.int32)
+        gen = "Gaussian mixture, 8 components, 4 classes, 1% uniform outliers in a 10x box, seed 20251006"
+    else:
+        n = args.n if args.n is not None else 200_000
+        T = args.trees if args.trees is not None else 2000
+        k, fmt, mtry, minnd, nclass = 64, 1, MTRY, 1, 7
+        X, y = synth.mixed_cover(n, seed=synth.SEED_BASE + 3)
+        cat = synth.detect_categorical(X)
+        gen = "mixed-type cover-shaped generator, seed 20251004"
     t0 = time.time()
-    f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
+    f = abi.grow_forest(X, y, T, mtry, minnd, cat=cat, nclass=nclass)
     grow_s = time.time() - t0
     ctx = abi.Context(0)
     ctx.load(f, X, y)
-    _, nout, _ = ctx.route_oob()
+    ctx.route_oob()
 
     phases = {0: {}, 1: {}}
 
@@ -237,27 +252,31 @@ def run_lowrank(args):
         t = time.perf_counter()
         A, ev = ctx.lowrank(k, oversample=16, power_iters=1, precision=precision)
         t1 = time.perf_counter()
-        ctx.lowrank_quantize(1)
+        ctx.lowrank_quantize(fmt)
         t2 = time.perf_counter()
         C, _ = ctx.mds_from_factors(3, use_quantized=True, precision=precision)
         torch.cuda.synchronize()
         t3 = time.perf_counter()
+        o = ctx.outlier_scores(use_quantized=True) if large else None
+        t4 = time.perf_counter()
         st, _ = ctx.profile_read()
         phases[precision] = {"factors_s": t1 - t, "quantize_s": t2 - t1, "mds_s": t3 - t2,
                              "operator_product_ms_avg": st["lowrank_product"], "orth_ms_avg": st["lowrank_orth"],
                              "mds_ms": st["mds_factors"], "route_ms": max(st["route"], 0.0),
                              "leaf_lists_ms": max(st["leaf_lists"], 0.0)}
-        return t3 - t, A, C
+        if large:
+            phases[precision]["outlier_s"] = t4 - t3
+        return t4 - t, A, C, o
 
     run(1)  # warm-up (module load, allocations; builds the leaf keys and member lists once)
-    once_ms = {k: phases[1][k] for k in ("route_ms", "leaf_lists_ms")}
+    once_ms = {key: phases[1][key] for key in ("route_ms", "leaf_lists_ms")}
     times = {0: [], 1: []}
     res = {}
     for rep in range(max(1, args.steps)):
         for prec in (0, 1):
-            dt, A, C = run(prec)
+            dt, A, C, o = run(prec)
             times[prec].append(dt)
-            res[prec] = (A, C)
+            res[prec] = (A, C, o)
     # exact FP64 proximity on a seeded subsample
     m = min(20_000, n)
     rng = np.random.default_rng(7)
@@ -289,18 +308,25 @@ def run_lowrank(args):
     ctx_s.close()
     ctx.close()
     t32, tmx = min(times[0]), min(times[1])
-    line = {"metric": "n=200K rank-64 prox+MDS sec, mixed vs FP32 form @same err", "value": tmx, "unit": "s",
-            "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "dtype": "bf16+fp32 (mixed) / fp32",
-            "data": "synthetic (seeded mixed-type cover-shaped generator, seed 20251004)",
-            "config": {"workload": f"low-rank proximity + 3D MDS: n={n} p=54 c=7 ntree={T} mtry=7 rank={k} "
-                                   "oversample=16 power_iters=1, INT8 per-column factors", "forest_grow_s": round(grow_s, 1),
-                       "per_forest_once_ms": once_ms,
-                       "timed": "factors (range finder), INT8 quantisation, 3-D MDS from the quantised factors; "
-                                "leaf keys and member lists are built once per loaded forest (per_forest_once_ms)"},
+    qname = "FP8 e4m3" if fmt == 2 else "INT8"
+    line = {"metric": f"n={n // 1000}K rank-{k} prox+MDS sec, mixed vs FP32 form @same err", "value": tmx,
+            "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+            "dtype": "bf16+fp32 (mixed) / fp32", "data": f"synthetic ({gen})",
+            "config": {"workload": f"low-rank proximity + 3D MDS{' + outlier scores' if large else ''}: n={n} "
+                                   f"p={X.shape[1]} c={nclass} ntree={T} mtry={mtry} nodesize={minnd} rank={k} "
+                                   f"oversample=16 power_iters=1, {qname} per-column factors",
+                       "forest_grow_s": round(grow_s, 1), "per_forest_once_ms": once_ms,
+                       "timed": f"factors (range finder), {qname} quantisation, 3-D MDS from the quantised factors"
+                                f"{', outlier scores' if large else ''}; leaf keys and member lists are built once "
+                                "per loaded forest (per_forest_once_ms)"},
             "fp32_seconds": t32, "mixed_seconds": tmx, "speedup_mixed_vs_fp32": t32 / tmx,
             "rel_frobenius_err_fp32": errs[0], "rel_frobenius_err_mixed": errs[1],
             "err_subsample_rows": m, "mds_procrustes_rel_mixed_vs_fp32": proc,
             "phases_fp32": phases[0], "phases_mixed": phases[1]}
+    if large:
+        o = res[1][2]
+        top = np.argsort(-o)[: len(outl)]
+        line["outlier_recall_top1pct"] = float(np.isin(top, outl).mean())
     print(json.dumps(line), flush=True)
     return 0
 
@@ -411,10 +437,10 @@ def main():
     ap.add_argument("--trees", type=int, default=None, help="trees (default 1000; 2000 for --workload lowrank)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="exact", choices=["exact", "lowrank", "batch"])
+    ap.add_argument("--workload", default="exact", choices=["exact", "lowrank", "large", "batch"])
     ap.add_argument("--forests", type=int, default=64, help="forests in the batch workload")
     args = ap.parse_args()
-    if args.workload == "lowrank":
+    if args.workload in ("lowrank", "large"):
         return run_lowrank(args)
     if args.workload == "batch":
         args.warmup = max(args.warmup, 3)

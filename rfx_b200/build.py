@@ -29,7 +29,7 @@ CPP_SOURCES = ["host/grow.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
               "--expt-relaxed-constexpr", "-I" + INC, "-I" + CSRC]
-CXX_FLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-std=c++17", "-I" + INC, "-pthread"]
+CXX_FLAGS = ["-O3", "-ffp-contract=off", "-fPIC", "-std=c++17", "-I" + INC, "-pthread"]
 
 LIB_PATH = os.path.join(PKG, "librfx_b200.so")
 

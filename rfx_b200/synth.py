@@ -93,8 +93,9 @@ def uneven_forests(count: int = 64, seed: int = SEED_BASE + 4, n_range=(1000, 50
 
 
 def large_gmm(n: int = 1_000_000, p: int = 32, seed: int = SEED_BASE + 5, n_comp: int = 8,
-              n_class: int = 4, outlier_frac: float = 0.01):
-    """8-component Gaussian mixture, 4 classes, 1% uniform outliers in a 10x box."""
+              n_class: int = 4, outlier_frac: float = 0.01, return_outliers: bool = False):
+    """8-component Gaussian mixture, 4 classes, 1% uniform outliers in a 10x box
+    (with return_outliers, also the sorted indices of the injected outliers)."""
     rng = np.random.default_rng(seed)
     centers = rng.normal(0.0, 3.0, size=(n_comp, p))
     comp_class = np.arange(n_comp) % n_class
@@ -107,6 +108,8 @@ def large_gmm(n: int = 1_000_000, p: int = 32, seed: int = SEED_BASE + 5, n_comp
     mid, half = 0.5 * (lo + hi), 0.5 * (hi - lo)
     X[idx] = mid + rng.uniform(-10.0, 10.0, size=(n_out, p)) * half
     y[idx] = rng.integers(0, n_class, size=n_out)
+    if return_outliers:
+        return np.ascontiguousarray(X, dtype=np.float32), y, np.sort(idx)
     return np.ascontiguousarray(X, dtype=np.float32), y
 
 

@@ -13,6 +13,9 @@ from conftest import has_reference
     ("cover", lambda: synth.mixed_cover(1200), 7, 1, 12),
     ("cover_minnd5", lambda: synth.mixed_cover(900, seed=5), 7, 5, 12),
     ("gmm", lambda: synth.large_gmm(800, 32), 5, 5, 10),
+    # nodes above 4096 samples take the radix-sort path of the split search
+    ("gmm_large_nodes", lambda: synth.large_gmm(12000, 32), 5, 5, 3),
+    ("cover_large_nodes", lambda: synth.mixed_cover(9000, seed=9), 7, 1, 2),
 ])
 def test_grow_identical(built, name, gen, mtry, minnd, T):
     from oracle import reference as ref
