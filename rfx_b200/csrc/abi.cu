@@ -173,8 +173,9 @@ rfx_status check_device_errors(Ctx* c) {
     if (bits & ERR_STALE_JVR)
         m += " a cpu_testreeimp walk ended without a terminal node (the reference would keep a stale vote);";
     if (bits & ERR_TRAVERSAL_LIMIT) m += " a walk hit its step limit;";
+    if (bits & ERR_WAIT_LIMIT) m += " a tensor-core pipeline wait gave up;";
     set_error(m);
-    return RFX_ERR_UNSUPPORTED;
+    return (bits & ERR_WAIT_LIMIT) ? RFX_ERR_TIMEOUT : RFX_ERR_UNSUPPORTED;
 }
 
 }  // namespace rfx

@@ -33,6 +33,7 @@ enum : uint32_t {
     ERR_STALE_JVR = 1u,       // testreeimp broke without assigning (stale jvr in the reference)
     ERR_TRAVERSAL_LIMIT = 2u, // a bounded walk hit its step limit
     ERR_SMEM_KEYS = 4u,       // per-tree key table exceeded its shared-memory budget
+    ERR_WAIT_LIMIT = 8u,      // a bounded mbarrier wait of a tensor-core pipeline gave up
 };
 
 enum Stage : int {

@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(TC_THREADS) mstack_tc_kernel(const float* __re
         }
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (!ok) {
-        if (lane == 0) atomicOr(err, ERR_TRAVERSAL_LIMIT);
+        if (lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
     } else if (issued > 0) {
         // warp w reads TMEM lanes 32w..32w+31 = tile rows; K_ columns
         const int r = warp * 32 + lane;
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(TC_THREADS) quadform_tc_kernel(const float* __
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
     }
-    if (!ok && lane == 0) atomicOr(err, ERR_TRAVERSAL_LIMIT);
+    if (!ok && lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
     if (warp == 0) tmem_dealloc(tmem, NP);
 }
 
