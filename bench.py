@@ -58,6 +58,19 @@ def dist_env():
     return ws, rank, local
 
 
+def replica_reduce(x: float, op: str, device=None) -> float:
+    """Max or sum of a per-rank number over the replicas (identity without a
+    process group).  Every rank calls it in the same order."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def make_forest(n, T, rank, ws, barrier):
     """Data + forest; rank 0 grows, other ranks read its export."""
     from rfx_b200 import abi, synth
@@ -513,12 +526,10 @@ def main():
     stage_ms, launches1 = ctx.profile_read()
     gpu_launches = launches1 - launches0
     ctx.profile(False)
-    ms_max = ms
-    if pg is not None:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = ws * U / (ms_max / 1000.0)
+    # whole-job throughput: every replica's pair updates over the slowest replica's time
+    ms_max = replica_reduce(ms, "max", dev)
+    U_all = replica_reduce(U, "sum", dev)
+    value = U_all / (ms_max / 1000.0)
 
     # roofline of the dominant kernel
     hbm, peak_src = peaks()
@@ -597,11 +608,8 @@ def main():
             e2e_step()
         te = (time.perf_counter() - t0) / ke
         ctx2.close()
-        if pg is not None:
-            t = torch.tensor([te], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            te = float(t.item())
-        line["e2e"] = {"value": ws * U / te, "unit": "pair-updates/s", "h2d_bytes_per_step": int(h2d),
+        te = replica_reduce(te, "max", dev)
+        line["e2e"] = {"value": U_all / te, "unit": "pair-updates/s", "h2d_bytes_per_step": int(h2d),
                        "d2h_bytes_per_step": int(d2h), "ms_per_step": te * 1000.0, "steps": ke}
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
