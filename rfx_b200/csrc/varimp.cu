@@ -135,9 +135,13 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         const float* xi = X + (size_t)i * p;
         const float* xp = X + (size_t)ip * p;
         const int yi = y[i];
-        int cls_tb;
-        walk_testreebag_src(xi, p, src, tc, nn, cat, cgl, maxcat, &cls_tb);
-        const int base_tb = (cls_tb == yi);
+        // The cpu_testreebag walk of the same sample follows the main path
+        // below node by node until the two rules disagree (categorical
+        // conventions, unsplit nodes, the step guard); it is decided along
+        // the way and walked on its own only when the paths part.
+        int cls_tb = -1;
+        bool tb_done = false, tb_sync = true;
+        int tb_steps = 0;
         uint64_t done[W], pcorr[W];
 #pragma unroll
         for (int q = 0; q < W; ++q) done[q] = pcorr[q] = 0ull;
@@ -145,14 +149,42 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         bool ok = false;
         for (int step = 0; step < nnv; ++step) {
             const DNode nd = src(kt);
-            if (node_status(nd.meta) == -1) {
+            const int st = node_status(nd.meta);
+            const int m = node_var(nd.meta);
+            if (tb_sync && !tb_done) {
+                if (st != 1) {
+                    cls_tb = (st == -1 || st == 2) ? __ldg(tc + kt) : __ldg(tc);
+                    tb_done = true;
+                } else if (++tb_steps >= 1000 || m >= p) {
+                    cls_tb = __ldg(tc);
+                    tb_done = true;
+                }
+            }
+            if (st == -1) {
                 jvr0 = __ldg(tc + kt);
                 ok = true;
                 break;
             }
-            const int m = node_var(nd.meta);
             if (m >= p) break;
-            const int dir_o = imp_decide(nd, kt, __ldg(xi + m), cgl, maxcat);
+            const float xv = __ldg(xi + m);
+            const int dir_o = imp_decide(nd, kt, xv, cgl, maxcat);
+            if (tb_sync && !tb_done) {
+                int tb_next;
+                if (!node_cat(nd.meta)) {
+                    tb_next = dir_o;  // numeric splits: the same comparison
+                } else {
+                    const int iv = __float2int_rz(xv);
+                    tb_next = (iv >= 0 && iv < __ldg(cat + m))
+                                  ? ((cgl_at(cgl, maxcat, kt, iv) == 1) ? nd.left : nd.right)
+                                  : nd.right;
+                }
+                if (tb_next < 0 || tb_next >= nn) {
+                    cls_tb = __ldg(tc);  // out-of-range child: the root's class
+                    tb_done = true;
+                } else if (tb_next != dir_o) {
+                    tb_sync = false;  // the walks part: cpu_testreebag is walked on its own below
+                }
+            }
             if (dir_o == DIR_BREAK) break;
             const int wq = m >> 6;
             const uint64_t bit = 1ull << (m & 63);
@@ -178,6 +210,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
             kt = dir_o;
         }
         if (!ok) my_err |= ERR_STALE_JVR;
+        if (!tb_done) walk_testreebag_src(xi, p, src, tc, nn, cat, cgl, maxcat, &cls_tb);
+        const int base_tb = (cls_tb == yi);
         const int base_imp = (ok && jvr0 == yi);
         const uint64_t bmask = base_imp ? ~0ull : 0ull;
         const size_t ti = (size_t)t * n + i;
