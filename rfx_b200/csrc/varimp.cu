@@ -107,6 +107,14 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                    int32_t* __restrict__ delta_out, uint32_t* __restrict__ err) {
     extern __shared__ int32_t delta[];  // p counters
     __shared__ int s_red[2];
+    // Side walks found along the main paths are queued and then shared out
+    // over the whole CTA, so a thread with many of them does not hold its
+    // warp: {thread, feature, start node, step budget}.
+    constexpr int QCAP = VW * 6;
+    __shared__ int4 q_ent[QCAP];
+    __shared__ int q_n;
+    __shared__ unsigned long long s_pcorr[VW][W];
+    __shared__ int s_i[VW], s_ip[VW], s_y[VW];
     const int t = blockIdx.y;
     const int noob = noob_arr[t];
     const int r0 = blockIdx.x * VW;
@@ -116,7 +124,10 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     if (tid == 0) {
         s_red[0] = 0;
         s_red[1] = 0;
+        q_n = 0;
     }
+#pragma unroll
+    for (int q = 0; q < W; ++q) s_pcorr[tid][q] = 0ull;
     __syncthreads();
     const int64_t o = offs[t];
     const DNode* tn = nodes + o;
@@ -129,12 +140,20 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     int my_right = 0, my_imp = 0;
     uint32_t my_err = 0;
     const int r = r0 + tid;
-    if (r < noob) {
-        const int i = joob[r];
+    const bool active = r < noob;
+    uint64_t done[W], pcorr[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) done[q] = pcorr[q] = 0ull;
+    int i = 0, yi = -1, base_tb = 0, base_imp = 0;
+    if (active) {
+        i = joob[r];
         const int ip = joob[__ldg(perm_all + permoff[t] + r)];
+        s_i[tid] = i;
+        s_ip[tid] = ip;
         const float* xi = X + (size_t)i * p;
         const float* xp = X + (size_t)ip * p;
-        const int yi = y[i];
+        yi = y[i];
+        s_y[tid] = yi;
         // The cpu_testreebag walk of the same sample follows the main path
         // below node by node until the two rules disagree (categorical
         // conventions, unsplit nodes, the step guard); it is decided along
@@ -142,9 +161,6 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         int cls_tb = -1;
         bool tb_done = false, tb_sync = true;
         int tb_steps = 0;
-        uint64_t done[W], pcorr[W];
-#pragma unroll
-        for (int q = 0; q < W; ++q) done[q] = pcorr[q] = 0ull;
         int kt = 0, jvr0 = -1;
         bool ok = false;
         for (int step = 0; step < nnv; ++step) {
@@ -195,10 +211,17 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
             if (!(dword & bit)) {
                 const int dir_p = imp_decide(nd, kt, __ldg(xp + m), cgl, maxcat);
                 if (dir_p != dir_o) {
-                    int cls_m = -1;
-                    if (dir_p != DIR_BREAK)
-                        cls_m = imp_side_walk(xi, xp, m, p, dir_p, nnv - step - 1, src, tc, cgl, maxcat);
-                    if (cls_m < 0) my_err |= ERR_STALE_JVR;
+                    int cls_m = -2;  // -2: queued, decided in the shared phase
+                    if (dir_p == DIR_BREAK) {
+                        cls_m = -1;
+                    } else {
+                        const int slot = atomicAdd(&q_n, 1);
+                        if (slot < QCAP)
+                            q_ent[slot] = make_int4(tid, m, dir_p, nnv - step - 1);
+                        else
+                            cls_m = imp_side_walk(xi, xp, m, p, dir_p, nnv - step - 1, src, tc, cgl, maxcat);
+                    }
+                    if (cls_m == -1) my_err |= ERR_STALE_JVR;
 #pragma unroll
                     for (int q = 0; q < W; ++q)
                         if (q == wq) {
@@ -211,8 +234,24 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         }
         if (!ok) my_err |= ERR_STALE_JVR;
         if (!tb_done) walk_testreebag_src(xi, p, src, tc, nn, cat, cgl, maxcat, &cls_tb);
-        const int base_tb = (cls_tb == yi);
-        const int base_imp = (ok && jvr0 == yi);
+        base_tb = (cls_tb == yi);
+        base_imp = (ok && jvr0 == yi);
+    }
+    __syncthreads();
+    // shared phase: every queued side walk, spread over the CTA's threads
+    const int qn = min(q_n, QCAP);
+    for (int e = tid; e < qn; e += VW) {
+        const int4 en = q_ent[e];
+        const int lt = en.x, m = en.y;
+        const int cls_m = imp_side_walk(X + (size_t)s_i[lt] * p, X + (size_t)s_ip[lt] * p, m, p, en.z, en.w, src,
+                                        tc, cgl, maxcat);
+        if (cls_m < 0) my_err |= ERR_STALE_JVR;
+        else if (cls_m == s_y[lt]) atomicOr(&s_pcorr[lt][m >> 6], 1ull << (m & 63));
+    }
+    __syncthreads();
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < W; ++q) pcorr[q] |= s_pcorr[tid][q];
         const uint64_t bmask = base_imp ? ~0ull : 0ull;
         const size_t ti = (size_t)t * n + i;
         vflags[ti] = (uint8_t)(1 | (base_tb << 1) | (base_imp << 2));
