@@ -342,6 +342,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, 
     return r;
 }
 
+// Ranges shorter than this are counted by the thread that loaded them.
+constexpr int PAIRS_SHORT = 16;
+
 // One CTA of NT threads per row.  Each round takes NT trees' member ranges of this row,
 // drops the empty ones, and cuts the rest into 32-member pieces; every warp
 // owns a contiguous run of pieces (so warps finish together whatever the range
@@ -378,7 +381,10 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
             len = v.y;
         }
         my_pairs += (unsigned long long)len;
-        const int np = (len + 31) >> 5;
+        // short ranges (most ranges, few members) are walked by their own
+        // thread below; only the long ones are cut into 32-member pieces
+        const bool shortr = len < PAIRS_SHORT;
+        const int np = shortr ? 0 : (len + 31) >> 5;
         int nseg, P;
         const int cidx = block_exclusive_scan<NW>(np > 0 ? 1 : 0, wtot, lane, w, &nseg);
         const int pfx = block_exclusive_scan<NW>(np, wtot, lane, w, &P);
@@ -389,6 +395,13 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
         }
         if (tid == 0) cp0[nseg] = P;
         __syncthreads();  // also orders the accumulator zeroing before any update
+        if (shortr && len > 0) {
+            const int32_t* mp = memb + b;
+            for (int q = 0; q < len; ++q) {
+                const int j = __ldg(mp + q);
+                atomicAdd(acc + (j >> 1), 1u << ((j & 1) << 4));
+            }
+        }
         // warp w owns pieces [q0, q1); walk the ranges they cover, 32 lanes on
         // consecutive members, four loads in flight per lane
         const int per = (P + NW - 1) / NW;
