@@ -343,7 +343,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, 
 }
 
 // Ranges shorter than this are counted by the thread that loaded them.
-constexpr int PAIRS_SHORT = 16;
+constexpr int PAIRS_SHORT = 32;
 
 // One CTA of NT threads per row.  Each round takes NT trees' member ranges of this row,
 // drops the empty ones, and cuts the rest into 32-member pieces; every warp
