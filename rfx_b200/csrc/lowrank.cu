@@ -68,12 +68,12 @@ __global__ void pack_x_kernel(const float* __restrict__ V, const float* __restri
     st_val(X + (size_t)i * 2 * w + w + c, __fmul_rn(v, dinv[i]));
 }
 
-// 16-byte chunks of a row: E values of type T per chunk.
-template <typename T>
+// Row chunks owned by one lane: E values of type T (16 bytes, or 8 bytes for
+// BF16 rows too narrow to give every lane a 16-byte chunk).
+template <typename T, int E>
 struct Chunk;
 template <>
-struct Chunk<float> {
-    static constexpr int E = 4;
+struct Chunk<float, 4> {
     __device__ static void load(const float* p, float* v) {
         const float4 x = __ldg(reinterpret_cast<const float4*>(p));
         v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
@@ -83,8 +83,7 @@ struct Chunk<float> {
     }
 };
 template <>
-struct Chunk<__nv_bfloat16> {
-    static constexpr int E = 8;
+struct Chunk<__nv_bfloat16, 8> {
     __device__ static void load(const __nv_bfloat16* p, float* v) {
         const uint4 x = __ldg(reinterpret_cast<const uint4*>(p));
         const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&x);
@@ -103,6 +102,26 @@ struct Chunk<__nv_bfloat16> {
         *reinterpret_cast<uint4*>(p) = x;
     }
 };
+template <>
+struct Chunk<__nv_bfloat16, 4> {
+    __device__ static void load(const __nv_bfloat16* p, float* v) {
+        const uint2 x = __ldg(reinterpret_cast<const uint2*>(p));
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&x);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const float2 f = __bfloat1622float2(h[q]);
+            v[2 * q] = f.x;
+            v[2 * q + 1] = f.y;
+        }
+    }
+    __device__ static void store(__nv_bfloat16* p, const float* v) {
+        uint2 x;
+        __nv_bfloat162* h = reinterpret_cast<__nv_bfloat162*>(&x);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+        *reinterpret_cast<uint2*>(p) = x;
+    }
+};
 
 // Leaf-key sums of X rows for trees [t0, t1): G[gofs[t-t0] + key][:] = sum
 // over members j of key of X[j][:].  The member list of each tree (keys in
@@ -115,68 +134,62 @@ struct Chunk<__nv_bfloat16> {
 // must be zero beforehand.
 constexpr int SEG_CH = 64;
 
-template <typename T>
+template <typename T, int E>
 __device__ __forceinline__ void add_row(const T* xr, int lane, bool c0ok, bool c1ok, float* a0, float* a1) {
-    constexpr int E = Chunk<T>::E;
     float v[E];
     if (c0ok) {
-        Chunk<T>::load(xr + lane * E, v);
+        Chunk<T, E>::load(xr + lane * E, v);
 #pragma unroll
         for (int e = 0; e < E; ++e) a0[e] += v[e];
     }
     if (c1ok) {
-        Chunk<T>::load(xr + (lane + 32) * E, v);
+        Chunk<T, E>::load(xr + (lane + 32) * E, v);
 #pragma unroll
         for (int e = 0; e < E; ++e) a1[e] += v[e];
     }
 }
 
-template <typename TO>
+template <typename TO, int E>
 __device__ __forceinline__ void store_row(TO* out, int lane, bool c0ok, bool c1ok, const float* a0, const float* a1) {
-    constexpr int E = Chunk<TO>::E;
-    static_assert(E == 4 || E == 8, "16-byte chunks");
-    if (c0ok) Chunk<TO>::store(out + lane * E, a0);
-    if (c1ok) Chunk<TO>::store(out + (lane + 32) * E, a1);
+    if (c0ok) Chunk<TO, E>::store(out + lane * E, a0);
+    if (c1ok) Chunk<TO, E>::store(out + (lane + 32) * E, a1);
 }
 
-// FP32 partial rows use 4-float chunks; with BF16 rows (8 values per chunk) a
-// partial row is stored as two float chunks per lane chunk.
-template <typename T>
+// FP32 partial rows use 4-float chunks; a lane chunk of E values is stored as
+// E / 4 float chunks.
+template <typename T, int E>
 __device__ __forceinline__ void store_partial(float* out, int lane, bool c0ok, bool c1ok, const float* a0,
                                               const float* a1) {
-    constexpr int E = Chunk<T>::E;
 #pragma unroll
     for (int h = 0; h < E / 4; ++h) {
-        if (c0ok) Chunk<float>::store(out + lane * E + 4 * h, a0 + 4 * h);
-        if (c1ok) Chunk<float>::store(out + (lane + 32) * E + 4 * h, a1 + 4 * h);
+        if (c0ok) Chunk<float, 4>::store(out + lane * E + 4 * h, a0 + 4 * h);
+        if (c1ok) Chunk<float, 4>::store(out + (lane + 32) * E + 4 * h, a1 + 4 * h);
     }
 }
 
-template <typename T>
+template <typename T, int E>
 __device__ __forceinline__ void add_partial(const float* in, int lane, bool c0ok, bool c1ok, float* a0, float* a1) {
-    constexpr int E = Chunk<T>::E;
     float v[4];
 #pragma unroll
     for (int h = 0; h < E / 4; ++h) {
         if (c0ok) {
-            Chunk<float>::load(in + lane * E + 4 * h, v);
+            Chunk<float, 4>::load(in + lane * E + 4 * h, v);
 #pragma unroll
             for (int e = 0; e < 4; ++e) a0[4 * h + e] += v[e];
         }
         if (c1ok) {
-            Chunk<float>::load(in + (lane + 32) * E + 4 * h, v);
+            Chunk<float, 4>::load(in + (lane + 32) * E + 4 * h, v);
 #pragma unroll
             for (int e = 0; e < 4; ++e) a1[4 * h + e] += v[e];
         }
     }
 }
 
-template <typename T>
+template <typename T, int E>
 __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
                               const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
                               int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
                               float* __restrict__ Pf, float* __restrict__ Pl, int32_t* __restrict__ fk) {
-    constexpr int E = Chunk<T>::E;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= (int64_t)(t1 - t0) * cpt) return;
@@ -216,14 +229,14 @@ __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32
         for (int q = pos; q < e; ++q) {
             const int r = q - cs;  // warp-uniform
             const int j = __shfl_sync(0xffffffffu, r < 32 ? m0 : m1, r & 31);
-            add_row<T>(X + (size_t)j * W, lane, c0ok, c1ok, a0, a1);
+            add_row<T, E>(X + (size_t)j * W, lane, c0ok, c1ok, a0, a1);
         }
         if (kbeg >= cs && kend <= ce) {
-            store_row<T>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
+            store_row<T, E>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
         } else if (pos == cs) {
-            store_partial<T>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+            store_partial<T, E>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
         } else {
-            store_partial<T>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+            store_partial<T, E>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
         }
         pos = e;
         if (pos < ce) {
@@ -235,12 +248,11 @@ __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32
 
 // Keys that cross chunk boundaries: the chunk after the one a key starts in
 // sums the key's partial rows in chunk order and writes its G row.
-template <typename T>
+template <typename T, int E>
 __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase,
                                   int t0, int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
                                   const float* __restrict__ Pf, const float* __restrict__ Pl,
                                   const int32_t* __restrict__ fk) {
-    constexpr int E = Chunk<T>::E;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= (int64_t)(t1 - t0) * cpt) return;
@@ -257,18 +269,17 @@ __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ sego
     float a0[E], a1[E];
 #pragma unroll
     for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
-    add_partial<T>((kbeg == cs - SEG_CH ? Pf : Pl) + (size_t)(warp - 1) * W, lane, c0ok, c1ok, a0, a1);
+    add_partial<T, E>((kbeg == cs - SEG_CH ? Pf : Pl) + (size_t)(warp - 1) * W, lane, c0ok, c1ok, a0, a1);
     for (int c2 = ch; c2 * SEG_CH < kend; ++c2)
-        add_partial<T>(Pf + (size_t)(warp - ch + c2) * W, lane, c0ok, c1ok, a0, a1);
-    store_row<T>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
+        add_partial<T, E>(Pf + (size_t)(warp - ch + c2) * W, lane, c0ok, c1ok, a0, a1);
+    store_row<T, E>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
 }
 
 // Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample,
 // 16-byte chunks per lane, 32 trees' keys fetched at once.
-template <typename T>
+template <typename T, int E>
 __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
                             const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate) {
-    constexpr int E = Chunk<T>::E;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
@@ -293,12 +304,12 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
             const T* gr = G + (size_t)r * W;
             float v[E];
             if (c0ok) {
-                Chunk<T>::load(gr + lane * E, v);
+                Chunk<T, E>::load(gr + lane * E, v);
 #pragma unroll
                 for (int e = 0; e < E; ++e) a0[e] += v[e];
             }
             if (c1ok) {
-                Chunk<T>::load(gr + (lane + 32) * E, v);
+                Chunk<T, E>::load(gr + (lane + 32) * E, v);
 #pragma unroll
                 for (int e = 0; e < E; ++e) a1[e] += v[e];
             }
@@ -479,11 +490,21 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
         const int cpt = (n + SEG_CH - 1) / SEG_CH;
         const int64_t chunks = (int64_t)(t1 - t0) * cpt;
         RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(TG) * (size_t)total_keys * W, s));
-        segsum_kernel<TX><<<nblk(chunks * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0, t1,
-                                                            cpt, gofs, G, Pf, Pl, fk);
-        segsum_fix_kernel<TG><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt, gofs, G,
-                                                                Pf, Pl, fk);
-        pull_kernel<TG><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0);
+        auto run = [&](auto e_tag) {
+            constexpr int E = decltype(e_tag)::value;
+            segsum_kernel<TX, E><<<nblk(chunks * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0,
+                                                                   t1, cpt, gofs, G, Pf, Pl, fk);
+            segsum_fix_kernel<TG, E><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt,
+                                                                       gofs, G, Pf, Pl, fk);
+            pull_kernel<TG, E><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0);
+        };
+        // BF16 rows narrower than 32 16-byte chunks use 8-byte chunks, so more lanes carry data
+        if constexpr (std::is_same<TX, float>::value) {
+            run(std::integral_constant<int, 4>{});
+        } else {
+            if (W / 8 > 16) run(std::integral_constant<int, 8>{});
+            else run(std::integral_constant<int, 4>{});
+        }
         c->launches += 3;
         RFX_CUDA(cudaGetLastError());
     }
