@@ -312,7 +312,37 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
 #pragma unroll
     for (int u = 0; u < VS_FEAT; ++u) acc[u] = 0.0f;
     float q = 0.0f;
-    for (int t = 0; t < T; ++t) {
+    // trees in blocks of TB: all loads of a block are issued before its sums
+    // (the flip words of in-bag units are read but not used), then the sums
+    // are added in tree order
+    constexpr int TB = 8;
+    int t0 = 0;
+    for (; t0 + TB <= T; t0 += TB) {
+        uint8_t ib[TB], fl[TB];
+        float inv[TB];
+        uint64_t fw[TB], ivw[TB];
+#pragma unroll
+        for (int u = 0; u < TB; ++u) {
+            const size_t ti = (size_t)(t0 + u) * n + i;
+            ib[u] = __ldg(inbag + ti);
+            fl[u] = __ldg(vflags + ti);
+            inv[u] = __ldg(invnoob + t0 + u);
+            fw[u] = __ldg(flips + ti * W + wq);
+            ivw[u] = __ldg(iv + (size_t)(t0 + u) * W + wq);
+        }
+#pragma unroll
+        for (int u = 0; u < TB; ++u) {
+            if (ib[u] != 0) continue;
+            const bool btb = (fl[u] >> 1) & 1, bimp = (fl[u] >> 2) & 1;
+            if (btb) q = __fadd_rn(q, inv[u]);
+            const uint64_t corr = (ivw[u] & ((bimp ? ~0ull : 0ull) ^ fw[u])) | (~ivw[u] & (btb ? ~0ull : 0ull));
+            const uint32_t cb = (uint32_t)(corr >> sh) & 0xffu;
+#pragma unroll
+            for (int v = 0; v < VS_FEAT; ++v)
+                if ((cb >> v) & 1u) acc[v] = __fadd_rn(acc[v], inv[u]);
+        }
+    }
+    for (int t = t0; t < T; ++t) {
         const size_t ti = (size_t)t * n + i;
         if (__ldg(inbag + ti) != 0) continue;
         const uint8_t fl = __ldg(vflags + ti);
