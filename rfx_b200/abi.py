@@ -181,7 +181,8 @@ class BatchGraph:
 
 TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk"}
 # launch shapes per stage, in the library's shape order
-TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees"], 1: ["256", "512", "1024"],
+TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
+                    "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight"], 1: ["256", "512", "1024"],
                 2: ["64", "128", "256"]}
 
 

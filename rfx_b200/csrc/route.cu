@@ -52,7 +52,164 @@ route_kernel(const float* __restrict__ X, int n, int p, int T, int nclass, const
     }
 }
 
-constexpr int ROUTE_SHAPES = 5;
+// One (tree, sample) walk advanced one node at a time, so that a thread can
+// keep two walks in flight: cpu_testreebag for an OOB sample, find_terminal_node
+// for an in-bag one, each restated exactly as in walks.cuh.
+struct Walk {
+    const DNode* tn;
+    const int32_t* tc;
+    const int32_t* cgl;
+    int nn, kt, steps, node, cls;
+    bool oob, done;
+    DNode nd;
+};
+
+__device__ __forceinline__ void walk_begin(Walk& w, const DNode* tn, const int32_t* tc, const int32_t* cgl, int nn,
+                                           bool oob) {
+    w.tn = tn;
+    w.tc = tc;
+    w.cgl = cgl;
+    w.nn = nn;
+    w.kt = 0;
+    w.steps = 0;
+    w.node = 0;
+    w.cls = -1;
+    w.oob = oob;
+    w.done = false;
+}
+
+// Decide at the current node w.nd (already loaded); on return either w.done
+// with node/cls set, or w.kt is the next node to load.
+__device__ __forceinline__ void walk_advance(Walk& w, const float* __restrict__ xrow, int p,
+                                             const int32_t* __restrict__ cat, int maxcat, int maxnode) {
+    const int st = node_status(w.nd.meta);
+    if (w.oob) {  // cpu_testreebag
+        if (st != 1) {
+            if (st == -1 || st == 2) {
+                w.cls = __ldg(w.tc + w.kt);
+                w.node = w.kt;
+            } else {
+                w.cls = __ldg(w.tc);
+                w.node = 0;
+            }
+            w.done = true;
+            return;
+        }
+        const int m = node_var(w.nd.meta);
+        if (++w.steps >= 1000 || m >= p) {
+            w.cls = __ldg(w.tc);
+            w.node = 0;
+            w.done = true;
+            return;
+        }
+        const float v = __ldg(xrow + m);
+        int nx;
+        if (!node_cat(w.nd.meta)) {
+            nx = (v <= w.nd.split) ? w.nd.left : w.nd.right;
+        } else {
+            const int iv = __float2int_rz(v);
+            nx = (iv >= 0 && iv < __ldg(cat + m)) ? ((cgl_at(w.cgl, maxcat, w.kt, iv) == 1) ? w.nd.left : w.nd.right)
+                                                 : w.nd.right;
+        }
+        if (nx < 0 || nx >= w.nn) {  // the root and its class
+            w.cls = __ldg(w.tc);
+            w.node = 0;
+            w.done = true;
+            return;
+        }
+        w.kt = nx;
+        return;
+    }
+    // find_terminal_node: at most maxnode nodes are examined
+    if (w.steps >= maxnode) {
+        w.node = 0;
+        w.done = true;
+        return;
+    }
+    ++w.steps;
+    if (st == -1) {
+        w.node = w.kt;
+        w.done = true;
+        return;
+    }
+    const int m = node_var(w.nd.meta);
+    if (m >= p) {
+        w.node = 0;
+        w.done = true;
+        return;
+    }
+    const float v = __ldg(xrow + m);
+    if (!node_cat(w.nd.meta)) {
+        w.kt = (v <= w.nd.split) ? w.nd.left : w.nd.right;
+    } else {
+        const int j = __double2int_rz(__dadd_rn((double)v, 0.5));
+        if (j >= 1 && j <= __ldg(cat + m)) {
+            w.kt = (cgl_at(w.cgl, maxcat, w.kt, j - 1) == 1) ? w.nd.left : w.nd.right;
+        } else {
+            w.node = 0;
+            w.done = true;
+        }
+    }
+}
+
+// Two trees per step of the loop: both walks' node loads are in flight at once.
+template <int RT, int TPC>
+__global__ void __launch_bounds__(RT)
+route2_kernel(const float* __restrict__ X, int n, int p, int T, int nclass, const DNode* __restrict__ nodes,
+              const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
+              const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+              const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
+              const int32_t* __restrict__ catgoleft, int maxcat, int32_t* __restrict__ key_out,
+              int32_t* __restrict__ leaf_out, int32_t* __restrict__ votes) {
+    static_assert(TPC % 2 == 0, "trees in pairs");
+    const int i = blockIdx.x * RT + threadIdx.x;
+    if (i >= n) return;
+    const float* xrow = X + (size_t)i * p;
+    const int maxnode = 2 * n + 1;
+#pragma unroll 1
+    for (int q = 0; q < TPC; q += 2) {
+        const int ta = blockIdx.y * TPC + q;
+        if (ta >= T) return;
+        const int tb = ta + 1 < T ? ta + 1 : -1;
+        Walk w[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int t = h == 0 ? ta : tb;
+            if (t < 0) {
+                w[h].done = true;
+                continue;
+            }
+            const int64_t o = offs[t];
+            walk_begin(w[h], nodes + o, nodeclass + o, catgoleft ? catgoleft + o * maxcat : nullptr, nnode_arr[t],
+                       inbag[(size_t)t * n + i] == 0);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (!w[h].done) w[h].nd = load_node(w[h].tn, 0);
+        while (!w[0].done || !w[1].done) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (!w[h].done) walk_advance(w[h], xrow, p, cat, maxcat, maxnode);
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (!w[h].done) w[h].nd = load_node(w[h].tn, w[h].kt);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int t = h == 0 ? ta : tb;
+            if (t < 0) continue;
+            const int64_t o = offs[t];
+            if (w[h].oob && w[h].cls >= 0 && w[h].cls < nclass) atomicAdd(votes + (size_t)i * nclass + w[h].cls, 1);
+            const int node = w[h].node;
+            const int li = (node >= 0 && node < w[h].nn) ? __ldg(leafidx + o + node) : -1;
+            const size_t ti = (size_t)t * n + i;
+            key_out[ti] = li >= 0 ? 2 * li + (w[h].oob ? 0 : 1) : -1;
+            if (leaf_out) leaf_out[ti] = node;
+        }
+    }
+}
+
+constexpr int ROUTE_SHAPES = 8;
 
 // votes must be zero beforehand (the kernel adds to them)
 void route_launch(Ctx* c, int shape, int32_t* d_leaf) {
@@ -67,6 +224,9 @@ void route_launch(Ctx* c, int shape, int32_t* d_leaf) {
         case 2: go(route_kernel<512, 1>, 512, 1); break;
         case 3: go(route_kernel<256, 2>, 256, 2); break;
         case 4: go(route_kernel<256, 4>, 256, 4); break;
+        case 5: go(route2_kernel<256, 2>, 256, 2); break;
+        case 6: go(route2_kernel<256, 4>, 256, 4); break;
+        case 7: go(route2_kernel<128, 4>, 128, 4); break;
         default: go(route_kernel<256, 1>, 256, 1); break;
     }
 }

@@ -38,7 +38,20 @@ bool tuning_enabled() {
 
 }  // namespace
 
+// RFX_TUNE_<STAGE>=<shape> (ROUTE, PAIRS, VWALK) forces a shape, e.g. to test
+// every shape against the oracle.
+int forced_shape(int kernel, int nvar) {
+    static const char* names[] = {"RFX_TUNE_ROUTE", "RFX_TUNE_PAIRS", "RFX_TUNE_VWALK"};
+    if (kernel < 0 || kernel > 2) return -1;
+    const char* e = std::getenv(names[kernel]);
+    if (!e || !*e) return -1;
+    const int v = std::atoi(e);
+    return (v >= 0 && v < nvar) ? v : -1;
+}
+
 rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<rfx_status(int)>& run) {
+    const int forced = forced_shape(kernel, nvar);
+    if (forced >= 0) return run(forced);
     const auto key = std::make_tuple(kernel, c->device, ilog2(c->n), ilog2(c->T), ilog2(c->p));
     {
         std::lock_guard<std::mutex> lk(g_mu);

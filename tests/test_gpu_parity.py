@@ -300,3 +300,25 @@ def test_full_size_properties(built):
 
 def ok_leaf(term, f, t, node):
     return bool(term[f.offs[t] + node])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("stage,count", [("ROUTE", 8), ("PAIRS", 3), ("VWALK", 3)])
+def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
+    """Each launch shape the autotuner can pick gives the oracle's results."""
+    from oracle import oracle as orc
+    from rfx_b200 import abi
+
+    X, y = synth.mixed_cover(2600, seed=23)
+    X, y, f = _grow(X, y, 9, 7)
+    O = orc.analyse(X, y, f, want_leaf=True)
+    for shape in range(count):
+        monkeypatch.setenv("RFX_TUNE_" + stage, str(shape))
+        ctx = abi.Context(0)
+        ctx.load(f, X, y)
+        q, nout, _ = ctx.route_oob()
+        assert np.array_equal(q.astype(np.float32), O["q_raw"]), shape
+        assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
+        avimp, sqsd, qimp, qimpm = ctx.varimp(True)
+        assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
+        ctx.close()
