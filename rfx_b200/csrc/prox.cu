@@ -342,6 +342,11 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, 
     return r;
 }
 
+// Counter words of the row kernel: ceil(n/2) rounded up to whole 4-counter
+// groups plus one zero group, so the write-out can read every group it
+// touches (and the one after) with aligned 8-byte loads.
+__host__ __device__ inline int r16_words(int n) { return (((n + 1) / 2 + 1) & ~1) + 2; }
+
 // Ranges shorter than this are counted by the thread that loaded them.
 constexpr int PAIRS_SHORT = 32;
 
@@ -355,14 +360,14 @@ __global__ void __launch_bounds__(NT)
 pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                    int n, int T, int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
     constexpr int NW = NT / 32;
-    extern __shared__ uint32_t acc[];  // ceil(n/2) words, two u16 counters each
+    extern __shared__ uint32_t acc[];  // r16_words(n) words, two u16 counters each
     __shared__ long long cb[NT];      // absolute start of each non-empty range
     __shared__ int clen[NT];          // its length
     __shared__ int cp0[NT + 1];       // its first piece index (+ sentinel)
     __shared__ int wtot[NW + 1];
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int words = (n + 1) >> 1;
+    const int words = r16_words(n);
     {
         uint4* a4 = reinterpret_cast<uint4*>(acc);
         const int w4 = words >> 2;
@@ -440,7 +445,41 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
     }
     const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
     const uint16_t* a16 = reinterpret_cast<const uint16_t*>(acc);
-    for (int j = i + tid; j < n; j += NT) S[rowoff + j] = (int32_t)a16[j];
+    // the row S[i][i..n) as 16-byte stores between a scalar head and tail
+    int32_t* srow = S + rowoff + i;
+    const int len = n - i;
+    int head = len, nv = 0;
+    if ((reinterpret_cast<uintptr_t>(S) & 15) == 0) {
+        head = min(len, (int)((4 - ((rowoff + i) & 3)) & 3));
+        nv = (len - head) >> 2;
+    }
+    for (int h = tid; h < head; h += NT) srow[h] = (int32_t)a16[i + h];
+    // body: lane L of a warp stores group v = v0 + L (entries jg + 4v ..+3);
+    // it reads the aligned 4-counter group containing its first entry, takes
+    // the next group from lane L + 1, and shifts by jg's offset in its group
+    // (one 8-byte shared load per 4 entries)
+    int4* s4 = reinterpret_cast<int4*>(srow + head);
+    const int jg = i + head;
+    const int sh = (jg & 3) * 16;
+    const int gb = jg >> 2;
+    const int ngroups = words >> 1;  // 4-counter groups in the array (the last one is padding)
+    const uint2* a64 = reinterpret_cast<const uint2*>(acc);
+    for (int v0 = w * 32; v0 < nv; v0 += NT) {
+        const int v = v0 + lane;
+        const int g = gb + v;
+        const uint2 cg = g < ngroups ? a64[g] : make_uint2(0u, 0u);
+        uint2 nx;
+        nx.x = __shfl_down_sync(0xffffffffu, cg.x, 1);
+        nx.y = __shfl_down_sync(0xffffffffu, cg.y, 1);
+        if (lane == 31) nx = g + 1 < ngroups ? a64[g + 1] : make_uint2(0u, 0u);
+        const unsigned long long lo = ((unsigned long long)cg.y << 32) | cg.x;
+        const unsigned long long hi = ((unsigned long long)nx.y << 32) | nx.x;
+        const unsigned long long e = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+        if (v < nv)
+            s4[v] = make_int4((int)(e & 0xffffu), (int)((e >> 16) & 0xffffu), (int)((e >> 32) & 0xffffu),
+                              (int)(e >> 48));
+    }
+    for (int j = i + head + 4 * nv + tid; j < n; j += NT) srow[j - i] = (int32_t)a16[j];
     if (pairs) {
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
@@ -552,7 +591,7 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
                                                         c->d_order);
             RFX_CUDA(cudaGetLastError());
         }
-        const size_t smem = ((size_t)c->n + 1) / 2 * sizeof(uint32_t);
+        const size_t smem = (size_t)r16_words(c->n) * sizeof(uint32_t);
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<256>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<512>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<1024>, dev_smem)) return s0;
@@ -608,7 +647,7 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
     RFX_CUDA(cudaGetLastError());
     row_order_kernel<<<1, 1024, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.order);
     RFX_CUDA(cudaGetLastError());
-    const size_t smem2 = ((size_t)a.n + 1) / 2 * sizeof(uint32_t);
+    const size_t smem2 = (size_t)r16_words(a.n) * sizeof(uint32_t);
     if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<R16_THREADS>, dev_smem)) return s0;
     pairs_row16_kernel<R16_THREADS><<<a.n, R16_THREADS, smem2, stream>>>(a.opp, a.memb, a.order, a.n, a.T, a.S,
                                                                          nullptr);
