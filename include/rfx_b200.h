@@ -237,10 +237,12 @@ rfx_status rfx_graph_destroy(rfx_graph* g);
  * identical results; the first run for a problem shape (device and
  * power-of-two buckets of n, ntree, p) times each once on the context stream
  * and keeps the fastest for the process.  Setting RFX_AUTOTUNE=0 keeps the
- * default shapes, and RFX_TUNE_ROUTE / RFX_TUNE_PAIRS / RFX_TUNE_VWALK = <shape>
- * force one shape; nothing is tuned while a stream is being captured.
+ * default shapes, and RFX_TUNE_ROUTE / RFX_TUNE_PAIRS / RFX_TUNE_VWALK /
+ * RFX_TUNE_ROUTE_LEAF = <shape> force one shape; nothing is tuned while a
+ * stream is being captured.
  * rfx_tuned_shapes copies up to `cap` records of 6 int32 {stage (0 routing,
- * 1 pair counts, 2 varimp walk), device, log2 n, log2 ntree, log2 p, shape}
+ * 1 pair counts, 2 varimp walk, 3 routing in leaf order), device, log2 n,
+ * log2 ntree, log2 p, shape}
  * and sets *count to the number of records. */
 rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count);
 

@@ -179,11 +179,11 @@ class BatchGraph:
             pass
 
 
-TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk"}
+TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order"}
 # launch shapes per stage, in the library's shape order
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
                     "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight"], 1: ["256", "512", "1024"],
-                2: ["64", "128", "256"]}
+                2: ["64", "128", "256"], 3: ["128", "256", "512"]}
 
 
 def tuned_shapes():

@@ -55,9 +55,12 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
     int32_t* ctr = use_smem ? cnt : so;
     for (int k = tid; k <= K; k += CSR_THREADS) ctr[k] = 0;
     __syncthreads();
+    // samples without a terminal node (key -1) go to the slot after the
+    // last key, so they follow every key's members (segoff[K] still marks
+    // the end of the keyed members)
     for (int i = tid; i < n; i += CSR_THREADS) {
         const int k = __ldg(kt + i);
-        if (k >= 0) atomicAdd(ctr + k, 1);
+        atomicAdd(ctr + (k >= 0 ? k : K), 1);
     }
     __syncthreads();
     // exclusive scan of K+1 counters: quarter q = [q*Q, min((q+1)*Q, K+1))
@@ -90,17 +93,20 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
     // stable scatter by one warp, samples in index order; the next batch of
     // keys is loaded while the current one is placed
     int kv[CSR_PREFETCH], kn[CSR_PREFETCH];
+    // slot per sample: its key, K for key -1, -1 past the end
 #pragma unroll
     for (int u = 0; u < CSR_PREFETCH; ++u) {
         const int i = u * 32 + lane;
-        kv[u] = i < n ? __ldg(kt + i) : -1;
+        const int k = i < n ? __ldg(kt + i) : 0;
+        kv[u] = i < n ? (k >= 0 ? k : K) : -1;
     }
     for (int base = 0; base < n; base += 32 * CSR_PREFETCH) {
         const int nb = base + 32 * CSR_PREFETCH;
 #pragma unroll
         for (int u = 0; u < CSR_PREFETCH; ++u) {
             const int i = nb + u * 32 + lane;
-            kn[u] = i < n ? __ldg(kt + i) : -1;
+            const int k = i < n ? __ldg(kt + i) : 0;
+            kn[u] = i < n ? (k >= 0 ? k : K) : -1;
         }
 #pragma unroll
         for (int u = 0; u < CSR_PREFETCH; ++u) {

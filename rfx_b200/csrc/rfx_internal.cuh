@@ -85,7 +85,8 @@ struct Ctx {
     // analysis scratch (allocated lazily)
     int32_t* d_key = nullptr;           // T*n: 2*leafidx + inbag, or -1
     int32_t* d_segoff = nullptr;        // segbase[T]: per-tree key offsets (+1 sentinel each)
-    int32_t* d_memb = nullptr;          // T*n: members grouped by key, ascending within a key
+    int32_t* d_memb = nullptr;          // T*n: members grouped by key, ascending within a key;
+                                        // samples without a terminal node follow the keyed members
     int2* d_opp = nullptr;              // n*T: opposite-status member range cut to members > i
     int32_t* d_order = nullptr;         // n: row processing order
     int32_t* d_votes = nullptr;         // n*nclass
@@ -268,7 +269,7 @@ rfx_status launch_route(Ctx* c);
 rfx_status launch_build_csr(Ctx* c);
 
 // Autotuned stages: kernel ids and the launch shapes each offers.
-enum TuneKernel : int { TK_ROUTE = 0, TK_PAIRS16 = 1, TK_VWALK = 2 };
+enum TuneKernel : int { TK_ROUTE = 0, TK_PAIRS16 = 1, TK_VWALK = 2, TK_ROUTE_LEAF = 3 };
 rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<rfx_status(int)>& run);
 rfx_status launch_pack_forest(cudaStream_t s, int T, int n, int p, const int64_t* d_offs, const int32_t* status,
                               const int32_t* bestvar, const float* split, const int32_t* treemap,

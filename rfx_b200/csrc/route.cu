@@ -209,6 +209,44 @@ route2_kernel(const float* __restrict__ X, int n, int p, int T, int nclass, cons
     }
 }
 
+// Routing in leaf order: when the member lists of this forest exist from an
+// earlier pass, tree t's samples are taken in that order (members of one leaf
+// and bag status together, then the samples without a terminal node), so the
+// threads of a warp follow the same path with the same walk rule.  Every
+// result is indexed by sample, so only the order of work changes.
+template <int RT>
+__global__ void __launch_bounds__(RT)
+route_leaf_order_kernel(const float* __restrict__ X, int n, int p, int nclass, const DNode* __restrict__ nodes,
+                        const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
+                        const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+                        const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
+                        const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ memb,
+                        int32_t* __restrict__ key_out, int32_t* __restrict__ votes) {
+    const int t = blockIdx.y;
+    const int q = blockIdx.x * RT + threadIdx.x;
+    if (q >= n) return;
+    const size_t tq = (size_t)t * n + q;
+    const int i = __ldg(memb + tq);
+    const float* xrow = X + (size_t)i * p;
+    const int64_t o = offs[t];
+    const DNode* tn = nodes + o;
+    const int32_t* tc = nodeclass + o;
+    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+    const int nn = nnode_arr[t];
+    const size_t ti = (size_t)t * n + i;
+    const bool ib = inbag[ti] != 0;
+    int node;
+    if (!ib) {
+        int cls;
+        node = walk_testreebag(xrow, p, tn, tc, nn, cat, cgl, maxcat, &cls);
+        if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
+    } else {
+        node = walk_terminal(xrow, p, tn, cat, cgl, maxcat, 2 * n + 1);
+    }
+    const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
+    key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
+}
+
 constexpr int ROUTE_SHAPES = 8;
 
 // votes must be zero beforehand (the kernel adds to them)
@@ -301,12 +339,31 @@ predict_kernel(const float* __restrict__ X, int m, int p, int nclass, int maxnod
 
 rfx_status launch_route(Ctx* c) {
     StageTimer st(c, ST_ROUTE, 2);
-    rfx_status r = autotune(c, TK_ROUTE, ROUTE_SHAPES, 0, [&](int shape) -> rfx_status {
-        RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
-        route_launch(c, shape, nullptr);
-        RFX_CUDA(cudaGetLastError());
-        return RFX_OK;
-    });
+    rfx_status r;
+    if (c->csr_built) {
+        // the member lists of an earlier pass over this forest give the order
+        r = autotune(c, TK_ROUTE_LEAF, 3, 1, [&](int shape) -> rfx_status {
+            RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
+            auto go = [&](auto kernel, int rt) {
+                dim3 grid((c->n + rt - 1) / rt, c->T);
+                kernel<<<grid, rt, 0, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
+                                                   c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+                                                   c->d_catgoleft, c->maxcat, c->d_memb, c->d_key, c->d_votes);
+            };
+            if (shape == 0) go(route_leaf_order_kernel<128>, 128);
+            else if (shape == 2) go(route_leaf_order_kernel<512>, 512);
+            else go(route_leaf_order_kernel<256>, 256);
+            RFX_CUDA(cudaGetLastError());
+            return RFX_OK;
+        });
+    } else {
+        r = autotune(c, TK_ROUTE, ROUTE_SHAPES, 0, [&](int shape) -> rfx_status {
+            RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
+            route_launch(c, shape, nullptr);
+            RFX_CUDA(cudaGetLastError());
+            return RFX_OK;
+        });
+    }
     if (r != RFX_OK) return r;
     nout_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_inbag, c->n, c->T, c->d_nout);
     RFX_CUDA(cudaGetLastError());

@@ -303,7 +303,7 @@ def ok_leaf(term, f, t, node):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("stage,count", [("ROUTE", 8), ("PAIRS", 3), ("VWALK", 3)])
+@pytest.mark.parametrize("stage,count", [("ROUTE", 8), ("PAIRS", 3), ("VWALK", 3), ("ROUTE_LEAF", 3)])
 def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
     """Each launch shape the autotuner can pick gives the oracle's results."""
     from oracle import oracle as orc
@@ -319,6 +319,10 @@ def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
         q, nout, _ = ctx.route_oob()
         assert np.array_equal(q.astype(np.float32), O["q_raw"]), shape
         assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
+        # a second pass routes in the leaf order of the first one
+        assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
+        q2, _, _ = ctx.route_oob()
+        assert np.array_equal(q2.astype(np.float32), O["q_raw"]), shape
         avimp, sqsd, qimp, qimpm = ctx.varimp(True)
         assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
         ctx.close()
