@@ -66,13 +66,15 @@ __device__ __forceinline__ int imp_side_walk(const float* __restrict__ xrow, con
 
 // OOB samples of every tree in ascending order (joob of cpu_varimp).
 __global__ void __launch_bounds__(VT)
-joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all) {
+joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all, int32_t* __restrict__ jrank_all,
+            const int32_t* __restrict__ memb, int32_t* __restrict__ ojr_all) {
     __shared__ int wsum[VT / 32];
     __shared__ int s_base;
     const int t = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint8_t* ib = inbag + (size_t)t * n;
     int32_t* joob = joob_all + (size_t)t * n;
+    int32_t* jrank = jrank_all ? jrank_all + (size_t)t * n : nullptr;
     if (tid == 0) s_base = 0;
     __syncthreads();
     for (int base = 0; base < n; base += VT) {
@@ -86,7 +88,35 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
             if (q < wid) woff += wsum[q];
             tot += wsum[q];
         }
-        if (f) joob[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = i;
+        if (f) {
+            const int pos = s_base + woff + __popc(bal & ((1u << lane) - 1u));
+            joob[pos] = i;
+            if (jrank) jrank[i] = pos;
+        }
+        __syncthreads();
+        if (tid == 0) s_base += tot;
+        __syncthreads();
+    }
+    if (!memb) return;
+    // the OOB positions again, in the order of the tree's member lists (one
+    // leaf's OOB members together): ojr[q] = position in joob
+    const int32_t* mt = memb + (size_t)t * n;
+    int32_t* ojr = ojr_all + (size_t)t * n;
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += VT) {
+        const int q = base + tid;
+        const int i = q < n ? __ldg(mt + q) : 0;
+        const int f = (q < n && ib[i] == 0) ? 1 : 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wsum[wid] = __popc(bal);
+        __syncthreads();
+        int woff = 0, tot = 0;
+        for (int u = 0; u < VT / 32; ++u) {
+            if (u < wid) woff += wsum[u];
+            tot += wsum[u];
+        }
+        if (f) ojr[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = jrank[i];
         __syncthreads();
         if (tid == 0) s_base += tot;
         __syncthreads();
@@ -103,8 +133,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                    const int32_t* __restrict__ noob_arr, const int32_t* __restrict__ cat,
                    const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ permoff,
                    const int32_t* __restrict__ perm_all, const int32_t* __restrict__ joob_all,
-                   uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips, int32_t* __restrict__ counts,
-                   int32_t* __restrict__ delta_out, uint32_t* __restrict__ err) {
+                   const int32_t* __restrict__ ojr_all, uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips,
+                   int32_t* __restrict__ counts, int32_t* __restrict__ delta_out, uint32_t* __restrict__ err) {
     extern __shared__ int32_t delta[];  // p counters
     __shared__ int s_red[2];
     // Side walks found along the main paths are queued and then shared out
@@ -139,8 +169,11 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     const GlobalNodes src{tn};
     int my_right = 0, my_imp = 0;
     uint32_t my_err = 0;
-    const int r = r0 + tid;
-    const bool active = r < noob;
+    // position r of this thread's OOB sample in joob: in leaf order when the
+    // member lists exist (neighbouring threads then share their main path)
+    const int qpos = r0 + tid;
+    const bool active = qpos < noob;
+    const int r = (active && ojr_all) ? __ldg(ojr_all + (size_t)t * n + qpos) : qpos;
     uint64_t done[W], pcorr[W];
 #pragma unroll
     for (int q = 0; q < W; ++q) done[q] = pcorr[q] = 0ull;
@@ -417,7 +450,9 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
     const size_t smem = (size_t)c->p * sizeof(int32_t);
     {
         StageTimer st(c, ST_VARIMP_TREE, 2);
-        joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob);
+        const bool ordered = c->csr_built && c->d_jrank && c->d_ojr;
+        joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, ordered ? c->d_jrank : nullptr,
+                                                ordered ? c->d_memb : nullptr, ordered ? c->d_ojr : nullptr);
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
@@ -425,7 +460,8 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
             dim3 grid((max_noob + vw - 1) / vw, c->T);
             kernel<<<grid, vw, smem, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
                                                  c->d_nnode, c->d_noob, c->d_cat, c->d_catgoleft, c->maxcat,
-                                                 c->d_permoff, c->d_perm, c->d_joob, c->d_vflags, c->d_flips,
+                                                 c->d_permoff, c->d_perm, c->d_joob, ordered ? c->d_ojr : nullptr,
+                                                 c->d_vflags, c->d_flips,
                                                  c->d_right, c->d_rightimp, c->d_err);
         };
         rfx_status r = autotune(c, TK_VWALK, 3, 1, [&](int shape) -> rfx_status {
