@@ -282,14 +282,20 @@ def run_lowrank(args):
         return t4 - t, A, C, o
 
     run(1)  # warm-up (module load, allocations; builds the leaf keys and member lists once)
+    run(0)
     once_ms = {key: phases[1][key] for key in ("route_ms", "leaf_lists_ms")}
     times = {0: [], 1: []}
+    best = {0: None, 1: None}
     res = {}
     for rep in range(max(1, args.steps)):
         for prec in (0, 1):
             dt, A, C, o = run(prec)
             times[prec].append(dt)
             res[prec] = (A, C, o)
+            # phases of the fastest repetition of each form
+            if best[prec] is None or dt <= min(times[prec]):
+                best[prec] = dict(phases[prec])
+    phases = best
     # exact FP64 proximity on a seeded subsample
     m = min(20_000, n)
     rng = np.random.default_rng(7)

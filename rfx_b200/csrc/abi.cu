@@ -919,9 +919,13 @@ rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int prec
     if (!coords || k < 1) return RFX_ERR_INVALID;
     const bool cdev = is_device_ptr(coords);
     double* dC = coords;
+    Scratch staging(c);
     if (!cdev) {
-        cudaError_t e = ctx_malloc(c, (void**)&dC, sizeof(double) * (size_t)c->n * k);
-        if (e != cudaSuccess) return cuda_fail(e, "rfx_mds_from_factors staging");
+        dC = staging.get<double>((size_t)c->n * k);
+        if (!dC) {
+            set_error("rfx_mds_from_factors: staging allocation failed");
+            return RFX_ERR_OOM;
+        }
     }
     std::vector<double> ev(8, 0.0);
     int iters = 0;
@@ -931,7 +935,6 @@ rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int prec
     if (st == RFX_OK && !cdev) st = copy_out(c, coords, dC, sizeof(double) * (size_t)c->n * k);
     if (st == RFX_OK) st = finish_host(c, true);
     cudaStreamSynchronize(c->stream);
-    if (!cdev) cudaFree(dC);
     if (st == RFX_OK && evals) std::copy(ev.begin(), ev.begin() + k, evals);
     return st;
 }

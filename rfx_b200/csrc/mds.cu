@@ -209,6 +209,24 @@ __global__ void coords_kernel(const double* __restrict__ V, const double* __rest
 
 }  // namespace
 
+// Seeded Gaussian start block on the device (counter hash splitmix64 and
+// Box-Muller); any full-rank start converges to the same subspace.
+__device__ __forceinline__ uint64_t start_mix(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void start_block_kernel(double* __restrict__ V, int64_t count, uint64_t seed) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const uint64_t h = start_mix(seed ^ start_mix((uint64_t)idx));
+    const double u1 = ((h >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+    const double u2 = (double)(start_mix(h) >> 11) * (1.0 / 9007199254740992.0);
+    V[idx] = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
 // Subspace iteration on the symmetric operator applied by `apply` (W = B V),
 // returning the k largest eigenpairs above 1e-10: coordinates n x k in `out`
 // (device) and eigenvalues in `evals_out` (host).  Shared by the full-matrix
@@ -238,12 +256,10 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
     if (warm_in) {
         RFX_CUDA(cudaMemcpyAsync(V, warm_in, sizeof(double) * (size_t)n * S_BLK, cudaMemcpyDeviceToDevice, s));
     } else {
-        std::vector<double> h((size_t)n * S_BLK);
-        std::mt19937_64 rng(seed);
-        std::normal_distribution<double> nd(0.0, 1.0);
-        for (auto& x : h) x = nd(rng);
-        RFX_CUDA(cudaMemcpyAsync(V, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, s));
-        RFX_CUDA(cudaStreamSynchronize(s));
+        const int64_t cnt = (int64_t)n * S_BLK;
+        start_block_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(V, cnt, seed);
+        c->launches += 1;
+        RFX_CUDA(cudaGetLastError());
     }
     RFX_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
     double* Xt = d.get<double>((size_t)n * S_BLK);
@@ -497,6 +513,64 @@ __global__ void __launch_bounds__(256) quadform_f32_kernel(const float* __restri
     }
 }
 
+// The same quadratic forms for k = 32 or 64 known at compile time: a_i stays in
+// registers (fully unrolled loops, no dynamic indexing) and every M row is
+// read from shared memory as float4 broadcasts.
+template <int K>
+__global__ void __launch_bounds__(256) quadform_f32k_kernel(const float* __restrict__ A, const float* __restrict__ M,
+                                                            int n, float* __restrict__ T2) {
+    extern __shared__ float Ms[];  // 4 * K * K
+    const int j0 = blockIdx.y * 4;
+    for (int e = threadIdx.x; e < 4 * K * K; e += blockDim.x) Ms[e] = M[(size_t)j0 * K * K + e];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float a[K];
+    const float4* ar = reinterpret_cast<const float4*>(A + (size_t)i * K);
+#pragma unroll
+    for (int q = 0; q < K / 4; ++q) {
+        const float4 v = __ldg(ar + q);
+        a[4 * q] = v.x;
+        a[4 * q + 1] = v.y;
+        a[4 * q + 2] = v.z;
+        a[4 * q + 3] = v.w;
+    }
+#pragma unroll 1
+    for (int jj = 0; jj < 4; ++jj) {
+        const float4* Mj = reinterpret_cast<const float4*>(Ms + jj * K * K);
+        float t = 0.0f;
+#pragma unroll
+        for (int r = 0; r < K; ++r) {
+            float v = 0.0f;
+#pragma unroll
+            for (int q = 0; q < K / 4; ++q) {
+                const float4 m = Mj[r * (K / 4) + q];
+                v = fmaf(m.x, a[4 * q], v);
+                v = fmaf(m.y, a[4 * q + 1], v);
+                v = fmaf(m.z, a[4 * q + 2], v);
+                v = fmaf(m.w, a[4 * q + 3], v);
+            }
+            t = fmaf(a[r], v, t);
+        }
+        T2[(size_t)i * S_BLK + j0 + jj] = t;
+    }
+}
+
+// T2 for any k <= 64 (the compile-time forms for 32 and 64)
+void quadform_f32(const float* dA, const float* M, int n, int k, float* T2, cudaStream_t s) {
+    const size_t qsm = 4 * (size_t)k * k * sizeof(float);
+    const dim3 grid((n + 255) / 256, S_BLK / 4);
+    if (k == 64) {
+        cudaFuncSetAttribute(quadform_f32k_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm);
+        quadform_f32k_kernel<64><<<grid, 256, qsm, s>>>(dA, M, n, T2);
+    } else if (k == 32) {
+        quadform_f32k_kernel<32><<<grid, 256, qsm, s>>>(dA, M, n, T2);
+    } else {
+        cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm);
+        quadform_f32_kernel<<<grid, 256, qsm, s>>>(dA, M, n, k, T2);
+    }
+}
+
 // W = T1 - T2/2 + c.u/2 with T1 = A (A^T u) (FP64 accumulation), before centring
 __global__ void factor_combine_kernel(const float* __restrict__ A, const double* __restrict__ AtU,
                                       const float* __restrict__ T2, const double* __restrict__ u, int n, int k,
@@ -599,7 +673,7 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
         } else {
             RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
             mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
-            quadform_f32_kernel<<<dim3((n + 255) / 256, S_BLK / 4), 256, qsm, s>>>(dA, M, n, k, T2);
+            quadform_f32(dA, M, n, k, T2, s);
             c->launches += 2;
         }
         factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
@@ -662,7 +736,7 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
         RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));
         RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
         mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
-        quadform_f32_kernel<<<dim3((n + 255) / 256, S_BLK / 4), 256, qsm, s>>>(dA, M, n, k, T2);
+        quadform_f32(dA, M, n, k, T2, s);
     }
     if (st != RFX_OK) return st;
     factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
