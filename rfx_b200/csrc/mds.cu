@@ -414,8 +414,9 @@ __global__ void __launch_bounds__(256) atu_part_kernel(const float* __restrict__
 #pragma unroll
     for (int j = 0; j < S_BLK; ++j) acc[j] = 0.0;
     if (a < k) {
+#pragma unroll 4
         for (int i = blockIdx.x * 4 + rg; i < n; i += gridDim.x * 4) {
-            const double x = (double)A[(size_t)i * k + a];
+            const double x = (double)__ldg(A + (size_t)i * k + a);
             const float4* ur = reinterpret_cast<const float4*>(u + (size_t)i * S_BLK);
 #pragma unroll
             for (int q = 0; q < S_BLK / 4; ++q) {
@@ -572,20 +573,33 @@ void quadform_f32(const float* dA, const float* M, int n, int k, float* T2, cuda
 }
 
 // W = T1 - T2/2 + c.u/2 with T1 = A (A^T u) (FP64 accumulation), before centring
-__global__ void factor_combine_kernel(const float* __restrict__ A, const double* __restrict__ AtU,
-                                      const float* __restrict__ T2, const double* __restrict__ u, int n, int k,
-                                      double* __restrict__ W) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)n * S_BLK) return;
-    const int i = (int)(idx / S_BLK), j = (int)(idx % S_BLK);
-    double t1 = 0.0, nrm = 0.0;
+__global__ void __launch_bounds__(256) factor_combine_kernel(const float* __restrict__ A,
+                                                             const double* __restrict__ AtU,
+                                                             const float* __restrict__ T2,
+                                                             const double* __restrict__ u, int n, int k,
+                                                             double* __restrict__ W) {
+    // one thread per row: the row of A is read once for all 16 columns and
+    // for |a_i|^2; A^T u sits in shared memory
+    __shared__ double s_atu[64 * S_BLK];
+    for (int e = threadIdx.x; e < k * S_BLK; e += blockDim.x) s_atu[e] = AtU[e];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double t1[S_BLK];
+#pragma unroll
+    for (int j = 0; j < S_BLK; ++j) t1[j] = 0.0;
+    double nrm = 0.0;
     for (int a = 0; a < k; ++a) {
         const double x = A[(size_t)i * k + a];
-        t1 += x * AtU[a * S_BLK + j];
         nrm += x * x;
+        const double* ar = s_atu + a * S_BLK;
+#pragma unroll
+        for (int j = 0; j < S_BLK; ++j) t1[j] += x * ar[j];
     }
     const double cc = (1.0 - nrm) * (1.0 - nrm);
-    W[idx] = t1 - 0.5 * (double)T2[idx] + 0.5 * cc * u[idx];
+    const size_t o = (size_t)i * S_BLK;
+#pragma unroll
+    for (int j = 0; j < S_BLK; ++j) W[o + j] = t1[j] - 0.5 * (double)T2[o + j] + 0.5 * cc * u[o + j];
 }
 
 __global__ void subtract_mean_kernel(double* __restrict__ W, const double* __restrict__ mean, int n) {
@@ -676,7 +690,7 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
             quadform_f32(dA, M, n, k, T2, s);
             c->launches += 2;
         }
-        factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
+        factor_combine_kernel<<<(n + 255) / 256, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
         col_mean(W, n, part, mean, s);
         subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
         c->launches += 9;
@@ -739,7 +753,7 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
         quadform_f32(dA, M, n, k, T2, s);
     }
     if (st != RFX_OK) return st;
-    factor_combine_kernel<<<gr, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
+    factor_combine_kernel<<<(n + 255) / 256, 256, 0, s>>>(dA, AtU, T2, u, n, k, W);
     col_mean(W, n, part, mean, s);
     subtract_mean_kernel<<<gr, 256, 0, s>>>(W, mean, n);
     RFX_CUDA(cudaGetLastError());
