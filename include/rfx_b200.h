@@ -86,8 +86,12 @@ rfx_status rfx_ctx_stream(rfx_ctx* ctx, void** stream);
 rfx_status rfx_synchronize(rfx_ctx* ctx);
 
 /* Validate and upload a forest (replaces the per-tree H2D copies of
- * cuda/rf_growtree.cu:2618-2657).  Rejects out-of-range children, bestvar or
- * labels before any launch.  The library keeps its own device copies. */
+ * cuda/rf_growtree.cu:2618-2657).  Labels and node counts are checked on the
+ * host; node status, bestvar, children and bootstrap counts by the packing
+ * kernels, before any analysis runs.  A forest that fails validation returns
+ * RFX_ERR_FOREST and leaves no forest loaded.  The library keeps its own
+ * device copies (pinned host arrays upload fastest); reloading a forest of the
+ * same shape reuses the context's device buffers. */
 rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* view);
 
 /* OOB routing + votes: cpu_testreebag (src/rf_testreebag.cpp:13-125) and the
