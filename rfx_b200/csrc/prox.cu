@@ -32,10 +32,31 @@ namespace {
 constexpr int CSR_THREADS = 128;
 constexpr int CSR_PREFETCH = 16;  // 32-sample groups loaded ahead by the scattering warp
 
+// Key counters of the CSR build: in shared memory as CT (16-bit when every
+// count and offset stays below 65536, so twice as many trees fit per SM), or
+// the tree's own 32-bit segment-offset table in global memory.
+template <typename CT>
+struct CsrCounters {
+    CT* s;
+    int32_t* g;
+    bool sm;
+    __device__ __forceinline__ int get(int k) const { return sm ? (int)s[k] : g[k]; }
+    __device__ __forceinline__ void set(int k, int v) {
+        if (sm) s[k] = (CT)v;
+        else g[k] = v;
+    }
+    __device__ __forceinline__ void inc(int k) {
+        if (!sm) atomicAdd(g + k, 1);
+        else if (sizeof(CT) == 2) atomicAdd(reinterpret_cast<unsigned int*>(s) + (k >> 1), 1u << ((k & 1) << 4));
+        else atomicAdd(reinterpret_cast<int*>(s) + k, 1);
+    }
+};
+
 // One CTA per tree.  All warps build the key histogram; the exclusive scan
 // runs over four quarters in parallel; warp 0 alone then scatters the samples
 // in index order (equal keys inside a 32-sample group are ranked by lane), so
 // every key's member list is ascending by sample id.
+template <typename CT>
 __global__ void __launch_bounds__(CSR_THREADS)
 build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restrict__ segbase,
                  int32_t* __restrict__ segoff, int32_t* __restrict__ memb, int smem_keys,
@@ -52,15 +73,16 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
     // counters: shared memory when the key table fits, else the tree's own
     // segment-offset table in global memory (slower, still exact)
     const bool use_smem = K + 1 <= smem_keys;
-    int32_t* ctr = use_smem ? cnt : so;
-    for (int k = tid; k <= K; k += CSR_THREADS) ctr[k] = 0;
+    CsrCounters<CT> ctr{reinterpret_cast<CT*>(cnt), so, use_smem};
+    for (int k = tid; k <= K; k += CSR_THREADS) ctr.set(k, 0);
+    if (use_smem && sizeof(CT) == 2 && tid == 0) ctr.s[K + 1] = 0;  // the other half of the last counter word
     __syncthreads();
     // samples without a terminal node (key -1) go to the slot after the
     // last key, so they follow every key's members (segoff[K] still marks
     // the end of the keyed members)
     for (int i = tid; i < n; i += CSR_THREADS) {
         const int k = __ldg(kt + i);
-        atomicAdd(ctr + (k >= 0 ? k : K), 1);
+        ctr.inc(k >= 0 ? k : K);
     }
     __syncthreads();
     // exclusive scan of K+1 counters: quarter q = [q*Q, min((q+1)*Q, K+1))
@@ -69,14 +91,14 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
     int carry = 0;
     for (int k0 = q0; k0 < q1; k0 += 32) {
         const int k = k0 + lane;
-        const int v = k < q1 ? ctr[k] : 0;
+        const int v = k < q1 ? ctr.get(k) : 0;
         int incl = v;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
             const int u = __shfl_up_sync(0xffffffffu, incl, d);
             if (lane >= d) incl += u;
         }
-        if (k < q1) ctr[k] = carry + incl - v;
+        if (k < q1) ctr.set(k, carry + incl - v);
         carry += __shfl_sync(0xffffffffu, incl, 31);
     }
     if (lane == 0) qtot[w] = carry;
@@ -84,8 +106,8 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
     int qoff = 0;
     for (int q = 0; q < w; ++q) qoff += qtot[q];
     for (int k = q0 + lane; k < q1; k += 32) {
-        const int v = ctr[k] + qoff;
-        ctr[k] = v;
+        const int v = ctr.get(k) + qoff;
+        ctr.set(k, v);
         if (use_smem) so[k] = v;
     }
     __syncthreads();
@@ -117,8 +139,8 @@ build_csr_kernel(const int32_t* __restrict__ key, int n, const int64_t* __restri
             const int rank = __popc(grp & ((1u << lane) - 1u));
             int start = 0;
             if (k >= 0 && lane == leader) {
-                start = ctr[k];
-                ctr[k] = start + __popc(grp);
+                start = ctr.get(k);
+                ctr.set(k, start + __popc(grp));
             }
             start = __shfl_sync(0xffffffffu, start, leader);
             if (k >= 0) mt[start + rank] = i;
@@ -549,12 +571,16 @@ rfx_status launch_build_csr(Ctx* c) {
     int dev_smem = 0;
     RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     // budget per tree-warp; several warps (trees) share an SM
-    int smem_keys = std::min(c->max_keys + 1, (dev_smem - 1024) / 4);
+    const bool narrow = c->n < 65536;  // counts and offsets fit 16 bits
+    const int csz = narrow ? 2 : 4;
+    int smem_keys = std::min(c->max_keys + 1, (dev_smem - 1024) / csz - 2);
     smem_keys = std::max(smem_keys, 32);
-    const size_t smem = (size_t)smem_keys * sizeof(int32_t);
+    const size_t smem = ((size_t)(smem_keys + 2) * csz + 3) & ~(size_t)3;
     StageTimer st(c, ST_CSR, c->max_keys + 1 > smem_keys ? 2 : 1);
-    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel, dev_smem)) return s0;
-    build_csr_kernel<<<c->T, CSR_THREADS, smem, c->stream>>>(c->d_key, c->n, c->d_segbase, c->d_segoff, c->d_memb, smem_keys,
+    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel<uint16_t>, dev_smem)) return s0;
+    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel<int32_t>, dev_smem)) return s0;
+    (narrow ? build_csr_kernel<uint16_t> : build_csr_kernel<int32_t>)<<<c->T, CSR_THREADS, smem, c->stream>>>(
+        c->d_key, c->n, c->d_segbase, c->d_segoff, c->d_memb, smem_keys,
                                                     c->d_err);
     RFX_CUDA(cudaGetLastError());
     if (c->max_keys + 1 > smem_keys) {
@@ -640,8 +666,8 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
     int smem_keys = std::min(max_keys + 1, (dev_smem - 1024) / 4);
     smem_keys = std::max(smem_keys, 32);
     const size_t smem = (size_t)smem_keys * sizeof(int32_t);
-    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel, dev_smem)) return s0;
-    build_csr_kernel<<<a.T, CSR_THREADS, smem, stream>>>(a.key, a.n, a.segbase, a.segoff, a.memb, smem_keys,
+    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel<int32_t>, dev_smem)) return s0;
+    build_csr_kernel<int32_t><<<a.T, CSR_THREADS, smem, stream>>>(a.key, a.n, a.segbase, a.segoff, a.memb, smem_keys,
                                                          a.err);
     RFX_CUDA(cudaGetLastError());
     if (max_keys + 1 > smem_keys) {
