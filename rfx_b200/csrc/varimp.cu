@@ -321,12 +321,12 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         if (delta[k]) atomicAdd(delta_out + (size_t)t * p + k, delta[k]);
 }
 
-// qimp / qimpm: one thread per (sample, group of 8 features); each thread
-// keeps its 8 running sums in registers and walks the trees in order, adding
+// qimp / qimpm: one thread per (sample, group of VS_FEAT features); each thread
+// keeps its running sums in registers and walks the trees in order, adding
 // 1/noob for every OOB tree where the feature's permuted vote is correct
 // (group 0 also sums qimp from the testreebag votes).  The float sums follow
 // the reference's tree order exactly.
-constexpr int VS_FEAT = 8;
+constexpr int VS_FEAT = 16;  // features per thread (a group never straddles a 64-bit word)
 
 template <int W>
 __global__ void __launch_bounds__(256)
@@ -340,7 +340,7 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
     const int i = (int)(idx / G);
     const int g = (int)(idx % G);
     const int k0 = g * VS_FEAT;
-    const int wq = k0 >> 6, sh = k0 & 63;  // 8-feature groups never straddle a 64-bit word
+    const int wq = k0 >> 6, sh = k0 & 63;  // groups never straddle a 64-bit word
     float acc[VS_FEAT];
 #pragma unroll
     for (int u = 0; u < VS_FEAT; ++u) acc[u] = 0.0f;
@@ -369,7 +369,7 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
             const bool btb = (fl[u] >> 1) & 1, bimp = (fl[u] >> 2) & 1;
             if (btb) q = __fadd_rn(q, inv[u]);
             const uint64_t corr = (ivw[u] & ((bimp ? ~0ull : 0ull) ^ fw[u])) | (~ivw[u] & (btb ? ~0ull : 0ull));
-            const uint32_t cb = (uint32_t)(corr >> sh) & 0xffu;
+            const uint32_t cb = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
 #pragma unroll
             for (int v = 0; v < VS_FEAT; ++v)
                 if ((cb >> v) & 1u) acc[v] = __fadd_rn(acc[v], inv[u]);
@@ -385,7 +385,7 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
         const uint64_t fw = __ldg(flips + ti * W + wq);
         const uint64_t ivw = __ldg(iv + (size_t)t * W + wq);
         const uint64_t corr = (ivw & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivw & (btb ? ~0ull : 0ull));
-        const uint32_t cb = (uint32_t)(corr >> sh) & 0xffu;
+        const uint32_t cb = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
 #pragma unroll
         for (int u = 0; u < VS_FEAT; ++u)
             if ((cb >> u) & 1u) acc[u] = __fadd_rn(acc[u], inv);
