@@ -100,8 +100,7 @@ struct Ctx {
 
     // varimp scratch
     int32_t* d_joob = nullptr;          // T*n
-    int32_t* d_jrank = nullptr;         // T*n: position of each OOB sample in its tree's joob
-    int32_t* d_ojr = nullptr;           // T*n: joob positions in leaf order
+    int32_t* d_partner = nullptr;       // T*n: permutation partner of each OOB sample
     uint8_t* d_vflags = nullptr;        // T*n: bit1 testreebag correct, bit2 testreeimp correct
     uint64_t* d_flips = nullptr;        // T*n*iv_words
     int32_t* d_right = nullptr;         // 2T: per tree #correct (testreebag), #correct (testreeimp)

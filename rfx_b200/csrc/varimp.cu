@@ -66,15 +66,15 @@ __device__ __forceinline__ int imp_side_walk(const float* __restrict__ xrow, con
 
 // OOB samples of every tree in ascending order (joob of cpu_varimp).
 __global__ void __launch_bounds__(VT)
-joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all, int32_t* __restrict__ jrank_all,
-            const int32_t* __restrict__ memb, int32_t* __restrict__ ojr_all) {
+joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all,
+            const int32_t* __restrict__ permoff, const int32_t* __restrict__ perm_all,
+            int32_t* __restrict__ partner_all) {
     __shared__ int wsum[VT / 32];
     __shared__ int s_base;
     const int t = blockIdx.x;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint8_t* ib = inbag + (size_t)t * n;
     int32_t* joob = joob_all + (size_t)t * n;
-    int32_t* jrank = jrank_all ? jrank_all + (size_t)t * n : nullptr;
     if (tid == 0) s_base = 0;
     __syncthreads();
     for (int base = 0; base < n; base += VT) {
@@ -88,39 +88,18 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
             if (q < wid) woff += wsum[q];
             tot += wsum[q];
         }
-        if (f) {
-            const int pos = s_base + woff + __popc(bal & ((1u << lane) - 1u));
-            joob[pos] = i;
-            if (jrank) jrank[i] = pos;
-        }
+        if (f) joob[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = i;
         __syncthreads();
         if (tid == 0) s_base += tot;
         __syncthreads();
     }
-    if (!memb) return;
-    // the OOB positions again, in the order of the tree's member lists (one
-    // leaf's OOB members together): ojr[q] = position in joob
-    const int32_t* mt = memb + (size_t)t * n;
-    int32_t* ojr = ojr_all + (size_t)t * n;
-    if (tid == 0) s_base = 0;
-    __syncthreads();
-    for (int base = 0; base < n; base += VT) {
-        const int q = base + tid;
-        const int i = q < n ? __ldg(mt + q) : 0;
-        const int f = (q < n && ib[i] == 0) ? 1 : 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) wsum[wid] = __popc(bal);
-        __syncthreads();
-        int woff = 0, tot = 0;
-        for (int u = 0; u < VT / 32; ++u) {
-            if (u < wid) woff += wsum[u];
-            tot += wsum[u];
-        }
-        if (f) ojr[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = jrank[i];
-        __syncthreads();
-        if (tid == 0) s_base += tot;
-        __syncthreads();
-    }
+    if (!partner_all) return;
+    // the permutation partner of every OOB sample, indexed by sample:
+    // partner[joob[r]] = joob[perm[r]] (cpu_permobmr's swap order)
+    const int noob = s_base;
+    const int32_t* perm = perm_all + permoff[t];
+    int32_t* partner = partner_all + (size_t)t * n;
+    for (int r = tid; r < noob; r += VT) partner[joob[r]] = joob[__ldg(perm + r)];
 }
 
 // One thread per (tree, OOB position r): grid = (ceil(max noob / VW), T),
@@ -133,7 +112,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                    const int32_t* __restrict__ noob_arr, const int32_t* __restrict__ cat,
                    const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ permoff,
                    const int32_t* __restrict__ perm_all, const int32_t* __restrict__ joob_all,
-                   const int32_t* __restrict__ ojr_all, uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips,
+                   const int32_t* __restrict__ memb, const int32_t* __restrict__ partner_all,
+                   const uint8_t* __restrict__ inbag, uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips,
                    int32_t* __restrict__ counts, int32_t* __restrict__ delta_out, uint32_t* __restrict__ err) {
     extern __shared__ int32_t delta[];  // p counters
     __shared__ int s_red[2];
@@ -148,8 +128,31 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     const int t = blockIdx.y;
     const int noob = noob_arr[t];
     const int r0 = blockIdx.x * VW;
-    if (r0 >= noob) return;
     const int tid = threadIdx.x, lane = tid & 31;
+    // This thread's OOB sample i and its permutation partner ip.  With member
+    // lists (memb != null) the threads run over all samples of the tree in
+    // leaf order, so neighbouring threads share their main path; in-bag ones
+    // idle and CTAs without an OOB sample leave at once.  Otherwise thread r
+    // takes joob position r.
+    int i = 0, ip = 0;
+    bool active;
+    if (memb) {
+        active = false;
+        if (r0 + tid < n) {
+            i = __ldg(memb + (size_t)t * n + r0 + tid);
+            active = __ldg(inbag + (size_t)t * n + i) == 0;
+            if (active) ip = __ldg(partner_all + (size_t)t * n + i);
+        }
+        if (!__syncthreads_or(active)) return;
+    } else {
+        if (r0 >= noob) return;
+        active = r0 + tid < noob;
+        if (active) {
+            const int32_t* joob = joob_all + (size_t)t * n;
+            i = joob[r0 + tid];
+            ip = joob[__ldg(perm_all + permoff[t] + r0 + tid)];
+        }
+    }
     for (int k = tid; k < p; k += VW) delta[k] = 0;
     if (tid == 0) {
         s_red[0] = 0;
@@ -165,22 +168,14 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
     const int nn = nnode_arr[t];
     const int nnv = nn > 0 ? nn : 1;
-    const int32_t* joob = joob_all + (size_t)t * n;
     const GlobalNodes src{tn};
     int my_right = 0, my_imp = 0;
     uint32_t my_err = 0;
-    // position r of this thread's OOB sample in joob: in leaf order when the
-    // member lists exist (neighbouring threads then share their main path)
-    const int qpos = r0 + tid;
-    const bool active = qpos < noob;
-    const int r = (active && ojr_all) ? __ldg(ojr_all + (size_t)t * n + qpos) : qpos;
     uint64_t done[W], pcorr[W];
 #pragma unroll
     for (int q = 0; q < W; ++q) done[q] = pcorr[q] = 0ull;
-    int i = 0, yi = -1, base_tb = 0, base_imp = 0;
+    int yi = -1, base_tb = 0, base_imp = 0;
     if (active) {
-        i = joob[r];
-        const int ip = joob[__ldg(perm_all + permoff[t] + r)];
         s_i[tid] = i;
         s_ip[tid] = ip;
         const float* xi = X + (size_t)i * p;
@@ -450,17 +445,18 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
     const size_t smem = (size_t)c->p * sizeof(int32_t);
     {
         StageTimer st(c, ST_VARIMP_TREE, 2);
-        const bool ordered = c->csr_built && c->d_jrank && c->d_ojr;
-        joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, ordered ? c->d_jrank : nullptr,
-                                                ordered ? c->d_memb : nullptr, ordered ? c->d_ojr : nullptr);
+        const bool ordered = c->csr_built && c->d_partner;
+        joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, c->d_permoff, c->d_perm,
+                                                ordered ? c->d_partner : nullptr);
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
         auto go = [&](auto kernel, int vw) {
-            dim3 grid((max_noob + vw - 1) / vw, c->T);
+            dim3 grid(((ordered ? c->n : max_noob) + vw - 1) / vw, c->T);
             kernel<<<grid, vw, smem, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
                                                  c->d_nnode, c->d_noob, c->d_cat, c->d_catgoleft, c->maxcat,
-                                                 c->d_permoff, c->d_perm, c->d_joob, ordered ? c->d_ojr : nullptr,
+                                                 c->d_permoff, c->d_perm, c->d_joob,
+                                                 ordered ? c->d_memb : nullptr, c->d_partner, c->d_inbag,
                                                  c->d_vflags, c->d_flips,
                                                  c->d_right, c->d_rightimp, c->d_err);
         };
