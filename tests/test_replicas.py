@@ -34,7 +34,7 @@ def _rank(rank, world, port, out):
 def test_replica_reduce_two_ranks():
     import torch.multiprocessing as mp
 
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     port = _free_port()
     mp.spawn(_rank, args=(2, port, out), nprocs=2, join=True)
