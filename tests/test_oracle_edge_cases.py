@@ -1,0 +1,131 @@
+"""The oracle against the reference's own CPU code on edge cases that grown
+forests rarely reach: single-leaf trees, trees with no OOB sample (the
+reference's 0/0 importance), trees with no in-bag sample, NaN feature values,
+and categorical values outside 0..cat-1 (negative, too large, fractional).
+
+Each case starts from a forest the reference grew and then changes the forest
+or the analysed X; both implementations analyse the same (forest, X).
+
+A categorical value that rounds outside 0..maxcat-1 makes cpu_testreeimp
+(src/rf_varimp.cpp:84-100) stop without a vote, and the permuted vote of that
+sample is then whatever the per-thread jvr buffer held from the previous
+feature the same OpenMP thread processed (src/rf_varimp.cpp:184-190).  That
+depends on how many threads the reference ran with; the oracle restates the
+one-thread order, so those cases run the reference on one thread.  The CUDA
+path refuses such inputs with an error instead of picking a thread count.
+"""
+import contextlib
+
+import numpy as np
+import pytest
+
+from rfx_b200 import synth
+from rfx_b200.forest import Forest
+from conftest import has_reference
+
+pytestmark = pytest.mark.skipif(not has_reference(), reason="reference library not built")
+
+
+def _leaf_tree(f: Forest, t: int, cls: int) -> Forest:
+    """Replace tree t by a single leaf of class cls."""
+    T = f.ntree
+    parts = lambda a, k=1: [a[k * f.offs[u]: k * f.offs[u + 1]] for u in range(T)]
+    ns, bv, xs, tm, nc = (parts(f.nodestatus), parts(f.bestvar), parts(f.xbestsplit),
+                          parts(f.treemap, 2), parts(f.nodeclass))
+    ns[t] = np.array([-1], np.int32)
+    bv[t] = np.array([0], np.int32)
+    xs[t] = np.array([0.0], np.float32)
+    tm[t] = np.array([0, 0], np.int32)
+    nc[t] = np.array([cls], np.int32)
+    nnode = f.nnode.copy()
+    nnode[t] = 1
+    offs = np.zeros(T + 1, np.int64)
+    offs[1:] = np.cumsum(nnode, dtype=np.int64)
+    cat = lambda a: np.ascontiguousarray(np.concatenate(a))
+    return Forest(f.n, f.p, f.nclass, f.maxcat, nnode, offs, cat(ns), cat(bv), cat(xs), cat(tm), cat(nc),
+                  f.nin.copy(), f.cat.copy(), None)
+
+
+@contextlib.contextmanager
+def _reference_threads(k):
+    from oracle import reference as ref
+
+    before = ref.set_threads(0)
+    ref.set_threads(k)
+    try:
+        yield
+    finally:
+        ref.set_threads(before)
+
+
+@pytest.fixture(scope="module")
+def grown(built):
+    from oracle import reference as ref
+
+    X, y = synth.mixed_cover(260, seed=17)
+    y = np.unique(y, return_inverse=True)[1].astype(np.int32)
+    cat = synth.detect_categorical(X)
+    f = ref.grow_forest(X, y, 12, 7, 1, cat=cat)
+    return X, y, f
+
+
+def _compare(X, y, f, threads=None):
+    """Votes, nout, leaf ids, importances and raw pair counts, bit for bit
+    (NaN where the reference divides 0 by 0 counts as equal)."""
+    from oracle import oracle as orc, reference as ref
+
+    with _reference_threads(threads) if threads else contextlib.nullcontext():
+        R = ref.analyse_trees(X, y, f, do_prox=True, want_leaf=True)
+    O = orc.analyse(X, y, f, want_leaf=True)
+    n = f.n
+    assert np.array_equal(O["q_raw"].reshape(-1), R["q"])
+    assert np.array_equal(O["nout"], R["nout"])
+    assert np.array_equal(O["leaf"], R["leaf"])
+    for k in ("qimp", "qimpm", "avimp", "sqsd"):
+        assert np.array_equal(O[k], R[k], equal_nan=True), k
+    # the reference adds 1 to prox[i + j*n] for OOB i and in-bag j in one leaf
+    C = R["prox"].reshape(n, n).T
+    assert np.array_equal(orc.upper_to_full(O["S"], n).astype(np.float64), C + C.T)
+    return O, R
+
+
+def test_single_leaf_trees(grown):
+    X, y, f = grown
+    g = _leaf_tree(_leaf_tree(f, 0, 0), 5, f.nclass - 1)
+    _compare(X, y, g)
+
+
+def test_tree_without_oob_samples(grown):
+    X, y, f = grown
+    g = f.subset(range(f.ntree))
+    g.nin[3] = np.maximum(g.nin[3], 1)
+    O, _ = _compare(X, y, g)
+    assert np.isnan(O["avimp"]).any()      # features split on in tree 3 get 0/0
+
+
+def test_tree_without_inbag_samples(grown):
+    X, y, f = grown
+    g = f.subset(range(f.ntree))
+    g.nin[2] = 0
+    _compare(X, y, g)
+
+
+def test_nan_in_continuous_features(grown):
+    X, y, f = grown
+    rng = np.random.default_rng(5)
+    X2 = X.copy()
+    cont = np.flatnonzero(f.cat == 1)
+    rows = rng.choice(f.n, size=40, replace=False)
+    X2[rows, rng.choice(cont, size=40)] = np.nan
+    _compare(X2, y, f)
+
+
+@pytest.mark.parametrize("value", [-1.0, -0.6, -0.4, 0.49, 0.5, 1.5, 2.0, 9.0, 9.6, 12.0])
+def test_categorical_values_out_of_range(grown, value):
+    X, y, f = grown
+    rng = np.random.default_rng(int(value * 10) + 100)
+    X2 = X.copy()
+    catcols = np.flatnonzero(f.cat > 1)
+    rows = rng.choice(f.n, size=60, replace=False)
+    X2[rows, rng.choice(catcols, size=60)] = np.float32(value)
+    _compare(X2, y, f, threads=1)
