@@ -20,30 +20,9 @@ import numpy as np
 import pytest
 
 from rfx_b200 import synth
-from rfx_b200.forest import Forest
-from conftest import has_reference
+from conftest import has_reference, single_leaf_tree
 
 pytestmark = pytest.mark.skipif(not has_reference(), reason="reference library not built")
-
-
-def _leaf_tree(f: Forest, t: int, cls: int) -> Forest:
-    """Replace tree t by a single leaf of class cls."""
-    T = f.ntree
-    parts = lambda a, k=1: [a[k * f.offs[u]: k * f.offs[u + 1]] for u in range(T)]
-    ns, bv, xs, tm, nc = (parts(f.nodestatus), parts(f.bestvar), parts(f.xbestsplit),
-                          parts(f.treemap, 2), parts(f.nodeclass))
-    ns[t] = np.array([-1], np.int32)
-    bv[t] = np.array([0], np.int32)
-    xs[t] = np.array([0.0], np.float32)
-    tm[t] = np.array([0, 0], np.int32)
-    nc[t] = np.array([cls], np.int32)
-    nnode = f.nnode.copy()
-    nnode[t] = 1
-    offs = np.zeros(T + 1, np.int64)
-    offs[1:] = np.cumsum(nnode, dtype=np.int64)
-    cat = lambda a: np.ascontiguousarray(np.concatenate(a))
-    return Forest(f.n, f.p, f.nclass, f.maxcat, nnode, offs, cat(ns), cat(bv), cat(xs), cat(tm), cat(nc),
-                  f.nin.copy(), f.cat.copy(), None)
 
 
 @contextlib.contextmanager
@@ -91,7 +70,7 @@ def _compare(X, y, f, threads=None):
 
 def test_single_leaf_trees(grown):
     X, y, f = grown
-    g = _leaf_tree(_leaf_tree(f, 0, 0), 5, f.nclass - 1)
+    g = single_leaf_tree(single_leaf_tree(f, 0, 0), 5, f.nclass - 1)
     _compare(X, y, g)
 
 
