@@ -146,47 +146,92 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_baseline_run(X, y, f, budget_s=15.0, min_trees=2):
-    """The reference's CPU path on a bounded sample of trees.
+def forest_pair_updates(X, y, f):
+    """Pair updates of the whole forest (the metric's unit count) on the CPU:
+    per tree, the sum over terminal nodes of OOB members x in-bag members,
+    from the oracle's leaf ids (OOB rows by testreebag, in-bag rows by
+    find_terminal_node; rows that end on a non-terminal node count nowhere,
+    as in cpu_proximity's dense branch, src/rf_proximity.cpp:108-231)."""
+    from oracle import oracle as orc
+
+    leaf = orc.analyse(X, y, f, do_imp=False, impn=False, do_prox=False, want_leaf=True)["leaf"]
+    U = 0
+    for t in range(f.ntree):
+        lf = leaf[t].astype(np.int64)
+        term = f.nodestatus[f.offs[t]: f.offs[t + 1]][lf] == -1
+        inb = f.nin[t] > 0
+        no = np.bincount(lf[term & ~inb], minlength=int(f.nnode[t]))
+        ni = np.bincount(lf[term & inb], minlength=int(f.nnode[t]))
+        U += int(no @ ni)
+    return U
+
+
+class CpuTrees:
+    """The reference's CPU path, one tree at a time, on the box's host cores.
 
     Per tree, as grow_tree_single does: cpu_testreebag, the vote loop,
     cpu_varimp (OpenMP over features) and find_terminal_node, all from
     oracle/_ref (the reference's own sources); the pair counts use the
-    oracle's restatement of cpu_proximity's dense branch, because the shipped
-    cpu_proximity takes its sparse branch above n = 5000 and its n*n int32
-    size overflows at n = 50,000.  Returns (pair updates/s, dict)."""
-    from oracle import oracle as orc, reference as ref
+    oracle's restatement of cpu_proximity's dense branch (the shipped
+    cpu_proximity takes its sparse branch above n = 5000, and its n*n int32
+    size overflows at n = 50,000), added into one upper-triangle array that is
+    allocated and touched once, as the reference accumulates one proximity
+    array over the forest.  Without oracle/_ref the oracle runs the whole
+    sequence ("port").  Trees are taken in a seeded random order: per-tree
+    pair counts are heavy-tailed (a tree with one large leaf has 100x the
+    median), so the first trees are not a fair sample."""
 
-    cores = os.cpu_count() or 1
-    if ref.available():
-        ref.set_threads(cores)
-        kind = "reference"
-    else:
-        kind = "port"
-    done = 0
-    t_total = 0.0
-    U = 0
-    while done < min_trees or t_total < budget_s:
-        if done >= f.ntree:
-            break
-        sub = f.subset([done])
-        t0 = time.perf_counter()
-        if kind == "reference":
-            ref.analyse_trees(X, y, sub, do_imp=True, impn=True, do_prox=False)
-            out = orc.analyse(X, y, sub, do_imp=False, impn=False, do_prox=True)
+    def __init__(self, X, y, f):
+        from oracle import reference as ref
+
+        self.X, self.y, self.f = X, y, f
+        self.cores = os.cpu_count() or 1
+        if ref.available():
+            ref.set_threads(self.cores)
+            self.kind = "reference"
         else:
-            out = orc.analyse(X, y, sub, do_imp=True, impn=True, do_prox=True)
-        t_total += time.perf_counter() - t0
-        U += int(out["S"].astype(np.int64).sum())
-        del out
+            self.kind = "port"
+        self.order = np.random.default_rng(0).permutation(f.ntree)
+        self.S = np.empty(f.n * (f.n + 1) // 2, np.int32)
+        self.S.fill(0)
+
+    def tree_seconds(self, k):
+        """Wall seconds of the k-th tree of the sample order."""
+        from oracle import oracle as orc, reference as ref
+
+        sub = self.f.subset([int(self.order[k % self.f.ntree])])
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            ref.analyse_trees(self.X, self.y, sub, do_imp=True, impn=True, do_prox=False)
+            orc.analyse(self.X, self.y, sub, do_imp=False, impn=False, do_prox=True, S=self.S)
+        else:
+            orc.analyse(self.X, self.y, sub, do_imp=True, impn=True, do_prox=True, S=self.S)
+        return time.perf_counter() - t0
+
+
+def cpu_baseline_run(X, y, f, budget_s=15.0, min_trees=2, pair_updates=None):
+    """The reference's CPU path (CpuTrees) on a bounded sample of trees:
+    the forest's rate = its total pair updates / (mean seconds per sampled
+    tree x ntree).  Returns (pair updates/s, dict)."""
+    U = forest_pair_updates(X, y, f) if pair_updates is None else int(pair_updates)
+    run = CpuTrees(X, y, f)
+    done, t_total = 0, 0.0
+    while done < f.ntree and (done < min_trees or t_total < budget_s):
+        t_total += run.tree_seconds(done)
         done += 1
-    return U / t_total, {"cores": cores if kind == "reference" else 1, "kind": kind,
-                         "sample": f"{done} of {f.ntree} trees at n={f.n} (testreebag + votes + cpu_varimp over "
-                                   f"{f.p} features + find_terminal_node + dense-branch pair counts), {t_total:.1f} s",
-                         "trees": done, "seconds": t_total, "pair_updates": U}
+    per_tree = t_total / done
+    return U / (per_tree * f.ntree), {
+        "cores": run.cores if run.kind == "reference" else 1, "kind": run.kind, "trees": done,
+        "seconds": t_total,
+        "sample": f"{done} of {f.ntree} trees (seeded random order) at n={f.n}, {t_total:.1f} s: testreebag + "
+                  f"votes + cpu_varimp over {f.p} features + find_terminal_node + dense-branch pair counts; "
+                  f"rate = the forest's {U} pair updates / ({per_tree:.3f} s per tree x {f.ntree} trees)"}
 
 
 def run_reference(args):
+    """The reference arm: each step is one tree of the forest (seeded random
+    order) through the reference's CPU path on all host cores; the rate is the
+    forest's pair updates per tree over the mean step time."""
     ws, rank, local = dist_env()
     if rank != 0:
         return 0
@@ -196,24 +241,25 @@ def run_reference(args):
     X, y = synth.mixed_cover(n)
     cat = synth.detect_categorical(X)
     f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
-    per_step = []
-    U_tot, t_tot = 0, 0.0
+    U = forest_pair_updates(X, y, f)
+    run = CpuTrees(X, y, f)
+    t_tot = 0.0
     for s in range(args.warmup + args.steps):
-        sub = f.subset([s % f.ntree])
-        v, info = cpu_baseline_run(X, y, sub, budget_s=0.0, min_trees=1)
+        dt = run.tree_seconds(s)
         if s >= args.warmup:
-            U_tot += info["pair_updates"]
-            t_tot += info["seconds"]
-            per_step.append(info["seconds"])
-    value = U_tot / t_tot
+            t_tot += dt
+    value = (U / T) * args.steps / t_tot
     line = {"metric": "prox pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD.format(n=n, T=T), "n": n, "ntree": T, "parallelism": "host cores (OpenMP)"},
-            "cpu_baseline": {"value": value, "unit": "pair-updates/s", "cores": info["cores"], "kind": info["kind"],
-                             "sample": f"each step = 1 tree of the {T}-tree forest at n={n} (reference per-tree "
-                                       "sequence; pair counts by the dense-branch restatement)"},
+            "config": {"workload": WORKLOAD.format(n=n, T=T), "n": n, "ntree": T,
+                       "pair_updates_per_forest": U, "parallelism": "host cores (OpenMP)"},
+            "cpu_baseline": {"value": value, "unit": "pair-updates/s",
+                             "cores": run.cores if run.kind == "reference" else 1, "kind": run.kind,
+                             "sample": f"each step = 1 tree of the {T}-tree forest at n={n} (seeded random "
+                                       "order; reference per-tree sequence, pair counts by the dense-branch "
+                                       "restatement); rate = the forest's pair updates per tree / mean step time"},
             "e2e": {"value": value, "unit": "pair-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -619,7 +665,7 @@ def main():
                        "d2h_bytes_per_step": int(d2h), "ms_per_step": te * 1000.0, "steps": ke}
 
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, info = cpu_baseline_run(X, y, f)
+        v, info = cpu_baseline_run(X, y, f, pair_updates=U)
         line["cpu_baseline"] = {"value": v, "unit": "pair-updates/s", "cores": info["cores"], "kind": info["kind"],
                                 "sample": info["sample"]}
     ctx.close()

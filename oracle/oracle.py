@@ -46,8 +46,12 @@ def bootstrap(n: int, tree: int) -> np.ndarray:
     return nin
 
 
-def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False, want_jtr=False):
-    """Whole-forest analysis in the reference's per-tree order (see orc_analyse)."""
+def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False, want_jtr=False, S=None):
+    """Whole-forest analysis in the reference's per-tree order (see orc_analyse).
+
+    With ``S`` (int32, n(n+1)/2, C-contiguous) the pair counts are added to
+    that buffer instead of a fresh zeroed one, as the reference accumulates
+    one proximity array over all trees."""
     X = np.ascontiguousarray(X, dtype=np.float32)
     y = np.ascontiguousarray(y, dtype=np.int32)
     f = forest
@@ -56,7 +60,12 @@ def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False,
         q_raw=np.zeros(n * c, np.float32), nout=np.zeros(n, np.int32),
         qimp=np.zeros(n, np.float32), qimpm=np.zeros(n * p, np.float32),
         avimp=np.zeros(p, np.float32), sqsd=np.zeros(p, np.float32))
-    S = np.zeros(n * (n + 1) // 2, np.int32) if do_prox else None
+    if not do_prox:
+        S = None
+    elif S is None:
+        S = np.zeros(n * (n + 1) // 2, np.int32)
+    elif S.dtype != np.int32 or S.size != n * (n + 1) // 2 or not S.flags.c_contiguous:
+        raise ValueError("S must be a C-contiguous int32 array of n(n+1)/2 entries")
     leaf = np.zeros(T * n, np.int32) if want_leaf else None
     jtr = np.zeros(T * n, np.int32) if want_jtr else None
     bad = ctypes.c_int(0)
