@@ -133,7 +133,11 @@ rfx_status rfx_finishprox(rfx_ctx* ctx, const int32_t* S, float* P, int full);
  * cpu_permobmr :16-30, accumulated as src/rf_random_forest.cpp:1217-1230).
  * avimp[p] = feature_importances_, sqsd[p], qimp[n], qimpm[n*p] (sample-major,
  * before localimp); impn = 1 computes qimp/qimpm (local importance), which may
- * then be NULL when impn = 0. */
+ * then be NULL when impn = 0.  A tree with no OOB sample gives the reference's
+ * 0/0 (NaN) for the features it splits on.  When a categorical value rounds
+ * outside 0..maxcat-1 in a permuted walk, cpu_testreeimp stops without a vote
+ * and the reference keeps a vote that depends on its OpenMP thread count; this
+ * call then returns RFX_ERR_UNSUPPORTED with a message naming the cause. */
 rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* qimp, float* qimpm);
 
 /* localimp (src/rf_utilities.cpp:28-43) as get_local_importance returns it:
