@@ -137,7 +137,9 @@ rfx_status rfx_finishprox(rfx_ctx* ctx, const int32_t* S, float* P, int full);
  * 0/0 (NaN) for the features it splits on.  When a categorical value rounds
  * outside 0..maxcat-1 in a permuted walk, cpu_testreeimp stops without a vote
  * and the reference keeps a vote that depends on its OpenMP thread count; this
- * call then returns RFX_ERR_UNSUPPORTED with a message naming the cause. */
+ * call then returns RFX_ERR_UNSUPPORTED with a message naming the cause.
+ * A walk decides up to 256 features at once (one bit each); with more
+ * features the walks run once per block of 256. */
 rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* qimp, float* qimpm);
 
 /* localimp (src/rf_utilities.cpp:28-43) as get_local_importance returns it:

@@ -684,11 +684,7 @@ rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* 
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     rfx_status st = need_forest(c);
     if (st) return st;
-    const int T = c->T, n = c->n, p = c->p, W = c->iv_words;
-    if (W > 4) {
-        set_error("rfx_varimp supports at most 256 features");
-        return RFX_ERR_UNSUPPORTED;
-    }
+    const int T = c->T, n = c->n, p = c->p, W = varimp_flip_words(c->iv_words);
 #define ALLOC(ptr, cnt) \
     if (st == RFX_OK) st = dalloc(c, &c->ptr, (size_t)(cnt));
     ALLOC(d_joob, (size_t)T * n);

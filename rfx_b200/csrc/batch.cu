@@ -54,11 +54,7 @@ rfx_status enqueue_item(Ctx* c, const rfx_batch_item& it) {
 
 // varimp's scratch buffers, allocated as rfx_varimp does
 rfx_status varimp_buffers(Ctx* c) {
-    const int T = c->T, n = c->n, p = c->p, W = c->iv_words;
-    if (W > 4) {
-        set_error("rfx_graph_capture_batch: permutation importance supports at most 256 features");
-        return RFX_ERR_UNSUPPORTED;
-    }
+    const int T = c->T, n = c->n, p = c->p, W = varimp_flip_words(c->iv_words);
     rfx_status st = RFX_OK;
     if (st == RFX_OK) st = dalloc(c, &c->d_joob, (size_t)T * n);
     if (st == RFX_OK) st = dalloc(c, &c->d_partner, (size_t)T * n);

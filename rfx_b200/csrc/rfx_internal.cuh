@@ -102,7 +102,7 @@ struct Ctx {
     int32_t* d_joob = nullptr;          // T*n
     int32_t* d_partner = nullptr;       // T*n: permutation partner of each OOB sample
     uint8_t* d_vflags = nullptr;        // T*n: bit1 testreebag correct, bit2 testreeimp correct
-    uint64_t* d_flips = nullptr;        // T*n*iv_words
+    uint64_t* d_flips = nullptr;        // T*n*varimp_flip_words(iv_words)
     int32_t* d_right = nullptr;         // 2T: per tree #correct (testreebag), #correct (testreeimp)
     int32_t* d_rightimp = nullptr;      // T*p: signed flip counts per tree and feature
     float* d_qimp = nullptr;            // n (internal accumulators)
@@ -280,6 +280,10 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS);
 rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full);
 rfx_status launch_oob_summary(Ctx* c, float* d_err_out, int32_t* d_pred, float* d_proba);
 rfx_status launch_varimp(Ctx* c, int impn);
+// Flip words per (tree, sample) of the varimp walk: one per 64 features, at
+// most four (features beyond 256 are decided in blocks of 256).
+constexpr int VARIMP_BLOCK_WORDS = 4;
+inline int varimp_flip_words(int iv_words) { return iv_words < VARIMP_BLOCK_WORDS ? iv_words : VARIMP_BLOCK_WORDS; }
 rfx_status launch_localimp(Ctx* c, const float* d_qimp, const float* d_qimpm, float* d_out);
 rfx_status launch_predict(Ctx* c, const float* dX, int m, int32_t* d_votes);
 rfx_status check_device_errors(Ctx* c);

@@ -104,7 +104,11 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
 
 // One thread per (tree, OOB position r): grid = (ceil(max noob / VW), T),
 // VW threads per CTA (a launch shape the autotuner picks: 64, 128 or 256).
-template <int W, int VW>
+// With FB (more than 64 W features) one launch decides the features of one
+// block [fb, fb + 64 W): flip bits and delta counters are block-local, other
+// features' splits are followed without a permuted decision, and the per-tree
+// correct counts are added by the fb == 0 launch only.
+template <int W, int VW, bool FB = false>
 __global__ void __launch_bounds__(VW, 1536 / VW)
 varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
                    const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
@@ -114,8 +118,9 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                    const int32_t* __restrict__ perm_all, const int32_t* __restrict__ joob_all,
                    const int32_t* __restrict__ memb, const int32_t* __restrict__ partner_all,
                    const uint8_t* __restrict__ inbag, uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips,
-                   int32_t* __restrict__ counts, int32_t* __restrict__ delta_out, uint32_t* __restrict__ err) {
-    extern __shared__ int32_t delta[];  // p counters
+                   int32_t* __restrict__ counts, int32_t* __restrict__ delta_out, uint32_t* __restrict__ err,
+                   int fb) {
+    extern __shared__ int32_t delta[];  // pw counters (the features of this launch)
     __shared__ int s_red[2];
     // Side walks found along the main paths are queued and then shared out
     // over the whole CTA, so a thread with many of them does not hold its
@@ -153,7 +158,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
             ip = joob[__ldg(perm_all + permoff[t] + r0 + tid)];
         }
     }
-    for (int k = tid; k < p; k += VW) delta[k] = 0;
+    const int pw = FB ? min(64 * W, p - fb) : p;
+    for (int k = tid; k < pw; k += VW) delta[k] = 0;
     if (tid == 0) {
         s_red[0] = 0;
         s_red[1] = 0;
@@ -230,13 +236,14 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                 }
             }
             if (dir_o == DIR_BREAK) break;
-            const int wq = m >> 6;
-            const uint64_t bit = 1ull << (m & 63);
+            const int mm = FB ? m - fb : m;  // the feature's bit within this launch's block
+            const int wq = mm >> 6;
+            const uint64_t bit = 1ull << (mm & 63);
             uint64_t dword = 0;
 #pragma unroll
             for (int q = 0; q < W; ++q)
                 if (q == wq) dword = done[q];
-            if (!(dword & bit)) {
+            if ((!FB || (unsigned)mm < (unsigned)(64 * W)) && !(dword & bit)) {
                 const int dir_p = imp_decide(nd, kt, __ldg(xp + m), cgl, maxcat);
                 if (dir_p != dir_o) {
                     int cls_m = -2;  // -2: queued, decided in the shared phase
@@ -274,7 +281,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         const int cls_m = imp_side_walk(X + (size_t)s_i[lt] * p, X + (size_t)s_ip[lt] * p, m, p, en.z, en.w, src,
                                         tc, cgl, maxcat);
         if (cls_m < 0) my_err |= ERR_STALE_JVR;
-        else if (cls_m == s_y[lt]) atomicOr(&s_pcorr[lt][m >> 6], 1ull << (m & 63));
+        const int mb = FB ? m - fb : m;
+        if (cls_m >= 0 && cls_m == s_y[lt]) atomicOr(&s_pcorr[lt][mb >> 6], 1ull << (mb & 63));
     }
     __syncthreads();
     if (active) {
@@ -308,19 +316,21 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     }
     if (my_err) atomicOr(err, my_err);
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && (!FB || fb == 0)) {
         if (s_red[0]) atomicAdd(counts + 2 * t, s_red[0]);
         if (s_red[1]) atomicAdd(counts + 2 * t + 1, s_red[1]);
     }
-    for (int k = tid; k < p; k += VW)
-        if (delta[k]) atomicAdd(delta_out + (size_t)t * p + k, delta[k]);
+    for (int k = tid; k < pw; k += VW)
+        if (delta[k]) atomicAdd(delta_out + (size_t)t * p + fb + k, delta[k]);
 }
 
 // qimp / qimpm: one thread per (sample, group of VS_FEAT features); each thread
 // keeps its running sums in registers and walks the trees in order, adding
 // 1/noob for every OOB tree where the feature's permuted vote is correct
 // (group 0 also sums qimp from the testreebag votes).  The float sums follow
-// the reference's tree order exactly.
+// the reference's tree order exactly.  One launch covers the pw features
+// [fb, fb + pw) whose flip bits the walk wrote (fb = 0 and pw = p unless the
+// features come in blocks); iv rows are ivw words long.
 constexpr int VS_FEAT = 16;  // features per thread (a group never straddles a 64-bit word)
 
 template <int W>
@@ -328,14 +338,16 @@ __global__ void __launch_bounds__(256)
 varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restrict__ vflags,
                      const uint64_t* __restrict__ flips, const uint64_t* __restrict__ iv,
                      const float* __restrict__ invnoob, int n, int p, int T, float* __restrict__ qimp,
-                     float* __restrict__ qimpm) {
-    const int G = (p + VS_FEAT - 1) / VS_FEAT;
+                     float* __restrict__ qimpm, int fb, int pw, int ivw) {
+    const int G = (pw + VS_FEAT - 1) / VS_FEAT;
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)n * G) return;
     const int i = (int)(idx / G);
     const int g = (int)(idx % G);
-    const int k0 = g * VS_FEAT;
-    const int wq = k0 >> 6, sh = k0 & 63;  // groups never straddle a 64-bit word
+    const int kl = g * VS_FEAT;  // first feature of the group within the block
+    const int k0 = fb + kl;
+    const int wq = kl >> 6, sh = kl & 63;  // groups never straddle a 64-bit word
+    const int iq = k0 >> 6;                // the group's word of the iv row
     float acc[VS_FEAT];
 #pragma unroll
     for (int u = 0; u < VS_FEAT; ++u) acc[u] = 0.0f;
@@ -348,7 +360,7 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
     for (; t0 + TB <= T; t0 += TB) {
         uint8_t ib[TB], fl[TB];
         float inv[TB];
-        uint64_t fw[TB], ivw[TB];
+        uint64_t fw[TB], ivv[TB];
 #pragma unroll
         for (int u = 0; u < TB; ++u) {
             const size_t ti = (size_t)(t0 + u) * n + i;
@@ -356,14 +368,14 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
             fl[u] = __ldg(vflags + ti);
             inv[u] = __ldg(invnoob + t0 + u);
             fw[u] = __ldg(flips + ti * W + wq);
-            ivw[u] = __ldg(iv + (size_t)(t0 + u) * W + wq);
+            ivv[u] = __ldg(iv + (size_t)(t0 + u) * ivw + iq);
         }
 #pragma unroll
         for (int u = 0; u < TB; ++u) {
             if (ib[u] != 0) continue;
             const bool btb = (fl[u] >> 1) & 1, bimp = (fl[u] >> 2) & 1;
             if (btb) q = __fadd_rn(q, inv[u]);
-            const uint64_t corr = (ivw[u] & ((bimp ? ~0ull : 0ull) ^ fw[u])) | (~ivw[u] & (btb ? ~0ull : 0ull));
+            const uint64_t corr = (ivv[u] & ((bimp ? ~0ull : 0ull) ^ fw[u])) | (~ivv[u] & (btb ? ~0ull : 0ull));
             const uint32_t cb = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
 #pragma unroll
             for (int v = 0; v < VS_FEAT; ++v)
@@ -378,17 +390,17 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
         const bool btb = (fl >> 1) & 1, bimp = (fl >> 2) & 1;
         if (btb) q = __fadd_rn(q, inv);
         const uint64_t fw = __ldg(flips + ti * W + wq);
-        const uint64_t ivw = __ldg(iv + (size_t)t * W + wq);
-        const uint64_t corr = (ivw & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivw & (btb ? ~0ull : 0ull));
+        const uint64_t ivt = __ldg(iv + (size_t)t * ivw + iq);
+        const uint64_t corr = (ivt & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivt & (btb ? ~0ull : 0ull));
         const uint32_t cb = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
 #pragma unroll
         for (int u = 0; u < VS_FEAT; ++u)
             if ((cb >> u) & 1u) acc[u] = __fadd_rn(acc[u], inv);
     }
-    if (g == 0) qimp[i] = q;
+    if (g == 0 && fb == 0) qimp[i] = q;
 #pragma unroll
     for (int u = 0; u < VS_FEAT; ++u)
-        if (k0 + u < p) qimpm[(size_t)i * p + k0 + u] = acc[u];
+        if (kl + u < pw) qimpm[(size_t)i * p + k0 + u] = acc[u];
 }
 
 // counts[2t] = #OOB correct by testreebag (right), counts[2t+1] = #OOB correct
@@ -458,7 +470,7 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
                                                  c->d_permoff, c->d_perm, c->d_joob,
                                                  ordered ? c->d_memb : nullptr, c->d_partner, c->d_inbag,
                                                  c->d_vflags, c->d_flips,
-                                                 c->d_right, c->d_rightimp, c->d_err);
+                                                 c->d_right, c->d_rightimp, c->d_err, 0);
         };
         rfx_status r = autotune(c, TK_VWALK, 3, 1, [&](int shape) -> rfx_status {
             // the walk adds to the per-tree counts: clear them for every run
@@ -477,12 +489,53 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         const long long G = (c->p + VS_FEAT - 1) / VS_FEAT;
         const long long threads = (long long)c->n * G;
         varimp_sample_kernel<W><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp, c->d_qimpm);
+            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp, c->d_qimpm, 0,
+            c->p, W);
         RFX_CUDA(cudaGetLastError());
     }
     StageTimer st(c, ST_VARIMP_FEATURE, 1);
     varimp_feature_kernel<<<(c->p + 3) / 4, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,
                                                                       W, c->p, c->T, c->d_avimp, c->d_sqsd);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+// More than 256 features: the walk and the per-sample sums run once per block
+// of 256 features (flip words and delta counters are per block; the flips
+// buffer holds one block), then the per-feature sums once for all features.
+// Launch shapes are the defaults (no tuning trials).
+rfx_status launch_varimp_blocked(Ctx* c, int impn) {
+    constexpr int W = VARIMP_BLOCK_WORDS, VW = 128, FW = 64 * W;
+    {
+        StageTimer st(c, ST_VARIMP_TREE, 1 + (impn ? 2 : 1) * ((c->p + FW - 1) / FW));
+        const bool ordered = c->csr_built && c->d_partner;
+        joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, c->d_permoff, c->d_perm,
+                                                ordered ? c->d_partner : nullptr);
+        RFX_CUDA(cudaGetLastError());
+        int max_noob = 1;
+        for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
+        RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
+        RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
+        const dim3 grid(((ordered ? c->n : max_noob) + VW - 1) / VW, c->T);
+        for (int fb = 0; fb < c->p; fb += FW) {
+            const int pw = std::min(FW, c->p - fb);
+            const long long threads = (long long)c->n * ((pw + VS_FEAT - 1) / VS_FEAT);
+            varimp_walk_kernel<W, VW, true><<<grid, VW, sizeof(int32_t) * pw, c->stream>>>(
+                c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs, c->d_nnode, c->d_noob, c->d_cat,
+                c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, ordered ? c->d_memb : nullptr,
+                c->d_partner, c->d_inbag, c->d_vflags, c->d_flips, c->d_right, c->d_rightimp, c->d_err, fb);
+            RFX_CUDA(cudaGetLastError());
+            if (impn) {
+                varimp_sample_kernel<W><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+                    c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp,
+                    c->d_qimpm, fb, pw, c->iv_words);
+                RFX_CUDA(cudaGetLastError());
+            }
+        }
+    }
+    StageTimer st(c, ST_VARIMP_FEATURE, 1);
+    varimp_feature_kernel<<<(c->p + 3) / 4, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,
+                                                                      c->iv_words, c->p, c->T, c->d_avimp, c->d_sqsd);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
 }
@@ -495,9 +548,7 @@ rfx_status launch_varimp(Ctx* c, int impn) {
         case 2: return launch_varimp_w<2>(c, impn);
         case 3: return launch_varimp_w<3>(c, impn);
         case 4: return launch_varimp_w<4>(c, impn);
-        default:
-            set_error("rfx_varimp supports at most 256 features");
-            return RFX_ERR_UNSUPPORTED;
+        default: return launch_varimp_blocked(c, impn);
     }
 }
 

@@ -31,6 +31,15 @@ def _with_catgoleft(f, seed=0):
     return f
 
 
+def _wide(n, pg, seed):
+    """pg pure-noise Gaussian features followed by the 54 cover-shaped ones,
+    which carry the labels (so the informative and categorical features sit
+    beyond index 256 when pg > 202)."""
+    Xc, y = synth.mixed_cover(n, seed=seed)
+    Xg = np.random.default_rng(seed).normal(size=(n, pg)).astype(np.float32)
+    return np.ascontiguousarray(np.concatenate([Xg, Xc], axis=1)), y
+
+
 CASES = {
     "gauss": lambda: _grow(*synth.gaussian_classes(500, 13, 3), 40, 3),
     "cover": lambda: _grow(*synth.mixed_cover(2000), 30, 7),
@@ -38,6 +47,9 @@ CASES = {
     "catgoleft": lambda: (lambda X, y, f: (X, y, _with_catgoleft(f)))(*_grow(*synth.mixed_cover(1200, seed=3), 20, 7)),
     "tiny": lambda: _grow(*synth.gaussian_classes(7, 3, 2, seed=5), 6, 1),
     "uneven": lambda: (lambda d: _grow(d["X"], d["y"], 12, d["mtry"]))(synth.uneven_forests(1, seed=21, n_range=(900, 900))[0]),
+    # more than 256 features: permutation importance runs in feature blocks
+    "wide_p304": lambda: _grow(*_wide(450, 250, 41), 24, 17),
+    "wide_p600": lambda: _grow(*synth.gaussian_classes(320, 600, 4, seed=43), 16, 24),
 }
 
 
