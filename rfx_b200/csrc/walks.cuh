@@ -24,17 +24,6 @@ __device__ __forceinline__ DNode load_node(const DNode* __restrict__ nodes, int 
     return as_node(__ldg(reinterpret_cast<const int4*>(nodes) + k));
 }
 
-// Node source with the first `ntop` nodes of the tree staged in shared memory
-// (nodes are numbered in creation order, so these are the top levels).
-struct TopCachedNodes {
-    const int4* top;
-    int ntop;
-    const DNode* g;
-    __device__ __forceinline__ DNode operator()(int k) const {
-        return k < ntop ? as_node(top[k]) : as_node(__ldg(reinterpret_cast<const int4*>(g) + k));
-    }
-};
-
 struct GlobalNodes {
     const DNode* g;
     __device__ __forceinline__ DNode operator()(int k) const { return load_node(g, k); }
