@@ -396,6 +396,98 @@ def run_lowrank(args):
     return 0
 
 
+def run_rows(args):
+    """The path's other rows, each timed on the device by the library's stage
+    events (mean over the timed launches, inputs and outputs in HBM):
+    finishprox (full n x n and packed upper) and test-set prediction at
+    n = 50,000 / 1,000 trees (the exact workload's forest), and the
+    full-matrix 3-D MDS at n = 2,000 (500 trees, 13 Gaussian features, the
+    reference's CPU-runnable size) and at n = 50,000."""
+    import torch
+
+    from rfx_b200 import abi, synth
+
+    hbm, peak_src = peaks()
+    dev = torch.device("cuda", 0)
+    reps = max(args.steps, 1)
+    warm = max(args.warmup, 3)
+
+    def timed(ctx, stage, fn):
+        ctx.profile(True)
+        for _ in range(warm):
+            fn()
+        ctx.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            fn()
+            ctx.synchronize()
+            tot += ctx.profile_read()[0][stage]
+        ctx.profile(False)
+        return tot / reps
+
+    rows = {}
+    n, T = 50_000, 1000
+    X, y, f, grow_s = make_forest(n, T, 0, 1, lambda: None)
+    ctx = abi.Context(0)
+    ctx.load(f, X, y)
+    L = n * (n + 1) // 2
+    S = torch.empty(L, dtype=torch.int32, device=dev)
+    ctx.proximity_upper(S)
+    ctx.synchronize()
+    for full in (True, False):
+        P = torch.empty((n, n) if full else (L,), dtype=torch.float32, device=dev)
+        ms = timed(ctx, "finishprox", lambda: ctx.finishprox(S, P, full=full))
+        nbytes = 4 * L + 4 * (n * n if full else L) + 4 * n
+        rows["finishprox_full" if full else "finishprox_upper"] = {
+            "ms": ms, "alg_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac": nbytes / ms / 1e6 / hbm,
+            "unit": "bytes: S read 4 B + P write 4 B per entry"}
+        del P
+    # test set: the training rows with Gaussian noise on the continuous columns
+    rng = np.random.default_rng(7)
+    Xt = X.copy()
+    Xt[:, :10] += rng.normal(0.0, 0.5, size=(n, 10)).astype(np.float32)
+    Xt_d = torch.from_numpy(Xt).to(dev)
+    votes = torch.empty((n, f.nclass), dtype=torch.int32, device=dev)
+    ms = timed(ctx, "predict", lambda: ctx.predict_votes(Xt_d, votes))
+    walks = n * T
+    nbytes = 4 * n * f.p + 4 * n * f.nclass + 16 * int(f.offs[-1])
+    rows["predict"] = {"ms": ms, "walks_per_s": walks / ms * 1e3, "alg_bytes": nbytes,
+                       "achieved_gbs": nbytes / ms / 1e6, "frac": nbytes / ms / 1e6 / hbm,
+                       "unit": "walk = one (test row, tree); bytes: X rows + votes + one pass over the 16-byte nodes"}
+    Pd = torch.empty((n, n), dtype=torch.float32, device=dev)
+    ctx.finishprox(S, Pd, full=True)
+    del S
+    coords = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    ms = timed(ctx, "mds_full", lambda: ctx.mds3d_full(Pd, coords))
+    rows["mds_full_n50000"] = {"ms": ms, "unit": "whole call: centring into an n x n FP64 matrix, subspace "
+                                                "iteration for the top 3 eigenpairs"}
+    del Pd, coords
+    ctx.close()
+    X1, y1 = synth.gaussian_classes(2000, 13, 3)
+    f1 = abi.grow_forest(X1, y1, 500, 3, 1, nclass=3)
+    ctx = abi.Context(0)
+    ctx.load(f1, X1, y1)
+    n1 = f1.n
+    S1 = torch.empty(n1 * (n1 + 1) // 2, dtype=torch.int32, device=dev)
+    ctx.proximity_upper(S1)
+    P1 = torch.empty((n1, n1), dtype=torch.float32, device=dev)
+    ctx.finishprox(S1, P1, full=True)
+    c1 = torch.empty((n1, 3), dtype=torch.float64, device=dev)
+    ms = timed(ctx, "mds_full", lambda: ctx.mds3d_full(P1, c1))
+    rows["mds_full_n2000"] = {"ms": ms, "unit": "whole call, n = 2,000, 500 trees"}
+    ctx.close()
+    line = {"metric": "per-row device time (finishprox, predict, full-matrix MDS)", "value": rows["finishprox_full"]["ms"],
+            "unit": "ms (finishprox full, n=50000)", "higher_is_better": False, "n_gpus": 1, "steps": reps,
+            "warmup": warm, "dtype": "int32 counts, fp64 normalisation and MDS, fp32 outputs",
+            "data": "synthetic (seeded cover-shaped and Gaussian generators)",
+            "config": {"workload": "rows a5/a7/a9: finishprox, predict at n=50000 ntree=1000; full-matrix 3-D MDS "
+                                   "at n=50000 and n=2000", "forest_grow_s": round(grow_s, 2),
+                       "peak_hbm_gbs": hbm, "peak_source": peak_src},
+            "rows": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """64 independent forests of uneven shape (n in [1000, 50000], p in
     [8, 100] with 30% noise features, 2..10 classes, 300 trees, mtry =
@@ -502,7 +594,7 @@ def main():
     ap.add_argument("--trees", type=int, default=None, help="trees (default 1000; 2000 for --workload lowrank)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="exact", choices=["exact", "lowrank", "large", "batch"])
+    ap.add_argument("--workload", default="exact", choices=["exact", "lowrank", "large", "batch", "rows"])
     ap.add_argument("--forests", type=int, default=64, help="forests in the batch workload")
     args = ap.parse_args()
     if args.workload in ("lowrank", "large"):
@@ -510,6 +602,8 @@ def main():
     if args.workload == "batch":
         args.warmup = max(args.warmup, 3)
         return run_batch(args)
+    if args.workload == "rows":
+        return run_rows(args)
     args.n = N_SAMPLES if args.n is None else args.n
     args.trees = N_TREES if args.trees is None else args.trees
     if args.warmup < 3:

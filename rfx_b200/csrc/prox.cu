@@ -519,49 +519,79 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
 // finishprox
 // ---------------------------------------------------------------------------
 constexpr int FP_TILE = 32;
+constexpr int FP_JT = 8;  // column tiles per CTA
 
+// S/2 is exact for an integer S, so it is formed as S * 0.5 (the same double
+// as the reference's division by 2).
 __device__ __forceinline__ double fp_value(int32_t s, double inv_i, double inv_j, bool sc_i, bool sc_j) {
-    const double h = __ddiv_rn((double)s, 2.0);
+    const double h = __dmul_rn((double)s, 0.5);
     const double a = sc_i ? __dmul_rn(h, inv_i) : h;
     const double b = sc_j ? __dmul_rn(h, inv_j) : h;
     return __dmul_rn(0.5, __dadd_rn(a, b));
 }
 
-// One CTA per (I, J) tile with I <= J; computes the 32x32 values from the
-// packed S rows of tile I and writes tile (I, J) and its mirror (J, I) of the
-// full matrix, or tile (I, J) of the packed triangle.
+// One CTA per row tile I and a run of FP_JT column tiles J >= I; computes the
+// 32x32 values of each tile (I, J) from the packed S rows of tile I and writes
+// tile (I, J) and its mirror (J, I) of the full matrix, or tile (I, J) of the
+// packed triangle.  The row tile's 1/nout factors are formed once per CTA.
 __global__ void __launch_bounds__(FP_TILE * 8)
 finishprox_kernel(const int32_t* __restrict__ S, const int32_t* __restrict__ nout, int n, int full,
                   float* __restrict__ P) {
     __shared__ float tile[FP_TILE][FP_TILE + 1];
-    const int I = blockIdx.y, J = blockIdx.x;
-    if (J < I) return;
+    __shared__ double s_inv[FP_TILE];
+    __shared__ int s_ni[FP_TILE];
+    const int I = blockIdx.y;
+    const int nt = (n + FP_TILE - 1) / FP_TILE;
+    const int J0 = blockIdx.x * FP_JT;
+    const int J1 = min(J0 + FP_JT, nt);
+    if (J1 <= I) return;  // the whole run lies left of the diagonal
     const int tx = threadIdx.x % FP_TILE, ty = threadIdx.x / FP_TILE;  // 32 x 8
-    const int j = J * FP_TILE + tx;
-    const bool jv = j < n;
-    const int nj = jv ? nout[j] : 0;
-    const double inv_j = nj > 0 ? __ddiv_rn(1.0, (double)nj) : 1.0;
-    for (int r = ty; r < FP_TILE; r += 8) {
-        const int i = I * FP_TILE + r;
-        float v = 0.0f;
-        if (i < n && jv && j >= i) {
-            const int ni = nout[i];
-            const double inv_i = ni > 0 ? __ddiv_rn(1.0, (double)ni) : 1.0;
-            const int64_t idx = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 + (j - i);
-            double d = (j == i) ? 1.0 : fp_value(S[idx], inv_i, inv_j, ni > 0, nj > 0);
-            v = __double2float_rn(d);
-            if (full) P[(size_t)i * n + j] = v;
-            else P[idx] = v;
-        }
-        tile[r][tx] = v;
+    if (threadIdx.x < FP_TILE) {
+        const int i = I * FP_TILE + threadIdx.x;
+        const int ni = i < n ? nout[i] : 0;
+        s_ni[threadIdx.x] = ni;
+        s_inv[threadIdx.x] = ni > 0 ? __ddiv_rn(1.0, (double)ni) : 1.0;
     }
-    if (!full) return;
     __syncthreads();
-    // mirror: P[j][i] for j in tile J rows, i in tile I columns (strictly lower part)
-    for (int r = ty; r < FP_TILE; r += 8) {
-        const int jj = J * FP_TILE + r;
-        const int ii = I * FP_TILE + tx;
-        if (jj < n && ii < n && jj > ii) P[(size_t)jj * n + ii] = tile[tx][r];
+    for (int J = max(J0, I); J < J1; ++J) {
+        const int j = J * FP_TILE + tx;
+        const bool jv = j < n;
+        const int nj = jv ? nout[j] : 0;
+        const double inv_j = nj > 0 ? __ddiv_rn(1.0, (double)nj) : 1.0;
+        // the four rows' loads are issued before any value is formed (four
+        // 128-byte row segments in flight per warp)
+        int32_t sv[FP_TILE / 8];
+        int64_t ix[FP_TILE / 8];
+#pragma unroll
+        for (int u = 0; u < FP_TILE / 8; ++u) {
+            const int i = I * FP_TILE + ty + 8 * u;
+            ix[u] = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 + (j - i);
+            sv[u] = (i < n && jv && j > i) ? __ldg(S + ix[u]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < FP_TILE / 8; ++u) {
+            const int r = ty + 8 * u;
+            const int i = I * FP_TILE + r;
+            float v = 0.0f;
+            if (i < n && jv && j >= i) {
+                const int ni = s_ni[r];
+                const double d = (j == i) ? 1.0 : fp_value(sv[u], s_inv[r], inv_j, ni > 0, nj > 0);
+                v = __double2float_rn(d);
+                if (full) P[(size_t)i * n + j] = v;
+                else P[ix[u]] = v;
+            }
+            tile[r][tx] = v;
+        }
+        if (full) {
+            __syncthreads();
+            // mirror: P[j][i] for j in tile J rows, i in tile I columns (strictly lower part)
+            for (int r = ty; r < FP_TILE; r += 8) {
+                const int jj = J * FP_TILE + r;
+                const int ii = I * FP_TILE + tx;
+                if (jj < n && ii < n && jj > ii) P[(size_t)jj * n + ii] = tile[tx][r];
+            }
+            __syncthreads();  // the tile is rewritten for the next J
+        }
     }
 }
 
@@ -690,7 +720,7 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
 rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full) {
     StageTimer st(c, ST_FINISHPROX, 1);
     const int nt = (c->n + FP_TILE - 1) / FP_TILE;
-    dim3 grid(nt, nt);
+    dim3 grid((nt + FP_JT - 1) / FP_JT, nt);
     finishprox_kernel<<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
