@@ -77,18 +77,33 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
     int32_t* joob = joob_all + (size_t)t * n;
     if (tid == 0) s_base = 0;
     __syncthreads();
-    for (int base = 0; base < n; base += VT) {
-        const int i = base + tid;
-        const int f = (i < n && ib[i] == 0) ? 1 : 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) wsum[wid] = __popc(bal);
+    // JB consecutive samples per thread (their flag loads in flight
+    // together), JB * VT samples per round
+    constexpr int JB = 4;
+    for (int base = 0; base < n; base += JB * VT) {
+        const int i0 = base + JB * tid;
+        unsigned fl = 0;
+#pragma unroll
+        for (int u = 0; u < JB; ++u)
+            if (i0 + u < n && ib[i0 + u] == 0) fl |= 1u << u;
+        const int cnt = __popc(fl);
+        int incl = cnt;  // inclusive warp scan of the per-thread counts
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        if (lane == 31) wsum[wid] = incl;
         __syncthreads();
         int woff = 0, tot = 0;
         for (int q = 0; q < VT / 32; ++q) {
             if (q < wid) woff += wsum[q];
             tot += wsum[q];
         }
-        if (f) joob[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = i;
+        int pos = s_base + woff + incl - cnt;
+#pragma unroll
+        for (int u = 0; u < JB; ++u)
+            if ((fl >> u) & 1u) joob[pos++] = i0 + u;
         __syncthreads();
         if (tid == 0) s_base += tot;
         __syncthreads();
@@ -334,7 +349,7 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
 constexpr int VS_FEAT = 16;  // features per thread (a group never straddles a 64-bit word)
 
 template <int W>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restrict__ vflags,
                      const uint64_t* __restrict__ flips, const uint64_t* __restrict__ iv,
                      const float* __restrict__ invnoob, int n, int p, int T, float* __restrict__ qimp,
