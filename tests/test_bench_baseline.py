@@ -45,3 +45,24 @@ def test_sampled_trees_accumulate_the_forest_counts(built):
     assert np.array_equal(run.S, S)
     v, info = bench.cpu_baseline_run(X, y, f, budget_s=0.0, min_trees=3)
     assert v > 0 and info["trees"] == 3
+
+
+def test_reference_arm_prints_the_contract_line(built):
+    """`bench.py --impl reference` on a small forest: one JSON line with the
+    contract's keys, the reference arm's own e2e and cpu_baseline."""
+    import json
+    import subprocess
+
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "600",
+                        "--trees", "8", "--steps", "2", "--warmup", "3"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["steps"] == 2 and d["warmup"] >= 3
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    assert "workload" in d["config"]
