@@ -100,23 +100,29 @@ __global__ void mds_b_kernel(const float* __restrict__ P, const int32_t* __restr
 
 // W[n x S] = B[n x n] V[n x S], FP64, 64-row tiles.
 constexpr int GT = 64;
+constexpr int BV_KSPLIT = 8;  // column ranges per row tile (enough CTAs to fill the GPU in several waves)
+
+// Partial products Wpart[ks] = B[rows, K_ks] V[K_ks, :] for row tile blockIdx.x
+// and column range ks = blockIdx.y of kchunk columns (a multiple of GT).
 __global__ void __launch_bounds__(256) dgemm_bv_kernel(const double* __restrict__ B, const double* __restrict__ V,
-                                                       int n, double* __restrict__ W) {
+                                                       int n, int kchunk, double* __restrict__ Wpart) {
     __shared__ double Bs[GT][GT + 1];
     __shared__ double Vs[GT][S_BLK];
     const int r0 = blockIdx.x * GT;
+    const int ks = blockIdx.y;
+    const int kbeg = ks * kchunk, kend = min(n, kbeg + kchunk);
     const int tid = threadIdx.x;
     // thread owns rows (tid / 4) and columns (tid % 4) * 4 .. +3
     const int rr = tid >> 2, cc = (tid & 3) * 4;
     double acc[4] = {0, 0, 0, 0};
-    for (int k0 = 0; k0 < n; k0 += GT) {
+    for (int k0 = kbeg; k0 < kend; k0 += GT) {
         for (int e = tid; e < GT * GT; e += 256) {
             const int r = e / GT, k = e % GT;
-            Bs[r][k] = (r0 + r < n && k0 + k < n) ? B[(size_t)(r0 + r) * n + k0 + k] : 0.0;
+            Bs[r][k] = (r0 + r < n && k0 + k < kend) ? B[(size_t)(r0 + r) * n + k0 + k] : 0.0;
         }
         for (int e = tid; e < GT * S_BLK; e += 256) {
             const int k = e / S_BLK, c = e % S_BLK;
-            Vs[k][c] = (k0 + k < n) ? V[(size_t)(k0 + k) * S_BLK + c] : 0.0;
+            Vs[k][c] = (k0 + k < kend) ? V[(size_t)(k0 + k) * S_BLK + c] : 0.0;
         }
         __syncthreads();
 #pragma unroll 8
@@ -129,7 +135,17 @@ __global__ void __launch_bounds__(256) dgemm_bv_kernel(const double* __restrict_
     }
     if (r0 + rr < n)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) W[(size_t)(r0 + rr) * S_BLK + cc + q] = acc[q];
+        for (int q = 0; q < 4; ++q) Wpart[((size_t)ks * n + r0 + rr) * S_BLK + cc + q] = acc[q];
+}
+
+// W = sum of the ksn partial products, added in range order (reproducible).
+__global__ void bv_reduce_kernel(const double* __restrict__ Wpart, int n, int ksn, double* __restrict__ W) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t cnt = (size_t)n * S_BLK;
+    if (idx >= cnt) return;
+    double a = Wpart[idx];
+    for (int s = 1; s < ksn; ++s) a += Wpart[(size_t)s * cnt + idx];
+    W[idx] = a;
 }
 
 // G[S x S] += X^T Y over rows (atomics into a zeroed G).
@@ -804,9 +820,17 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
     mds_b_kernel<<<2048, 256, 0, s>>>(dP, c->d_nout, n, mx, rowmean, grand, B);
     c->launches += 4;
     RFX_CUDA(cudaGetLastError());
+    const int kchunk = ((n + BV_KSPLIT - 1) / BV_KSPLIT + GT - 1) / GT * GT;
+    const int ksn = (n + kchunk - 1) / kchunk;
+    double* Wpart = d.get<double>((size_t)ksn * n * S_BLK);
+    if (!Wpart) {
+        set_error("rfx_mds3d_full: device allocation failed");
+        return RFX_ERR_OOM;
+    }
     auto apply = [&](const double* V, double* W) -> rfx_status {
-        dgemm_bv_kernel<<<(n + GT - 1) / GT, 256, 0, s>>>(B, V, n, W);
-        c->launches += 1;
+        dgemm_bv_kernel<<<dim3((n + GT - 1) / GT, ksn), 256, 0, s>>>(B, V, n, kchunk, Wpart);
+        bv_reduce_kernel<<<(unsigned)(((size_t)n * S_BLK + 255) / 256), 256, 0, s>>>(Wpart, n, ksn, W);
+        c->launches += 2;
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
