@@ -277,7 +277,7 @@ struct TreeView {
 };
 
 static void expand_tree(TreeView& v, int maxnode, int maxcat, int nn, const int* ns, const int* bv,
-                        const float* xs, const int* tm, const int* nc) {
+                        const float* xs, const int* tm, const int* nc, const int* cgl = nullptr) {
     v.ns.assign(maxnode, 0);
     v.bv.assign(maxnode, 0);
     v.xs.assign(maxnode, 0.0f);
@@ -289,17 +289,20 @@ static void expand_tree(TreeView& v, int maxnode, int maxcat, int nn, const int*
     std::memcpy(v.xs.data(), xs, sizeof(float) * nn);
     std::memcpy(v.tm.data(), tm, sizeof(int) * 2 * nn);
     std::memcpy(v.nc.data(), nc, sizeof(int) * nn);
+    if (cgl) std::memcpy(v.cgl.data(), cgl, sizeof(int) * (size_t)maxcat * nn);
 }
 
 // The per-tree analysis sequence of grow_tree_single (src/rf_random_forest.cpp:1043-1309)
 // for trees [t0, t1): testreebag, OOB votes, varimp, in-bag routing, proximity.
 // Accumulators follow the reference types: q float, nout int (incremented twice
 // per OOB tree as the reference does), qimp/qimpm/avimp/sqsd float.
-// prox: n*n FP64 column-major, or null to skip proximity.
+// prox: n*n FP64 column-major, or null to skip proximity.  catgoleft: maxcat
+// entries per node in the compact layout (tree t from offs[t] * maxcat), or
+// null for the all-zero table the reference's CPU grower leaves.
 extern "C" int rh_analyse_trees(const float* X, const int* y, const int* cat, int n, int p, int nclass,
                                 int maxcat, int t0, int t1, const long long* offs, const int* nnode,
                                 const int* nodestatus, const int* bestvar, const float* xbestsplit,
-                                const int* treemap, const int* nodeclass, const int* nin_all,
+                                const int* treemap, const int* nodeclass, const int* catgoleft, const int* nin_all,
                                 int do_imp, int impn,
                                 float* q, int* nout, float* qimp, float* qimpm, float* avimp, float* sqsd,
                                 double* prox, int* leaf_out) {
@@ -318,7 +321,7 @@ extern "C" int rh_analyse_trees(const float* X, const int* y, const int* cat, in
             const long long o = offs[t];
             const int nn = nnode[t];
             expand_tree(v, maxnode, maxcat, nn, nodestatus + o, bestvar + o, xbestsplit + o, treemap + 2 * o,
-                        nodeclass + o);
+                        nodeclass + o, catgoleft ? catgoleft + o * maxcat : nullptr);
             const int* nin = nin_all + (size_t)t * n;
             // cpu_bootstrap's own nout increment (src/rf_bootstrap.cpp:60-61)
             for (int i = 0; i < n; ++i) if (nin[i] == 0) nout[i]++;

@@ -121,7 +121,7 @@ def analyse_trees(X, y, forest, t0=0, t1=None, do_imp=True, impn=True, do_prox=F
     offs = np.ascontiguousarray(f.offs[:-1], dtype=np.int64)
     _check(lib().rh_analyse_trees(
         _p(X), _p(y), _p(f.cat), n, p, c, f.maxcat, t0, t1, _p(offs), _p(f.nnode), _p(f.nodestatus), _p(f.bestvar),
-        _p(f.xbestsplit), _p(f.treemap), _p(f.nodeclass), _p(f.nin), int(do_imp), int(impn),
+        _p(f.xbestsplit), _p(f.treemap), _p(f.nodeclass), _p(f.catgoleft), _p(f.nin), int(do_imp), int(impn),
         _p(state["q"]), _p(state["nout"]), _p(state["qimp"]), _p(state["qimpm"]), _p(state["avimp"]),
         _p(state["sqsd"]), _p(state["prox"]), _p(leaf)))
     if want_leaf:

@@ -108,3 +108,17 @@ def test_categorical_values_out_of_range(grown, value):
     rows = rng.choice(f.n, size=60, replace=False)
     X2[rows, rng.choice(catcols, size=60)] = np.float32(value)
     _compare(X2, y, f, threads=1)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_nonzero_catgoleft(grown, seed):
+    """Random go-left tables: the three walks index them differently
+    (testreebag by the truncated value, find_terminal_node by the 1-based
+    rounded value, testreeimp by the rounded value), and the oracle follows
+    each as the reference does."""
+    X, y, f = grown
+    g = f.subset(range(f.ntree))
+    rng = np.random.default_rng(seed)
+    g.catgoleft = rng.integers(0, 2, size=g.total_nodes * g.maxcat).astype(np.int32)
+    O, _ = _compare(X, y, g, threads=1)
+    assert O["S"].any()
