@@ -173,15 +173,16 @@ extern "C" int rh_fit_capture(const float* X, const int* y, const int* cat,
 
 // Reference predict / predict_proba on held-out rows, using a fitted forest
 // rebuilt from caller arrays (padded to maxnode = 2n+1 per tree).
-static void load_forest(rf::RandomForest& m, int T, int maxnode, const int* nnode,
+static void load_forest(rf::RandomForest& m, int T, int maxnode, int maxcat, const int* nnode,
                         const int* nodestatus, const int* bestvar, const float* xbestsplit,
-                        const int* treemap, const int* nodeclass) {
+                        const int* treemap, const int* nodeclass, const int* catgoleft) {
     for (int t = 0; t < T; ++t) m.nnode_[t] = nnode[t];
     std::memcpy(m.nodestatus_.data(), nodestatus, sizeof(int) * (size_t)T * maxnode);
     std::memcpy(m.bestvar_.data(), bestvar, sizeof(int) * (size_t)T * maxnode);
     std::memcpy(m.xbestsplit_.data(), xbestsplit, sizeof(float) * (size_t)T * maxnode);
     std::memcpy(m.treemap_.data(), treemap, sizeof(int) * (size_t)T * 2 * maxnode);
     std::memcpy(m.nodeclass_.data(), nodeclass, sizeof(int) * (size_t)T * maxnode);
+    if (catgoleft) std::memcpy(m.catgoleft_.data(), catgoleft, sizeof(int) * (size_t)T * maxnode * maxcat);
 }
 
 static rf::RandomForestConfig make_cfg(int n, int p, int nclass, int T, int maxcat) {
@@ -202,12 +203,13 @@ static rf::RandomForestConfig make_cfg(int n, int p, int nclass, int T, int maxc
 extern "C" int rh_predict(int n_train, int p, int nclass, int T, int maxcat, const int* cat,
                           const int* nnode, const int* nodestatus, const int* bestvar,
                           const float* xbestsplit, const int* treemap, const int* nodeclass,
-                          const float* Xtest, int m, int* pred, float* proba) {
+                          const int* catgoleft, const float* Xtest, int m, int* pred, float* proba) {
     try {
         rf::RandomForestConfig cfg = make_cfg(n_train, p, nclass, T, maxcat);
         rf::RandomForest model(cfg);
         model.set_categorical_features(cat, p);
-        load_forest(model, T, cfg.maxnode, nnode, nodestatus, bestvar, xbestsplit, treemap, nodeclass);
+        load_forest(model, T, cfg.maxnode, maxcat, nnode, nodestatus, bestvar, xbestsplit, treemap, nodeclass,
+                    catgoleft);
         model.predict_classification(Xtest, m, pred);
         model.predict_proba(Xtest, m, proba);
         return 0;

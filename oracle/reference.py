@@ -172,5 +172,6 @@ def predict(Xt, forest):
     proba = np.zeros(m * f.nclass, np.float32)
     _check(lib().rh_predict(n, f.p, f.nclass, T, f.maxcat, _p(f.cat), _p(f.nnode), _p(pad(f.nodestatus)),
                             _p(pad(f.bestvar)), _p(pad(f.xbestsplit)), _p(pad(f.treemap, 2)), _p(pad(f.nodeclass)),
+                            _p(None if f.catgoleft is None else pad(f.catgoleft, f.maxcat)),
                             _p(Xt), m, _p(pred), _p(proba)))
     return pred, proba.reshape(m, f.nclass)

@@ -122,3 +122,21 @@ def test_nonzero_catgoleft(grown, seed):
     g.catgoleft = rng.integers(0, 2, size=g.total_nodes * g.maxcat).astype(np.int32)
     O, _ = _compare(X, y, g, threads=1)
     assert O["S"].any()
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_predict_with_catgoleft_and_invalid_codes(grown, seed):
+    """predict / predict_proba through random go-left tables, with test codes
+    outside 1..cat (the reference votes 0 for those)."""
+    from oracle import oracle as orc, reference as ref
+
+    X, y, f = grown
+    g = f.subset(range(f.ntree))
+    rng = np.random.default_rng(seed)
+    g.catgoleft = rng.integers(0, 2, size=g.total_nodes * g.maxcat).astype(np.int32)
+    Xt = (X[:90] + rng.normal(0, 0.4, size=X[:90].shape)).astype(np.float32)
+    Xt[:, g.cat > 1] = np.round(Xt[:, g.cat > 1] * 2.0)  # codes -2..4, some outside 1..cat
+    _, pred, proba = orc.predict(Xt, g)
+    rp, rpr = ref.predict(Xt, g)
+    assert np.array_equal(pred, rp)
+    assert np.array_equal(proba, rpr)
