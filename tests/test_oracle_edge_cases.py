@@ -140,3 +140,21 @@ def test_predict_with_catgoleft_and_invalid_codes(grown, seed):
     rp, rpr = ref.predict(Xt, g)
     assert np.array_equal(pred, rp)
     assert np.array_equal(proba, rpr)
+
+
+def test_status2_nodes(grown):
+    """Created-but-unsplit nodes (status 2, children 0): testreebag stops on
+    them, find_terminal_node walks through them back to the root, and the
+    permuted walks of cpu_testreeimp pass through them without a vote (the
+    one-thread stale order, as above)."""
+    X, y, f = grown
+    g = f.subset(range(f.ntree))
+    rng = np.random.default_rng(4)
+    for t in range(g.ntree):
+        o = g.offs[t]
+        leaves = np.flatnonzero(g.nodestatus[o:g.offs[t + 1]] == -1)
+        pick = o + rng.choice(leaves, size=max(1, leaves.size // 4), replace=False)
+        g.nodestatus[pick] = 2
+        g.treemap[2 * pick] = 0
+        g.treemap[2 * pick + 1] = 0
+    _compare(X, y, g, threads=1)
