@@ -92,3 +92,12 @@ def test_no_device_fails_loudly(rfx):
     m = rfx.RandomForestClassifier(nsample=40, ntree=3, mdim=3, show_progress=False)
     with pytest.raises(RuntimeError, match="CUDA context"):
         m.fit(X, y)
+
+
+def test_package_reads_like_rfx(built):
+    """`import rfx_b200 as rfx` exposes the reference module's names."""
+    import rfx_b200 as rfx
+    from rfx_b200 import _rfx
+
+    for name in ("RandomForestClassifier", "confusion_matrix", "cuda_is_available", "TaskType"):
+        assert getattr(rfx, name) is getattr(_rfx, name)
