@@ -1,4 +1,6 @@
-// Permutation importance for all trees and all features in three launches.
+// Permutation importance for all trees and all features in four launches (with
+// more than 256 features the walk and the per-sample sums run once per block of
+// 256 features).
 //
 // cpu_varimp (src/rf_varimp.cpp:106-302) re-routes every OOB sample once per
 // used feature k, with x[pjoob[r]][k] in place of x[joob[r]][k], where pjoob is
