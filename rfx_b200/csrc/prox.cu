@@ -6,16 +6,20 @@
 // of the same leaf.  Here S = C + C^T is produced directly in its packed
 // upper-triangle form.
 //
-// Stage 1 (build_csr_kernel, one warp per tree): a stable counting sort of the
+// Stage 1 (build_csr_kernel, one CTA per tree): a stable counting sort of the
 //   tree's samples by key = 2*leaf + inbag.  seg[t][k] .. seg[t][k+1] is the
 //   member range of key k in memb[t*n ...], members ascending by sample id.
-//   A single warp walks the samples in order, so equal keys keep index order.
-// Stage 2 (pairs_row_kernel, row-owner): one CTA owns row i of S restricted to
-//   a column window; for every tree it binary-searches, in the member list of
-//   the opposite bag status of i's leaf, the members j in (i, window) and adds 1
-//   to a shared-memory accumulator per member; the accumulated row segment is
-//   then written once, coalesced.  Work is proportional to the pair updates,
-//   and S is written exactly once.
+//   The CTA counts and scans the keys; a single warp then places the samples
+//   in index order, so equal keys keep index order.
+// Stage 2, row-owner: one CTA owns row i of S; for every tree it takes, in the
+//   member list of the opposite bag status of i's leaf, the members j > i and
+//   adds 1 to a shared-memory counter per member; the accumulated row is then
+//   written once, coalesced.  Work is proportional to the pair updates, and S
+//   is written exactly once.  The full-row form (opp_kernel, row_order_kernel,
+//   pairs_row16_kernel: u16 counters for the whole row) is used when a row of
+//   counters fits in shared memory and ntree < 65536; otherwise the windowed
+//   form (pairs_row_kernel: u32 counters over a column window, binary searches
+//   per window) runs.
 #include "rfx_internal.cuh"
 
 #include <algorithm>
