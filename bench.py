@@ -14,9 +14,14 @@ metric = pair updates per second (sum over trees and leaves of
 #OOB x #in-bag members; counted exactly by the kernel) of that step.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--workload exact|lowrank|large|batch|rows]
 Under torchrun (N > 1) every rank runs an independent replica on its own GPU
 (the path needs no exchange between replicas); value is the sum over ranks,
-timed as the max over ranks.
+timed as the max over ranks.  The other workloads print their own line: the
+low-rank proximity + MDS in the mixed and the FP32 form (lowrank: n = 200,000;
+large: n = 1,000,000 with outlier scores), 64 uneven forests in one CUDA graph
+(batch), and the device time of finishprox, prediction and the full-matrix MDS
+(rows).
 """
 from __future__ import annotations
 
