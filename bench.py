@@ -76,26 +76,77 @@ def replica_reduce(x: float, op: str, device=None) -> float:
     return float(t.item())
 
 
-def make_forest(n, T, rank, ws, barrier):
-    """Data + forest; rank 0 grows, other ranks read its export."""
+def forest_cache_path(n, T):
+    """Where the bench forest of (n, T) is kept between the two arms' runs."""
+    from rfx_b200 import synth
+
+    return os.path.join(tempfile.gettempdir(),
+                        f"rfx_bench_forest_n{n}_t{T}_mtry{MTRY}_seed{synth.SEED_BASE + 2}_v1.npz")
+
+
+def grow_forest_file(n, T, path):
+    """Grow the bench forest with the library's grower and save it (run in a
+    child process by `cached_forest`)."""
     from rfx_b200 import abi, synth
-    from rfx_b200.forest import Forest
 
     X, y = synth.mixed_cover(n)
     cat = synth.detect_categorical(X)
-    path = os.path.join(tempfile.gettempdir(), f"rfx_bench_forest_{n}_{T}_{os.getpid() if ws == 1 else 'dist'}.npz")
+    f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    f.save(tmp)
+    os.replace(tmp, path)
+
+
+def cached_forest(n, T):
+    """Data + forest of the exact workload, identical in both arms.
+
+    The forest is grown once per (n, T) by a child process (the library's
+    restatement of the reference grower) and read back here with the
+    numpy-only loader, so this process maps no native library for it: the
+    reference arm's timed process then runs only the reference's code and
+    the oracle.  Returns (X, y, forest, seconds spent obtaining it)."""
+    from rfx_b200 import synth
+    from rfx_b200.forest import Forest
+
+    X, y = synth.mixed_cover(n)
+    path = forest_cache_path(n, T)
+    t0 = time.time()
+    f = None
+    if os.path.exists(path):
+        try:
+            f = Forest.load(path)
+            if f.n != n or f.ntree != T:
+                f = None
+        except Exception:
+            f = None
+    if f is None:
+        subprocess.run([sys.executable, os.path.abspath(__file__), "--grow-forest", path, "--n", str(n),
+                        "--trees", str(T)], check=True)
+        f = Forest.load(path)
+    return X, y, f, time.time() - t0
+
+
+def make_forest(n, T, rank, ws, barrier):
+    """Data + forest; rank 0 obtains it (grown once, kept on disk), the other
+    ranks read the same file after a barrier."""
+    from rfx_b200 import synth
+    from rfx_b200.forest import Forest
+
     t0 = time.time()
     if rank == 0:
-        f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
-        if ws > 1:
-            f.save(path)
+        X, y, f, _ = cached_forest(n, T)
     barrier()
     if rank != 0:
-        f = Forest.load(path)
+        X, y = synth.mixed_cover(n)
+        f = Forest.load(forest_cache_path(n, T))
     barrier()
-    if rank == 0 and ws > 1 and os.path.exists(path):
-        os.remove(path)
     return X, y, f, time.time() - t0
+
+
+def exact_config(n, p, T, U):
+    """The `config` of the exact workload, printed identically by both arms."""
+    return {"workload": WORKLOAD.format(n=n, T=T), "n": n, "p": p, "ntree": T, "pair_updates_per_step": int(U),
+            "l2": "inputs larger than L2 (S 5.0 GB written per step; nodes and leaf keys > 126 MB)"}
 
 
 class Clocks:
@@ -151,24 +202,29 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def forest_pair_updates(X, y, f):
-    """Pair updates of the whole forest (the metric's unit count) on the CPU:
-    per tree, the sum over terminal nodes of OOB members x in-bag members,
-    from the oracle's leaf ids (OOB rows by testreebag, in-bag rows by
+def tree_pair_updates(X, y, f):
+    """Pair updates of every tree (the metric's unit count) on the CPU: per
+    tree, the sum over terminal nodes of OOB members x in-bag members, from
+    the oracle's leaf ids (OOB rows by testreebag, in-bag rows by
     find_terminal_node; rows that end on a non-terminal node count nowhere,
     as in cpu_proximity's dense branch, src/rf_proximity.cpp:108-231)."""
     from oracle import oracle as orc
 
     leaf = orc.analyse(X, y, f, do_imp=False, impn=False, do_prox=False, want_leaf=True)["leaf"]
-    U = 0
+    U = np.zeros(f.ntree, np.int64)
     for t in range(f.ntree):
         lf = leaf[t].astype(np.int64)
         term = f.nodestatus[f.offs[t]: f.offs[t + 1]][lf] == -1
         inb = f.nin[t] > 0
         no = np.bincount(lf[term & ~inb], minlength=int(f.nnode[t]))
         ni = np.bincount(lf[term & inb], minlength=int(f.nnode[t]))
-        U += int(no @ ni)
+        U[t] = int(no @ ni)
     return U
+
+
+def forest_pair_updates(X, y, f):
+    """Pair updates of the whole forest (see tree_pair_updates)."""
+    return int(tree_pair_updates(X, y, f).sum())
 
 
 class CpuTrees:
@@ -234,37 +290,51 @@ def cpu_baseline_run(X, y, f, budget_s=15.0, min_trees=2, pair_updates=None):
 
 
 def run_reference(args):
-    """The reference arm: each step is one tree of the forest (seeded random
-    order) through the reference's CPU path on all host cores; the rate is the
-    forest's pair updates per tree over the mean step time."""
+    """The reference arm: the reference's own CPU path (CpuTrees) on all host
+    cores over the same forest as the repository arm.
+
+    The forest's trees are taken in a seeded random order and dealt out in
+    equal blocks over the warm-up and timed steps, so that the timed steps
+    together cover most of the forest once (about 150 s at n = 50,000 on 16
+    cores); a step is one block.  Rate = the timed trees' exact pair updates
+    over their summed wall time.  This process loads only the reference's
+    build (oracle/_ref) and the oracle: the forest comes from `cached_forest`
+    (a child process grows it when it is not on disk yet)."""
     ws, rank, local = dist_env()
     if rank != 0:
         return 0
-    from rfx_b200 import abi, synth
-
     n, T = args.n, args.trees
-    X, y = synth.mixed_cover(n)
-    cat = synth.detect_categorical(X)
-    f = abi.grow_forest(X, y, T, MTRY, 1, cat=cat, nclass=7)
-    U = forest_pair_updates(X, y, f)
+    X, y, f, _ = cached_forest(n, T)
+    Ut = tree_pair_updates(X, y, f)
+    U = int(Ut.sum())
     run = CpuTrees(X, y, f)
-    t_tot = 0.0
-    for s in range(args.warmup + args.steps):
-        dt = run.tree_seconds(s)
+    nsteps = args.warmup + args.steps
+    block = max(1, T // nsteps)
+    t_tot, u_tot, trees = 0.0, 0, 0
+    for s in range(nsteps):
+        dt, du = 0.0, 0
+        for k in range(s * block, (s + 1) * block):
+            dt += run.tree_seconds(k)
+            du += int(Ut[run.order[k % T]])
         if s >= args.warmup:
             t_tot += dt
-    value = (U / T) * args.steps / t_tot
+            u_tot += du
+            trees += block
+    value = u_tot / t_tot
+    cores = run.cores if run.kind == "reference" else 1
     line = {"metric": "prox pair-updates/s", "value": value, "unit": "pair-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD.format(n=n, T=T), "n": n, "ntree": T,
-                       "pair_updates_per_forest": U, "parallelism": "host cores (OpenMP)"},
-            "cpu_baseline": {"value": value, "unit": "pair-updates/s",
-                             "cores": run.cores if run.kind == "reference" else 1, "kind": run.kind,
-                             "sample": f"each step = 1 tree of the {T}-tree forest at n={n} (seeded random "
-                                       "order; reference per-tree sequence, pair counts by the dense-branch "
-                                       "restatement); rate = the forest's pair updates per tree / mean step time"},
+            "data": "synthetic (seeded mixed-type cover-shaped generator; forest grown by the library's "
+                    "restatement of the reference grower)",
+            "impl": "reference", "config": exact_config(n, f.p, T, U),
+            "parallelism": f"host cores (OpenMP, {cores} threads)",
+            "cpu_baseline": {"value": value, "unit": "pair-updates/s", "cores": cores, "kind": run.kind,
+                             "sample": f"{trees} of the {T} trees (seeded random order, {block} per step) at n={n}: "
+                                       "testreebag + votes + cpu_varimp over all features + find_terminal_node "
+                                       "(the reference's own build) + dense-branch pair counts into one "
+                                       "upper-triangle array; rate = those trees' exact pair updates "
+                                       f"({u_tot}) / their summed time ({t_tot:.1f} s)"},
             "e2e": {"value": value, "unit": "pair-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -601,7 +671,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="exact", choices=["exact", "lowrank", "large", "batch", "rows"])
     ap.add_argument("--forests", type=int, default=64, help="forests in the batch workload")
+    ap.add_argument("--grow-forest", default=None, metavar="PATH",
+                    help="grow the exact workload's forest and save it to PATH (used by the forest cache)")
     args = ap.parse_args()
+    if args.grow_forest:
+        grow_forest_file(args.n or N_SAMPLES, args.trees or N_TREES, args.grow_forest)
+        return 0
     if args.workload in ("lowrank", "large"):
         return run_lowrank(args)
     if args.workload == "batch":
@@ -713,10 +788,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded mixed-type cover-shaped generator; forest grown by the library's "
                     "restatement of the reference grower)",
-            "config": {"workload": WORKLOAD.format(n=n, T=T), "n": n, "p": p, "ntree": T, "pair_updates_per_step": U,
-                       "l2": "inputs larger than L2 (S 5.0 GB written per step; nodes and leaf keys > 126 MB)",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "forest_grow_s": round(grow_s, 2)},
+            "config": exact_config(n, p, T, U),
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU", "forest_obtain_s": round(grow_s, 2),
             "roofline": roofline, "gpu_launches": gpu_launches,
             "breakdown_ms": {k: round(v, 4) for k, v in kernels.items()},
             "tuned_shapes": abi.tuned_shapes()}

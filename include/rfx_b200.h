@@ -267,16 +267,24 @@ rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count);
  *                  nodes numbered 0.. in node order), or -1 to leave it out;
  *   inbag[t*n + i] nonzero when sample i is in-bag in tree t;
  *   S[len]         output, len = n(n+1)/2.
- * All three must be device memory; the work runs on `stream` (a cudaStream_t,
- * NULL = default stream) and the call returns when it has finished.  It calls
- * no cudaMalloc, cudaFree or allocating library routine: its temporaries live
- * in one fixed array of about 26 MB inside the library, which every GPU that
- * loads the library holds until the process exits.  Limits: n <= 32768,
- * ntree <= 65535, ntree * n <= 1048576, 1 <= max_leaves <= n; larger inputs are
- * rejected with RFX_ERR_INVALID.  The first call on a device looks up that
- * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Every call uses the same array, so calls whose work
- * overlaps on a GPU race with each other: serialise them. */
+ * All three must be device memory of the current device; the work runs on
+ * `stream` (a cudaStream_t, NULL = default stream) and the call waits for that
+ * stream before it returns.  It calls no cudaMalloc, cudaFree or allocating
+ * library routine: its temporaries live in one fixed array of about 26 MB
+ * inside the library.  CUDA creates that array, and loads the kernels' code,
+ * on a device when the library is first used there (lazy module loading, the
+ * default since CUDA 12.2), so the FIRST call on each device is where that
+ * device memory is taken: a caller that reserves the GPU's memory for its own
+ * arena should make one call per device before it reserves the rest (or set
+ * CUDA_MODULE_LOADING=EAGER); the device then holds the array until its
+ * context is destroyed.  The first call on a device (and the first after the
+ * device's context was reset) also looks up the array's device address with
+ * cudaGetSymbolAddress, and should come before any stream capture.  Limits:
+ * n <= 32768, ntree <= 65535, ntree * n <= 1048576, 1 <= max_leaves <= n; larger
+ * inputs are rejected with RFX_ERR_INVALID, as is a leaf index >= max_leaves
+ * (those samples are left out of S).  Every call uses the same array and it
+ * keeps the last call's contents, so calls whose work overlaps on a GPU race
+ * with each other: serialise them. */
 rfx_status rfx_pair_counts_noalloc(const int32_t* leaf, const uint8_t* inbag, int32_t n, int32_t ntree,
                                    int32_t max_leaves, int32_t* S, size_t len, void* stream);
 

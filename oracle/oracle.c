@@ -429,6 +429,55 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
     return 0;
 }
 
+/* ------------------------------------------------------------------------ */
+/* cpu_proximity's dense branch (src/rf_proximity.cpp:108-231) from leaf      */
+/* indices the caller supplies instead of routing a forest: per tree t,        */
+/* leaf[t*n+i] is sample i's terminal index (0..max_leaves-1, the nod[] map    */
+/* of :108-115 already applied) or -1 to leave it out, and inbag[t*n+i] its    */
+/* bag flag.  Members of a leaf are bucketed stable by sample index (:116-140)*/
+/* and every OOB i adds 1 for every in-bag kk of its leaf (:173-230), into    */
+/* S[min][max] of the packed upper triangle.  Indices >= max_leaves are left  */
+/* out and counted in the return value.                                        */
+/* ------------------------------------------------------------------------ */
+int64_t orc_pairs_from_leaves(int n, int T, int max_leaves, const int32_t* leaf, const uint8_t* inbag,
+                              int32_t* S) {
+    int32_t* ncount = (int32_t*)malloc(sizeof(int32_t) * (size_t)(max_leaves + 1));
+    int32_t* ndbegin = (int32_t*)malloc(sizeof(int32_t) * (size_t)(max_leaves + 1));
+    int32_t* npcase = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+    int64_t bad = 0;
+    for (int t = 0; t < T; ++t) {
+        const int32_t* lf = leaf + (size_t)t * n;
+        const uint8_t* ib = inbag + (size_t)t * n;
+        for (int k = 0; k <= max_leaves; ++k) ncount[k] = 0;
+        for (int i = 0; i < n; ++i) {
+            if (lf[i] >= max_leaves) bad++;
+            else if (lf[i] >= 0) ncount[lf[i]]++;
+        }
+        ndbegin[0] = 0;
+        for (int k = 1; k <= max_leaves; ++k) ndbegin[k] = ndbegin[k - 1] + ncount[k - 1];
+        for (int k = 0; k < max_leaves; ++k) ncount[k] = 0;
+        for (int i = 0; i < n; ++i) {
+            const int k = lf[i];
+            if (k >= 0 && k < max_leaves) npcase[ndbegin[k] + ncount[k]++] = i;
+        }
+        for (int i = 0; i < n; ++i) {
+            const int k = lf[i];
+            if (ib[i] || k < 0 || k >= max_leaves) continue;
+            for (int jj = ndbegin[k]; jj < ndbegin[k + 1]; ++jj) {
+                const int kk = npcase[jj];
+                if (ib[kk]) {
+                    const int a = i < kk ? i : kk, b = i < kk ? kk : i;
+                    S[upidx(n, a, b)] += 1;
+                }
+            }
+        }
+    }
+    free(ncount);
+    free(ndbegin);
+    free(npcase);
+    return bad;
+}
+
 /* OOB error / predictions / probabilities from raw votes                    */
 /* (compute_classification_error :2413-2462, compute_oob_predictions          */
 /* :2246-2301; argmax with >=, so ties go to the higher class).               */

@@ -84,6 +84,21 @@ def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False,
     return out
 
 
+def pairs_from_leaves(leaf, inbag, max_leaves):
+    """Pair counts (packed upper triangle, int32) from per-(tree, sample)
+    terminal indices and bag flags: cpu_proximity's dense branch without the
+    routing (see orc_pairs_from_leaves).  Returns (S, number of indices
+    >= max_leaves that were left out)."""
+    leaf = np.ascontiguousarray(leaf, dtype=np.int32)
+    inbag = np.ascontiguousarray(inbag != 0, dtype=np.uint8)
+    T, n = leaf.shape
+    S = np.zeros(n * (n + 1) // 2, np.int32)
+    f = lib().orc_pairs_from_leaves
+    f.restype = ctypes.c_int64
+    bad = f(ctypes.c_int(n), ctypes.c_int(T), ctypes.c_int(max_leaves), _p(leaf), _p(inbag), _p(S))
+    return S, int(bad)
+
+
 def oob_summary(q_raw, nout, y):
     n, c = q_raw.shape
     err = ctypes.c_float(0)

@@ -1,7 +1,7 @@
 """ctypes front-end of oracle/_ref/librfxref.so — the reference's own CPU code.
 
 Test infrastructure only (tests/, smoke(), bench.py's reference arm).  The
-library is built by ``make -f oracle/Makefile ref`` from the reference's
+library is built by ``make -f oracle/Makefile REF_DIR=<reference checkout> ref`` from the reference's
 sources where they lie; it is absent when the reference tree was not available
 at build time, in which case ``available()`` is False.
 """

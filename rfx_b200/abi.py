@@ -1,6 +1,6 @@
 """ctypes binding of the C ABI (include/rfx_b200.h) — the call path the parity
-tests and bench.py use.  It mirrors the ctypes stub a reference maintainer
-would add.
+tests and bench.py use.  It is the kind of ctypes stub a maintainer of the
+reference would add to call the library from Python.
 
 Device outputs may be given as torch CUDA tensors (or raw device addresses);
 host outputs as numpy arrays.  There is no CPU fallback: if the library or a

@@ -8,8 +8,18 @@
 // them rfx_pair_counts_noalloc computes the same packed upper-triangle pair
 // counts as rfx_proximity_upper_i32, from per-(tree, sample) leaf indices the
 // caller already holds on the device, and keeps all of its temporary data in
-// one fixed-size array defined in this file (a __device__ variable, so every
-// GPU that loads the library reserves it until the process exits).
+// one fixed-size array defined in this file (a __device__ variable).
+//
+// CUDA loads a module's code and its __device__ variables into a device's
+// context when the module is first used there (lazy module loading, the
+// default since CUDA 12.2), not when the library is opened.  The first call
+// on each device is that first use: it looks up the array's device address
+// and launches the kernels for the first time, and that is when the array and
+// the kernels' code take their device memory.  A caller that reserves the
+// GPU's memory up front should therefore make one call per device before it
+// reserves the rest (or run with CUDA_MODULE_LOADING=EAGER, which loads
+// everything when the context is created); from then on the device holds the
+// array until the context is destroyed and calls allocate nothing.
 #include <mutex>
 
 #include "rfx_internal.cuh"
@@ -38,7 +48,52 @@ static __device__ __align__(256) int32_t g_noalloc_scratch[NA_WORDS];
 
 constexpr int NA_MAX_DEVICES = 64;
 std::mutex g_na_mutex;
+// Per device: the scratch array's device address and the id of the context it
+// was looked up in.  A context destroyed and created again (cudaDeviceReset)
+// gets a new id, so the address is looked up again instead of reusing a stale
+// one.
 int32_t* g_na_addr[NA_MAX_DEVICES] = {};
+unsigned long long g_na_ctx[NA_MAX_DEVICES] = {};
+
+// Current context id through the driver entry points (cuCtxGetCurrent and
+// cuCtxGetId, CUDA 12.0+), fetched once; 0 when they are unavailable, in which
+// case the address is looked up on every call.
+typedef int (*na_ctx_get_current_t)(void**);
+typedef int (*na_ctx_get_id_t)(void*, unsigned long long*);
+
+unsigned long long current_ctx_id() {
+    static na_ctx_get_current_t get_cur = nullptr;
+    static na_ctx_get_id_t get_id = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0 = cudaDriverEntryPointSymbolNotFound, q1 = q0;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q0 == cudaDriverEntryPointSuccess && q1 == cudaDriverEntryPointSuccess) {
+            get_cur = reinterpret_cast<na_ctx_get_current_t>(f0);
+            get_id = reinterpret_cast<na_ctx_get_id_t>(f1);
+        }
+        cudaGetLastError();
+    }
+    if (!get_cur || !get_id) return 0;
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// True when p is device memory of device `dev` (managed memory counts).
+bool on_device(const void* p, int dev) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice && a.device == dev) || a.type == cudaMemoryTypeManaged;
+}
 
 __global__ void na_keys_kernel(const int32_t* __restrict__ leaf, const uint8_t* __restrict__ inbag, int64_t cells,
                                int max_leaves, int32_t* __restrict__ key, uint32_t* __restrict__ err) {
@@ -82,26 +137,29 @@ extern "C" rfx_status rfx_pair_counts_noalloc(const int32_t* leaf, const uint8_t
         set_error("rfx_pair_counts_noalloc: S must hold n(n+1)/2 entries");
         return RFX_ERR_INVALID;
     }
-    if (!is_device_ptr(leaf) || !is_device_ptr(inbag) || !is_device_ptr(S)) {
-        set_error("rfx_pair_counts_noalloc: leaf, inbag and S must be device memory");
-        return RFX_ERR_INVALID;
-    }
     int dev = 0;
     RFX_CUDA(cudaGetDevice(&dev));
+    if (!on_device(leaf, dev) || !on_device(inbag, dev) || !on_device(S, dev)) {
+        set_error("rfx_pair_counts_noalloc: leaf, inbag and S must be device memory of the current device");
+        return RFX_ERR_INVALID;
+    }
     if (dev < 0 || dev >= NA_MAX_DEVICES) {
         set_error("rfx_pair_counts_noalloc: device ordinal beyond the address table");
         return RFX_ERR_UNSUPPORTED;
     }
     int32_t* base = nullptr;
     {
-        // first call on this device: look up the device address of the
-        // scratch array (host code cannot use the symbol itself)
+        // set-up, once per device and context: look up the device address of
+        // the scratch array with this device current (host code cannot use
+        // the symbol itself; it names a host-side stand-in)
         std::lock_guard<std::mutex> lk(g_na_mutex);
-        if (!g_na_addr[dev]) {
+        const unsigned long long cid = current_ctx_id();
+        if (!g_na_addr[dev] || cid == 0 || cid != g_na_ctx[dev]) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess) return cuda_fail(e, "rfx_pair_counts_noalloc: cudaGetSymbolAddress");
             g_na_addr[dev] = static_cast<int32_t*>(p);
+            g_na_ctx[dev] = cid;
         }
         base = g_na_addr[dev];
     }

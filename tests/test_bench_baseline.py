@@ -66,3 +66,27 @@ def test_reference_arm_prints_the_contract_line(built):
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
     assert "workload" in d["config"]
+
+
+def test_reference_arm_maps_no_library_of_this_package(built):
+    """The reference arm's process runs the reference's build and the oracle
+    only: the forest comes from a child process through the numpy loader, so
+    librfx_b200.so is never mapped into it; both arms print the same config."""
+    import json
+    import subprocess
+
+    code = ("import sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--n', '500', '--trees', '6', "
+            "'--steps', '2', '--warmup', '3']; sys.path.insert(0, %r); import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'maps_rfx': 'librfx_b200' in maps, 'maps_pyrfx': '_rfx.' in maps}))" % ROOT)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    line, maps = lines[0], lines[-1]
+    assert maps == {"maps_rfx": False, "maps_pyrfx": False}
+    sys.path.insert(0, ROOT)
+    import bench
+
+    X, y, f, _ = bench.cached_forest(500, 6)
+    U = bench.forest_pair_updates(X, y, f)
+    assert line["config"] == json.loads(json.dumps(bench.exact_config(500, f.p, 6, U)))
