@@ -94,6 +94,39 @@ rfx_status rfx_synchronize(rfx_ctx* ctx);
  * same shape reuses the context's device buffers. */
 rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* view);
 
+/* A forest left in device memory by a GPU grower, in the reference's padded
+ * layout: tree t owns slots [t*maxnode, t*maxnode + nnode[t]) of nodestatus,
+ * bestvar, xbestsplit and nodeclass, 2*maxnode slots per tree of treemap and
+ * maxnode*maxcat of catgoleft (NULL = all zero); nin is ntree x n, X n x p
+ * row-major, y n labels, cat p feature kinds.  nnode is a HOST array of
+ * ntree node counts (the reference keeps nnode_all on the host); every other
+ * array is device memory of the context's device. */
+typedef struct rfx_forest_device_view {
+    int32_t n, p, nclass, maxcat, ntree, maxnode;
+    const int32_t* nnode;       /* host, ntree */
+    const int32_t* nodestatus;  /* device, ntree * maxnode */
+    const int32_t* bestvar;     /* device, ntree * maxnode */
+    const float* xbestsplit;    /* device, ntree * maxnode */
+    const int32_t* treemap;     /* device, ntree * 2 * maxnode */
+    const int32_t* nodeclass;   /* device, ntree * maxnode */
+    const int32_t* catgoleft;   /* device, ntree * maxnode * maxcat, or NULL */
+    const int32_t* nin;         /* device, ntree * n */
+    const float* X;             /* device, n * p */
+    const int32_t* y;           /* device, n */
+    const int32_t* cat;         /* device, p */
+} rfx_forest_device_view;
+
+/* Load a device-resident forest without a round trip through the host: the
+ * hand-off from the reference's GPU grower (gpu_growtree_batch,
+ * cuda/rf_growtree.cu:888 and :2706-2771, whose node arrays stay on the device
+ * with tree_offset = tree_id * maxnode) to the analysis path.  The trees are
+ * gathered into the compact layout on the device (device-to-device copies and
+ * one gather kernel), then validated and packed exactly as rfx_forest_load
+ * does; the labels and feature kinds are read back (n + p ints) for the
+ * host-side checks.  Results are identical to loading the same forest from
+ * host arrays. */
+rfx_status rfx_forest_load_device(rfx_ctx* ctx, const rfx_forest_device_view* view);
+
 /* OOB routing + votes: cpu_testreebag (src/rf_testreebag.cpp:13-125) and the
  * vote loop of grow_tree_single (src/rf_random_forest.cpp:1107-1153) over all
  * trees.  q[n*nclass] receives integer vote counts; nout[n] the reference's
@@ -181,9 +214,15 @@ typedef struct rfx_lowrank_opts {
 rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* opts, float* A, float* evals);
 
 /* Quantised factors with one scale per column (format 1: INT8, q = round(A/s),
- * s = max|A[:,c]|/127; format 2: FP8 e4m3, s = max|A[:,c]|/448).  q is n x rank
- * bytes, scales rank floats (either may be NULL).  The reference quantises with
- * one per-tensor scale (cuda/rf_quantization_kernels.cu:107-120). */
+ * s = max|A[:,c]|/127; format 2: FP8 e4m3, s = max|A[:,c]|/448; format 3:
+ * NF4, the reference's 16-level code of A/s with s = max|A[:,c]|, two codes
+ * per byte over the row-major entries, the lower nibble first; format 4: FP16
+ * with scales 1).  q is n x rank bytes (NF4: ceil(n x rank / 2), FP16:
+ * 2 x n x rank), scales
+ * rank floats (either may be NULL).  The reference quantises INT8 with one
+ * per-tensor scale (cuda/rf_quantization_kernels.cu:107-120), NF4 without a
+ * scale (cuda/rf_proximity_lowrank.cu:353-411) and FP16 without a scale; the
+ * factors of P ~= I + A A^T are what is quantised. */
 rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales);
 
 /* k-dimensional classical MDS from the factors (compute_mds_from_factors,
@@ -296,8 +335,10 @@ rfx_status rfx_pair_counts_noalloc(const int32_t* leaf, const uint8_t* inbag, in
  * created.  Stage order: route, leaf lists, pair counts,
  * finishprox, varimp per-tree, varimp per-sample, varimp per-feature, predict,
  * oob summary, localimp, pair-range table, low-rank operator product,
- * low-rank orthonormalisation, MDS from factors, full-matrix MDS. */
-enum { RFX_NUM_STAGES = 15 };
+ * low-rank orthonormalisation, MDS from factors, full-matrix MDS, hub-leaf
+ * pair counts on the tensor cores (the pair counts of one call are the hub
+ * stage plus the pair-count stage). */
+enum { RFX_NUM_STAGES = 16 };
 rfx_status rfx_profile_enable(rfx_ctx* ctx, int enable);
 rfx_status rfx_profile_read(rfx_ctx* ctx, float* stage_ms, int64_t* kernel_launches);
 

@@ -206,6 +206,31 @@ static int route_testreeimp(const float* xrow, const float* xperm, int mr, int p
     return 0;
 }
 
+/* The in-bag walk of grow_tree_single's casewise tnodewt block
+ * (src/rf_random_forest.cpp:1052-1095): categorical splits take
+ * idx = (int)(x + 0.5f) and go left iff 0 <= idx < maxcat and the go-left
+ * table says 1 (otherwise right); numeric splits go left iff x <= split; the
+ * walk runs while the node status is 1 and stops at a child outside
+ * [0, nnode).  Returns the node reached (checked by the caller).            */
+static int route_tnodewt(const float* xrow, int p, const int32_t* ns, const int32_t* bv, const float* xs,
+                         const int32_t* tm, const int32_t* cat, const int32_t* cgl, int maxcat, int nnode) {
+    int cur = 0;
+    while (ns[cur] == 1) {
+        int m = bv[cur];
+        int numcat = (cat == NULL || m >= p) ? 1 : cat[m];
+        int left;
+        if (numcat > 1) {
+            int idx = (int)(xrow[m] + 0.5f);
+            left = (idx >= 0 && idx < maxcat && cgl != NULL && cgl[(size_t)cur * maxcat + idx] == 1);
+        } else {
+            left = xrow[m] <= xs[cur];
+        }
+        cur = tm[2 * cur + (left ? 0 : 1)];
+        if (cur < 0 || cur >= nnode) break;
+    }
+    return cur;
+}
+
 /* Predict traversal (src/rf_random_forest.cpp:1959-2013): returns the voted
  * class (0 on every invalid path), as predict_classification counts it.     */
 static int route_predict(const float* xrow, int p, int nclass, const int32_t* ns, const int32_t* bv,
@@ -269,9 +294,9 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
                 int T, const int64_t* offs, const int32_t* nnode, const int32_t* nodestatus,
                 const int32_t* bestvar, const float* xbestsplit, const int32_t* treemap,
                 const int32_t* nodeclass, const int32_t* catgoleft, const int32_t* nin_all,
-                int do_imp, int impn, int do_prox,
+                int do_imp, int impn, int do_prox, int casewise,
                 float* q_raw, int32_t* nout, float* qimp, float* qimpm, float* avimp, float* sqsd,
-                int32_t* S, int32_t* leaf, int32_t* jtr_out, int32_t* perm_bad) {
+                int32_t* S, double* Cw, int32_t* leaf, int32_t* jtr_out, int32_t* perm_bad) {
     const int maxnode = 2 * n + 1;
     int32_t* jtr = (int32_t*)calloc((size_t)n, sizeof(int32_t));
     int32_t* nodextr = (int32_t*)calloc((size_t)n, sizeof(int32_t));
@@ -286,6 +311,10 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
     int32_t* npcase = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
     float* qimpm_t = (float*)malloc(sizeof(float) * (size_t)n * p);
     int32_t* iv = (int32_t*)malloc(sizeof(int32_t) * (size_t)p);
+    int32_t* nodexvr = (int32_t*)calloc((size_t)n, sizeof(int32_t));
+    float* tnodewt = (float*)calloc((size_t)maxnode, sizeof(float));
+    float* wsum = (float*)malloc(sizeof(float) * (size_t)maxnode);
+    int32_t* wcnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)maxnode);
     if (perm_bad) *perm_bad = 0;
 
     for (int t = 0; t < T; ++t) {
@@ -310,32 +339,62 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
             nodextr[i] = route_testreebag(X + (size_t)i * p, p, ns, bv, xs, tm, nc, nn, cat, cgl, maxcat, &c);
             jtr[i] = c;
         }
-        /* OOB votes and the two nout increments */
+        /* casewise: tnodewt = mean bootstrap multiplicity of the in-bag
+         * samples that reach each terminal node (src/rf_random_forest.cpp:
+         * 1049-1102); 0 for every other node */
+        if (casewise) {
+            for (int k = 0; k < maxnode; ++k) {
+                tnodewt[k] = 0.0f;
+                wsum[k] = 0.0f;
+                wcnt[k] = 0;
+            }
+            for (int i = 0; i < n; ++i) {
+                if (nin[i] <= 0) continue;
+                int nd = route_tnodewt(X + (size_t)i * p, p, ns, bv, xs, tm, cat, cgl, maxcat, nn);
+                if (nd >= 0 && nd < nn && ns[nd] == -1) {
+                    wsum[nd] += (float)nin[i];
+                    wcnt[nd]++;
+                }
+            }
+            for (int k = 0; k < nn; ++k)
+                if (wcnt[k] > 0) tnodewt[k] = wsum[k] / (float)wcnt[k];
+        }
+        /* OOB votes (weight tnodewt[nodextr] when casewise, :1107-1153) and
+         * the two nout increments */
         for (int i = 0; i < n; ++i) {
             if (nin[i] != 0) continue;
             if (nout) nout[i] += 2;
-            if (q_raw && jtr[i] >= 0 && jtr[i] < nclass) q_raw[(size_t)i * nclass + jtr[i]] += 1.0f;
+            if (q_raw && jtr[i] >= 0 && jtr[i] < nclass) {
+                float w = 1.0f;
+                if (casewise && nodextr[i] >= 0 && nodextr[i] < nn) w = tnodewt[nodextr[i]];
+                q_raw[(size_t)i * nclass + jtr[i]] += w;
+            }
         }
         if (jtr_out) memcpy(jtr_out + (size_t)t * n, jtr, sizeof(int32_t) * (size_t)n);
 
         /* cpu_varimp (src/rf_varimp.cpp:106-302), non-casewise */
         if (do_imp) {
+            /* weight of an OOB vote that lands on node nd (src/rf_varimp.cpp:
+             * 138-148, 203-217): tnodewt[nd] when casewise and nd is a node
+             * of the tree, else 1 */
+#define ORC_W(nd) ((casewise && (nd) >= 0 && (nd) < nn) ? tnodewt[(nd)] : 1.0f)
             int noob = 0;
             float right = 0.0f;
             for (int i = 0; i < n; ++i) {
                 if (nin[i] == 0) {
-                    if (jtr[i] == y[i]) right += 1.0f;
+                    if (jtr[i] == y[i]) right += ORC_W(nodextr[i]);
                     joob[noob++] = i;
                 }
             }
             const float fnoob = (float)noob;
-            /* jvr is a fresh zero vector per cpu_varimp call */
+            /* jvr and nodexvr are fresh zero vectors per cpu_varimp call */
             memset(jvr, 0, sizeof(int32_t) * (size_t)n);
+            memset(nodexvr, 0, sizeof(int32_t) * (size_t)n);
             if (impn == 1) {
                 for (int r = 0; r < noob; ++r) {
                     int i = joob[r];
-                    /* qimp_temp[i] = 0 + 1/noob, then qimp_[i] += qimp_temp[i] */
-                    if (jtr[i] == y[i]) qimp[i] += 0.0f + 1.0f / fnoob;
+                    /* qimp_temp[i] = 0 + w/noob, then qimp_[i] += qimp_temp[i] */
+                    if (jtr[i] == y[i]) qimp[i] += 0.0f + ORC_W(nodextr[i]) / fnoob;
                 }
             }
             for (int k = 0; k < p; ++k) iv[k] = 0;
@@ -353,12 +412,16 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
                         int ip = joob[perm[r]];
                         int32_t c, node;
                         if (route_testreeimp(X + (size_t)i * p, X + (size_t)ip * p, k, p, ns, bv, xs, tm, nc,
-                                             nnv, cat, cgl, maxcat, &c, &node))
+                                             nnv, cat, cgl, maxcat, &c, &node)) {
                             jvr[r] = c;
-                        /* else: jvr[r] keeps its previous (stale) value, as in the reference */
+                            nodexvr[r] = node;
+                        }
+                        /* else: jvr[r] and nodexvr[r] keep their previous (stale)
+                         * values, as in the reference */
                         if (jvr[r] == y[i]) {
-                            if (impn == 1) qimpm_t[(size_t)i * p + k] += 1.0f / fnoob;
-                            rightimp += 1.0f;
+                            const float w = ORC_W(nodexvr[r]);
+                            if (impn == 1) qimpm_t[(size_t)i * p + k] += w / fnoob;
+                            rightimp += w;
                         }
                     }
                     rr = (right - rightimp) / fnoob;
@@ -368,22 +431,23 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
                 } else if (impn == 1) {
                     for (int r = 0; r < noob; ++r) {
                         int i = joob[r];
-                        if (jtr[i] == y[i]) qimpm_t[(size_t)i * p + k] += 1.0f / fnoob;
+                        if (jtr[i] == y[i]) qimpm_t[(size_t)i * p + k] += ORC_W(nodextr[i]) / fnoob;
                     }
                 }
             }
             if (impn == 1)
                 for (size_t e = 0; e < (size_t)n * p; ++e) qimpm[e] += qimpm_t[e];
+#undef ORC_W
         }
 
         /* in-bag routing, then cpu_proximity's dense branch */
-        if (do_prox || leaf) {
+        if (do_prox || leaf || Cw) {
             for (int i = 0; i < n; ++i)
                 if (nin[i] > 0)
                     nodextr[i] = route_terminal(X + (size_t)i * p, p, ns, bv, xs, tm, cat, cgl, maxcat, maxnode);
             if (leaf) memcpy(leaf + (size_t)t * n, nodextr, sizeof(int32_t) * (size_t)n);
         }
-        if (do_prox) {
+        if (do_prox || Cw) {
             int nterm = 0;
             for (int k = 0; k < nn; ++k) nod[k] = (ns[k] == -1) ? nterm++ : -1;
             for (int i = 0; i < n; ++i) {
@@ -413,12 +477,23 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
                 if (nin[i] != 0) continue;
                 int k = nodexb[i];
                 if (k < 0 || k >= nterm) continue;
+                /* nodesize = sum of the in-bag multiplicities of the leaf (:195-204) */
+                int nodesize = 0;
+                for (int jj = ndbegin[k]; jj < ndbegin[k + 1]; ++jj)
+                    if (npcase[jj] >= 0 && nin[npcase[jj]] > 0) nodesize += nin[npcase[jj]];
                 for (int jj = ndbegin[k]; jj < ndbegin[k + 1]; ++jj) {
                     int kk = npcase[jj];
                     if (kk >= 0 && nin[kk] > 0) {
-                        /* C[i][kk] += 1  ->  S[min][max] += 1 */
-                        int a = i < kk ? i : kk, b = i < kk ? kk : i;
-                        S[upidx(n, a, b)] += 1;
+                        if (S) {
+                            /* C[i][kk] += 1  ->  S[min][max] += 1 */
+                            int a = i < kk ? i : kk, b = i < kk ? kk : i;
+                            S[upidx(n, a, b)] += 1;
+                        }
+                        if (Cw && (nodesize > 0 || !casewise)) {
+                            /* C[i][kk] += nin[kk] / nodesize (casewise) or 1, FP64 (:205-222) */
+                            double w = (casewise && nodesize > 0) ? (double)nin[kk] / (double)nodesize : 1.0;
+                            Cw[(size_t)i * n + kk] += w;
+                        }
                     }
                 }
             }
@@ -426,6 +501,7 @@ int orc_analyse(const float* X, const int32_t* y, const int32_t* cat, int n, int
     }
     free(jtr); free(nodextr); free(joob); free(perm); free(jvr); free(nod); free(ncount);
     free(ncn); free(nodexb); free(ndbegin); free(npcase); free(qimpm_t); free(iv);
+    free(nodexvr); free(tnodewt); free(wsum); free(wcnt);
     return 0;
 }
 
@@ -476,6 +552,85 @@ int64_t orc_pairs_from_leaves(int n, int T, int max_leaves, const int32_t* leaf,
     free(ndbegin);
     free(npcase);
     return bad;
+}
+
+/* ------------------------------------------------------------------------ */
+/* cpu_finishprox (src/rf_finishprox.cpp:12-74) from FP64 sums: Sd is the     */
+/* packed upper triangle of C + C^T (C the raw FP64 matrix cpu_proximity     */
+/* accumulates, e.g. casewise weights), the same arithmetic as               */
+/* orc_finishprox.                                                            */
+/* ------------------------------------------------------------------------ */
+void orc_finishprox_f64(int n, const double* Sd, const int32_t* nout, int full, float* P, double* Pd) {
+    double* inv = (double*)malloc(sizeof(double) * (size_t)n);
+    for (int i = 0; i < n; ++i) inv[i] = nout[i] > 0 ? 1.0 / (double)nout[i] : 1.0;
+    for (int64_t i = 0; i < n; ++i) {
+        for (int64_t j = i; j < n; ++j) {
+            double v;
+            if (i == j) {
+                v = 1.0;
+            } else {
+                double h = Sd[upidx(n, i, j)] / 2.0;
+                double a = nout[i] > 0 ? h * inv[i] : h;
+                double b = nout[j] > 0 ? h * inv[j] : h;
+                v = 0.5 * (a + b);
+            }
+            if (full) {
+                if (P) { P[i * n + j] = (float)v; P[j * n + i] = (float)v; }
+                if (Pd) { Pd[i * n + j] = v; Pd[j * n + i] = v; }
+            } else {
+                if (P) P[upidx(n, i, j)] = (float)v;
+                if (Pd) Pd[upidx(n, i, j)] = v;
+            }
+        }
+    }
+    free(inv);
+}
+
+/* ------------------------------------------------------------------------ */
+/* RF-GAP proximity, cpu_proximity_rfgap (src/rf_proximity.cpp:238-391):      */
+/*   pGAP(i,j) = (1/|S_i|) sum_{t in S_i} c_j(t) [j in-bag in i's node] /     */
+/*               |M_i(t)|                                                     */
+/* S_i = trees where i is OOB, c_j(t) = j's bootstrap multiplicity, |M_i(t)| */
+/* = the multiplicities of the in-bag samples in i's node summed.  Nodes are */
+/* the per-tree node ids the reference stores (OOB: testreebag, in-bag:      */
+/* find_terminal_node; any node id matches, the root included).  A sample    */
+/* never OOB gets 1 on the diagonal.  Then P = (pGAP + pGAP^T) / 2 off the   */
+/* diagonal.  node and nin are T x n; P is n x n row-major (FP64).           */
+/* ------------------------------------------------------------------------ */
+void orc_rfgap(int n, int T, const int32_t* nin, const int32_t* node, double* P) {
+    memset(P, 0, sizeof(double) * (size_t)n * n);
+    for (int i = 0; i < n; ++i) {
+        int noob_i = 0;
+        for (int t = 0; t < T; ++t)
+            if (nin[(size_t)t * n + i] == 0) noob_i++;
+        if (noob_i == 0) {
+            P[(size_t)i * n + i] = 1.0;
+            continue;
+        }
+        double* row = P + (size_t)i * n;
+        for (int t = 0; t < T; ++t) {
+            const int32_t* nt = nin + (size_t)t * n;
+            const int32_t* dt = node + (size_t)t * n;
+            if (nt[i] != 0) continue;
+            const int v = dt[i];
+            if (v < 0) continue;
+            int64_t m = 0;
+            for (int j = 0; j < n; ++j)
+                if (nt[j] > 0 && dt[j] == v) m += nt[j];
+            if (m == 0) continue;
+            const double inv = 1.0 / (double)m;
+            for (int j = 0; j < n; ++j)
+                if (nt[j] > 0 && dt[j] == v) row[j] += (double)nt[j] * inv;
+        }
+        const double norm = 1.0 / (double)noob_i;
+        for (int j = 0; j < n; ++j) row[j] *= norm;
+    }
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            const double avg = (P[(size_t)i * n + j] + P[(size_t)j * n + i]) / 2.0;
+            P[(size_t)i * n + j] = avg;
+            P[(size_t)j * n + i] = avg;
+        }
 }
 
 /* OOB error / predictions / probabilities from raw votes                    */

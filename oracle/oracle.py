@@ -46,12 +46,17 @@ def bootstrap(n: int, tree: int) -> np.ndarray:
     return nin
 
 
-def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False, want_jtr=False, S=None):
+def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False, want_jtr=False, S=None,
+            casewise=False, want_cw=False):
     """Whole-forest analysis in the reference's per-tree order (see orc_analyse).
 
     With ``S`` (int32, n(n+1)/2, C-contiguous) the pair counts are added to
     that buffer instead of a fresh zeroed one, as the reference accumulates
-    one proximity array over all trees."""
+    one proximity array over all trees.  ``casewise`` weights votes,
+    importance and the FP64 proximity sums as the reference's
+    use_casewise=True; ``want_cw`` returns those FP64 sums as ``Cw`` (n x n,
+    row = OOB sample, column = in-bag sample) and their packed symmetric
+    upper triangle ``Sd`` = C + C^T."""
     X = np.ascontiguousarray(X, dtype=np.float32)
     y = np.ascontiguousarray(y, dtype=np.int32)
     f = forest
@@ -66,6 +71,7 @@ def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False,
         S = np.zeros(n * (n + 1) // 2, np.int32)
     elif S.dtype != np.int32 or S.size != n * (n + 1) // 2 or not S.flags.c_contiguous:
         raise ValueError("S must be a C-contiguous int32 array of n(n+1)/2 entries")
+    Cw = np.zeros(n * n, np.float64) if want_cw else None
     leaf = np.zeros(T * n, np.int32) if want_leaf else None
     jtr = np.zeros(T * n, np.int32) if want_jtr else None
     bad = ctypes.c_int(0)
@@ -73,11 +79,16 @@ def analyse(X, y, forest, do_imp=True, impn=True, do_prox=True, want_leaf=False,
     lib().orc_analyse(
         _p(X), _p(y), _p(f.cat), n, p, c, f.maxcat, T, _p(offs), _p(f.nnode), _p(f.nodestatus),
         _p(f.bestvar), _p(f.xbestsplit), _p(f.treemap), _p(f.nodeclass), _p(f.catgoleft), _p(f.nin),
-        int(bool(do_imp)), int(bool(impn)), int(bool(do_prox)),
+        int(bool(do_imp)), int(bool(impn)), int(bool(do_prox)), int(bool(casewise)),
         _p(out["q_raw"]), _p(out["nout"]), _p(out["qimp"]), _p(out["qimpm"]), _p(out["avimp"]),
-        _p(out["sqsd"]), _p(S), _p(leaf), _p(jtr), ctypes.byref(bad))
+        _p(out["sqsd"]), _p(S), _p(Cw), _p(leaf), _p(jtr), ctypes.byref(bad))
     out["q_raw"] = out["q_raw"].reshape(n, c)
     out["S"] = S
+    if want_cw:
+        C = Cw.reshape(n, n)
+        iu = np.triu_indices(n)
+        out["Cw"] = C
+        out["Sd"] = np.ascontiguousarray((C + C.T)[iu])
     out["leaf"] = None if leaf is None else leaf.reshape(T, n)
     out["jtr"] = None if jtr is None else jtr.reshape(T, n)
     out["perm_bad"] = int(bad.value)
@@ -118,6 +129,26 @@ def finishprox(S, nout, full=True, double=False):
                          int(bool(full)), _p(P), _p(Pd))
     R = Pd if double else P
     return R.reshape(n, n) if full else R
+
+
+def finishprox_f64(Sd, nout, full=True):
+    """orc_finishprox_f64: cpu_finishprox from the packed FP64 sums C + C^T."""
+    n = nout.size
+    P = np.zeros(n * n if full else n * (n + 1) // 2, np.float32)
+    lib().orc_finishprox_f64(n, _p(np.ascontiguousarray(Sd, np.float64)), _p(np.ascontiguousarray(nout, np.int32)),
+                             int(bool(full)), _p(P), None)
+    return P.reshape(n, n) if full else P
+
+
+def rfgap(nin, node):
+    """orc_rfgap: the RF-GAP proximity matrix (n x n FP64) from per-tree
+    multiplicities and node ids (T x n each)."""
+    nin = np.ascontiguousarray(nin, np.int32)
+    node = np.ascontiguousarray(node, np.int32)
+    T, n = nin.shape
+    P = np.zeros(n * n, np.float64)
+    lib().orc_rfgap(n, T, _p(nin), _p(node), _p(P))
+    return P.reshape(n, n)
 
 
 def localimp(qimp, qimpm, n, p, T):

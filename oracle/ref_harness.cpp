@@ -72,7 +72,9 @@ extern "C" int rh_set_threads(int n) {
 //   q_raw[n*c] (raw OOB votes, before finalize), nout[n],
 //   scalars[0] = oob_error, oob_pred[n], oob_proba[n*c],
 //   importances[p], qimp[n], qimpm[n*p] (after localimp), avimp[p], sqsd[p],
-//   prox[n*n] (finalised, column-major FP64) or null.
+//   prox[n*n] (finalised, column-major FP64; with use_rfgap the RF-GAP
+//   matrix of cpu_proximity_rfgap) or null.
+// use_casewise / use_rfgap set the reference's config flags of the same names.
 // ---------------------------------------------------------------------------
 struct CaptureState {
     rf::RandomForest* rfp;
@@ -89,6 +91,7 @@ extern "C" int rh_fit_capture(const float* X, const int* y, const int* cat,
                               int n, int p, int ntree, int mtry, int minndsize,
                               int maxcat, int iseed,
                               int compute_prox, int compute_imp, int compute_local_imp,
+                              int use_casewise, int use_rfgap,
                               int* nclass_out,
                               int* nnode, int* nodestatus, int* bestvar, float* xbestsplit,
                               int* treemap, int* nodeclass,
@@ -123,7 +126,8 @@ extern "C" int rh_fit_capture(const float* X, const int* y, const int* cat,
         cfg.compute_local_importance = compute_local_imp != 0;
         cfg.use_gpu = false;
         cfg.use_qlora = false;
-        cfg.use_casewise = false;
+        cfg.use_casewise = use_casewise != 0;
+        cfg.use_rfgap = use_rfgap != 0;
         *nclass_out = cfg.nclass;
 
         rf::RandomForest model(cfg);

@@ -45,7 +45,8 @@ def set_threads(n: int) -> int:
 
 
 def fit_capture(X, y, cat, ntree, mtry=0, minndsize=1, maxcat=10, iseed=12345,
-                compute_proximity=True, compute_importance=True, compute_local_importance=True):
+                compute_proximity=True, compute_importance=True, compute_local_importance=True,
+                use_casewise=False, use_rfgap=False):
     """Run rf::RandomForest::fit on the CPU path and capture everything."""
     X = np.ascontiguousarray(X, np.float32)
     y = np.ascontiguousarray(y, np.int32)
@@ -66,7 +67,8 @@ def fit_capture(X, y, cat, ntree, mtry=0, minndsize=1, maxcat=10, iseed=12345,
     nclass = ctypes.c_int(0)
     _check(lib().rh_fit_capture(
         _p(X), _p(y), _p(cat), n, p, T, mtry, minndsize, maxcat, iseed,
-        int(compute_proximity), int(compute_importance), int(compute_local_importance), ctypes.byref(nclass),
+        int(compute_proximity), int(compute_importance), int(compute_local_importance), int(use_casewise),
+        int(use_rfgap), ctypes.byref(nclass),
         *[_p(a[k]) for k in ("nnode", "nodestatus", "bestvar", "xbestsplit", "treemap", "nodeclass", "nin", "jtr",
                              "nodextr", "q_raw", "nout", "scalars", "oob_pred", "oob_proba", "importances", "qimp",
                              "qimpm", "avimp", "sqsd")], _p(prox)))

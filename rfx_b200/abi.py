@@ -25,7 +25,7 @@ STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ER
 
 # Every symbol include/rfx_b200.h declares (checked by the CPU tests).
 EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
-           "rfx_forest_load", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
+           "rfx_forest_load", "rfx_forest_load_device", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
            "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
            "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_factor_mds_operator", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest", "rfx_graph_capture_batch",
@@ -33,7 +33,7 @@ EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_strea
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
           "predict", "oob_summary", "localimp", "pair_ranges", "lowrank_product", "lowrank_orth", "mds_factors",
-          "mds_full"]
+          "mds_full", "pair_hubs"]
 
 
 class RfxError(RuntimeError):
@@ -53,6 +53,14 @@ class _ForestView(ctypes.Structure):
                 ("bestvar", ctypes.c_void_p), ("xbestsplit", ctypes.c_void_p), ("treemap", ctypes.c_void_p),
                 ("nodeclass", ctypes.c_void_p), ("catgoleft", ctypes.c_void_p), ("nin", ctypes.c_void_p),
                 ("X", ctypes.c_void_p), ("y", ctypes.c_void_p), ("cat", ctypes.c_void_p)]
+
+
+class _ForestDeviceView(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("p", ctypes.c_int32), ("nclass", ctypes.c_int32), ("maxcat", ctypes.c_int32),
+                ("ntree", ctypes.c_int32), ("maxnode", ctypes.c_int32), ("nnode", ctypes.c_void_p),
+                ("nodestatus", ctypes.c_void_p), ("bestvar", ctypes.c_void_p), ("xbestsplit", ctypes.c_void_p),
+                ("treemap", ctypes.c_void_p), ("nodeclass", ctypes.c_void_p), ("catgoleft", ctypes.c_void_p),
+                ("nin", ctypes.c_void_p), ("X", ctypes.c_void_p), ("y", ctypes.c_void_p), ("cat", ctypes.c_void_p)]
 
 
 class _LowrankOpts(ctypes.Structure):
@@ -179,7 +187,7 @@ class BatchGraph:
             pass
 
 
-TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order"}
+TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order", 4: "pair_counts_hub"}
 # launch shapes per stage, in the library's shape order
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
                     "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight"], 1: ["256", "512", "1024"],
@@ -262,6 +270,23 @@ class Context:
         self.forest = f
         self.n, self.p, self.nclass, self.ntree = f.n, f.p, f.nclass, f.ntree
 
+    def load_device(self, forest: Forest, arrays: dict, maxnode: int):
+        """Load a forest held in device memory in the padded per-tree layout
+        (rfx_forest_load_device).  ``arrays`` maps nodestatus, bestvar,
+        xbestsplit, treemap, nodeclass, nin, X, y, cat (and optionally
+        catgoleft) to device buffers (torch CUDA tensors or addresses); node
+        counts come from ``forest.nnode`` (host)."""
+        nnode = np.ascontiguousarray(forest.nnode, dtype=np.int32)
+        g = lambda k: _ptr(arrays.get(k))
+        v = _ForestDeviceView(n=forest.n, p=forest.p, nclass=forest.nclass, maxcat=forest.maxcat,
+                              ntree=forest.ntree, maxnode=int(maxnode), nnode=_ptr(nnode),
+                              nodestatus=g("nodestatus"), bestvar=g("bestvar"), xbestsplit=g("xbestsplit"),
+                              treemap=g("treemap"), nodeclass=g("nodeclass"), catgoleft=g("catgoleft"),
+                              nin=g("nin"), X=g("X"), y=g("y"), cat=g("cat"))
+        _check(lib().rfx_forest_load_device(self._h, ctypes.byref(v)))
+        self.forest = forest
+        self.n, self.p, self.nclass, self.ntree = forest.n, forest.p, forest.nclass, forest.ntree
+
     # --- analysis ---------------------------------------------------------
     def route_oob(self, q=None, nout=None, leaf=None):
         """Integer OOB votes q (n, c), doubled nout (n,), optional leaf (T, n)."""
@@ -340,9 +365,16 @@ class Context:
         return A, ev
 
     def lowrank_quantize(self, fmt):
-        """fmt 1 = INT8, 2 = FP8 e4m3: (q as uint8 bytes n x rank, scales)."""
+        """fmt 1 = INT8, 2 = FP8 e4m3 (q: n x rank bytes), 3 = NF4 (q:
+        ceil(n * rank / 2) bytes, two codes per byte), 4 = FP16 (q: n x rank
+        uint16); returns (q, per-column scales)."""
         r = self._rank_guess
-        q = np.zeros((self.n, r), np.uint8)
+        if fmt == 3:
+            q = np.zeros((self.n * r + 1) // 2, np.uint8)
+        elif fmt == 4:
+            q = np.zeros((self.n, r), np.uint16)
+        else:
+            q = np.zeros((self.n, r), np.uint8)
         sc = np.zeros(r, np.float32)
         _check(lib().rfx_lowrank_quantize(self._h, int(fmt), _vp(q), _vp(sc)))
         return q, sc

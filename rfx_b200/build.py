@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # The system compilers: the environment's CXX wrapper lacks the OpenMP spec.
 HOST_CXX = "/usr/bin/g++"
 
-CU_SOURCES = ["abi.cu", "load.cu", "route.cu", "prox.cu", "varimp.cu", "noalloc.cu", "mds.cu", "tc_mds.cu", "lowrank.cu", "batch.cu", "tune.cu"]
+CU_SOURCES = ["abi.cu", "load.cu", "route.cu", "prox.cu", "varimp.cu", "noalloc.cu", "hubs.cu", "mds.cu", "tc_mds.cu", "lowrank.cu", "batch.cu", "tune.cu"]
 CPP_SOURCES = ["host/grow.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,

@@ -118,6 +118,7 @@ void free_forest(Ctx* c) {
     dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_partner); dfree(c, c->d_vflags); dfree(c, c->d_flips);
     dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
     dfree(c, c->d_sqsd); dfree(c, c->d_opp); dfree(c, c->d_order);
+    dfree(c, c->d_hubflag); dfree(c, c->d_hubtiles); dfree(c, c->d_hubstate);
     dfree(c, c->d_lrA); dfree(c, c->d_lrAq); dfree(c, c->d_lrScale);
     if (c->d_lrQ) cudaFree(c->d_lrQ);
     c->d_lrQ = nullptr;
@@ -265,56 +266,64 @@ rfx_status rfx_synchronize(rfx_ctx* ctx) {
     return check_device_errors(c);
 }
 
-rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
-    Ctx* c = reinterpret_cast<Ctx*>(ctx);
-    if (!c || !v) {
-        set_error("rfx_forest_load: null argument");
-        return RFX_ERR_INVALID;
-    }
+// What a forest load needs besides the context: sizes, the compact node
+// offsets on the host, host copies of the labels and feature kinds (checked
+// here), and a function that fills the device buffers from the caller's
+// arrays (host arrays: H2D copies; device arrays: D2D copies and a gather of
+// padded trees).
+struct LoadInput {
+    int n = 0, p = 0, nclass = 0, maxcat = 0, T = 0;
+    const int64_t* offs = nullptr;  // host, T + 1
+    const int32_t* y = nullptr;     // host, n
+    const int32_t* cat = nullptr;   // host, p
+    bool has_catgoleft = false;
+    const char* who = "rfx_forest_load";
+    // fills c->d_X, d_y, d_cat, d_nodeclass, d_catgoleft (if any) and the
+    // compact raw node arrays and nin; c->d_offs is already on the device
+    std::function<cudaError_t(cudaStream_t, Ctx*, int32_t*, int32_t*, float*, int32_t*, int32_t*)> upload;
+};
+
+static rfx_status load_forest(Ctx* c, const LoadInput& in) {
+    const std::string who = in.who;
     try {
         cudaSetDevice(c->device);
-        const int n = v->n, p = v->p, nclass = v->nclass, T = v->ntree;
-        const int maxcat = v->maxcat;
+        const int n = in.n, p = in.p, nclass = in.nclass, T = in.T;
+        const int maxcat = in.maxcat;
         if (n < 1 || p < 1 || nclass < 1 || T < 1 || maxcat < 1) {
-            set_error("rfx_forest_load: n, p, nclass, ntree and maxcat must be >= 1");
+            set_error(who + ": n, p, nclass, ntree and maxcat must be >= 1");
             return RFX_ERR_INVALID;
         }
         if (p > 65535) {
-            set_error("rfx_forest_load: at most 65535 features");
+            set_error(who + ": at most 65535 features");
             return RFX_ERR_UNSUPPORTED;
         }
-        if (!v->offs || !v->nodestatus || !v->bestvar || !v->xbestsplit || !v->treemap || !v->nodeclass || !v->nin ||
-            !v->X || !v->y || !v->cat) {
-            set_error("rfx_forest_load: a required array is null");
-            return RFX_ERR_INVALID;
-        }
-        if (v->offs[0] != 0) {
-            set_error("rfx_forest_load: offs[0] must be 0");
+        if (in.offs[0] != 0) {
+            set_error(who + ": offs[0] must be 0");
             return RFX_ERR_FOREST;
         }
         for (int i = 0; i < n; ++i)
-            if (v->y[i] < 0 || v->y[i] >= nclass) {
-                set_error("rfx_forest_load: label out of [0, nclass) at sample " + std::to_string(i));
+            if (in.y[i] < 0 || in.y[i] >= nclass) {
+                set_error(who + ": label out of [0, nclass) at sample " + std::to_string(i));
                 return RFX_ERR_INVALID;
             }
-        if (v->catgoleft)
+        if (in.has_catgoleft)
             for (int m = 0; m < p; ++m)
-                if (v->cat[m] != 1 && v->cat[m] > maxcat) {
-                    set_error("rfx_forest_load: cat[m] exceeds maxcat with a catgoleft table");
+                if (in.cat[m] != 1 && in.cat[m] > maxcat) {
+                    set_error(who + ": cat[m] exceeds maxcat with a catgoleft table");
                     return RFX_ERR_FOREST;
                 }
         std::vector<int32_t> nnode(T), nleaf(T), noob(T);
         for (int t = 0; t < T; ++t) {
-            const int64_t a = v->offs[t], b = v->offs[t + 1];
+            const int64_t a = in.offs[t], b = in.offs[t + 1];
             // trees may come from a larger training set than the rows loaded
             // here (a row subsample), so only positivity and int32 range are checked
             if (b <= a || b - a > (int64_t)INT32_MAX / 2) {
-                set_error("rfx_forest_load: tree " + std::to_string(t) + " has an invalid node count");
+                set_error(who + ": tree " + std::to_string(t) + " has an invalid node count");
                 return RFX_ERR_FOREST;
             }
             nnode[t] = (int)(b - a);
         }
-        const int64_t N = v->offs[T];
+        const int64_t N = in.offs[T];
         const int W = (p + 63) / 64;
 
         // device buffers (from the pool when a forest of this shape was loaded
@@ -330,7 +339,7 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
         ALLOC(d_nodes, N);
         ALLOC(d_nodeclass, N);
         ALLOC(d_leafidx, N);
-        if (v->catgoleft) ALLOC(d_catgoleft, (size_t)N * maxcat);
+        if (in.has_catgoleft) ALLOC(d_catgoleft, (size_t)N * maxcat);
         ALLOC(d_offs, T + 1);
         ALLOC(d_nnode, T);
         ALLOC(d_inbag, (size_t)T * n);
@@ -365,22 +374,12 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
             return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
         };
         cudaError_t e = cudaMemsetAsync(r_err, 0, sizeof(LoadError), s);
-        if (e == cudaSuccess) e = up(c->d_X, v->X, sizeof(float) * (size_t)n * p);
-        if (e == cudaSuccess) e = up(c->d_y, v->y, sizeof(int32_t) * n);
-        if (e == cudaSuccess) e = up(c->d_cat, v->cat, sizeof(int32_t) * p);
-        if (e == cudaSuccess) e = up(c->d_offs, v->offs, sizeof(int64_t) * (T + 1));
+        if (e == cudaSuccess) e = up(c->d_offs, in.offs, sizeof(int64_t) * (T + 1));
         if (e == cudaSuccess) e = up(c->d_nnode, nnode.data(), sizeof(int32_t) * T);
-        if (e == cudaSuccess) e = up(r_status, v->nodestatus, sizeof(int32_t) * (size_t)N);
-        if (e == cudaSuccess) e = up(r_bestvar, v->bestvar, sizeof(int32_t) * (size_t)N);
-        if (e == cudaSuccess) e = up(r_split, v->xbestsplit, sizeof(float) * (size_t)N);
-        if (e == cudaSuccess) e = up(r_treemap, v->treemap, sizeof(int32_t) * 2 * (size_t)N);
-        if (e == cudaSuccess) e = up(c->d_nodeclass, v->nodeclass, sizeof(int32_t) * (size_t)N);
-        if (e == cudaSuccess && v->catgoleft)
-            e = up(c->d_catgoleft, v->catgoleft, sizeof(int32_t) * (size_t)N * maxcat);
-        if (e == cudaSuccess) e = up(r_nin, v->nin, sizeof(int32_t) * (size_t)T * n);
+        if (e == cudaSuccess) e = in.upload(s, c, r_status, r_bestvar, r_split, r_treemap, r_nin);
         if (e != cudaSuccess) {
             free_forest(c);
-            return cuda_fail(e, "rfx_forest_load upload");
+            return cuda_fail(e, (who + " upload").c_str());
         }
         st = launch_pack_forest(s, T, n, p, c->d_offs, r_status, r_bestvar, r_split, r_treemap, c->d_cat, r_nin,
                                 c->d_nodes, c->d_leafidx, c->d_iv, r_nleaf, c->d_inbag, c->d_noob, r_err);
@@ -392,16 +391,16 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
                 e = cudaMemcpyAsync(noob.data(), c->d_noob, sizeof(int32_t) * T, cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, r_err, sizeof(LoadError), cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess) st = cuda_fail(e, "rfx_forest_load pack");
+            if (e != cudaSuccess) st = cuda_fail(e, (who + " pack").c_str());
         }
         if (st == RFX_OK && herr.code) {
             const std::string where = " at tree " + std::to_string(herr.tree) + " node " + std::to_string(herr.node);
             switch (herr.code) {
-                case 1: set_error("rfx_forest_load: nodestatus out of range" + where); break;
-                case 2: set_error("rfx_forest_load: bestvar out of range" + where); break;
-                case 3: set_error("rfx_forest_load: child out of range" + where); break;
+                case 1: set_error(who + ": nodestatus out of range" + where); break;
+                case 2: set_error(who + ": bestvar out of range" + where); break;
+                case 3: set_error(who + ": child out of range" + where); break;
                 default:
-                    set_error("rfx_forest_load: negative nin at tree " + std::to_string(herr.tree) + " sample " +
+                    set_error(who + ": negative nin at tree " + std::to_string(herr.tree) + " sample " +
                               std::to_string(herr.node));
             }
             st = RFX_ERR_FOREST;
@@ -425,7 +424,7 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
         }
         if (total > INT32_MAX) {
             free_forest(c);
-            set_error("rfx_forest_load: permutation tables too large");
+            set_error(who + ": permutation tables too large");
             return RFX_ERR_UNSUPPORTED;
         }
         if (!c->d_perm || distinct != c->perm_noobs) {
@@ -453,7 +452,7 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             if (e != cudaSuccess) {
                 free_forest(c);
-                return cuda_fail(e, "rfx_forest_load permutation upload");
+                return cuda_fail(e, (who + " permutation upload").c_str());
             }
             c->perm_noobs = distinct;
         }
@@ -464,7 +463,7 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
             volatile float f = (float)noob[t];
             invnoob[t] = 1.0f / f;
         }
-        c->h_offs.assign(v->offs, v->offs + T + 1);
+        c->h_offs.assign(in.offs, in.offs + T + 1);
         c->h_nnode = nnode;
         c->h_nleaf = nleaf;
         c->h_segbase = segbase;
@@ -488,16 +487,119 @@ rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) {
             free_forest(c);
-            return cuda_fail(e, "rfx_forest_load upload");
+            return cuda_fail(e, (who + " upload").c_str());
         }
         c->loaded = true;
         return RFX_OK;
     } catch (const std::bad_alloc&) {
-        set_error("rfx_forest_load: host allocation failed");
+        set_error(who + ": host allocation failed");
         return RFX_ERR_OOM;
     } catch (const std::exception& ex) {
-        set_error(std::string("rfx_forest_load: ") + ex.what());
+        set_error(who + ": " + ex.what());
         return RFX_ERR_INVALID;
+    }
+}
+
+rfx_status rfx_forest_load(rfx_ctx* ctx, const rfx_forest_view* v) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !v) {
+        set_error("rfx_forest_load: null argument");
+        return RFX_ERR_INVALID;
+    }
+    if (!v->offs || !v->nodestatus || !v->bestvar || !v->xbestsplit || !v->treemap || !v->nodeclass || !v->nin ||
+        !v->X || !v->y || !v->cat) {
+        set_error("rfx_forest_load: a required array is null");
+        return RFX_ERR_INVALID;
+    }
+    LoadInput in;
+    in.n = v->n; in.p = v->p; in.nclass = v->nclass; in.maxcat = v->maxcat; in.T = v->ntree;
+    in.offs = v->offs; in.y = v->y; in.cat = v->cat; in.has_catgoleft = v->catgoleft != nullptr;
+    in.upload = [v](cudaStream_t s, Ctx* c, int32_t* r_status, int32_t* r_bestvar, float* r_split, int32_t* r_treemap,
+                    int32_t* r_nin) -> cudaError_t {
+        const int n = v->n, p = v->p, T = v->ntree;
+        const size_t N = (size_t)v->offs[T];
+        auto up = [&](void* d, const void* h, size_t bytes) {
+            return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
+        };
+        cudaError_t e = up(c->d_X, v->X, sizeof(float) * (size_t)n * p);
+        if (e == cudaSuccess) e = up(c->d_y, v->y, sizeof(int32_t) * n);
+        if (e == cudaSuccess) e = up(c->d_cat, v->cat, sizeof(int32_t) * p);
+        if (e == cudaSuccess) e = up(r_status, v->nodestatus, sizeof(int32_t) * N);
+        if (e == cudaSuccess) e = up(r_bestvar, v->bestvar, sizeof(int32_t) * N);
+        if (e == cudaSuccess) e = up(r_split, v->xbestsplit, sizeof(float) * N);
+        if (e == cudaSuccess) e = up(r_treemap, v->treemap, sizeof(int32_t) * 2 * N);
+        if (e == cudaSuccess) e = up(c->d_nodeclass, v->nodeclass, sizeof(int32_t) * N);
+        if (e == cudaSuccess && v->catgoleft) e = up(c->d_catgoleft, v->catgoleft, sizeof(int32_t) * N * v->maxcat);
+        if (e == cudaSuccess) e = up(r_nin, v->nin, sizeof(int32_t) * (size_t)T * n);
+        return e;
+    };
+    return load_forest(c, in);
+}
+
+rfx_status rfx_forest_load_device(rfx_ctx* ctx, const rfx_forest_device_view* v) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (!c || !v) {
+        set_error("rfx_forest_load_device: null argument");
+        return RFX_ERR_INVALID;
+    }
+    if (!v->nnode || !v->nodestatus || !v->bestvar || !v->xbestsplit || !v->treemap || !v->nodeclass || !v->nin ||
+        !v->X || !v->y || !v->cat) {
+        set_error("rfx_forest_load_device: a required array is null");
+        return RFX_ERR_INVALID;
+    }
+    const int n = v->n, p = v->p, T = v->ntree, maxnode = v->maxnode, maxcat = v->maxcat;
+    if (n < 1 || p < 1 || T < 1 || maxnode < 1 || maxcat < 1) {
+        set_error("rfx_forest_load_device: n, p, ntree, maxnode and maxcat must be >= 1");
+        return RFX_ERR_INVALID;
+    }
+    cudaSetDevice(c->device);
+    const void* dev_arrays[] = {v->nodestatus, v->bestvar, v->xbestsplit, v->treemap, v->nodeclass, v->nin,
+                                v->X, v->y, v->cat};
+    for (const void* a : dev_arrays)
+        if (!is_device_ptr(a)) {
+            set_error("rfx_forest_load_device: the forest and data arrays must be device memory (nnode stays on the host)");
+            return RFX_ERR_INVALID;
+        }
+    if (v->catgoleft && !is_device_ptr(v->catgoleft)) {
+        set_error("rfx_forest_load_device: catgoleft must be device memory");
+        return RFX_ERR_INVALID;
+    }
+    try {
+        std::vector<int64_t> offs(T + 1, 0);
+        for (int t = 0; t < T; ++t) {
+            if (v->nnode[t] < 1 || v->nnode[t] > maxnode) {
+                set_error("rfx_forest_load_device: nnode[" + std::to_string(t) + "] outside [1, maxnode]");
+                return RFX_ERR_FOREST;
+            }
+            offs[t + 1] = offs[t] + v->nnode[t];
+        }
+        std::vector<int32_t> y(n), cat(p);
+        RFX_CUDA(cudaMemcpy(y.data(), v->y, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        RFX_CUDA(cudaMemcpy(cat.data(), v->cat, sizeof(int32_t) * p, cudaMemcpyDeviceToHost));
+        LoadInput in;
+        in.n = n; in.p = p; in.nclass = v->nclass; in.maxcat = maxcat; in.T = T;
+        in.offs = offs.data(); in.y = y.data(); in.cat = cat.data(); in.has_catgoleft = v->catgoleft != nullptr;
+        in.who = "rfx_forest_load_device";
+        in.upload = [v](cudaStream_t s, Ctx* c, int32_t* r_status, int32_t* r_bestvar, float* r_split,
+                        int32_t* r_treemap, int32_t* r_nin) -> cudaError_t {
+            const int n = v->n, p = v->p, T = v->ntree;
+            auto cp = [&](void* d, const void* src, size_t bytes) {
+                return cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, s);
+            };
+            cudaError_t e = cp(c->d_X, v->X, sizeof(float) * (size_t)n * p);
+            if (e == cudaSuccess) e = cp(c->d_y, v->y, sizeof(int32_t) * n);
+            if (e == cudaSuccess) e = cp(c->d_cat, v->cat, sizeof(int32_t) * p);
+            if (e == cudaSuccess) e = cp(r_nin, v->nin, sizeof(int32_t) * (size_t)T * n);
+            if (e == cudaSuccess)
+                e = launch_gather_padded(s, T, v->maxnode, v->maxcat, c->d_offs, v->nodestatus, v->bestvar,
+                                         v->xbestsplit, v->treemap, v->nodeclass, v->catgoleft, r_status, r_bestvar,
+                                         r_split, r_treemap, c->d_nodeclass, c->d_catgoleft);
+            return e;
+        };
+        return load_forest(c, in);
+    } catch (const std::bad_alloc&) {
+        set_error("rfx_forest_load_device: host allocation failed");
+        return RFX_ERR_OOM;
     }
 }
 
@@ -872,15 +974,17 @@ rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales
         set_error("rfx_lowrank_quantize: no factors (call rfx_lowrank first)");
         return RFX_ERR_STATE;
     }
-    if (format != 1 && format != 2) {
-        set_error("rfx_lowrank_quantize: format must be 1 (INT8) or 2 (FP8 e4m3)");
+    if (format < 1 || format > 4) {
+        set_error("rfx_lowrank_quantize: format must be 1 (INT8), 2 (FP8 e4m3), 3 (NF4) or 4 (FP16)");
         return RFX_ERR_INVALID;
     }
     const int k = c->lr_rank;
     const size_t nk = (size_t)c->n * k;
+    // stored bytes: INT8 / FP8 one per entry, NF4 half, FP16 two
+    const size_t qbytes = format == 3 ? (nk + 1) / 2 : format == 4 ? 2 * nk : nk;
     if (c->d_lrQ) cudaFree(c->d_lrQ);
     c->d_lrQ = nullptr;
-    if (ctx_malloc(c, (void**)&c->d_lrQ, nk) != cudaSuccess) {
+    if (ctx_malloc(c, (void**)&c->d_lrQ, qbytes) != cudaSuccess) {
         cudaGetLastError();
         set_error("rfx_lowrank_quantize: allocation failed");
         return RFX_ERR_OOM;
@@ -890,7 +994,7 @@ rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales
     if ((st = lowrank_quantize(c, c->d_lrA, k, format, c->d_lrQ, c->d_lrScale))) return st;
     if ((st = lowrank_dequantize(c, c->d_lrQ, c->d_lrScale, k, format, c->d_lrAq))) return st;
     c->lr_qformat = format;
-    if (q && (st = copy_out(c, q, c->d_lrQ, nk))) return st;
+    if (q && (st = copy_out(c, q, c->d_lrQ, qbytes))) return st;
     if (scales && (st = copy_out(c, scales, c->d_lrScale, sizeof(float) * k))) return st;
     RFX_CUDA(cudaStreamSynchronize(c->stream));
     return RFX_OK;

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <cstring>
 #include <cstdint>
 #include <set>
 #include <stdexcept>
@@ -46,6 +47,33 @@ void check(rfx_status st, const std::string& what) {
 std::string lower(std::string s) {
     std::transform(s.begin(), s.end(), s.begin(), [](unsigned char c) { return (char)std::tolower(c); });
     return s;
+}
+
+// IEEE binary16 bits -> float (FP16 factor storage read back on the host).
+float half_to_float(uint16_t h) {
+    const uint32_t sign = (uint32_t)(h >> 15) << 31;
+    const int e = (h >> 10) & 31;
+    uint32_t m = h & 1023u;
+    uint32_t bits;
+    if (e == 0) {
+        if (m == 0) {
+            bits = sign;
+        } else {  // subnormal: normalise
+            int k = -1;
+            do {
+                ++k;
+                m <<= 1;
+            } while (!(m & 1024u));
+            bits = sign | ((uint32_t)(127 - 15 - k) << 23) | ((m & 1023u) << 13);
+        }
+    } else if (e == 31) {
+        bits = sign | 0x7f800000u | (m << 13);
+    } else {
+        bits = sign | ((uint32_t)(e - 15 + 127) << 23) | (m << 13);
+    }
+    float f;
+    std::memcpy(&f, &bits, sizeof(f));
+    return f;
 }
 
 // quantization_string_to_int (python/randomforest_py.cpp:271-287)
@@ -468,16 +496,20 @@ class RandomForestClassifier {
         lowrank_ready_ = false;
     }
 
-    // Low-rank proximity factors: rank `rank`, 16 extra sketch columns, one
-    // power iteration; BF16 sketch storage with FP32 accumulation unless
-    // quant_mode is 'fp32'.  'int8' and 'nf4' store INT8 factors with one
-    // scale per column; 'fp16' and 'fp32' keep the FP32 factors.
+    // Low-rank proximity factors of P ~= I + A A^T: rank `rank`, 16 extra
+    // sketch columns, one power iteration; BF16 sketch storage with FP32
+    // accumulation unless quant_mode is 'fp32'.  The factors are then stored
+    // in the quant_mode's format ('fp16': FP16; 'int8': INT8 with one scale
+    // per column; 'nf4': the reference's 4-bit code, two per byte, with one
+    // scale per column) and every later use (get_lowrank_factors, MDS) reads
+    // the stored values back; 'fp32' keeps the FP32 factors.
     void compute_lowrank() {
         ensure_ctx();
-        const int n = nsample_, r = std::max(1, std::min(rank_, 64));
+        const int n = nsample_;
+        const int r = std::max(1, std::min(rank_, 64));
         lr_rank_ = r;
         lr_precision_ = quant_code_ == 0 ? 0 : 1;
-        lr_quantized_ = quant_code_ >= 2;
+        lr_quantized_ = quant_code_ >= 1;
         factors_.assign((size_t)n * r, 0.0f);
         NoGil ng;
         rfx_lowrank_opts o{};
@@ -489,12 +521,30 @@ class RandomForestClassifier {
         std::vector<float> ev(r);
         check(rfx_lowrank(ctx_, &o, factors_.data(), ev.data()), "low-rank proximity");
         if (lr_quantized_) {
-            std::vector<int8_t> q((size_t)n * r);
+            const size_t nk = (size_t)n * r;
             std::vector<float> sc(r);
-            check(rfx_lowrank_quantize(ctx_, 1, q.data(), sc.data()), "low-rank quantisation");
-            for (int i = 0; i < n; ++i)
-                for (int col = 0; col < r; ++col)
-                    factors_[(size_t)i * r + col] = (float)q[(size_t)i * r + col] * sc[col];
+            if (quant_code_ == 1) {  // FP16
+                std::vector<uint16_t> q(nk);
+                check(rfx_lowrank_quantize(ctx_, 4, q.data(), sc.data()), "low-rank quantisation");
+                for (size_t e = 0; e < nk; ++e) factors_[e] = half_to_float(q[e]);
+            } else if (quant_code_ == 2) {  // INT8
+                std::vector<int8_t> q(nk);
+                check(rfx_lowrank_quantize(ctx_, 1, q.data(), sc.data()), "low-rank quantisation");
+                for (int i = 0; i < n; ++i)
+                    for (int col = 0; col < r; ++col)
+                        factors_[(size_t)i * r + col] = (float)q[(size_t)i * r + col] * sc[col];
+            } else {  // NF4
+                std::vector<uint8_t> q((nk + 1) / 2);
+                check(rfx_lowrank_quantize(ctx_, 3, q.data(), sc.data()), "low-rank quantisation");
+                for (int i = 0; i < n; ++i)
+                    for (int col = 0; col < r; ++col) {
+                        const size_t e = (size_t)i * r + col;
+                        const unsigned b = q[e >> 1];
+                        const unsigned code = (e & 1) ? (b >> 4) : (b & 15u);
+                        const float v = code <= 7 ? (float)code / 7.0f : -(float)(code - 8) / 7.0f;
+                        factors_[e] = v * sc[col];
+                    }
+            }
         }
         lowrank_ready_ = true;
     }

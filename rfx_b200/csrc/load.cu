@@ -113,7 +113,43 @@ bag_kernel(const int32_t* __restrict__ nin, int n, uint8_t* __restrict__ inbag, 
     }
 }
 
+// Padded device trees (tree t at slots t*maxnode.., as the reference's GPU
+// grower leaves them, cuda/rf_growtree.cu:888-) gathered into the compact
+// layout (tree t at offs[t]..offs[t+1]); one CTA per tree.
+__global__ void __launch_bounds__(LD_THREADS)
+gather_padded_kernel(const int64_t* __restrict__ offs, int maxnode, int maxcat, const int32_t* __restrict__ ps,
+                     const int32_t* __restrict__ pbv, const float* __restrict__ pxs, const int32_t* __restrict__ ptm,
+                     const int32_t* __restrict__ pnc, const int32_t* __restrict__ pcg, int32_t* __restrict__ status,
+                     int32_t* __restrict__ bestvar, float* __restrict__ split, int32_t* __restrict__ treemap,
+                     int32_t* __restrict__ nodeclass, int32_t* __restrict__ catgoleft) {
+    const int t = blockIdx.x;
+    const int64_t o = offs[t];
+    const int nn = (int)(offs[t + 1] - o);
+    const size_t src = (size_t)t * maxnode;
+    for (int k = threadIdx.x; k < nn; k += LD_THREADS) {
+        status[o + k] = ps[src + k];
+        bestvar[o + k] = pbv[src + k];
+        split[o + k] = pxs[src + k];
+        nodeclass[o + k] = pnc[src + k];
+    }
+    for (int k = threadIdx.x; k < 2 * nn; k += LD_THREADS) treemap[2 * o + k] = ptm[2 * src + k];
+    if (pcg)
+        for (long long k = threadIdx.x; k < (long long)nn * maxcat; k += LD_THREADS)
+            catgoleft[o * maxcat + k] = pcg[src * maxcat + k];
+}
+
 }  // namespace
+
+cudaError_t launch_gather_padded(cudaStream_t s, int T, int maxnode, int maxcat, const int64_t* d_offs,
+                                 const int32_t* status_p, const int32_t* bestvar_p, const float* split_p,
+                                 const int32_t* treemap_p, const int32_t* nodeclass_p, const int32_t* catgoleft_p,
+                                 int32_t* status, int32_t* bestvar, float* split, int32_t* treemap,
+                                 int32_t* nodeclass, int32_t* catgoleft) {
+    gather_padded_kernel<<<T, LD_THREADS, 0, s>>>(d_offs, maxnode, maxcat, status_p, bestvar_p, split_p, treemap_p,
+                                                  nodeclass_p, catgoleft_p, status, bestvar, split, treemap, nodeclass,
+                                                  catgoleft);
+    return cudaGetLastError();
+}
 
 rfx_status launch_pack_forest(cudaStream_t s, int T, int n, int p, const int64_t* d_offs, const int32_t* status,
                               const int32_t* bestvar, const float* split, const int32_t* treemap,

@@ -18,6 +18,7 @@
 //           Rayleigh-Ritz projection, in FP32.
 // FP64 is used for the k' x k' Gram (CholeskyQR2) and the eigensolve only.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_fp8.h>
 
 #include <algorithm>
@@ -454,6 +455,58 @@ __global__ void quant_fp8_kernel(const float* __restrict__ A, int n, int k, cons
     q[idx] = __nv_fp8_e4m3(s > 0.0f ? A[idx] / s : 0.0f);
 }
 
+// NF4 storage: the reference's 16-level code (fp32_to_nf4 / nf4_to_fp32,
+// include/rf_quantization_kernels.hpp:37-65: codes 0..7 hold v/7 for v in
+// [0, 1], codes 8..15 hold -(code - 8)/7 for v in [-1, 0)), applied to A / s
+// with one scale s = max |A[:, c]| per column so that every column uses the
+// whole code range (the reference applies the code to unscaled factors);
+// two codes per byte, the lower nibble first, over the row-major n x k entries
+// (cuda/rf_proximity_lowrank.cu:353-383 packs its flat factor array the same
+// way); an odd count leaves the last upper nibble 0.
+__device__ __forceinline__ uint32_t nf4_code(float v) {
+    if (v >= 0.0f) return (uint32_t)fminf(7.0f, roundf(v * 7.0f));
+    return (uint32_t)fmaxf(8.0f, roundf(8.0f - v * 7.0f));
+}
+
+__device__ __forceinline__ float nf4_value(uint32_t code) {
+    return code <= 7 ? (float)code / 7.0f : -(float)(code - 8) / 7.0f;
+}
+
+__global__ void quant_nf4_kernel(const float* __restrict__ A, int n, int k, const unsigned int* __restrict__ mx,
+                                 uint8_t* __restrict__ q, float* __restrict__ scale) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // one byte = two entries
+    if (idx < k) scale[idx] = __uint_as_float(mx[idx]);
+    const int64_t count = (int64_t)n * k;
+    if (idx >= (count + 1) / 2) return;
+    const int64_t e = 2 * idx;
+    const float s0 = __uint_as_float(mx[e % k]);
+    const uint32_t lo = nf4_code(s0 > 0.0f ? A[e] / s0 : 0.0f);
+    uint32_t hi = 0;
+    if (e + 1 < count) {
+        const float s1 = __uint_as_float(mx[(e + 1) % k]);
+        hi = nf4_code(s1 > 0.0f ? A[e + 1] / s1 : 0.0f);
+    }
+    q[idx] = (uint8_t)(lo | (hi << 4));
+}
+
+__global__ void dequant_nf4_kernel(const uint8_t* __restrict__ q, const float* __restrict__ scale, int n, int k,
+                                   float* __restrict__ A) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)n * k) return;
+    const uint32_t b = q[idx >> 1];
+    A[idx] = nf4_value((idx & 1) ? (b >> 4) : (b & 15u)) * scale[idx % k];
+}
+
+// FP16 storage (the reference's FP16 level stores the factors as __half with
+// no scale, cuda/rf_proximity_lowrank.cu:300-331); the scales are 1.
+__global__ void quant_f16_kernel(const float* __restrict__ A, int n, int k, __half* __restrict__ q,
+                                 float* __restrict__ scale) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < k) scale[idx] = 1.0f;
+    if (idx >= (int64_t)n * k) return;
+    q[idx] = __float2half_rn(A[idx]);
+}
+
 template <typename TQ>
 __global__ void dequant_kernel(const TQ* __restrict__ q, const float* __restrict__ scale, int n, int k,
                                float* __restrict__ A) {
@@ -689,8 +742,13 @@ rfx_status lowrank_quantize(Ctx* c, const float* dA, int k, int format, void* dq
     colmax_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, mx);
     if (format == 1)
         quant_i8_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, mx, (int8_t*)dq, dscale);
-    else
+    else if (format == 2)
         quant_fp8_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, mx, (__nv_fp8_e4m3*)dq, dscale);
+    else if (format == 3)
+        quant_nf4_kernel<<<nblk(std::max<int64_t>(((int64_t)n * k + 1) / 2, k)), 256, 0, s>>>(dA, n, k, mx,
+                                                                                             (uint8_t*)dq, dscale);
+    else
+        quant_f16_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>(dA, n, k, (__half*)dq, dscale);
     c->launches += 2;
     RFX_CUDA(cudaGetLastError());
     RFX_CUDA(cudaStreamSynchronize(s));
@@ -702,9 +760,13 @@ rfx_status lowrank_dequantize(Ctx* c, const void* dq, const float* dscale, int k
     const int n = c->n;
     if (format == 1)
         dequant_kernel<int8_t><<<nblk((int64_t)n * k), 256, 0, s>>>((const int8_t*)dq, dscale, n, k, dA);
-    else
+    else if (format == 2)
         dequant_kernel<__nv_fp8_e4m3><<<nblk((int64_t)n * k), 256, 0, s>>>((const __nv_fp8_e4m3*)dq, dscale, n, k,
                                                                            dA);
+    else if (format == 3)
+        dequant_nf4_kernel<<<nblk((int64_t)n * k), 256, 0, s>>>((const uint8_t*)dq, dscale, n, k, dA);
+    else
+        dequant_kernel<__half><<<nblk((int64_t)n * k), 256, 0, s>>>((const __half*)dq, dscale, n, k, dA);
     c->launches += 1;
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;

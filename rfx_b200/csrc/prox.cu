@@ -280,7 +280,8 @@ constexpr int OPP_TILE = 32;
 
 __global__ void __launch_bounds__(OPP_TILE * 8)
 opp_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase,
-           const int32_t* __restrict__ memb, int n, int T, int2* __restrict__ opp) {
+           const int32_t* __restrict__ memb, int n, int T, const uint8_t* __restrict__ keyflag,
+           int2* __restrict__ opp) {
     __shared__ int2 tile[OPP_TILE][OPP_TILE + 1];
     const int i0 = blockIdx.x * OPP_TILE, t0 = blockIdx.y * OPP_TILE;
     const int tx = threadIdx.x % OPP_TILE, ty = threadIdx.x / OPP_TILE;
@@ -289,7 +290,8 @@ opp_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ segoff, 
         int2 v = make_int2(0, 0);
         if (t < T && i < n) {
             const int k = __ldg(key + (size_t)t * n + i);
-            if (k >= 0) {
+            // keys of hub leaves (counted on the tensor cores, hubs.cu) are left out
+            if (k >= 0 && !(keyflag && keyflag[segbase[t] + k])) {
                 const int32_t* so = segoff + segbase[t];
                 int lo = __ldg(so + (k ^ 1)), hi = __ldg(so + (k ^ 1) + 1);
                 const int s1 = hi;
@@ -341,9 +343,12 @@ row_order_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ se
     }
 }
 
-// Launch shapes of the row kernel the autotuner chooses from (threads per
-// CTA); 512 is the default.
+// Launch shapes of the row kernels the autotuner chooses from: 0..2
+// pairs_row16_kernel with 256/512/1024 threads, 3..5 pairs_row2_kernel with
+// 256/512/1024 threads.
 constexpr int R16_THREADS = 512;
+constexpr int PAIRS_SHAPES = 6;
+constexpr int PAIRS_DEFAULT_SHAPE = 4;
 
 template <int NW>
 __device__ __forceinline__ int block_exclusive_scan(int v, int* wtot, int lane, int w, int* total) {
@@ -520,6 +525,209 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
 }
 
 // ---------------------------------------------------------------------------
+// Stage 2, full-row form without per-round block barriers (pairs_row2_kernel).
+//   One CTA per row, u16 counters for the whole row as in pairs_row16_kernel.
+//   Phase A: warps claim chunks of 32 trees from a CTA counter (lane = tree)
+//     and count the chunk's ranges themselves: ranges shorter than 32 members
+//     are expanded element by element over the warp (a lane finds its range
+//     by a binary search over the warp's inclusive length scan, so no lane
+//     idles on a short range), ranges of 32..V2_LONG-1 members are walked by
+//     the whole warp with four loads in flight per lane, and ranges of
+//     V2_LONG or more are put on a per-CTA list.
+//   Phase B (after one barrier): the listed ranges are cut into pieces of
+//     V2_PIECE members dealt round-robin over the warps (the running piece
+//     count of the ranges before a range fixes where its first piece goes),
+//     eight loads in flight per lane.
+//   Three barriers per row: after zeroing, between the phases, before the
+//   write-out.
+// ---------------------------------------------------------------------------
+constexpr int V2_LONG = 256;
+constexpr int V2_PIECE = 256;  // 8 members per lane
+constexpr int V2_LIST = 256;   // listed long ranges per row (more are walked in phase A)
+
+__device__ __forceinline__ void count16(uint32_t* acc, int j) { atomicAdd(acc + (j >> 1), 1u << ((j & 1) << 4)); }
+
+template <int NT>
+__global__ void __launch_bounds__(NT)
+pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
+                  int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
+                  int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+    constexpr int NW = NT / 32;
+    extern __shared__ uint32_t acc[];  // `words` words, two u16 counters each
+    __shared__ long long lbase[V2_LIST];
+    __shared__ int llen[V2_LIST];
+    __shared__ int s_nlong, s_chunk;
+    const int i = order[blockIdx.x];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (hubt && hub_state[1] > 0) {
+        // counters start from the hub leaves' counts: row i of the S_hub tiles
+        // (row block I = i / 128, column tiles J = i / 256 .. NJ - 1; 16-byte
+        // chunk q of a tile row stored at slot q ^ (row % 16)), u8 -> u16
+        const int NJ = (n + 255) >> 8, I = i >> 7, r = i & 127, J0 = i >> 8;
+        const uint8_t* rowt = hubt + (size_t)(hub_row_start(I, NJ) - (I >> 1)) * 32768u + (size_t)r * 256u;
+        const int nch = (NJ - J0) * 16;
+        for (int k = tid; k < nch; k += NT) {
+            const int J = J0 + (k >> 4), slot = k & 15, q = slot ^ (r & 15);
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(rowt + (size_t)J * 32768u + slot * 16));
+            const uint32_t b[4] = {v.x, v.y, v.z, v.w};
+            uint32_t o[8];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                o[2 * h] = (b[h] & 0xffu) | ((b[h] & 0xff00u) << 8);
+                o[2 * h + 1] = ((b[h] >> 16) & 0xffu) | ((b[h] >> 8) & 0xff0000u);
+            }
+            uint4* dst = reinterpret_cast<uint4*>(acc + (size_t)J * 128 + q * 8);
+            dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+            dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+        }
+        for (int k = NJ * 128 + tid; k < words; k += NT) acc[k] = 0u;
+    } else {
+        uint4* a4 = reinterpret_cast<uint4*>(acc);
+        const int w4 = words >> 2;
+        for (int k = tid; k < w4; k += NT) a4[k] = make_uint4(0u, 0u, 0u, 0u);
+        for (int k = (w4 << 2) + tid; k < words; k += NT) acc[k] = 0u;
+    }
+    if (tid == 0) {
+        s_nlong = 0;
+        s_chunk = 0;
+    }
+    __syncthreads();
+    unsigned long long my_pairs = 0;
+    const int2* orow = opp + (size_t)i * T;
+    const int nchunks = (T + 31) >> 5;
+    for (;;) {
+        int ch = 0;
+        if (lane == 0) ch = atomicAdd(&s_chunk, 1);
+        ch = __shfl_sync(0xffffffffu, ch, 0);
+        if (ch >= nchunks) break;
+        const int t = (ch << 5) + lane;
+        const int2 v = t < T ? __ldg(orow + t) : make_int2(0, 0);
+        int len = v.y;
+        my_pairs += (unsigned long long)len;
+        if (len >= V2_LONG) {
+            const int slot = atomicAdd(&s_nlong, 1);
+            if (slot < V2_LIST) {
+                lbase[slot] = (long long)t * n + v.x;
+                llen[slot] = len;
+                len = 0;
+            }
+        }
+        // ranges of 32 members or more that stayed here: the whole warp walks each
+        unsigned med = __ballot_sync(0xffffffffu, len >= 32);
+        while (med) {
+            const int src = __ffs(med) - 1;
+            med &= med - 1;
+            const int ml = __shfl_sync(0xffffffffu, len, src);
+            const int ts = (ch << 5) + src;
+            const int xs = __shfl_sync(0xffffffffu, v.x, src);
+            const int32_t* mp = memb + (size_t)ts * n + xs;
+            int off = lane;
+            for (; off + 96 < ml; off += 128) {
+                const int j0 = __ldg(mp + off), j1 = __ldg(mp + off + 32);
+                const int j2 = __ldg(mp + off + 64), j3 = __ldg(mp + off + 96);
+                count16(acc, j0);
+                count16(acc, j1);
+                count16(acc, j2);
+                count16(acc, j3);
+            }
+            for (; off < ml; off += 32) count16(acc, __ldg(mp + off));
+        }
+        if (len >= 32) len = 0;
+        // the short ranges, element by element over the warp
+        int incl = len;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        const int xoff = v.x - (incl - len);  // member index = tree base + xoff + element
+        for (int base = 0; base < total; base += 64) {
+            int e[2], j[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                e[u] = base + (u << 5) + lane;
+                const int ec = min(e[u], total - 1);
+                int c = 0;  // number of lanes whose inclusive end is <= ec
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) {
+                    const int x = __shfl_sync(0xffffffffu, incl, c + d - 1);
+                    if (x <= ec) c += d;
+                }
+                const int xo = __shfl_sync(0xffffffffu, xoff, c);
+                j[u] = e[u] < total ? __ldg(memb + (size_t)((ch << 5) + c) * n + (xo + e[u])) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                if (j[u] >= 0) count16(acc, j[u]);
+        }
+    }
+    __syncthreads();
+    // phase B: the listed long ranges, pieces dealt round-robin over the warps
+    const int L = min(s_nlong, V2_LIST);
+    int run = 0;
+    for (int c = 0; c < L; ++c) {
+        const long long b = lbase[c];
+        const int len = llen[c];
+        const int np = (len + V2_PIECE - 1) / V2_PIECE;
+        int k = w - run;
+        if (k < 0) k += NW;
+        for (; k < np; k += NW) {
+            const int32_t* mp = memb + b + (long long)k * V2_PIECE;
+            const int lim = min(V2_PIECE, len - k * V2_PIECE);
+            int j[V2_PIECE / 32];
+#pragma unroll
+            for (int u = 0; u < V2_PIECE / 32; ++u) {
+                const int o = (u << 5) + lane;
+                j[u] = o < lim ? __ldg(mp + o) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < V2_PIECE / 32; ++u)
+                if (j[u] >= 0) count16(acc, j[u]);
+        }
+        run = (run + np) % NW;
+    }
+    __syncthreads();
+    const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
+    const uint16_t* a16 = reinterpret_cast<const uint16_t*>(acc);
+    int32_t* srow = S + rowoff + i;
+    const int len = n - i;
+    int head = len, nv = 0;
+    if ((reinterpret_cast<uintptr_t>(S) & 15) == 0) {
+        head = min(len, (int)((4 - ((rowoff + i) & 3)) & 3));
+        nv = (len - head) >> 2;
+    }
+    for (int h = tid; h < head; h += NT) srow[h] = (int32_t)a16[i + h];
+    int4* s4 = reinterpret_cast<int4*>(srow + head);
+    const int jg = i + head;
+    const int sh = (jg & 3) * 16;
+    const int gb = jg >> 2;
+    const int ngroups = words >> 1;
+    const uint2* a64 = reinterpret_cast<const uint2*>(acc);
+    for (int v0 = w * 32; v0 < nv; v0 += NT) {
+        const int v = v0 + lane;
+        const int g = gb + v;
+        const uint2 cg = g < ngroups ? a64[g] : make_uint2(0u, 0u);
+        uint2 nx;
+        nx.x = __shfl_down_sync(0xffffffffu, cg.x, 1);
+        nx.y = __shfl_down_sync(0xffffffffu, cg.y, 1);
+        if (lane == 31) nx = g + 1 < ngroups ? a64[g + 1] : make_uint2(0u, 0u);
+        const unsigned long long lo = ((unsigned long long)cg.y << 32) | cg.x;
+        const unsigned long long hi = ((unsigned long long)nx.y << 32) | nx.x;
+        const unsigned long long e = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
+        if (v < nv)
+            s4[v] = make_int4((int)(e & 0xffffu), (int)((e >> 16) & 0xffffu), (int)((e >> 32) & 0xffffu),
+                              (int)(e >> 48));
+    }
+    for (int j = i + head + 4 * nv + tid; j < n; j += NT) srow[j - i] = (int32_t)a16[j];
+    if (pairs) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
+        if (lane == 0 && my_pairs) atomicAdd(pairs, my_pairs);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // finishprox
 // ---------------------------------------------------------------------------
 constexpr int FP_TILE = 32;
@@ -639,32 +847,74 @@ bool use_row16(const Ctx* c, int dev_smem) {
     return c->T < 65536 && words * 4 + 20 * 1024 <= (size_t)dev_smem;
 }
 
+// Hub leaves on the tensor cores (hubs.cu): by default from n = 16,384 (at
+// smaller n the dense n x n tiles cost more than the few hub updates they
+// save); RFX_PAIRS_HUBS=0 turns the part off, =1 forces it on at any n.  The
+// counts are the same either way.
+bool use_hubs(const Ctx* c) {
+    const char* e = getenv("RFX_PAIRS_HUBS");
+    if (e && std::string(e) == "0") return false;
+    if (e && std::string(e) == "1") return true;
+    return c->n >= 16384 && c->T >= 16;
+}
+
 rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
     int dev_smem = 0;
     RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
     if (use_row16(c, dev_smem)) {
+        const int NJ = hub_tiles_nj(c->n);
+        const int hub_words = NJ * 128 + 2;
+        const bool hubs = use_hubs(c) && (size_t)hub_words * 4 + 20 * 1024 <= (size_t)dev_smem;
         rfx_status st0 = dalloc(c, &c->d_opp, (size_t)c->T * c->n);
         if (st0 == RFX_OK) st0 = dalloc(c, &c->d_order, (size_t)c->n);
+        if (st0 == RFX_OK && hubs) st0 = dalloc(c, &c->d_hubflag, (size_t)c->h_segbase[c->T]);
+        if (st0 == RFX_OK && hubs) st0 = dalloc(c, &c->d_hubtiles, hub_tile_bytes(c->n));
+        if (st0 == RFX_OK && hubs) st0 = dalloc(c, &c->d_hubstate, (size_t)8);
         if (st0 != RFX_OK) return st0;
-        RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
+        unsigned long long* hub_pairs = reinterpret_cast<unsigned long long*>(c->d_hubstate + 4);
+        if (hubs) {
+            RFX_CUDA(cudaMemsetAsync(c->d_hubstate, 0, 8 * sizeof(int32_t), c->stream));
+            StageTimer st(c, ST_HUBS, 5);
+            if (rfx_status s1 = launch_hub_tiles(c, c->d_hubflag, c->d_hubtiles, c->d_hubstate, hub_pairs)) return s1;
+        }
         {
             StageTimer st(c, ST_OPP, 2);
             dim3 g((c->n + OPP_TILE - 1) / OPP_TILE, (c->T + OPP_TILE - 1) / OPP_TILE);
             opp_kernel<<<g, OPP_TILE * 8, 0, c->stream>>>(c->d_key, c->d_segoff, c->d_segbase, c->d_memb, c->n,
-                                                           c->T, c->d_opp);
+                                                           c->T, hubs ? c->d_hubflag : nullptr, c->d_opp);
             RFX_CUDA(cudaGetLastError());
             row_order_kernel<<<1, 1024, 0, c->stream>>>(c->d_key, c->d_segoff, c->d_segbase, c->d_memb, c->n,
                                                         c->d_order);
             RFX_CUDA(cudaGetLastError());
         }
-        const size_t smem = (size_t)r16_words(c->n) * sizeof(uint32_t);
+        const int words = hubs ? std::max(r16_words(c->n), hub_words) : r16_words(c->n);
+        const size_t smem = (size_t)words * sizeof(uint32_t);
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<256>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<512>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<1024>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<256>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<512>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<1024>, dev_smem)) return s0;
         StageTimer st(c, ST_PAIRS, 1);
-        return autotune(c, TK_PAIRS16, 3, 1, [&](int shape) -> rfx_status {
-            RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
-            if (shape == 0)
+        // with hub tiles only the second row kernel (which starts from them) runs
+        const int tk = hubs ? TK_PAIRS_HUB : TK_PAIRS16;
+        const int nshape = hubs ? 3 : PAIRS_SHAPES;
+        const int defshape = hubs ? 1 : PAIRS_DEFAULT_SHAPE;
+        return autotune(c, tk, nshape, defshape, [&](int shape) -> rfx_status {
+            // the pair counter restarts from the hub leaves' pair updates
+            if (hubs)
+                RFX_CUDA(cudaMemcpyAsync(c->d_pairs, hub_pairs, sizeof(unsigned long long), cudaMemcpyDeviceToDevice,
+                                         c->stream));
+            else
+                RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
+            if (hubs) shape += 3;
+            if (shape >= 3) {
+                const int nt = 256 << (shape - 3);
+                auto kern = shape == 3 ? pairs_row2_kernel<256> : shape == 4 ? pairs_row2_kernel<512>
+                                                                             : pairs_row2_kernel<1024>;
+                kern<<<c->n, nt, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, words,
+                                                    hubs ? c->d_hubtiles : nullptr, c->d_hubstate, dS, c->d_pairs);
+            } else if (shape == 0)
                 pairs_row16_kernel<256><<<c->n, 256, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T,
                                                                        dS, c->d_pairs);
             else if (shape == 2)
@@ -709,7 +959,7 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
         RFX_CUDA(cudaGetLastError());
     }
     dim3 g((a.n + OPP_TILE - 1) / OPP_TILE, (a.T + OPP_TILE - 1) / OPP_TILE);
-    opp_kernel<<<g, OPP_TILE * 8, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.T, a.opp);
+    opp_kernel<<<g, OPP_TILE * 8, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.T, nullptr, a.opp);
     RFX_CUDA(cudaGetLastError());
     row_order_kernel<<<1, 1024, 0, stream>>>(a.key, a.segoff, a.segbase, a.memb, a.n, a.order);
     RFX_CUDA(cudaGetLastError());

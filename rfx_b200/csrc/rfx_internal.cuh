@@ -38,7 +38,8 @@ enum : uint32_t {
 
 enum Stage : int {
     ST_ROUTE = 0, ST_CSR, ST_PAIRS, ST_FINISHPROX, ST_VARIMP_TREE, ST_VARIMP_SAMPLE, ST_VARIMP_FEATURE,
-    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_OPP, ST_LR_PRODUCT, ST_LR_ORTH, ST_MDS_FACTORS, ST_MDS_FULL, ST_COUNT
+    ST_PREDICT, ST_OOB, ST_LOCALIMP, ST_OPP, ST_LR_PRODUCT, ST_LR_ORTH, ST_MDS_FACTORS, ST_MDS_FULL, ST_HUBS,
+    ST_COUNT
 };
 
 struct Ctx {
@@ -88,6 +89,9 @@ struct Ctx {
     int32_t* d_memb = nullptr;          // T*n: members grouped by key, ascending within a key;
                                         // samples without a terminal node follow the keyed members
     int2* d_opp = nullptr;              // n*T: opposite-status member range cut to members > i
+    uint8_t* d_hubflag = nullptr;       // segbase[T]: 1 for the keys of hub leaves (hubs.cu)
+    uint8_t* d_hubtiles = nullptr;      // S_hub upper-triangle tiles, one byte per entry
+    int32_t* d_hubstate = nullptr;      // [0] threshold bin, [1] hub count, [4..5] hub pair updates (u64)
     int32_t* d_order = nullptr;         // n: row processing order
     int32_t* d_votes = nullptr;         // n*nclass
     int32_t* d_nout = nullptr;          // n
@@ -270,13 +274,30 @@ rfx_status launch_route(Ctx* c);
 rfx_status launch_build_csr(Ctx* c);
 
 // Autotuned stages: kernel ids and the launch shapes each offers.
-enum TuneKernel : int { TK_ROUTE = 0, TK_PAIRS16 = 1, TK_VWALK = 2, TK_ROUTE_LEAF = 3 };
+enum TuneKernel : int { TK_ROUTE = 0, TK_PAIRS16 = 1, TK_VWALK = 2, TK_ROUTE_LEAF = 3, TK_PAIRS_HUB = 4 };
 rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<rfx_status(int)>& run);
 rfx_status launch_pack_forest(cudaStream_t s, int T, int n, int p, const int64_t* d_offs, const int32_t* status,
                               const int32_t* bestvar, const float* split, const int32_t* treemap,
                               const int32_t* d_cat, const int32_t* nin, DNode* nodes, int32_t* leafidx,
                               uint64_t* iv, int32_t* nleaf, uint8_t* inbag, int32_t* noob, LoadError* err);
+cudaError_t launch_gather_padded(cudaStream_t s, int T, int maxnode, int maxcat, const int64_t* d_offs,
+                                 const int32_t* status_p, const int32_t* bestvar_p, const float* split_p,
+                                 const int32_t* treemap_p, const int32_t* nodeclass_p, const int32_t* catgoleft_p,
+                                 int32_t* status, int32_t* bestvar, float* split, int32_t* treemap,
+                                 int32_t* nodeclass, int32_t* catgoleft);
 rfx_status launch_pairs_upper(Ctx* c, int32_t* dS);
+// S_hub tiles of the hub leaves (hubs.cu)
+int hub_tiles_nj(int n);
+size_t hub_tile_bytes(int n);
+// first tile of row block I (128 rows) in the S_hub tile list: the tiles
+// (I, J), J = I/2 .. NJ-1 (256 columns each), row block after row block
+__host__ __device__ inline long long hub_row_start(int I, int NJ) {
+    if (I <= 0) return 0;
+    const long long a = (long long)(I - 1);
+    return (long long)I * NJ - (a * a) / 4;
+}
+rfx_status launch_hub_tiles(Ctx* c, uint8_t* keyflag, uint8_t* tiles, int32_t* hub_state,
+                            unsigned long long* hub_pairs);
 rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full);
 rfx_status launch_oob_summary(Ctx* c, float* d_err_out, int32_t* d_pred, float* d_proba);
 rfx_status launch_varimp(Ctx* c, int impn);

@@ -5,7 +5,9 @@
 //                       D[(j,a), b] = sum_i (u_ij A_ia) A_ib, M = s*k rows,
 //                       N = k, reduction over the n samples split across CTAs
 //                       (each CTA owns one 128-row M tile and one K range and
-//                       adds its FP32 tile into the global stack).
+//                       writes its FP32 tile to its own slot of a partial
+//                       stack; mstack_reduce_kernel adds the slots in K-range
+//                       order, so the result does not depend on CTA timing).
 //   quadform_tc_kernel: T2_ij = a_i^T M_j a_i: D[i, (j,b)] = sum_a A_ia M_j[b][a]
 //                       for a 128-sample tile in TMEM, then the epilogue reads
 //                       each row from TMEM and dots every 64-column block with
@@ -99,7 +101,8 @@ constexpr int KCH = 64;  // samples per K chunk
 // grid: (s*k/128 M tiles, K splits); k in {16, 32, 64}; u is n x S (S = 16)
 template <int K_, int S_>
 __global__ void __launch_bounds__(TC_THREADS) mstack_tc_kernel(const float* __restrict__ A, const float* __restrict__ u,
-                                                              int n, float* __restrict__ M, uint32_t* __restrict__ err) {
+                                                              int n, float* __restrict__ Mpart,
+                                                              uint32_t* __restrict__ err) {
     constexpr int JT = 128 / K_;  // j values per M tile
     constexpr uint32_t A_BYTES = 128 * KCH * 2, B_BYTES = K_ * KCH * 2;
     constexpr uint32_t TM_COLS = K_ < 32 ? 32 : K_;
@@ -171,23 +174,37 @@ __global__ void __launch_bounds__(TC_THREADS) mstack_tc_kernel(const float* __re
             phase[st] ^= 1u;
         }
     asm volatile("tcgen05.fence::after_thread_sync;");
+    // this K range's slot of the partial stack
+    float* M = Mpart + (size_t)blockIdx.y * S_ * K_ * K_;
+    const int r = warp * 32 + lane;
+    const int j = j0 + r / K_, a = r % K_;
     if (!ok) {
         if (lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
     } else if (issued > 0) {
         // warp w reads TMEM lanes 32w..32w+31 = tile rows; K_ columns
-        const int r = warp * 32 + lane;
-        const int j = j0 + r / K_, a = r % K_;
 #pragma unroll
         for (int c = 0; c < K_; c += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, v);
+            float4* dst = reinterpret_cast<float4*>(M + ((size_t)j * K_ + a) * K_ + c);
 #pragma unroll
-            for (int q = 0; q < 16; ++q) atomicAdd(M + ((size_t)j * K_ + a) * K_ + c + q, v[q]);
+            for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
         }
+    } else {
+        for (int c = 0; c < K_; ++c) M[((size_t)j * K_ + a) * K_ + c] = 0.0f;  // an empty K range adds nothing
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, TM_COLS);
+}
+
+// M = sum over the K ranges of their partial stacks, in K-range order
+__global__ void mstack_reduce_kernel(const float* __restrict__ Mpart, int parts, size_t count, float* __restrict__ M) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    float acc = 0.0f;
+    for (int p = 0; p < parts; ++p) acc += Mpart[(size_t)p * count + e];
+    M[e] = acc;
 }
 
 // grid: n/128 sample tiles; the s*k rows of the M stack in passes of NP rows
@@ -283,14 +300,21 @@ rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32
     cudaStream_t s = c->stream;
     const int n = c->n;
     constexpr int S = 16;
-    RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S * k * k, s));
-    const int ksplit = 37;  // 296 CTAs for rank 64: two per SM, few partial-tile atomics
+    const int ksplit = 37;  // 296 CTAs for rank 64: two per SM
+    Scratch sc(c);
+    const size_t count = (size_t)S * k * k;
+    float* Mpart = sc.get<float>(count * ksplit);
+    if (!Mpart) {
+        set_error("tensor-core factor MDS: scratch allocation failed");
+        return RFX_ERR_OOM;
+    }
     auto run = [&](auto mk, auto qk, int K) -> rfx_status {
         const int sm_m = 2 * (128 * KCH * 2 + K * KCH * 2);
         const int sm_q = 128 * K * 2 + 256 * K * 2;
         RFX_CUDA(cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_m));
         RFX_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_q));
-        mk<<<dim3(S * K / 128, ksplit), TC_THREADS, sm_m, s>>>(dA, u32, n, M, c->d_err);
+        mk<<<dim3(S * K / 128, ksplit), TC_THREADS, sm_m, s>>>(dA, u32, n, Mpart, c->d_err);
+        mstack_reduce_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(Mpart, ksplit, count, M);
         qk<<<(n + 127) / 128, TC_THREADS, sm_q, s>>>(dA, M, n, T2, c->d_err);
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
@@ -308,7 +332,7 @@ rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32
             return RFX_ERR_UNSUPPORTED;
     }
     if (st != RFX_OK) return st;
-    c->launches += 2;
+    c->launches += 3;
     return RFX_OK;
 }
 
