@@ -48,7 +48,10 @@ typedef struct rfx_ctx rfx_ctx;
  * rf::g_config, include/rf_config.hpp:17-114, has no counterpart here). */
 typedef struct rfx_config {
     int32_t device;          /* CUDA device ordinal */
-    int32_t use_casewise;    /* must be 0: case-wise weighting is rejected */
+    int32_t use_casewise;    /* 1: the reference's use_casewise=True weighting
+                                (votes, importance and pair sums weighted by
+                                bootstrap multiplicities; see rfx_casewise_votes,
+                                rfx_proximity_upper_f64) */
     int32_t n_threads_cpu;   /* host threads for rfx_grow_forest (0 = all) */
     int32_t reserved[5];
 } rfx_config;
@@ -326,6 +329,44 @@ rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count);
  * with each other: serialise them. */
 rfx_status rfx_pair_counts_noalloc(const int32_t* leaf, const uint8_t* inbag, int32_t n, int32_t ntree,
                                    int32_t max_leaves, int32_t* S, size_t len, void* stream);
+
+/* Case-wise weighting (use_casewise = 1 in rfx_config; the reference's
+ * bootstrap-frequency weighting, src/rf_random_forest.cpp:1049-1153,
+ * src/rf_varimp.cpp:138-236, src/rf_proximity.cpp:195-222).  tnodewt of a
+ * terminal node = the mean bootstrap multiplicity of the in-bag samples that
+ * reach it; an OOB vote counts tnodewt of the node it ends on.
+ * rfx_casewise_votes writes the weighted OOB votes q (n x nclass float, the
+ * reference's q_) and optionally the doubled nout; rfx_oob_summary and
+ * rfx_varimp of a case-wise context use these weights (importance: right,
+ * rightimp, qimp, qimpm weighted by tnodewt of the node each (permuted) walk
+ * reaches).  In a case-wise context rfx_route_oob refuses an int32 q and
+ * rfx_proximity_upper_i32 refuses (the pair weights are FP64).  Every sum runs
+ * in the reference's order: results are bit-identical to it. */
+rfx_status rfx_casewise_votes(rfx_ctx* ctx, float* q, int32_t* nout);
+
+/* FP64 pair sums S = C + C^T (packed upper triangle with the diagonal, 0 on
+ * it): C[i][j] += nin[j] / nodesize for every tree where i is OOB and j is
+ * in-bag in i's leaf (nodesize = the leaf's in-bag multiplicities summed) in a
+ * case-wise context, += 1 otherwise (then S equals the INT32 counts);
+ * cpu_proximity's dense branch, src/rf_proximity.cpp:99-231, summed tree by
+ * tree as the reference does.  S: host or device, n(n+1)/2 doubles. */
+rfx_status rfx_proximity_upper_f64(rfx_ctx* ctx, double* S, size_t len);
+
+/* cpu_finishprox (src/rf_finishprox.cpp:12-74) of FP64 sums from
+ * rfx_proximity_upper_f64; S and P host or device memory, P as in
+ * rfx_finishprox (full n x n or the packed upper triangle, float32). */
+rfx_status rfx_finishprox_f64(rfx_ctx* ctx, const double* S, float* P, int full);
+
+/* RF-GAP proximity (cpu_proximity_rfgap, src/rf_proximity.cpp:238-391, the
+ * reference's use_rfgap=True): pGAP(i,j) = (1/|S_i|) sum over the trees where
+ * i is OOB of c_j / |M_i| for the in-bag samples j of i's node (c_j = j's
+ * bootstrap multiplicity, |M_i| = the multiplicities of those samples summed,
+ * nodes = the node ids of testreebag for OOB samples and of
+ * find_terminal_node for in-bag ones), P = (pGAP + pGAP^T) / 2 off the
+ * diagonal, 1 on the diagonal of a sample never OOB (else 0).  P: host or
+ * device, the packed upper triangle with the diagonal, FP64 — the final
+ * matrix (no finishprox).  Bit-identical to the reference. */
+rfx_status rfx_proximity_rfgap(rfx_ctx* ctx, double* P, size_t len);
 
 /* Per-stage device timing.  With profiling enabled, every stage launch is
  * bracketed by CUDA events on the context stream; rfx_profile_read waits for

@@ -29,7 +29,8 @@ EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_strea
            "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
            "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_factor_mds_operator", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest", "rfx_graph_capture_batch",
-           "rfx_graph_launch", "rfx_graph_destroy", "rfx_tuned_shapes"]
+           "rfx_graph_launch", "rfx_graph_destroy", "rfx_tuned_shapes", "rfx_casewise_votes",
+           "rfx_proximity_upper_f64", "rfx_finishprox_f64", "rfx_proximity_rfgap"]
 
 STAGES = ["route", "leaf_lists", "pair_counts", "finishprox", "varimp_tree", "varimp_sample", "varimp_feature",
           "predict", "oob_summary", "localimp", "pair_ranges", "lowrank_product", "lowrank_orth", "mds_factors",
@@ -296,6 +297,38 @@ class Context:
             nout = np.zeros(self.n, np.int32)
         _check(lib().rfx_route_oob(self._h, _vp(q), _vp(nout), _vp(leaf)))
         return q, nout, leaf
+
+    def casewise_votes(self, q=None, nout=None):
+        """Case-wise weighted OOB votes q (n, c) float32 and doubled nout."""
+        if q is None:
+            q = np.zeros((self.n, self.nclass), np.float32)
+        if nout is None:
+            nout = np.zeros(self.n, np.int32)
+        _check(lib().rfx_casewise_votes(self._h, _vp(q), _vp(nout)))
+        return q, nout
+
+    def proximity_upper_f64(self, S=None):
+        """FP64 pair sums C + C^T, packed upper triangle (n(n+1)/2,)."""
+        L = self.n * (self.n + 1) // 2
+        if S is None:
+            S = np.zeros(L, np.float64)
+        _check(lib().rfx_proximity_upper_f64(self._h, _vp(S), ctypes.c_size_t(L)))
+        return S
+
+    def finishprox_f64(self, S, P=None, full=True):
+        """finishprox of FP64 sums (host or device buffers)."""
+        if P is None:
+            P = np.zeros((self.n, self.n) if full else (self.n * (self.n + 1) // 2,), np.float32)
+        _check(lib().rfx_finishprox_f64(self._h, _vp(S), _vp(P), int(bool(full))))
+        return P
+
+    def proximity_rfgap(self, P=None):
+        """RF-GAP proximity, packed upper triangle FP64 (n(n+1)/2,)."""
+        L = self.n * (self.n + 1) // 2
+        if P is None:
+            P = np.zeros(L, np.float64)
+        _check(lib().rfx_proximity_rfgap(self._h, _vp(P), ctypes.c_size_t(L)))
+        return P
 
     def oob_summary(self, err=None, pred=None, proba=None):
         """OOB error, predictions and probabilities; with any output given

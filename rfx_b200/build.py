@@ -24,7 +24,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # The system compilers: the environment's CXX wrapper lacks the OpenMP spec.
 HOST_CXX = "/usr/bin/g++"
 
-CU_SOURCES = ["abi.cu", "load.cu", "route.cu", "prox.cu", "varimp.cu", "noalloc.cu", "hubs.cu", "mds.cu", "tc_mds.cu", "lowrank.cu", "batch.cu", "tune.cu"]
+CU_SOURCES = ["abi.cu", "load.cu", "route.cu", "prox.cu", "varimp.cu", "noalloc.cu", "hubs.cu", "weighted.cu", "mds.cu", "tc_mds.cu", "lowrank.cu", "batch.cu", "tune.cu"]
 CPP_SOURCES = ["host/grow.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", HOST_CXX,
@@ -83,7 +83,8 @@ def build_lib(verbose: bool = False, ptxas_info: bool = False) -> str:
             if o.strip():
                 print(o)
     if _stale(LIB_PATH, objs) or jobs:
-        _run([NVCC] + GENCODE + ["-shared", "-ccbin", HOST_CXX, "-o", LIB_PATH] + objs + ["-lpthread"])
+        _run([NVCC] + GENCODE + ["-shared", "-ccbin", HOST_CXX, "-Xlinker", "--no-undefined", "-o", LIB_PATH] + objs +
+             ["-lpthread"])
     return LIB_PATH
 
 

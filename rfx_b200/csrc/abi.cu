@@ -119,6 +119,7 @@ void free_forest(Ctx* c) {
     dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
     dfree(c, c->d_sqsd); dfree(c, c->d_opp); dfree(c, c->d_order);
     dfree(c, c->d_hubflag); dfree(c, c->d_hubtiles); dfree(c, c->d_hubstate);
+    dfree(c, c->d_nin); dfree(c, c->d_tnodewt);
     dfree(c, c->d_lrA); dfree(c, c->d_lrAq); dfree(c, c->d_lrScale);
     if (c->d_lrQ) cudaFree(c->d_lrQ);
     c->d_lrQ = nullptr;
@@ -183,6 +184,28 @@ rfx_status check_device_errors(Ctx* c) {
 
 using namespace rfx;
 
+// Device or host FP64 output of n(n+1)/2 entries through pooled staging.
+template <typename F>
+static rfx_status with_f64_out(Ctx* c, double* out, size_t len, const char* who, F&& fill) {
+    const bool dev = is_device_ptr(out);
+    Scratch staging(c);
+    double* d = out;
+    if (!dev) {
+        d = staging.get<double>(len);
+        if (!d) {
+            set_error(std::string(who) + ": device staging allocation failed");
+            return RFX_ERR_OOM;
+        }
+    }
+    rfx_status st = fill(d);
+    if (st == RFX_OK && !dev) {
+        st = copy_out(c, out, d, sizeof(double) * len);
+        if (st == RFX_OK) st = finish_host(c, true);
+    }
+    cudaStreamSynchronize(c->stream);
+    return st;
+}
+
 extern "C" {
 
 const char* rfx_last_error(void) { return g_last_error.c_str(); }
@@ -195,10 +218,6 @@ rfx_status rfx_ctx_create(const rfx_config* cfg, rfx_ctx** out) {
     *out = nullptr;
     rfx_config conf{};
     if (cfg) conf = *cfg;
-    if (conf.use_casewise) {
-        set_error("use_casewise=True is not supported (case-wise weighting is out of scope)");
-        return RFX_ERR_UNSUPPORTED;
-    }
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) {
@@ -361,7 +380,8 @@ static rfx_status load_forest(Ctx* c, const LoadInput& in) {
         int32_t* r_bestvar = raw.get<int32_t>(N);
         float* r_split = raw.get<float>(N);
         int32_t* r_treemap = raw.get<int32_t>(2 * (size_t)N);
-        int32_t* r_nin = raw.get<int32_t>((size_t)T * n);
+        ALLOC(d_nin, (size_t)T * n);  // kept: case-wise weights and RF-GAP read the multiplicities
+        int32_t* r_nin = c->d_nin;
         int32_t* r_nleaf = raw.get<int32_t>(T);
         LoadError* r_err = raw.get<LoadError>(1);
         if (!r_status || !r_bestvar || !r_split || !r_treemap || !r_nin || !r_nleaf || !r_err) {
@@ -603,6 +623,8 @@ rfx_status rfx_forest_load_device(rfx_ctx* ctx, const rfx_forest_device_view* v)
     }
 }
 
+static rfx_status casewise_votes_into(Ctx* c, float* dq);
+
 static rfx_status need_forest(Ctx* c) {
     if (!c) {
         set_error("null context");
@@ -620,6 +642,10 @@ rfx_status rfx_route_oob(rfx_ctx* ctx, int32_t* q, int32_t* nout, int32_t* leaf)
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     rfx_status st = need_forest(c);
     if (st) return st;
+    if (q && c->cfg.use_casewise) {
+        set_error("rfx_route_oob: a case-wise context weighs the votes (float): use rfx_casewise_votes");
+        return RFX_ERR_STATE;
+    }
     bool any_host = false;
     if (leaf) {
         int32_t* dleaf = leaf;
@@ -682,7 +708,17 @@ rfx_status rfx_oob_summary(rfx_ctx* ctx, float* oob_error, int32_t* pred, float*
         set_error("rfx_oob_summary: staging allocation failed");
         return RFX_ERR_OOM;
     }
-    st = launch_oob_summary(c, d_e, d_p, d_pr);
+    if (c->cfg.use_casewise) {
+        // the weighted votes of rfx_casewise_votes (computed here)
+        Scratch sq(c);
+        float* dq = sq.get<float>((size_t)c->n * c->nclass);
+        if (!dq) st = RFX_ERR_OOM;
+        if (st == RFX_OK) st = casewise_votes_into(c, dq);
+        if (st == RFX_OK) st = launch_oob_summary_f32(c, dq, d_e, d_p, d_pr);
+        if (st == RFX_OK) cudaStreamSynchronize(c->stream);
+    } else {
+        st = launch_oob_summary(c, d_e, d_p, d_pr);
+    }
     if (st == RFX_OK && he) st = copy_out(c, oob_error, d_e, sizeof(float));
     if (st == RFX_OK && hp) st = copy_out(c, pred, d_p, sizeof(int32_t) * c->n);
     if (st == RFX_OK && hpr) st = copy_out(c, proba, d_pr, sizeof(float) * (size_t)c->n * c->nclass);
@@ -696,6 +732,10 @@ rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     rfx_status st = need_forest(c);
     if (st) return st;
+    if (c->cfg.use_casewise) {
+        set_error("rfx_proximity_upper_i32: a case-wise context weighs the pairs (FP64): use rfx_proximity_upper_f64");
+        return RFX_ERR_STATE;
+    }
     if (!S || len != (size_t)upper_len(c->n)) {
         set_error("rfx_proximity_upper_i32: S must hold n(n+1)/2 entries");
         return RFX_ERR_INVALID;
@@ -724,6 +764,153 @@ rfx_status rfx_proximity_upper_i32(rfx_ctx* ctx, int32_t* S, size_t len) {
     }
     if (!dev) cudaStreamSynchronize(c->stream);
     return st;
+}
+
+// Case-wise weighted OOB votes (n x nclass float) into device memory.
+static rfx_status casewise_votes_into(Ctx* c, float* dq) {
+    Scratch sl(c);
+    int32_t* dleaf = sl.get<int32_t>((size_t)c->T * c->n);
+    if (!dleaf) {
+        set_error("case-wise votes: scratch allocation failed");
+        return RFX_ERR_OOM;
+    }
+    rfx_status st = launch_route_leaf(c, dleaf);  // node ids, and nout
+    if (st == RFX_OK) st = launch_route(c);
+    if (st == RFX_OK) {
+        c->routed = true;
+        c->csr_built = false;
+        st = launch_tnodewt(c);
+    }
+    if (st == RFX_OK) st = launch_casewise_votes(c, dleaf, dq);
+    if (st == RFX_OK) RFX_CUDA(cudaStreamSynchronize(c->stream));  // the scratch goes back to the pool
+    return st;
+}
+
+rfx_status rfx_casewise_votes(rfx_ctx* ctx, float* q, int32_t* nout) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!c->cfg.use_casewise) {
+        set_error("rfx_casewise_votes: the context was created without use_casewise");
+        return RFX_ERR_STATE;
+    }
+    if (!q) {
+        set_error("rfx_casewise_votes: q is null");
+        return RFX_ERR_INVALID;
+    }
+    const size_t nq = (size_t)c->n * c->nclass;
+    Scratch sq(c);
+    const bool dev = is_device_ptr(q);
+    float* dq = dev ? q : sq.get<float>(nq);
+    if (!dq) return RFX_ERR_OOM;
+    if ((st = casewise_votes_into(c, dq))) return st;
+    bool any_host = false;
+    if (!dev) {
+        if ((st = copy_out(c, q, dq, sizeof(float) * nq))) return st;
+        any_host = true;
+    }
+    if (nout) {
+        any_host |= !is_device_ptr(nout);
+        if ((st = copy_out(c, nout, c->d_nout, sizeof(int32_t) * (size_t)c->n))) return st;
+    }
+    st = finish_host(c, any_host);
+    cudaStreamSynchronize(c->stream);
+    return st;
+}
+
+rfx_status rfx_proximity_upper_f64(rfx_ctx* ctx, double* S, size_t len) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!S || len != (size_t)upper_len(c->n)) {
+        set_error("rfx_proximity_upper_f64: S must hold n(n+1)/2 entries");
+        return RFX_ERR_INVALID;
+    }
+    return with_f64_out(c, S, len, "rfx_proximity_upper_f64", [&](double* dS) -> rfx_status {
+        rfx_status s = launch_route(c);
+        if (s == RFX_OK) s = launch_build_csr(c);
+        if (s != RFX_OK) return s;
+        c->routed = true;
+        c->csr_built = true;
+        StageTimer stt(c, ST_PAIRS, 0);
+        return launch_weighted_rows(c, c->cfg.use_casewise ? 0 : 2, c->d_key, c->d_segbase, c->d_segoff, c->d_memb,
+                                    c->h_segbase[c->T], dS);
+    });
+}
+
+rfx_status rfx_finishprox_f64(rfx_ctx* ctx, const double* S, float* P, int full) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!S || !P) {
+        set_error("rfx_finishprox_f64: null argument");
+        return RFX_ERR_INVALID;
+    }
+    if (!c->routed) {
+        if ((st = launch_route(c))) return st;
+        c->routed = true;
+    }
+    const size_t slen = (size_t)upper_len(c->n);
+    const size_t plen = full ? (size_t)c->n * c->n : slen;
+    const bool sdev = is_device_ptr(S), pdev = is_device_ptr(P);
+    Scratch sc(c);
+    const double* dS = S;
+    float* dP = P;
+    if (!sdev) {
+        double* t = sc.get<double>(slen);
+        if (!t) return RFX_ERR_OOM;
+        RFX_CUDA(cudaMemcpyAsync(t, S, sizeof(double) * slen, cudaMemcpyHostToDevice, c->stream));
+        dS = t;
+    }
+    if (!pdev) {
+        dP = sc.get<float>(plen);
+        if (!dP) return RFX_ERR_OOM;
+    }
+    st = launch_finishprox_f64(c, dS, dP, full);
+    if (st == RFX_OK && !pdev) st = copy_out(c, P, dP, sizeof(float) * plen);
+    if (st == RFX_OK) st = finish_host(c, !sdev || !pdev);
+    cudaStreamSynchronize(c->stream);
+    return st;
+}
+
+rfx_status rfx_proximity_rfgap(rfx_ctx* ctx, double* P, size_t len) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!P || len != (size_t)upper_len(c->n)) {
+        set_error("rfx_proximity_rfgap: P must hold n(n+1)/2 entries");
+        return RFX_ERR_INVALID;
+    }
+    return with_f64_out(c, P, len, "rfx_proximity_rfgap", [&](double* dP) -> rfx_status {
+        const int T = c->T, n = c->n;
+        Scratch sc(c);
+        int32_t* leaf = sc.get<int32_t>((size_t)T * n);
+        int32_t* key = sc.get<int32_t>((size_t)T * n);
+        int32_t* memb = sc.get<int32_t>((size_t)T * n);
+        // node-id keys: 2 * nnode + 1 slots per tree
+        std::vector<int64_t> sb(T + 1, 0);
+        for (int t = 0; t < T; ++t) sb[t + 1] = sb[t] + 2 * (int64_t)c->h_nnode[t] + 1;
+        int64_t* dsb = sc.get<int64_t>((size_t)T + 1);
+        int32_t* segoff = sc.get<int32_t>((size_t)sb[T]);
+        if (!leaf || !key || !memb || !dsb || !segoff) {
+            set_error("rfx_proximity_rfgap: scratch allocation failed");
+            return RFX_ERR_OOM;
+        }
+        RFX_CUDA(cudaMemcpyAsync(dsb, sb.data(), sizeof(int64_t) * (T + 1), cudaMemcpyHostToDevice, c->stream));
+        rfx_status s = launch_route_leaf(c, leaf);  // node ids (and nout)
+        if (s == RFX_OK) s = launch_route(c);
+        if (s != RFX_OK) return s;
+        c->routed = true;
+        c->csr_built = false;
+        if ((s = launch_gap_keys(c, leaf, key))) return s;
+        if ((s = launch_build_csr_raw(c->stream, c->device, key, n, T, dsb, segoff, memb, 2 * c->max_nnode,
+                                      c->d_err)))
+            return s;
+        StageTimer stt(c, ST_PAIRS, 0);
+        s = launch_weighted_rows(c, 1, key, dsb, segoff, memb, sb[T], dP);
+        if (s == RFX_OK) RFX_CUDA(cudaStreamSynchronize(c->stream));  // the scratch goes back to the pool
+        return s;
+    });
 }
 
 rfx_status rfx_pair_updates(rfx_ctx* ctx, int64_t* count) {
@@ -801,7 +988,25 @@ rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* 
     ALLOC(d_sqsd, p);
 #undef ALLOC
     if (st) return st;
-    if ((st = launch_varimp(c, impn ? 1 : 0))) return st;
+    if (c->cfg.use_casewise) {
+        // weights of the testreebag nodes; OOB lists and permutation partners
+        Scratch sl(c);
+        int32_t* dleaf = sl.get<int32_t>((size_t)T * n);
+        if (!dleaf) return RFX_ERR_OOM;
+        if ((st = launch_route_leaf(c, dleaf))) return st;
+        if ((st = launch_tnodewt(c))) return st;
+        if ((st = launch_joob_partner(c))) return st;
+        RFX_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(uint32_t), c->stream));
+        {
+            StageTimer stt(c, ST_VARIMP_TREE, 0);
+            if ((st = launch_casewise_varimp(c, dleaf, impn ? 1 : 0, c->d_avimp, c->d_sqsd, c->d_qimp, c->d_qimpm)))
+                return st;
+        }
+        RFX_CUDA(cudaStreamSynchronize(c->stream));
+        if ((st = check_device_errors(c))) return st;
+    } else if ((st = launch_varimp(c, impn ? 1 : 0))) {
+        return st;
+    }
     bool any_host = false;
     auto out = [&](float* dst, const float* src, size_t cnt) -> rfx_status {
         if (!dst) return RFX_OK;

@@ -12,7 +12,9 @@
 //   * get_local_importance returns localimp's feature-major reading of the
 //     sample-major buffer as an (n, p) array;
 //   * get_lowrank_factors returns (A, B, r) with B == A and a column-major
-//     buffer behind the C-order (n, r) arrays.
+//     buffer behind the C-order (n, r) arrays; the factors are those of
+//     P ~= I + A A^T (the identity is not part of them: a caller rebuilding P
+//     adds it).
 // Every call into the library releases the GIL; the library never calls back
 // into Python.  All analysis runs on CUDA device 0; fit() raises when no
 // usable device or library is present (there is no CPU fallback).
@@ -164,10 +166,10 @@ class RandomForestClassifier {
             c = (int)u.size();
         }
         check_loss(gpu_loss_function_);
-        if (use_casewise_)
-            throw std::runtime_error("use_casewise=True (bootstrap-frequency weighting) is not supported by rfx_b200");
-        if (compute_proximity_ && use_rfgap_)
-            throw std::runtime_error("use_rfgap=True (RF-GAP proximity) is not supported by rfx_b200");
+        if (compute_proximity_ && use_rfgap_ && use_qlora_)
+            throw std::runtime_error(
+                "use_rfgap=True with use_qlora=True is not supported by rfx_b200: RF-GAP proximity is computed as "
+                "the full matrix (use_qlora=False)");
         if (compute_importance_ && compute_local_importance_ && importance_method_ == "clique")
             throw std::runtime_error(
                 "CLIQUE importance is not available in v1.0. Use importance_method='local_imp' instead.");
@@ -207,11 +209,17 @@ class RandomForestClassifier {
         importances_.assign(p, 0.0f);
         local_imp_.clear();
         S_.clear();
+        Sd_.clear();
         lowrank_ready_ = false;
         {
             NoGil ng;
-            std::vector<int32_t> q((size_t)n * c);
-            check(rfx_route_oob(ctx_, q.data(), nout_.data(), nullptr), "fit (OOB routing)");
+            if (use_casewise_) {  // votes weighted by tnodewt
+                std::vector<float> q((size_t)n * c);
+                check(rfx_casewise_votes(ctx_, q.data(), nout_.data()), "fit (OOB routing)");
+            } else {
+                std::vector<int32_t> q((size_t)n * c);
+                check(rfx_route_oob(ctx_, q.data(), nout_.data(), nullptr), "fit (OOB routing)");
+            }
             check(rfx_oob_summary(ctx_, &oob_error_, oob_pred_.data(), oob_proba_.data()), "fit (OOB summary)");
             if (compute_importance_) {
                 std::vector<float> sqsd(p), qimp(n), qimpm;
@@ -231,8 +239,16 @@ class RandomForestClassifier {
             } else {
                 NoGil ng;
                 const size_t len = (size_t)n * (n + 1) / 2;
-                S_.resize(len);
-                check(rfx_proximity_upper_i32(ctx_, S_.data(), len), "fit (proximity)");
+                if (use_rfgap_) {  // the final RF-GAP matrix
+                    Sd_.resize(len);
+                    check(rfx_proximity_rfgap(ctx_, Sd_.data(), len), "fit (RF-GAP proximity)");
+                } else if (use_casewise_) {  // FP64 weighted sums, finished on request
+                    Sd_.resize(len);
+                    check(rfx_proximity_upper_f64(ctx_, Sd_.data(), len), "fit (proximity)");
+                } else {
+                    S_.resize(len);
+                    check(rfx_proximity_upper_i32(ctx_, S_.data(), len), "fit (proximity)");
+                }
             }
         }
         fitted_ = true;
@@ -336,7 +352,20 @@ class RandomForestClassifier {
             throw py::error_already_set();
         ensure_ctx();
         NoGil ng;
-        check(rfx_finishprox(ctx_, S_.data(), o, 1), "get_proximity_matrix");
+        if (use_rfgap_) {
+            // the RF-GAP matrix is final: float32 copy of the packed triangle
+            const int64_t nn = n;
+            for (int64_t i = 0; i < nn; ++i)
+                for (int64_t j = i; j < nn; ++j) {
+                    const float v = (float)Sd_[(size_t)(i * nn - i * (i - 1) / 2 + (j - i))];
+                    o[i * nn + j] = v;
+                    o[j * nn + i] = v;
+                }
+        } else if (use_casewise_) {
+            check(rfx_finishprox_f64(ctx_, Sd_.data(), o, 1), "get_proximity_matrix");
+        } else {
+            check(rfx_finishprox(ctx_, S_.data(), o, 1), "get_proximity_matrix");
+        }
         return out;
     }
 
@@ -456,7 +485,7 @@ class RandomForestClassifier {
         if (ctx_) return;
         rfx_config cfg{};
         cfg.device = 0;
-        cfg.use_casewise = 0;
+        cfg.use_casewise = use_casewise_ ? 1 : 0;
         cfg.n_threads_cpu = n_threads_cpu_;
         rfx_forest_view v{};
         v.n = nsample_;
@@ -611,6 +640,7 @@ class RandomForestClassifier {
     std::vector<int32_t> nout_, oob_pred_;
     std::vector<float> oob_proba_, importances_, local_imp_;
     std::vector<int32_t> S_;  // packed upper-triangle pair counts (full proximity mode)
+    std::vector<double> Sd_;  // case-wise FP64 pair sums, or the RF-GAP matrix (packed upper triangle)
     bool lowrank_ready_ = false, lr_quantized_ = false;
     int lr_rank_ = 0, lr_precision_ = 0;
     std::vector<float> factors_;  // n x r row-major, as stored (dequantised when quantised)
@@ -655,7 +685,9 @@ PYBIND11_MODULE(_rfx, m) {
         .def("compute_proximity_matrix", &RandomForestClassifier::get_proximity_matrix,
              "Alias for get_proximity_matrix()")
         .def("get_oob_predictions", &RandomForestClassifier::get_oob_predictions)
-        .def("get_lowrank_factors", &RandomForestClassifier::get_lowrank_factors)
+        .def("get_lowrank_factors", &RandomForestClassifier::get_lowrank_factors,
+             "(A, B, r): factors of the low-rank proximity P ~= I + A A^T, float64 (n, r) arrays over a column-major "
+             "buffer, B == A; quantised modes return the stored (dequantised) values.")
         .def("compute_mds_3d_cpu", &RandomForestClassifier::compute_mds_3d_cpu,
              "3-D MDS coordinates (n, 3) of the full proximity matrix; needs compute_proximity=True.")
         .def("compute_mds_from_factors", &RandomForestClassifier::compute_mds_from_factors, py::arg("k") = 3,

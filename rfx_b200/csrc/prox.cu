@@ -735,7 +735,8 @@ constexpr int FP_JT = 8;  // column tiles per CTA
 
 // S/2 is exact for an integer S, so it is formed as S * 0.5 (the same double
 // as the reference's division by 2).
-__device__ __forceinline__ double fp_value(int32_t s, double inv_i, double inv_j, bool sc_i, bool sc_j) {
+template <typename TS>
+__device__ __forceinline__ double fp_value(TS s, double inv_i, double inv_j, bool sc_i, bool sc_j) {
     const double h = __dmul_rn((double)s, 0.5);
     const double a = sc_i ? __dmul_rn(h, inv_i) : h;
     const double b = sc_j ? __dmul_rn(h, inv_j) : h;
@@ -746,8 +747,9 @@ __device__ __forceinline__ double fp_value(int32_t s, double inv_i, double inv_j
 // 32x32 values of each tile (I, J) from the packed S rows of tile I and writes
 // tile (I, J) and its mirror (J, I) of the full matrix, or tile (I, J) of the
 // packed triangle.  The row tile's 1/nout factors are formed once per CTA.
+template <typename TS>
 __global__ void __launch_bounds__(FP_TILE * 8)
-finishprox_kernel(const int32_t* __restrict__ S, const int32_t* __restrict__ nout, int n, int full,
+finishprox_kernel(const TS* __restrict__ S, const int32_t* __restrict__ nout, int n, int full,
                   float* __restrict__ P) {
     __shared__ float tile[FP_TILE][FP_TILE + 1];
     __shared__ double s_inv[FP_TILE];
@@ -772,13 +774,13 @@ finishprox_kernel(const int32_t* __restrict__ S, const int32_t* __restrict__ nou
         const double inv_j = nj > 0 ? __ddiv_rn(1.0, (double)nj) : 1.0;
         // the four rows' loads are issued before any value is formed (four
         // 128-byte row segments in flight per warp)
-        int32_t sv[FP_TILE / 8];
+        TS sv[FP_TILE / 8];
         int64_t ix[FP_TILE / 8];
 #pragma unroll
         for (int u = 0; u < FP_TILE / 8; ++u) {
             const int i = I * FP_TILE + ty + 8 * u;
             ix[u] = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 + (j - i);
-            sv[u] = (i < n && jv && j > i) ? __ldg(S + ix[u]) : 0;
+            sv[u] = (i < n && jv && j > i) ? __ldg(S + ix[u]) : (TS)0;
         }
 #pragma unroll
         for (int u = 0; u < FP_TILE / 8; ++u) {
@@ -808,6 +810,25 @@ finishprox_kernel(const int32_t* __restrict__ S, const int32_t* __restrict__ nou
 }
 
 }  // namespace
+
+// Leaf lists of arbitrary keys (key per (tree, sample) in [0, K_t), or -1),
+// for callers with their own key tables (RF-GAP's node-id keys).
+rfx_status launch_build_csr_raw(cudaStream_t s, int device, const int32_t* key, int n, int T, const int64_t* segbase,
+                                int32_t* segoff, int32_t* memb, int max_keys, uint32_t* err) {
+    int dev_smem = 0;
+    RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    int smem_keys = std::min(max_keys + 1, (dev_smem - 1024) / 4);
+    smem_keys = std::max(smem_keys, 32);
+    const size_t smem = (size_t)smem_keys * sizeof(int32_t);
+    if (rfx_status s0 = allow_dyn_smem(build_csr_kernel<int32_t>, dev_smem)) return s0;
+    build_csr_kernel<int32_t><<<T, CSR_THREADS, smem, s>>>(key, n, segbase, segoff, memb, smem_keys, err);
+    RFX_CUDA(cudaGetLastError());
+    if (max_keys + 1 > smem_keys) {
+        fix_global_segoff_kernel<<<T, 32, 0, s>>>(segbase, segoff, smem_keys);
+        RFX_CUDA(cudaGetLastError());
+    }
+    return RFX_OK;
+}
 
 rfx_status launch_build_csr(Ctx* c) {
     int dev_smem = 0;
@@ -975,7 +996,18 @@ rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full) {
     StageTimer st(c, ST_FINISHPROX, 1);
     const int nt = (c->n + FP_TILE - 1) / FP_TILE;
     dim3 grid((nt + FP_JT - 1) / FP_JT, nt);
-    finishprox_kernel<<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
+    finishprox_kernel<int32_t><<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+// finishprox of FP64 sums (case-wise weights): the same arithmetic on
+// S = C + C^T in double
+rfx_status launch_finishprox_f64(Ctx* c, const double* dS, float* dP, int full) {
+    StageTimer st(c, ST_FINISHPROX, 1);
+    const int nt = (c->n + FP_TILE - 1) / FP_TILE;
+    dim3 grid((nt + FP_JT - 1) / FP_JT, nt);
+    finishprox_kernel<double><<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
 }

@@ -76,6 +76,8 @@ struct Ctx {
     int64_t* d_offs = nullptr;          // T+1
     int32_t* d_nnode = nullptr;         // T
     uint8_t* d_inbag = nullptr;         // T*n
+    int32_t* d_nin = nullptr;           // T*n bootstrap multiplicities (case-wise weights, RF-GAP)
+    float* d_tnodewt = nullptr;         // N: case-wise terminal-node weights
     int64_t* d_segbase = nullptr;       // T+1
     uint64_t* d_iv = nullptr;           // T*iv_words: features used by non-terminal nodes
     int32_t* d_noob = nullptr;          // T
@@ -286,6 +288,20 @@ cudaError_t launch_gather_padded(cudaStream_t s, int T, int maxnode, int maxcat,
                                  int32_t* status, int32_t* bestvar, float* split, int32_t* treemap,
                                  int32_t* nodeclass, int32_t* catgoleft);
 rfx_status launch_pairs_upper(Ctx* c, int32_t* dS);
+rfx_status launch_build_csr_raw(cudaStream_t s, int device, const int32_t* key, int n, int T, const int64_t* segbase,
+                                int32_t* segoff, int32_t* memb, int max_keys, uint32_t* err);
+rfx_status launch_joob_partner(Ctx* c);
+// case-wise weighting and RF-GAP (weighted.cu)
+rfx_status launch_tnodewt(Ctx* c);
+rfx_status launch_casewise_votes(Ctx* c, const int32_t* d_leafnode, float* d_q);
+rfx_status launch_weighted_rows(Ctx* c, int mode, const int32_t* key, const int64_t* segbase, const int32_t* segoff,
+                                const int32_t* memb, int64_t nkeys, double* out);
+rfx_status launch_gap_keys(Ctx* c, const int32_t* d_leafnode, int32_t* d_key);
+rfx_status launch_casewise_varimp(Ctx* c, const int32_t* d_leafnode, int impn, float* d_avimp, float* d_sqsd,
+                                  float* d_qimp, float* d_qimpm);
+rfx_status launch_route_leaf(Ctx* c, int32_t* d_leaf);
+rfx_status launch_oob_summary_f32(Ctx* c, const float* d_q, float* d_errout, int32_t* d_pred, float* d_proba);
+rfx_status launch_finishprox_f64(Ctx* c, const double* dS, float* dP, int full);
 // S_hub tiles of the hub leaves (hubs.cu)
 int hub_tiles_nj(int n);
 size_t hub_tile_bytes(int n);

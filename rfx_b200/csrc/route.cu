@@ -282,12 +282,13 @@ __global__ void nout_kernel(const uint8_t* __restrict__ inbag, int n, int T, int
 // OOB error / prediction / probability from integer votes, with the
 // reference's float arithmetic: argmax with >= (ties to the higher class),
 // total votes summed in float, probability = q / total (or 1/nclass).
-__global__ void oob_summary_kernel(const int32_t* __restrict__ votes, const int32_t* __restrict__ nout,
+template <typename TV>
+__global__ void oob_summary_kernel(const TV* __restrict__ votes, const int32_t* __restrict__ nout,
                                    const int32_t* __restrict__ y, int n, int nclass, int32_t* __restrict__ pred,
                                    float* __restrict__ proba, unsigned int* __restrict__ counts) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int32_t* q = votes + (size_t)i * nclass;
+    const TV* q = votes + (size_t)i * nclass;
     const float uni = __double2float_rn(1.0 / (double)nclass);
     if (nout[i] > 0) {
         int best = 0;
@@ -383,8 +384,23 @@ rfx_status launch_oob_summary(Ctx* c, float* d_errout, int32_t* d_pred, float* d
     StageTimer st(c, ST_OOB, d_errout ? 2 : 1);
     unsigned int* counts = reinterpret_cast<unsigned int*>(c->d_pairs) + 2;  // scratch words after the pair counter
     RFX_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), c->stream));
-    oob_summary_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_votes, c->d_nout, c->d_y, c->n, c->nclass,
-                                                                   d_pred, d_proba, counts);
+    oob_summary_kernel<int32_t><<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_votes, c->d_nout, c->d_y, c->n,
+                                                                            c->nclass, d_pred, d_proba, counts);
+    RFX_CUDA(cudaGetLastError());
+    if (d_errout) {
+        oob_error_kernel<<<1, 1, 0, c->stream>>>(counts, d_errout);
+        RFX_CUDA(cudaGetLastError());
+    }
+    return RFX_OK;
+}
+
+// the same from float votes (case-wise weights)
+rfx_status launch_oob_summary_f32(Ctx* c, const float* d_q, float* d_errout, int32_t* d_pred, float* d_proba) {
+    StageTimer st(c, ST_OOB, d_errout ? 2 : 1);
+    unsigned int* counts = reinterpret_cast<unsigned int*>(c->d_pairs) + 2;  // scratch words after the pair counter
+    RFX_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), c->stream));
+    oob_summary_kernel<float><<<(c->n + 255) / 256, 256, 0, c->stream>>>(d_q, c->d_nout, c->d_y, c->n,
+                                                                            c->nclass, d_pred, d_proba, counts);
     RFX_CUDA(cudaGetLastError());
     if (d_errout) {
         oob_error_kernel<<<1, 1, 0, c->stream>>>(counts, d_errout);

@@ -559,6 +559,14 @@ rfx_status launch_varimp_blocked(Ctx* c, int impn) {
 
 }  // namespace
 
+// OOB lists and permutation partners of every tree (case-wise importance).
+rfx_status launch_joob_partner(Ctx* c) {
+    joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, c->d_permoff, c->d_perm, c->d_partner);
+    RFX_CUDA(cudaGetLastError());
+    c->launches += 1;
+    return RFX_OK;
+}
+
 rfx_status launch_varimp(Ctx* c, int impn) {
     switch (c->iv_words) {
         case 1: return launch_varimp_w<1>(c, impn);

@@ -70,10 +70,8 @@ def test_confusion_matrix(rfx):
 def test_unsupported_options_raise(rfx):
     X = np.zeros((8, 2), np.float32)
     y = np.array([0, 1] * 4, np.int32)
-    with pytest.raises(RuntimeError, match="use_casewise"):
-        rfx.RandomForestClassifier(ntree=2, use_casewise=True).fit(X, y)
-    with pytest.raises(RuntimeError, match="RF-GAP"):
-        rfx.RandomForestClassifier(ntree=2, compute_proximity=True, use_rfgap=True).fit(X, y)
+    with pytest.raises(RuntimeError, match="use_rfgap=True with use_qlora=True"):
+        rfx.RandomForestClassifier(ntree=2, compute_proximity=True, use_rfgap=True, use_qlora=True).fit(X, y)
     with pytest.raises(RuntimeError, match="CLIQUE"):
         rfx.RandomForestClassifier(ntree=2, compute_local_importance=True, importance_method="clique").fit(X, y)
     with pytest.raises(RuntimeError, match="2-dimensional"):
