@@ -10,7 +10,11 @@
 // All arithmetic in FP64.  The eigenpairs come from subspace iteration on B
 // with a block of S_BLK vectors, CholeskyQR2 re-orthonormalisation and a
 // Rayleigh-Ritz step (Jacobi on the S_BLK x S_BLK projection) instead of a full
-// dsyevd; eigenvectors are defined up to sign.
+// dsyevd; eigenvectors are defined up to sign.  The full-matrix form filters
+// the block with Chebyshev polynomials of B (degree 8) between Rayleigh-Ritz
+// steps, so that a third eigenvalue close to a cluster below it (the plain
+// method at n = 2,000 / 500 trees has lambda3 / lambda17 = 1.02) still
+// converges in a few hundred products.
 #include <algorithm>
 #include <cmath>
 #include <random>
@@ -234,6 +238,17 @@ __device__ __forceinline__ uint64_t start_mix(uint64_t z) {
     return z ^ (z >> 31);
 }
 
+// out = a X + b Y + c Z over an n x S_BLK block (Z may be null); the
+// three-term recurrence of the Chebyshev filter.
+__global__ void block_axpby_kernel(double a, const double* __restrict__ X, double b, const double* __restrict__ Y,
+                                   double c, const double* __restrict__ Z, int64_t count, double* __restrict__ out) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= count) return;
+    double v = __dadd_rn(__dmul_rn(a, X[e]), __dmul_rn(b, Y[e]));
+    if (Z) v = __dadd_rn(v, __dmul_rn(c, Z[e]));
+    out[e] = v;
+}
+
 __global__ void start_block_kernel(double* __restrict__ V, int64_t count, uint64_t seed) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= count) return;
@@ -250,7 +265,7 @@ __global__ void start_block_kernel(double* __restrict__ V, int64_t count, uint64
 template <typename Apply>
 rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double* d_out, double* evals_out,
                          uint64_t seed, double tol = 1e-14, const double* warm_in = nullptr, double* keep_out = nullptr,
-                         int* iters_out = nullptr, bool floor_stop = false) {
+                         int* iters_out = nullptr, bool floor_stop = false, int cheb = 0) {
     cudaStream_t s = c->stream;
     Scratch d(c);
     double* V = d.get<double>((size_t)n * S_BLK);
@@ -303,6 +318,86 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
     if ((st = orth(V, V)) != RFX_OK) return st;  // src and Out may alias: Xt sits between
     std::vector<double> prev(S_BLK, 0.0), cur(S_BLK, 0.0), hist;
     std::vector<double> hU(S_BLK * S_BLK);
+    // Rayleigh-Ritz on span(V) with W = B V: eigenvalues into cur, change of
+    // the k largest against the previous check into *delta
+    auto ritz = [&](double* delta) -> rfx_status {
+        RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * S_BLK * S_BLK, s));
+        dgram_kernel<<<std::min(1024, (n + 63) / 64), 256, 0, s>>>(V, W, n, G);
+        rr_kernel<<<1, 128, 0, s>>>(G, ev, U);
+        c->launches += 2;
+        RFX_CUDA(cudaMemcpyAsync(cur.data(), ev, sizeof(double) * S_BLK, cudaMemcpyDeviceToHost, s));
+        RFX_CUDA(cudaStreamSynchronize(s));
+        std::vector<double> a = cur, b = prev;
+        std::sort(a.rbegin(), a.rend());
+        std::sort(b.rbegin(), b.rend());
+        double dl = 0.0;
+        for (int q = 0; q < k; ++q) dl = std::max(dl, std::fabs(a[q] - b[q]) / std::max(std::fabs(a[q]), 1e-300));
+        prev = cur;
+        *delta = dl;
+        return RFX_OK;
+    };
+    if (cheb > 0) {
+        // Chebyshev-filtered subspace iteration: after a few plain steps, each
+        // outer step applies T_cheb of B mapped so that [-|theta|max,
+        // theta_min] (theta = the block's Ritz values; |lambda_min| <= the
+        // largest |Ritz value| for the operators used here) goes to [-1, 1]:
+        // the components below the block's smallest Ritz value are damped,
+        // the top ones grow like cosh(cheb * acosh(x)), so a cluster of close
+        // eigenvalues below the wanted ones costs far fewer products than
+        // plain powers.  The stop rule is the eigenvalue change < tol.
+        Scratch dc(c);
+        double* Y0 = dc.get<double>((size_t)n * S_BLK);
+        double* Y1 = dc.get<double>((size_t)n * S_BLK);
+        double* Y2 = dc.get<double>((size_t)n * S_BLK);
+        if (!Y0 || !Y1 || !Y2) {
+            set_error("MDS: device allocation failed");
+            return RFX_ERR_OOM;
+        }
+        const int64_t cnt = (int64_t)n * S_BLK;
+        const unsigned gb = (unsigned)((cnt + 255) / 256);
+        for (int q = 0; q < 10; ++q) {
+            if ((st = apply(V, W)) != RFX_OK) return st;
+            if ((st = orth(W, V)) != RFX_OK) return st;
+        }
+        int matvecs = 10;
+        for (int outer = 0; matvecs < max_iter; ++outer) {
+            if ((st = apply(V, W)) != RFX_OK) return st;
+            ++matvecs;
+            double delta = 0.0;
+            if ((st = ritz(&delta)) != RFX_OK) return st;
+            if (iters_out) *iters_out = matvecs;
+            // also stop at the rounding floor: below 1e-9 a change that is no
+            // smaller than the last three means the products' rounding, not
+            // the iteration, sets it
+            hist.push_back(delta);
+            const size_t hn = hist.size();
+            const bool floor = hn >= 4 && delta < 1e-9 &&
+                               delta >= std::min(hist[hn - 2], std::min(hist[hn - 3], hist[hn - 4]));
+            if (delta < tol || floor || matvecs + cheb > max_iter) break;
+            double thmax = 0.0, thmin = cur[0];
+            for (double v : cur) {
+                thmax = std::max(thmax, std::fabs(v));
+                thmin = std::min(thmin, v);
+            }
+            const double lo = -thmax, hi = thmin;
+            const double cc = 0.5 * (lo + hi), ee = 0.5 * (hi - lo);
+            if (!(ee > 0.0)) break;
+            // Y0 = V, Y1 = (B V - cc V) / ee, Y_{j+1} = 2 (B Y_j - cc Y_j) / ee - Y_{j-1}
+            RFX_CUDA(cudaMemcpyAsync(Y0, V, sizeof(double) * cnt, cudaMemcpyDeviceToDevice, s));
+            block_axpby_kernel<<<gb, 256, 0, s>>>(1.0 / ee, W, -cc / ee, V, 0.0, nullptr, cnt, Y1);
+            c->launches += 1;
+            for (int j = 2; j <= cheb; ++j) {
+                if ((st = apply(Y1, W)) != RFX_OK) return st;
+                ++matvecs;
+                block_axpby_kernel<<<gb, 256, 0, s>>>(2.0 / ee, W, -2.0 * cc / ee, Y1, -1.0, Y0, cnt, Y2);
+                c->launches += 1;
+                std::swap(Y0, Y1);
+                std::swap(Y1, Y2);
+            }
+            RFX_CUDA(cudaGetLastError());
+            if ((st = orth(Y1, V)) != RFX_OK) return st;
+        }
+    } else
     for (int it = 1; it <= max_iter; ++it) {
         if ((st = apply(V, W)) != RFX_OK) return st;
         const bool check = (it % 10 == 0) || it == max_iter;
@@ -834,7 +929,10 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
-    return subspace_topk(c, n, 3, apply, 600, d_coords, evals, 12345);
+    // Chebyshev degree 8; up to 4000 products (the eigenvalue-change
+    // criterion of 1e-14 ends it far earlier unless the third eigenvalue sits
+    // in a tight cluster)
+    return subspace_topk(c, n, 3, apply, 4000, d_coords, evals, 12345, 1e-14, nullptr, nullptr, nullptr, false, 8);
 }
 
 }  // namespace rfx
