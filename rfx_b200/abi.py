@@ -191,8 +191,9 @@ class BatchGraph:
 TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order", 4: "pair_counts_hub"}
 # launch shapes per stage, in the library's shape order
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
-                    "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight"], 1: ["256", "512", "1024"],
-                2: ["64", "128", "256"], 3: ["128", "256", "512"]}
+                    "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight"],
+                1: ["row16 256", "row16 512", "row16 1024", "row2 256", "row2 512", "row2 1024"],
+                2: ["64", "128", "256"], 3: ["128", "256", "512"], 4: ["row2 256", "row2 512", "row2 1024"]}
 
 
 def tuned_shapes():
@@ -205,7 +206,7 @@ def tuned_shapes():
     for r in buf[: 6 * cnt.value].reshape(-1, 6):
         st = int(r[0])
         out.append({"stage": TUNED_STAGES.get(st, str(st)), "device": int(r[1]), "log2_n": int(r[2]),
-                    "log2_ntree": int(r[3]), "log2_p": int(r[4]), "shape": TUNED_SHAPES[st][int(r[5])]})
+                    "log2_ntree": int(r[3]), "log2_p": int(r[4]), "shape": TUNED_SHAPES.get(st, [])[int(r[5])] if int(r[5]) < len(TUNED_SHAPES.get(st, [])) else str(int(r[5]))})
     return out
 
 

@@ -44,3 +44,13 @@ def test_casewise_context_without_device(built):
         abi.Context(0, use_casewise=True)
     except abi.RfxError as e:
         assert e.status in (2, 8)
+
+
+def test_tuned_shape_names_cover_every_stage_and_shape(built):
+    """Every launch shape the autotuner can record has a name in the binding's
+    table (stage ids and shape counts as csrc/tune.cu and the launchers use)."""
+    from rfx_b200 import abi
+
+    counts = {0: 8, 1: 6, 2: 3, 3: 3, 4: 3}
+    for st, k in counts.items():
+        assert len(abi.TUNED_SHAPES[st]) == k, st
