@@ -193,7 +193,14 @@ TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_o
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
                     "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight"],
                 1: ["row16 256", "row16 512", "row16 1024", "row2 256", "row2 512", "row2 1024"],
-                2: ["64", "128", "256"], 3: ["128", "256", "512"], 4: ["row2 256", "row2 512", "row2 1024"]}
+                2: ["64", "128", "256", "64 staged rows", "128 staged rows", "256 staged rows"],
+                3: ["128", "256", "512", "64 staged rows", "128 staged rows", "256 staged rows"],
+                4: ["row2 256", "row2 512", "row2 1024"]}
+
+
+def _shape_name(kernel: int, shape: int) -> str:
+    names = TUNED_SHAPES.get(kernel, [])
+    return names[shape] if 0 <= shape < len(names) else str(shape)
 
 
 def tuned_shapes():
@@ -206,7 +213,7 @@ def tuned_shapes():
     for r in buf[: 6 * cnt.value].reshape(-1, 6):
         st = int(r[0])
         out.append({"stage": TUNED_STAGES.get(st, str(st)), "device": int(r[1]), "log2_n": int(r[2]),
-                    "log2_ntree": int(r[3]), "log2_p": int(r[4]), "shape": TUNED_SHAPES.get(st, [])[int(r[5])] if int(r[5]) < len(TUNED_SHAPES.get(st, [])) else str(int(r[5]))})
+                    "log2_ntree": int(r[3]), "log2_p": int(r[4]), "shape": _shape_name(st, int(r[5]))})
     return out
 
 

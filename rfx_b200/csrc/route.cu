@@ -247,6 +247,54 @@ route_leaf_order_kernel(const float* __restrict__ X, int n, int p, int nclass, c
     key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
 }
 
+// The same with the CTA's feature rows staged in shared memory first (row
+// stride p | 1 floats, so that the lanes of a warp reading one feature hit
+// different banks): each walk step then waits for one node load (L1, the
+// CTA's samples share a tree) instead of a node load and an L2 feature load.
+template <int RT>
+__global__ void __launch_bounds__(RT)
+route_leaf_staged_kernel(const float* __restrict__ X, int n, int p, int nclass, const DNode* __restrict__ nodes,
+                         const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
+                         const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+                         const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
+                         const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ memb,
+                         int32_t* __restrict__ key_out, int32_t* __restrict__ votes) {
+    extern __shared__ float xs[];  // RT rows of ps floats
+    const int ps = p | 1;
+    const int t = blockIdx.y;
+    const int q = blockIdx.x * RT + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = q < n ? __ldg(memb + (size_t)t * n + q) : -1;
+    // each warp stages its 32 rows, one row at a time across the lanes
+    for (int r = 0; r < 32; ++r) {
+        const int ir = __shfl_sync(0xffffffffu, i, r);
+        if (ir < 0) continue;
+        float* dst = xs + (size_t)(w * 32 + r) * ps;
+        const float* src = X + (size_t)ir * p;
+        for (int m = lane; m < p; m += 32) dst[m] = __ldg(src + m);
+    }
+    __syncwarp();
+    if (q >= n) return;
+    const SharedRow xrow{xs + (size_t)threadIdx.x * ps};
+    const int64_t o = offs[t];
+    const DNode* tn = nodes + o;
+    const int32_t* tc = nodeclass + o;
+    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+    const int nn = nnode_arr[t];
+    const size_t ti = (size_t)t * n + i;
+    const bool ib = inbag[ti] != 0;
+    int node;
+    if (!ib) {
+        int cls;
+        node = walk_testreebag_x(xrow, p, GlobalNodes{tn}, tc, nn, cat, cgl, maxcat, &cls);
+        if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
+    } else {
+        node = walk_terminal_x(xrow, p, GlobalNodes{tn}, cat, cgl, maxcat, 2 * n + 1);
+    }
+    const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
+    key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
+}
+
 constexpr int ROUTE_SHAPES = 8;
 
 // votes must be zero beforehand (the kernel adds to them)
@@ -343,17 +391,37 @@ rfx_status launch_route(Ctx* c) {
     rfx_status r;
     if (c->csr_built) {
         // the member lists of an earlier pass over this forest give the order
-        r = autotune(c, TK_ROUTE_LEAF, 3, 1, [&](int shape) -> rfx_status {
+        // shapes 0-2: 128 / 256 / 512 threads; 3-5: 64 / 128 / 256 threads
+        // with the feature rows staged in shared memory (when they fit in
+        // 96 KB; otherwise the unstaged kernel of that width runs)
+        const size_t row_bytes = sizeof(float) * (size_t)(c->p | 1);
+        int dev_smem = 0;
+        RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+        if (rfx_status s0 = allow_dyn_smem(route_leaf_staged_kernel<64>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(route_leaf_staged_kernel<128>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(route_leaf_staged_kernel<256>, dev_smem)) return s0;
+        r = autotune(c, TK_ROUTE_LEAF, 6, 1, [&](int shape) -> rfx_status {
             RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
-            auto go = [&](auto kernel, int rt) {
+            auto go = [&](auto kernel, int rt, size_t smem) {
                 dim3 grid((c->n + rt - 1) / rt, c->T);
-                kernel<<<grid, rt, 0, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
-                                                   c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
-                                                   c->d_catgoleft, c->maxcat, c->d_memb, c->d_key, c->d_votes);
+                kernel<<<grid, rt, smem, c->stream>>>(c->d_X, c->n, c->p, c->nclass, c->d_nodes, c->d_nodeclass,
+                                                      c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+                                                      c->d_catgoleft, c->maxcat, c->d_memb, c->d_key, c->d_votes);
             };
-            if (shape == 0) go(route_leaf_order_kernel<128>, 128);
-            else if (shape == 2) go(route_leaf_order_kernel<512>, 512);
-            else go(route_leaf_order_kernel<256>, 256);
+            const int srt = shape == 3 ? 64 : shape == 4 ? 128 : 256;
+            const bool staged = shape >= 3 && (size_t)srt * row_bytes <= 96 * 1024;
+            if (staged) {
+                const size_t sm = (size_t)srt * row_bytes;
+                if (srt == 64) go(route_leaf_staged_kernel<64>, 64, sm);
+                else if (srt == 128) go(route_leaf_staged_kernel<128>, 128, sm);
+                else go(route_leaf_staged_kernel<256>, 256, sm);
+            } else if (shape == 0 || shape == 4) {
+                go(route_leaf_order_kernel<128>, 128, 0);
+            } else if (shape == 2) {
+                go(route_leaf_order_kernel<512>, 512, 0);
+            } else {
+                go(route_leaf_order_kernel<256>, 256, 0);
+            }
             RFX_CUDA(cudaGetLastError());
             return RFX_OK;
         });

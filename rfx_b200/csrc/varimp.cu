@@ -36,6 +36,15 @@ constexpr int VT = 256;  // threads of the per-tree OOB-list kernel
 
 enum { DIR_BREAK = -2 };
 
+// A sample's feature row for the walks: staged in shared memory (SX) or read
+// from global memory through the read-only cache.
+template <bool SX>
+struct RowSel {
+    const float* g;
+    const float* s;
+    __device__ __forceinline__ float operator()(int m) const { return SX ? s[m] : __ldg(g + m); }
+};
+
 // One decision of the cpu_testreeimp walk at node nd (local id kt) for value x.
 __device__ __forceinline__ int imp_decide(const DNode& nd, int kt, float x, const int32_t* __restrict__ cgl,
                                           int maxcat) {
@@ -48,17 +57,16 @@ __device__ __forceinline__ int imp_decide(const DNode& nd, int kt, float x, cons
 // Side walk of the permuted traversal from node kt with feature mr taken from
 // xperm; budget = remaining loop iterations of the reference's k < nnode loop.
 // Returns the class, or -1 when the reference would break without assigning.
-template <typename Src>
-__device__ __forceinline__ int imp_side_walk(const float* __restrict__ xrow, const float* __restrict__ xperm, int mr,
-                                             int p, int kt, int budget, const Src& nodes,
-                                             const int32_t* __restrict__ nclass_of, const int32_t* __restrict__ cgl,
-                                             int maxcat) {
+template <typename Src, typename XR>
+__device__ __forceinline__ int imp_side_walk(const XR& xrow, const XR& xperm, int mr, int p, int kt, int budget,
+                                             const Src& nodes, const int32_t* __restrict__ nclass_of,
+                                             const int32_t* __restrict__ cgl, int maxcat) {
     for (int s = 0; s < budget; ++s) {
         const DNode nd = nodes(kt);
         if (node_status(nd.meta) == -1) return __ldg(nclass_of + kt);
         const int m = node_var(nd.meta);
         if (m >= p) return -1;
-        const float x = __ldg((m == mr ? xperm : xrow) + m);
+        const float x = m == mr ? xperm(m) : xrow(m);
         const int nx = imp_decide(nd, kt, x, cgl, maxcat);
         if (nx == DIR_BREAK) return -1;
         kt = nx;
@@ -125,7 +133,7 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
 // block [fb, fb + 64 W): flip bits and delta counters are block-local, other
 // features' splits are followed without a permuted decision, and the per-tree
 // correct counts are added by the fb == 0 launch only.
-template <int W, int VW, bool FB = false>
+template <int W, int VW, bool FB = false, bool SX = false>
 __global__ void __launch_bounds__(VW, 1536 / VW)
 varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
                    const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
@@ -137,7 +145,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                    const uint8_t* __restrict__ inbag, uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips,
                    int32_t* __restrict__ counts, int32_t* __restrict__ delta_out, uint32_t* __restrict__ err,
                    int fb) {
-    extern __shared__ int32_t delta[];  // pw counters (the features of this launch)
+    extern __shared__ int32_t delta[];  // pw counters (the features of this launch), then with SX the
+                                        // staged feature rows: VW own rows and VW partner rows of p | 1 floats
     __shared__ int s_red[2];
     // Side walks found along the main paths are queued and then shared out
     // over the whole CTA, so a thread with many of them does not hold its
@@ -177,6 +186,26 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     }
     const int pw = FB ? min(64 * W, p - fb) : p;
     for (int k = tid; k < pw; k += VW) delta[k] = 0;
+    // with SX: every warp stages its lanes' own and partner rows (one row at
+    // a time across the lanes), so each walk step reads features from shared
+    // memory; without it the rows are read through the read-only cache
+    const int ps = p | 1;
+    float* xs_own = reinterpret_cast<float*>(delta + ((pw + 3) & ~3));
+    float* xs_par = xs_own + (size_t)VW * ps;
+    if (SX) {
+        const int w = tid >> 5;
+        for (int r = 0; r < 32; ++r) {
+            const int ir = __shfl_sync(0xffffffffu, active ? i : -1, r);
+            const int pr = __shfl_sync(0xffffffffu, ip, r);
+            if (ir < 0) continue;
+            float* d0 = xs_own + (size_t)(w * 32 + r) * ps;
+            float* d1 = xs_par + (size_t)(w * 32 + r) * ps;
+            for (int m = lane; m < p; m += 32) {
+                d0[m] = __ldg(X + (size_t)ir * p + m);
+                d1[m] = __ldg(X + (size_t)pr * p + m);
+            }
+        }
+    }
     if (tid == 0) {
         s_red[0] = 0;
         s_red[1] = 0;
@@ -201,8 +230,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     if (active) {
         s_i[tid] = i;
         s_ip[tid] = ip;
-        const float* xi = X + (size_t)i * p;
-        const float* xp = X + (size_t)ip * p;
+        const RowSel<SX> xi{X + (size_t)i * p, xs_own + (size_t)tid * ps};
+        const RowSel<SX> xp{X + (size_t)ip * p, xs_par + (size_t)tid * ps};
         yi = y[i];
         s_y[tid] = yi;
         // The cpu_testreebag walk of the same sample follows the main path
@@ -233,7 +262,7 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                 break;
             }
             if (m >= p) break;
-            const float xv = __ldg(xi + m);
+            const float xv = xi(m);
             const int dir_o = imp_decide(nd, kt, xv, cgl, maxcat);
             if (tb_sync && !tb_done) {
                 int tb_next;
@@ -261,7 +290,7 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
             for (int q = 0; q < W; ++q)
                 if (q == wq) dword = done[q];
             if ((!FB || (unsigned)mm < (unsigned)(64 * W)) && !(dword & bit)) {
-                const int dir_p = imp_decide(nd, kt, __ldg(xp + m), cgl, maxcat);
+                const int dir_p = imp_decide(nd, kt, xp(m), cgl, maxcat);
                 if (dir_p != dir_o) {
                     int cls_m = -2;  // -2: queued, decided in the shared phase
                     if (dir_p == DIR_BREAK) {
@@ -285,7 +314,7 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
             kt = dir_o;
         }
         if (!ok) my_err |= ERR_STALE_JVR;
-        if (!tb_done) walk_testreebag_src(xi, p, src, tc, nn, cat, cgl, maxcat, &cls_tb);
+        if (!tb_done) walk_testreebag_x(xi, p, src, tc, nn, cat, cgl, maxcat, &cls_tb);
         base_tb = (cls_tb == yi);
         base_imp = (ok && jvr0 == yi);
     }
@@ -295,7 +324,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     for (int e = tid; e < qn; e += VW) {
         const int4 en = q_ent[e];
         const int lt = en.x, m = en.y;
-        const int cls_m = imp_side_walk(X + (size_t)s_i[lt] * p, X + (size_t)s_ip[lt] * p, m, p, en.z, en.w, src,
+        const int cls_m = imp_side_walk(RowSel<SX>{X + (size_t)s_i[lt] * p, xs_own + (size_t)lt * ps},
+                                        RowSel<SX>{X + (size_t)s_ip[lt] * p, xs_par + (size_t)lt * ps}, m, p, en.z, en.w, src,
                                         tc, cgl, maxcat);
         if (cls_m < 0) my_err |= ERR_STALE_JVR;
         const int mb = FB ? m - fb : m;
@@ -480,22 +510,42 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
-        auto go = [&](auto kernel, int vw) {
+        // staged shapes hold VW own rows and VW partner rows of p | 1 floats
+        // after the counters (offset rounded to 16 bytes)
+        const size_t cnt_bytes = sizeof(int32_t) * (((size_t)c->p + 3) & ~(size_t)3);
+        auto staged_smem = [&](int vw) { return cnt_bytes + 2 * sizeof(float) * (size_t)vw * (size_t)(c->p | 1); };
+        auto go = [&](auto kernel, int vw, size_t sm) -> rfx_status {
+            if (sm > 48 * 1024)
+                RFX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             dim3 grid(((ordered ? c->n : max_noob) + vw - 1) / vw, c->T);
-            kernel<<<grid, vw, smem, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
+            kernel<<<grid, vw, sm, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
                                                  c->d_nnode, c->d_noob, c->d_cat, c->d_catgoleft, c->maxcat,
                                                  c->d_permoff, c->d_perm, c->d_joob,
                                                  ordered ? c->d_memb : nullptr, c->d_partner, c->d_inbag,
                                                  c->d_vflags, c->d_flips,
                                                  c->d_right, c->d_rightimp, c->d_err, 0);
+            return RFX_OK;
         };
-        rfx_status r = autotune(c, TK_VWALK, 3, 1, [&](int shape) -> rfx_status {
+        // shapes 0-2: rows through the read-only cache at 64/128/256 threads;
+        // 3-5: the same with staged rows, where they fit in 96 KB
+        rfx_status r = autotune(c, TK_VWALK, 6, 1, [&](int shape) -> rfx_status {
             // the walk adds to the per-tree counts: clear them for every run
             RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
             RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
-            if (shape == 0) go(varimp_walk_kernel<W, 64>, 64);
-            else if (shape == 2) go(varimp_walk_kernel<W, 256>, 256);
-            else go(varimp_walk_kernel<W, 128>, 128);
+            const int vw = (shape % 3) == 0 ? 64 : (shape % 3) == 2 ? 256 : 128;
+            const bool staged = shape >= 3 && staged_smem(vw) <= 96 * 1024;
+            rfx_status g;
+            if (staged) {
+                const size_t sm = staged_smem(vw);
+                g = vw == 64 ? go(varimp_walk_kernel<W, 64, false, true>, 64, sm)
+                    : vw == 256 ? go(varimp_walk_kernel<W, 256, false, true>, 256, sm)
+                                : go(varimp_walk_kernel<W, 128, false, true>, 128, sm);
+            } else {
+                g = vw == 64 ? go(varimp_walk_kernel<W, 64>, 64, smem)
+                    : vw == 256 ? go(varimp_walk_kernel<W, 256>, 256, smem)
+                                : go(varimp_walk_kernel<W, 128>, 128, smem);
+            }
+            if (g != RFX_OK) return g;
             RFX_CUDA(cudaGetLastError());
             return RFX_OK;
         });

@@ -33,13 +33,24 @@ __device__ __forceinline__ int cgl_at(const int32_t* __restrict__ cgl, int maxca
     return cgl ? __ldg(cgl + (size_t)node * maxcat + idx) : 0;
 }
 
+// A sample's feature row: in global memory (read through the read-only
+// cache) or staged in shared memory by the calling kernel.
+struct GlobalRow {
+    const float* r;
+    __device__ __forceinline__ float operator()(int m) const { return __ldg(r + m); }
+};
+struct SharedRow {
+    const float* r;
+    __device__ __forceinline__ float operator()(int m) const { return r[m]; }
+};
+
 // Returns the node id; *cls receives the class (nodeclass of the final node,
 // or of the root on the fallback path).
-template <typename Src>
-__device__ __forceinline__ int walk_testreebag_src(const float* __restrict__ xrow, int p, const Src& nodes,
-                                                   const int32_t* __restrict__ nclass_of, int nnode,
-                                                   const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
-                                                   int maxcat, int* cls) {
+template <typename Src, typename XR>
+__device__ __forceinline__ int walk_testreebag_x(const XR& xrow, int p, const Src& nodes,
+                                                 const int32_t* __restrict__ nclass_of, int nnode,
+                                                 const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                 int maxcat, int* cls) {
     int kt = 0;
     int steps = 0;
     DNode nd = nodes(0);
@@ -48,7 +59,7 @@ __device__ __forceinline__ int walk_testreebag_src(const float* __restrict__ xro
         if (steps >= 1000) break;
         const int m = node_var(nd.meta);
         if (m >= p) break;
-        const float v = __ldg(xrow + m);
+        const float v = xrow(m);
         if (!node_cat(nd.meta)) {
             kt = (v <= nd.split) ? nd.left : nd.right;
         } else {
@@ -76,6 +87,14 @@ __device__ __forceinline__ int walk_testreebag_src(const float* __restrict__ xro
     return 0;
 }
 
+template <typename Src>
+__device__ __forceinline__ int walk_testreebag_src(const float* __restrict__ xrow, int p, const Src& nodes,
+                                                   const int32_t* __restrict__ nclass_of, int nnode,
+                                                   const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                   int maxcat, int* cls) {
+    return walk_testreebag_x(GlobalRow{xrow}, p, nodes, nclass_of, nnode, cat, cgl, maxcat, cls);
+}
+
 __device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,
                                                const int32_t* __restrict__ nclass_of, int nnode,
                                                const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
@@ -85,17 +104,17 @@ __device__ __forceinline__ int walk_testreebag(const float* __restrict__ xrow, i
 
 // find_terminal_node: stops only at status -1; invalid category or variable
 // returns the root.  maxnode is the reference's loop bound (2n+1).
-template <typename Src>
-__device__ __forceinline__ int walk_terminal_src(const float* __restrict__ xrow, int p, const Src& nodes,
-                                                 const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
-                                                 int maxcat, int maxnode) {
+template <typename Src, typename XR>
+__device__ __forceinline__ int walk_terminal_x(const XR& xrow, int p, const Src& nodes,
+                                               const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                               int maxcat, int maxnode) {
     int cur = 0;
     for (int k = 0; k < maxnode; ++k) {
         const DNode nd = nodes(cur);
         if (node_status(nd.meta) == -1) return cur;
         const int m = node_var(nd.meta);
         if (m >= p) return 0;
-        const float v = __ldg(xrow + m);
+        const float v = xrow(m);
         if (!node_cat(nd.meta)) {
             cur = (v <= nd.split) ? nd.left : nd.right;
         } else {
@@ -108,6 +127,13 @@ __device__ __forceinline__ int walk_terminal_src(const float* __restrict__ xrow,
         }
     }
     return 0;
+}
+
+template <typename Src>
+__device__ __forceinline__ int walk_terminal_src(const float* __restrict__ xrow, int p, const Src& nodes,
+                                                 const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                 int maxcat, int maxnode) {
+    return walk_terminal_x(GlobalRow{xrow}, p, nodes, cat, cgl, maxcat, maxnode);
 }
 
 __device__ __forceinline__ int walk_terminal(const float* __restrict__ xrow, int p, const DNode* __restrict__ nodes,

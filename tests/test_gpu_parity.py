@@ -315,7 +315,7 @@ def ok_leaf(term, f, t, node):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("stage,count", [("ROUTE", 8), ("PAIRS", 6), ("VWALK", 3), ("ROUTE_LEAF", 3)])
+@pytest.mark.parametrize("stage,count", [("ROUTE", 8), ("PAIRS", 6), ("VWALK", 6), ("ROUTE_LEAF", 6)])
 def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
     """Each launch shape the autotuner can pick gives the oracle's results."""
     from oracle import oracle as orc
@@ -330,6 +330,9 @@ def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
         ctx.load(f, X, y)
         q, nout, _ = ctx.route_oob()
         assert np.array_equal(q.astype(np.float32), O["q_raw"]), shape
+        # before any pair counts the walk runs over the OOB lists, after them in leaf order
+        avimp, sqsd, qimp, qimpm = ctx.varimp(True)
+        assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
         assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
         # a second pass routes in the leaf order of the first one
         assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
