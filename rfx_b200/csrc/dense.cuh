@@ -58,9 +58,13 @@ __device__ inline void cta_tri_inverse(const double* L, double* Linv, int s, int
 // eigenvalues on the diagonal of A, eigenvectors in the columns of V.
 // Rotations of disjoint index pairs are applied in parallel (round-robin
 // ordering); at most `sweeps` full sweeps, fewer once every off-diagonal entry
-// is at FP64 rounding relative to its diagonal pair.  A leading dimension
-// ld = s + 1 keeps the column passes free of shared-memory bank conflicts.
-__device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweeps, int* pairs) {
+// is at FP64 rounding relative to its diagonal pair, or (abs_tol > 0) below
+// abs_tol times the largest diagonal magnitude: the absolute stop ends a
+// spectrum with eigenvalues near zero, whose relative test rounding keeps
+// open, and leaves the large eigenpairs accurate to abs_tol.  A leading
+// dimension ld = s + 1 keeps the column passes free of shared-memory bank
+// conflicts.
+__device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweeps, int* pairs, double abs_tol = 0.0) {
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = tid; e < s * s; e += nt) V[(e / s) * ld + (e % s)] = ((e / s) == (e % s)) ? 1.0 : 0.0;
     __syncthreads();
@@ -70,12 +74,18 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
         // converged when every off-diagonal entry is negligible against its
         // diagonal pair, |a_pq| <= 1e-16 sqrt(|a_pp a_qq|) (the relative
         // criterion, which keeps small eigenvalues accurate)
+        double floor2 = 0.0;
+        if (abs_tol > 0.0) {
+            double dmax = 0.0;
+            for (int r = 0; r < s; ++r) dmax = fmax(dmax, fabs(A[r * ld + r]));
+            floor2 = (abs_tol * dmax) * (abs_tol * dmax);
+        }
         int active = 0;
         for (int e = tid; e < s * s; e += nt) {
             const int r = e / s, q = e % s;
             if (r < q) {
                 const double v = A[r * ld + q];
-                if (v * v > 1e-32 * fabs(A[r * ld + r] * A[q * ld + q])) active = 1;
+                if (v * v > 1e-32 * fabs(A[r * ld + r] * A[q * ld + q]) && v * v > floor2) active = 1;
             }
         }
         if (!__syncthreads_or(active)) break;

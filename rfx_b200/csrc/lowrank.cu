@@ -425,7 +425,9 @@ __global__ void eig_w_kernel(const double* __restrict__ H, int w, double* __rest
         A[i * ld + j] = 0.5 * (H[i * w + j] + H[j * w + i]);
     }
     __syncthreads();
-    cta_jacobi(A, U, w, ld, 30, pairs);
+    // the top k of w eigenpairs are kept: an absolute stop at 1e-15 of the
+    // largest eigenvalue
+    cta_jacobi(A, U, w, ld, 30, pairs, 1e-15);
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) evecs[e] = U[(e / w) * ld + (e % w)];
     for (int i = threadIdx.x; i < w; i += blockDim.x) evals[i] = A[i * ld + i];
 }

@@ -88,58 +88,179 @@ __global__ void mds_grand_kernel(const double* __restrict__ rowmean, int n, doub
     }
 }
 
-__global__ void mds_b_kernel(const float* __restrict__ P, const int32_t* __restrict__ nout, int n,
+// B with leading dimension npad (>= n); the pad rows and columns are zero.
+__global__ void mds_b_kernel(const float* __restrict__ P, const int32_t* __restrict__ nout, int n, int npad,
                              const unsigned long long* __restrict__ maxbits, const double* __restrict__ rowmean,
                              const double* __restrict__ grand, double* __restrict__ B) {
     const double mx = __longlong_as_double((long long)*maxbits);
     const double g = *grand;
-    const size_t total = (size_t)n * n;
+    const size_t total = (size_t)npad * npad;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e / n), j = (int)(e % n);
+        const int i = (int)(e / npad), j = (int)(e % npad);
+        if (i >= n || j >= n) {
+            B[e] = 0.0;
+            continue;
+        }
         const double d = (i == j) ? 0.0 : __dsub_rn(mx, q_value(P, nout, n, i, j));
         const double v = __dadd_rn(__dsub_rn(__dsub_rn(__dmul_rn(d, d), rowmean[i]), rowmean[j]), g);
         B[e] = __dmul_rn(-0.5, v);
     }
 }
 
-// W[n x S] = B[n x n] V[n x S], FP64, 64-row tiles.
+// W[n x S] = B[n x n] V[n x S] in FP64 on the tensor cores (mma.sync
+// m16n8k4 .f64; Blackwell's tcgen05 has no FP64 kind).  B is stored with a
+// padded leading dimension npad (a multiple of 64, pads zero), so every
+// 64 x 64 tile row is one 512-byte bulk copy.  A CTA of four warps owns 64
+// rows and one range of kchunk columns; each 64-column step brings the B tile
+// (64 row copies into rows 544 bytes apart, which makes the fragment reads
+// conflict-free) and the matching 64 x 16 block of V (pre-arranged in
+// fragment order by bv_pack_kernel) through a DB_STAGES-deep mbarrier
+// pipeline.  Warp w multiplies rows 16w..16w+15 by both 8-column halves of V.
+// The partial products go to Wpart[range] and are added in range order.
 constexpr int GT = 64;
 constexpr int BV_KSPLIT = 8;  // column ranges per row tile (enough CTAs to fill the GPU in several waves)
+constexpr int DB_STAGES = 4;
+constexpr int DB_RS = GT * 8 + 32;                          // bytes between tile rows in shared memory
+constexpr int DB_VBYTES = GT * S_BLK * 8;                   // one 64 x 16 block of V
+constexpr int DB_STAGE = GT * DB_RS + DB_VBYTES;            // 43,008 bytes
+constexpr size_t DB_SMEM = (size_t)DB_STAGES * DB_STAGE;    // 172,032 bytes
+constexpr int DB_WAIT_LIMIT = 1 << 24;
 
-// Partial products Wpart[ks] = B[rows, K_ks] V[K_ks, :] for row tile blockIdx.x
-// and column range ks = blockIdx.y of kchunk columns (a multiple of GT).
-__global__ void __launch_bounds__(256) dgemm_bv_kernel(const double* __restrict__ B, const double* __restrict__ V,
-                                                       int n, int kchunk, double* __restrict__ Wpart) {
-    __shared__ double Bs[GT][GT + 1];
-    __shared__ double Vs[GT][S_BLK];
-    const int r0 = blockIdx.x * GT;
-    const int ks = blockIdx.y;
-    const int kbeg = ks * kchunk, kend = min(n, kbeg + kchunk);
-    const int tid = threadIdx.x;
-    // thread owns rows (tid / 4) and columns (tid % 4) * 4 .. +3
-    const int rr = tid >> 2, cc = (tid & 3) * 4;
-    double acc[4] = {0, 0, 0, 0};
-    for (int k0 = kbeg; k0 < kend; k0 += GT) {
-        for (int e = tid; e < GT * GT; e += 256) {
-            const int r = e / GT, k = e % GT;
-            Bs[r][k] = (r0 + r < n && k0 + k < kend) ? B[(size_t)(r0 + r) * n + k0 + k] : 0.0;
-        }
-        for (int e = tid; e < GT * S_BLK; e += 256) {
-            const int k = e / S_BLK, c = e % S_BLK;
-            Vs[k][c] = (k0 + k < kend) ? V[(size_t)(k0 + k) * S_BLK + c] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll 8
-        for (int k = 0; k < GT; ++k) {
-            const double b = Bs[rr][k];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = fma(b, Vs[k][cc + q], acc[q]);
-        }
-        __syncthreads();
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void db_mbar_init(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
+}
+
+__device__ __forceinline__ void db_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(mbar),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the completion with parity `parity`
+__device__ __forceinline__ bool db_wait(uint32_t mbar, uint32_t parity) {
+    for (int it = 0; it < DB_WAIT_LIMIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (done) return true;
     }
-    if (r0 + rr < n)
+    return false;
+}
+
+__device__ __forceinline__ void db_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+
+// D += A B for one m16n8k4 FP64 tile: a0/a1 = A[g][t], A[g+8][t]; b = B[t][g];
+// c0..c3 = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1] (g = lane / 4,
+// t = lane % 4)
+__device__ __forceinline__ void dmma(double* c, double a0, double a1, double b) {
+    asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+                 : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+                 : "d"(a0), "d"(a1), "d"(b));
+}
+
+// Vf = V in fragment order, npad rows (rows >= n zero): within each 4-row
+// step, element (k, c) sits at (c / 8) * 32 + (c % 8) * 4 + k % 4, so the
+// lanes of a warp read 32 consecutive doubles per fragment.
+__global__ void bv_pack_kernel(const double* __restrict__ V, int n, int npad, double* __restrict__ Vf) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)npad * S_BLK) return;
+    const int k = (int)(idx / S_BLK), c = (int)(idx % S_BLK);
+    const size_t dst = (size_t)(k >> 2) * 64 + (c >> 3) * 32 + (c & 7) * 4 + (k & 3);
+    Vf[dst] = k < n ? V[idx] : 0.0;
+}
+
+__global__ void __launch_bounds__(128, 1) dgemm_bv_kernel(const double* __restrict__ B, int ldb,
+                                                         const double* __restrict__ Vf, int n, int kchunk,
+                                                         double* __restrict__ Wpart, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t dsm[];
+    __shared__ __align__(8) uint64_t full[DB_STAGES];
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = blockIdx.x * GT;
+    const int kbeg = blockIdx.y * kchunk, kend = min(n, kbeg + kchunk);
+    const int ntile = (kend - kbeg + GT - 1) / GT;  // >= 1: every range starts below n
+    const uint32_t base = su32(dsm);
+    if (tid == 0) {
+        for (int s = 0; s < DB_STAGES; ++s) db_mbar_init(su32(&full[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    __syncthreads();
+    // warp 0 brings tile `it` into its stage: 64 row copies and the V block
+    auto issue = [&](int it) {
+        const int s = it % DB_STAGES;
+        const int k0 = kbeg + it * GT;
+        const uint32_t dst = base + (uint32_t)(s * DB_STAGE);
+        const uint32_t bar = su32(&full[s]);
+        if (lane == 0) db_expect_tx(bar, GT * GT * 8 + DB_VBYTES);
+        __syncwarp();
+        for (int r = lane; r < GT; r += 32)
+            db_g2s(dst + (uint32_t)(r * DB_RS), B + (size_t)(r0 + r) * ldb + k0, GT * 8, bar);
+        if (lane == 0) db_g2s(dst + (uint32_t)(GT * DB_RS), Vf + (size_t)k0 * S_BLK, DB_VBYTES, bar);
+    };
+    int issued = 0;
+    if (warp == 0)
+        for (; issued < min(DB_STAGES - 1, ntile); ++issued) issue(issued);
+    double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+    const int arow = (warp * 16 + g) * (DB_RS / 8) + t;  // A[g][t] of this warp's rows, in doubles
+    int it = 0;
+    for (; it < ntile; ++it) {
+        // every warp is done with tile it - 1, so its stage can be refilled
+        __syncthreads();
+        if (s_fail) break;
+        if (warp == 0 && it + DB_STAGES - 1 < ntile) {
+            issue(it + DB_STAGES - 1);
+            issued = it + DB_STAGES;
+        }
+        const int s = it % DB_STAGES;
+        if (!db_wait(su32(&full[s]), (uint32_t)((it / DB_STAGES) & 1))) {
+            if (lane == 0) {
+                s_fail = 1;
+                atomicOr(err, ERR_WAIT_LIMIT);
+            }
+            continue;  // the next barrier ends the loop for every warp
+        }
+        const double* Bs = reinterpret_cast<const double*>(dsm + s * DB_STAGE);
+        const double* Vs = reinterpret_cast<const double*>(dsm + s * DB_STAGE + GT * DB_RS);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) Wpart[((size_t)ks * n + r0 + rr) * S_BLK + cc + q] = acc[q];
+        for (int ks = 0; ks < GT / 4; ++ks) {
+            const double a0 = Bs[arow + ks * 4];
+            const double a1 = Bs[arow + 8 * (DB_RS / 8) + ks * 4];
+            const double b0 = Vs[ks * 64 + g * 4 + t];
+            const double b1 = Vs[ks * 64 + 32 + g * 4 + t];
+            dmma(acc[0], a0, a1, b0);
+            dmma(acc[1], a0, a1, b1);
+        }
+    }
+    __syncthreads();
+    if (s_fail) {
+        // a wait gave up at tile it - 1 (or at the last tile): the copies
+        // issued from there on land before the CTA leaves (bounded waits;
+        // a completed tile's wait returns at once)
+        if (warp == 0 && lane == 0)
+            for (int q = max(0, it - 1); q < issued; ++q)
+                db_wait(su32(&full[q % DB_STAGES]), (uint32_t)((q / DB_STAGES) & 1));
+        return;
+    }
+    double* out = Wpart + ((size_t)blockIdx.y * n) * S_BLK;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int col = h * 8 + 2 * t;
+        const int ra = r0 + warp * 16 + g, rb = ra + 8;
+        if (ra < n) *reinterpret_cast<double2*>(out + (size_t)ra * S_BLK + col) = make_double2(acc[h][0], acc[h][1]);
+        if (rb < n) *reinterpret_cast<double2*>(out + (size_t)rb * S_BLK + col) = make_double2(acc[h][2], acc[h][3]);
+    }
 }
 
 // W = sum of the ksn partial products, added in range order (reproducible).
@@ -900,7 +1021,8 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
         return RFX_ERR_UNSUPPORTED;
     }
     Scratch d(c);
-    double* B = d.get<double>((size_t)n * n);
+    const int npad = (n + GT - 1) / GT * GT;
+    double* B = d.get<double>((size_t)npad * npad);
     double* rowmean = d.get<double>(n);
     double* grand = d.get<double>(1);
     unsigned long long* mx = d.get<unsigned long long>(1);
@@ -912,20 +1034,23 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
     mds_max_kernel<<<1024, 256, 0, s>>>(dP, c->d_nout, n, mx);
     mds_rowsum_kernel<<<n, 256, 0, s>>>(dP, c->d_nout, n, mx, rowmean);
     mds_grand_kernel<<<1, 1024, 0, s>>>(rowmean, n, grand);
-    mds_b_kernel<<<2048, 256, 0, s>>>(dP, c->d_nout, n, mx, rowmean, grand, B);
+    mds_b_kernel<<<2048, 256, 0, s>>>(dP, c->d_nout, n, npad, mx, rowmean, grand, B);
     c->launches += 4;
     RFX_CUDA(cudaGetLastError());
     const int kchunk = ((n + BV_KSPLIT - 1) / BV_KSPLIT + GT - 1) / GT * GT;
     const int ksn = (n + kchunk - 1) / kchunk;
     double* Wpart = d.get<double>((size_t)ksn * n * S_BLK);
-    if (!Wpart) {
+    double* Vf = d.get<double>((size_t)npad * S_BLK);
+    if (!Wpart || !Vf) {
         set_error("rfx_mds3d_full: device allocation failed");
         return RFX_ERR_OOM;
     }
+    RFX_CUDA(cudaFuncSetAttribute(dgemm_bv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DB_SMEM));
     auto apply = [&](const double* V, double* W) -> rfx_status {
-        dgemm_bv_kernel<<<dim3((n + GT - 1) / GT, ksn), 256, 0, s>>>(B, V, n, kchunk, Wpart);
+        bv_pack_kernel<<<(unsigned)(((size_t)npad * S_BLK + 255) / 256), 256, 0, s>>>(V, n, npad, Vf);
+        dgemm_bv_kernel<<<dim3(npad / GT, ksn), 128, DB_SMEM, s>>>(B, npad, Vf, n, kchunk, Wpart, c->d_err);
         bv_reduce_kernel<<<(unsigned)(((size_t)n * S_BLK + 255) / 256), 256, 0, s>>>(Wpart, n, ksn, W);
-        c->launches += 2;
+        c->launches += 3;
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };

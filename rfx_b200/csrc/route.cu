@@ -295,12 +295,69 @@ route_leaf_staged_kernel(const float* __restrict__ X, int n, int p, int nclass, 
     key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
 }
 
-constexpr int ROUTE_SHAPES = 8;
+// The first KN nodes of tree t (the top levels: the grower numbers nodes in
+// the order it creates them, level by level) staged in shared memory; a CTA
+// then walks SUB x RT samples of that tree, so the staging is paid once per
+// RT * SUB samples.  Deeper nodes are read from global memory.
+struct StagedNodes {
+    const DNode* g;
+    const int4* s;
+    int k;
+    __device__ __forceinline__ DNode operator()(int j) const { return j < k ? as_node(s[j]) : load_node(g, j); }
+};
+
+template <int RT, int SUB, int KN>
+__global__ void __launch_bounds__(RT)
+route_nodes_kernel(const float* __restrict__ X, int n, int p, int T, int nclass, const DNode* __restrict__ nodes,
+                   const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
+                   const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
+                   const uint8_t* __restrict__ inbag, const int32_t* __restrict__ cat,
+                   const int32_t* __restrict__ catgoleft, int maxcat, int32_t* __restrict__ key_out,
+                   int32_t* __restrict__ leaf_out, int32_t* __restrict__ votes) {
+    __shared__ int4 sn[KN];
+    const int t = blockIdx.y;
+    const int64_t o = offs[t];
+    const int nn = nnode_arr[t];
+    const int kn = min(KN, nn);
+    const DNode* tn = nodes + o;
+    for (int j = threadIdx.x; j < kn; j += RT) sn[j] = __ldg(reinterpret_cast<const int4*>(tn) + j);
+    __syncthreads();
+    const StagedNodes src{tn, sn, kn};
+    const int32_t* tc = nodeclass + o;
+    const int32_t* cgl = catgoleft ? catgoleft + o * maxcat : nullptr;
+#pragma unroll 1
+    for (int s = 0; s < SUB; ++s) {
+        const int i = (blockIdx.x * SUB + s) * RT + threadIdx.x;
+        if (i >= n) return;
+        const float* xrow = X + (size_t)i * p;
+        const size_t ti = (size_t)t * n + i;
+        const bool ib = inbag[ti] != 0;
+        int node;
+        if (!ib) {
+            int cls;
+            node = walk_testreebag_src(xrow, p, src, tc, nn, cat, cgl, maxcat, &cls);
+            if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
+        } else {
+            node = walk_terminal_src(xrow, p, src, cat, cgl, maxcat, 2 * n + 1);
+        }
+        const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
+        key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
+        if (leaf_out) leaf_out[ti] = node;
+    }
+}
+
+constexpr int ROUTE_SHAPES = 10;
 
 // votes must be zero beforehand (the kernel adds to them)
 void route_launch(Ctx* c, int shape, int32_t* d_leaf) {
     auto go = [&](auto kernel, int rt, int tpc) {
         dim3 grid((c->n + rt - 1) / rt, (c->T + tpc - 1) / tpc);
+        kernel<<<grid, rt, 0, c->stream>>>(c->d_X, c->n, c->p, c->T, c->nclass, c->d_nodes, c->d_nodeclass,
+                                           c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
+                                           c->d_catgoleft, c->maxcat, c->d_key, d_leaf, c->d_votes);
+    };
+    auto go_nodes = [&](auto kernel, int rt, int sub) {
+        dim3 grid((c->n + rt * sub - 1) / (rt * sub), c->T);
         kernel<<<grid, rt, 0, c->stream>>>(c->d_X, c->n, c->p, c->T, c->nclass, c->d_nodes, c->d_nodeclass,
                                            c->d_leafidx, c->d_offs, c->d_nnode, c->d_inbag, c->d_cat,
                                            c->d_catgoleft, c->maxcat, c->d_key, d_leaf, c->d_votes);
@@ -313,6 +370,8 @@ void route_launch(Ctx* c, int shape, int32_t* d_leaf) {
         case 5: go(route2_kernel<256, 2>, 256, 2); break;
         case 6: go(route2_kernel<256, 4>, 256, 4); break;
         case 7: go(route2_kernel<128, 4>, 128, 4); break;
+        case 8: go_nodes(route_nodes_kernel<256, 8, 2048>, 256, 8); break;
+        case 9: go_nodes(route_nodes_kernel<256, 4, 1024>, 256, 4); break;
         default: go(route_kernel<256, 1>, 256, 1); break;
     }
 }
