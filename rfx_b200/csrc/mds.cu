@@ -871,7 +871,11 @@ __global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __
 
 }  // namespace
 
-rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32, float* M, float* T2);
+rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const uint8_t* Aq, const uint8_t* At,
+                                const float* u32, float* M, float* T2);
+rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* At);
+size_t factor_tc_aq_bytes(int n, int k);
+size_t factor_tc_at_bytes(int n, int k);
 
 namespace {
 void col_mean(const double* V, int n, double* part, double* mean, cudaStream_t s) {
@@ -908,13 +912,15 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     const size_t qsm = 4 * (size_t)k * k * sizeof(float);
     RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));
     bool tensor = false;
+    uint8_t* Aq = nullptr;
+    uint8_t* At = nullptr;
     auto apply = [&](const double* V, double* W) -> rfx_status {
         const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
         col_mean(V, n, part, mean, s);
         center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
         at_u(dA, u32, n, k, part, AtU, s);
         if (tensor) {
-            rfx_status st = launch_factor_ops_tc(c, dA, k, u32, M, T2);
+            rfx_status st = launch_factor_ops_tc(c, dA, k, Aq, At, u32, M, T2);
             if (st != RFX_OK) return st;
         } else {
             RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
@@ -934,7 +940,14 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     // mixed: BF16 tensor-core iterations to the BF16 rounding floor, then one
     // FP32 refinement step from that basis
     double* basis = d.get<double>((size_t)n * S_BLK);
-    if (!basis) return RFX_ERR_OOM;
+    Aq = d.get<uint8_t>(factor_tc_aq_bytes(n, k));
+    At = d.get<uint8_t>(factor_tc_at_bytes(n, k));
+    if (!basis || !Aq || !At) {
+        set_error("compute_mds_from_factors: device allocation failed");
+        return RFX_ERR_OOM;
+    }
+    // the factor's BF16 tensor-core operands, packed once for every product
+    if (rfx_status pst = pack_factor_tc(c, dA, k, Aq, At)) return pst;
     tensor = true;
     int it1 = 0, it2 = 0;
     rfx_status st =
@@ -976,7 +989,11 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
     at_u(dA, u32, n, k, part, AtU, s);
     rfx_status st = RFX_OK;
     if (precision) {
-        st = launch_factor_ops_tc(c, dA, k, u32, M, T2);
+        uint8_t* Aq = d.get<uint8_t>(factor_tc_aq_bytes(n, k));
+        uint8_t* At = d.get<uint8_t>(factor_tc_at_bytes(n, k));
+        if (!Aq || !At) return RFX_ERR_OOM;
+        st = pack_factor_tc(c, dA, k, Aq, At);
+        if (st == RFX_OK) st = launch_factor_ops_tc(c, dA, k, Aq, At, u32, M, T2);
     } else {
         const size_t qsm = 4 * (size_t)k * k * sizeof(float);
         RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));

@@ -1,31 +1,46 @@
 // Tensor-core (tcgen05, BF16 inputs, FP32 accumulation in TMEM) kernels of the
-// factor-space MDS operator (mds.cu):
+// factor-space MDS operator (mds.cu), for rank k = 32 or 64 and a block of
+// S = 16 vectors:
 //
 //   mstack_tc_kernel:   M_j = A^T diag(u_j) A for all j, as one GEMM
-//                       D[(j,a), b] = sum_i (u_ij A_ia) A_ib, M = s*k rows,
-//                       N = k, reduction over the n samples split across CTAs
-//                       (each CTA owns one 128-row M tile and one K range and
-//                       writes its FP32 tile to its own slot of a partial
-//                       stack; mstack_reduce_kernel adds the slots in K-range
-//                       order, so the result does not depend on CTA timing).
+//                       D[(j,a), b] = sum_i (u_ij A_ia) A_ib with M = S*k rows
+//                       (4 or 8 tiles of 128, all resident in TMEM), N = k and
+//                       the n samples as the reduction, in chunks of 32.  A
+//                       persistent CTA per SM owns one contiguous range of
+//                       chunks and writes its FP32 partial; mstack_reduce_kernel
+//                       adds the partials in CTA order (reproducible) and lays
+//                       M out as the next kernel's BF16 operand.
 //   quadform_tc_kernel: T2_ij = a_i^T M_j a_i: D[i, (j,b)] = sum_a A_ia M_j[b][a]
-//                       for a 128-sample tile in TMEM, then the epilogue reads
-//                       each row from TMEM and dots every 64-column block with
-//                       a_i; the n x (s*k) product never leaves the SM.
+//                       for a 128-sample tile, N = S*k in passes of 256 TMEM
+//                       columns (two buffers, so the epilogue of one pass
+//                       overlaps the MMAs of the next); the epilogue dots every
+//                       k-column block of a row with a_i, so the n x (S*k)
+//                       product never leaves the SM.  Persistent CTAs load the
+//                       whole M stack once.
 //
-// Operands are staged in shared memory by the CTA's threads in the canonical
-// K-major, no-swizzle UMMA layout: 8-row x 16-byte core matrices, the two
-// 8-element K halves of a 16-wide K step 128 bytes apart (leading byte offset)
-// and consecutive 8-row groups 256 bytes apart (stride byte offset).  One
-// elected thread issues tcgen05.mma and commits to an mbarrier; two operand
-// stages let the next tile be built while the tensor core works.  Every
-// mbarrier wait is bounded and records a timeout in the error word.
+// Operands sit in shared memory in the canonical K-major, no-swizzle UMMA
+// layout: 8-row x 16-byte core matrices, the two 8-element K halves of a
+// 16-wide K step 128 bytes apart (leading byte offset) and consecutive 8-row
+// groups 256 bytes apart (stride byte offset).  The factor A, which is fixed
+// for a whole MDS call, is packed once into that layout in two forms (128-
+// sample tiles with K = rank for the quadratic forms, and 32-sample chunks
+// with K = samples for the M stack), so every operand tile arrives by one
+// cp.async.bulk copy.  Roles: one thread issues the bulk copies, one the
+// MMAs (tcgen05.commit to mbarriers), four warps build the scaled operand or
+// run the epilogue.  Every mbarrier wait is bounded; a wait that gives up
+// raises ERR_WAIT_LIMIT, and the CTA drains its copies and MMAs (again with
+// bounded waits) before it frees TMEM and returns.
 #include <cuda_bf16.h>
 
 #include "rfx_internal.cuh"
 
 namespace rfx {
 namespace {
+
+constexpr int S_ = 16;    // vectors per block
+constexpr int CH = 32;    // samples per M-stack chunk
+constexpr int NP = 256;   // TMEM columns per quadratic-form pass
+constexpr int WAIT_LIMIT = 1 << 24;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -38,9 +53,9 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// byte offset of (row r, k) inside an R-row tile of 64 K: four 16-wide K steps
-// of R*32 bytes each
-__device__ __forceinline__ uint32_t tile_off(int r, int k, int R) {
+// byte offset of (row r, k) in a canonical tile of R rows: 16-wide K steps of
+// R * 32 bytes each
+__host__ __device__ __forceinline__ uint32_t canon_off(int r, int k, int R) {
     return (uint32_t)((k >> 4) * (R * 32) + (r >> 3) * 256 + ((k >> 3) & 1) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
@@ -52,16 +67,27 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar));
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count));
 }
 
-// bounded wait for phase `parity` of the mbarrier
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(mbar),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the phase with parity `parity` to complete
 __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < WAIT_LIMIT; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -74,6 +100,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -83,256 +115,490 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
+// 16 consecutive columns of this thread's TMEM lane (no wait)
+__device__ __forceinline__ void tmem_ld16_nw(uint32_t taddr, uint32_t* r) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;");
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-constexpr int TC_THREADS = 128;
-constexpr int KCH = 64;  // samples per K chunk
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// grid: (s*k/128 M tiles, K splits); k in {16, 32, 64}; u is n x S (S = 16)
-template <int K_, int S_>
-__global__ void __launch_bounds__(TC_THREADS) mstack_tc_kernel(const float* __restrict__ A, const float* __restrict__ u,
-                                                              int n, float* __restrict__ Mpart,
-                                                              uint32_t* __restrict__ err) {
-    constexpr int JT = 128 / K_;  // j values per M tile
-    constexpr uint32_t A_BYTES = 128 * KCH * 2, B_BYTES = K_ * KCH * 2;
-    constexpr uint32_t TM_COLS = K_ < 32 ? 32 : K_;
-    extern __shared__ __align__(1024) uint8_t sm[];  // 2 * (A_BYTES + B_BYTES)
-    __shared__ __align__(8) uint64_t mbar[2];
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// ---------------------------------------------------------------------------
+// Packing (once per MDS call for A, once per product for u)
+
+// Aq: 128-sample tiles of A (K = rank), canonical, rows >= n zero.
+template <int K_>
+__global__ void pack_aq_kernel(const float* __restrict__ A, int n, int ntiles, uint8_t* __restrict__ Aq) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // one (tile row, 8-wide K group)
+    const size_t total = (size_t)ntiles * 128 * (K_ / 8);
+    if (idx >= total) return;
+    const int kg = (int)(idx % (K_ / 8));
+    const size_t row = idx / (K_ / 8);
+    const int tile = (int)(row / 128), r = (int)(row % 128);
+    const size_t i = row;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = i < (size_t)n ? A[i * K_ + kg * 8 + q] : 0.0f;
+    uint4 o;
+    o.x = pack_bf16x2(v[0], v[1]);
+    o.y = pack_bf16x2(v[2], v[3]);
+    o.z = pack_bf16x2(v[4], v[5]);
+    o.w = pack_bf16x2(v[6], v[7]);
+    *reinterpret_cast<uint4*>(Aq + (size_t)tile * (128 * K_ * 2) + canon_off(r, kg * 8, 128)) = o;
+}
+
+// At: 32-sample chunks of A^T (rows = rank index, K = samples), canonical,
+// samples >= n zero.
+template <int K_>
+__global__ void pack_at_kernel(const float* __restrict__ A, int n, int nch, uint8_t* __restrict__ At) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // one (chunk, a, 8-sample group)
+    const size_t total = (size_t)nch * K_ * (CH / 8);
+    if (idx >= total) return;
+    const int g = (int)(idx % (CH / 8));
+    const int a = (int)((idx / (CH / 8)) % K_);
+    const size_t ch = idx / ((size_t)(CH / 8) * K_);
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const size_t i = ch * CH + g * 8 + q;
+        v[q] = i < (size_t)n ? A[i * K_ + a] : 0.0f;
+    }
+    uint4 o;
+    o.x = pack_bf16x2(v[0], v[1]);
+    o.y = pack_bf16x2(v[2], v[3]);
+    o.z = pack_bf16x2(v[4], v[5]);
+    o.w = pack_bf16x2(v[6], v[7]);
+    *reinterpret_cast<uint4*>(At + ch * (size_t)(K_ * CH * 2) + canon_off(a, g * 8, K_)) = o;
+}
+
+// uT: 32-sample chunks of u^T in FP32, [chunk][j][32], samples >= n zero.
+__global__ void pack_ut_kernel(const float* __restrict__ u, int n, int nch, float* __restrict__ uT) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (size_t)nch * CH * S_) return;
+    const size_t i = idx / S_;
+    const int j = (int)(idx % S_);
+    const size_t ch = i / CH;
+    const int w = (int)(i % CH);
+    uT[(ch * S_ + j) * CH + w] = i < (size_t)n ? u[idx] : 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// M stack
+
+template <int K_>
+struct MsCfg {
+    static constexpr int MT = S_ * K_ / 128;               // M tiles
+    static constexpr uint32_t AOP = MT * 128 * CH * 2;     // scaled operand per stage
+    static constexpr uint32_t ATB = K_ * CH * 2;           // A^T chunk
+    static constexpr uint32_t UTB = S_ * CH * 4;           // u^T chunk
+    static constexpr uint32_t STB = AOP + ATB + UTB;
+    static constexpr int ST = K_ == 64 ? 3 : 4;            // stages
+    static constexpr uint32_t SMEM = ST * STB;
+    static constexpr uint32_t TMC = MT * K_ < 32 ? 32 : MT * K_;  // TMEM columns
+};
+
+// 192 threads: warps 0-3 build the scaled operand and run the epilogue, warp 4
+// lane 0 loads, warp 5 lane 0 issues the MMAs.  CTA b owns chunks
+// [b * per, min(nch, (b + 1) * per)) and writes partial b.
+template <int K_>
+__global__ void __launch_bounds__(192, 1) mstack_tc_kernel(const uint8_t* __restrict__ At, const float* __restrict__ uT,
+                                                          int nch, int per, float* __restrict__ Mpart,
+                                                          uint32_t* __restrict__ err) {
+    using C = MsCfg<K_>;
+    extern __shared__ __align__(1024) uint8_t sm[];
+    __shared__ __align__(8) uint64_t full[C::ST], aready[C::ST], empty[C::ST], done;
     __shared__ uint32_t tmem_base;
+    __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int j0 = blockIdx.x * JT;
-    const int chunks = (n + KCH - 1) / KCH;
-    const int per = (chunks + gridDim.y - 1) / gridDim.y;
-    const int c0 = blockIdx.y * per, c1 = min(chunks, c0 + per);
-    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), TM_COLS);
+    const int c0 = blockIdx.x * per, c1 = min(nch, c0 + per);
+    const int cnt = max(0, c1 - c0);
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), C::TMC);
     if (tid == 0) {
-        mbar_init(smem_u32(&mbar[0]), 1);
-        mbar_init(smem_u32(&mbar[1]), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;");
+        for (int s = 0; s < C::ST; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&aready[s]), 128);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        mbar_init(smem_u32(&done), 1);
+        s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-    constexpr uint32_t idesc = idesc_bf16_f32(128, K_);
-    uint32_t phase[2] = {0u, 0u};
+    const uint32_t base = smem_u32(sm);
     bool ok = true;
-    int it = 0;
-    for (int ch = c0; ch < c1; ++ch, ++it) {
-        const int st = it & 1;
-        uint8_t* As = sm + st * (A_BYTES + B_BYTES);
-        uint8_t* Bs = As + A_BYTES;
-        if (it >= 2) {  // the MMAs that read this stage must have finished
-            ok = ok && mbar_wait(smem_u32(&mbar[st]), phase[st]);
-            phase[st] ^= 1u;
-        }
-        // build the tiles: thread -> (sample kk, half of the a range)
-        const int kk = tid & 63, half = tid >> 6;
-        const int i = ch * KCH + kk;
-        const bool valid = i < n;
-        float uj[JT];
-#pragma unroll
-        for (int jj = 0; jj < JT; ++jj) uj[jj] = valid ? u[(size_t)i * S_ + j0 + jj] : 0.0f;
-#pragma unroll 4
-        for (int a = half * (K_ / 2); a < (half + 1) * (K_ / 2); ++a) {
-            const float x = valid ? A[(size_t)i * K_ + a] : 0.0f;
-            *reinterpret_cast<__nv_bfloat16*>(Bs + tile_off(a, kk, K_)) = __float2bfloat16_rn(x);
-#pragma unroll
-            for (int jj = 0; jj < JT; ++jj)
-                *reinterpret_cast<__nv_bfloat16*>(As + tile_off(jj * K_ + a, kk, 128)) =
-                    __float2bfloat16_rn(uj[jj] * x);
-        }
-        asm volatile("fence.proxy.async.shared::cta;");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-#pragma unroll
-            for (int ks = 0; ks < KCH / 16; ++ks) {
-                const uint64_t ad = umma_desc(smem_u32(As) + ks * 128 * 32);
-                const uint64_t bd = umma_desc(smem_u32(Bs) + ks * K_ * 32);
-                mma_bf16(tmem, ad, bd, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+    if (warp == 4) {
+        if (lane == 0) {
+            int it = 0;
+            for (; it < cnt; ++it) {
+                const int s = it % C::ST;
+                if (it >= C::ST && !mbar_wait(smem_u32(&empty[s]), (uint32_t)((it / C::ST - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t st = base + s * C::STB;
+                mbar_expect_tx(smem_u32(&full[s]), C::ATB + C::UTB);
+                bulk_g2s(st + C::AOP, At + (size_t)(c0 + it) * C::ATB, C::ATB, smem_u32(&full[s]));
+                bulk_g2s(st + C::AOP + C::ATB, uT + (size_t)(c0 + it) * S_ * CH, C::UTB, smem_u32(&full[s]));
             }
-            mma_commit(smem_u32(&mbar[st]));
+            // the last copies land before the CTA can leave
+            for (int q = max(0, it - C::ST); q < it; ++q)
+                mbar_wait(smem_u32(&full[q % C::ST]), (uint32_t)((q / C::ST) & 1));
         }
-        __syncwarp();
-    }
-    // drain: each used stage has exactly one commit not yet waited for
-    const int issued = it;
-    for (int st = 0; st < 2; ++st)
-        if (issued > st) {
-            ok = ok && mbar_wait(smem_u32(&mbar[st]), phase[st]);
-            phase[st] ^= 1u;
-        }
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    // this K range's slot of the partial stack
-    float* M = Mpart + (size_t)blockIdx.y * S_ * K_ * K_;
-    const int r = warp * 32 + lane;
-    const int j = j0 + r / K_, a = r % K_;
-    if (!ok) {
-        if (lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
-    } else if (issued > 0) {
-        // warp w reads TMEM lanes 32w..32w+31 = tile rows; K_ columns
+    } else if (warp == 5) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16_f32(128, K_);
+            for (int it = 0; it < cnt && ok; ++it) {
+                const int s = it % C::ST;
+                if (!mbar_wait(smem_u32(&aready[s]), (uint32_t)((it / C::ST) & 1))) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t st = base + s * C::STB;
 #pragma unroll
-        for (int c = 0; c < K_; c += 16) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, v);
-            float4* dst = reinterpret_cast<float4*>(M + ((size_t)j * K_ + a) * K_ + c);
+                for (int m = 0; m < C::MT; ++m)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    for (int ks = 0; ks < CH / 16; ++ks)
+                        mma_bf16(tmem + m * K_, umma_desc(st + m * (128 * CH * 2) + ks * (128 * 32)),
+                                 umma_desc(st + C::AOP + ks * (K_ * 32)), idesc, (it > 0 || ks > 0) ? 1u : 0u);
+                mma_commit(smem_u32(&empty[s]));
+            }
+            mma_commit(smem_u32(&done));  // arrives once every MMA issued above has finished
         }
     } else {
-        for (int c = 0; c < K_; ++c) M[((size_t)j * K_ + a) * K_ + c] = 0.0f;  // an empty K range adds nothing
+        // scaled operand: thread r builds row r of every M tile, (j, a) =
+        // (m * 128 / K_ + r / K_, r % K_), 8 samples per 16-byte store
+        const int r = tid;
+        const int a = r % K_, jr = r / K_;
+        for (int it = 0; it < cnt; ++it) {
+            const int s = it % C::ST;
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((it / C::ST) & 1))) {
+                ok = false;
+                break;
+            }
+            uint8_t* st = sm + s * C::STB;
+            const uint8_t* at = st + C::AOP;
+            const float* ut = reinterpret_cast<const float*>(st + C::AOP + C::ATB);
+#pragma unroll
+            for (int g = 0; g < CH / 8; ++g) {
+                const uint4 av = *reinterpret_cast<const uint4*>(at + canon_off(a, g * 8, K_));
+                const __nv_bfloat162* ab = reinterpret_cast<const __nv_bfloat162*>(&av);
+                float x[8];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float2 f = __bfloat1622float2(ab[q]);
+                    x[2 * q] = f.x;
+                    x[2 * q + 1] = f.y;
+                }
+#pragma unroll
+                for (int m = 0; m < C::MT; ++m) {
+                    const int j = m * (128 / K_) + jr;
+                    const float4 u0 = *reinterpret_cast<const float4*>(ut + j * CH + g * 8);
+                    const float4 u1 = *reinterpret_cast<const float4*>(ut + j * CH + g * 8 + 4);
+                    uint4 o;
+                    o.x = pack_bf16x2(u0.x * x[0], u0.y * x[1]);
+                    o.y = pack_bf16x2(u0.z * x[2], u0.w * x[3]);
+                    o.z = pack_bf16x2(u1.x * x[4], u1.y * x[5]);
+                    o.w = pack_bf16x2(u1.z * x[6], u1.w * x[7]);
+                    *reinterpret_cast<uint4*>(st + m * (128 * CH * 2) + canon_off(r, g * 8, 128)) = o;
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(smem_u32(&aready[s]));
+        }
+        if (!ok) s_fail = 1;
+    }
+    if (!ok) {
+        s_fail = 1;
+        atomicOr(err, ERR_WAIT_LIMIT);
+    }
+    __syncthreads();
+    // epilogue (warps 0-3: TMEM lanes 32w..32w+31), or the drain after a failure
+    if (warp < 4) {
+        const bool fin = mbar_wait(smem_u32(&done), 0u);
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (!fin) {
+            if (lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
+        } else if (!s_fail) {
+            float* M = Mpart + (size_t)blockIdx.x * (S_ * K_ * K_);
+#pragma unroll 1
+            for (int m = 0; m < C::MT; ++m) {
+                const int row = m * 128 + warp * 32 + lane;
+#pragma unroll
+                for (int c = 0; c < K_; c += 16) {
+                    uint32_t v[16];
+                    if (cnt > 0) {
+                        tmem_ld16_nw(tmem + ((uint32_t)(warp * 32) << 16) + m * K_ + c, v);
+                        tmem_wait_ld();
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) v[q] = 0u;  // an empty range adds nothing
+                    }
+                    float4* dst = reinterpret_cast<float4*>(M + (size_t)row * K_ + c);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                             __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+                }
+            }
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem, TM_COLS);
+    if (warp == 0) tmem_dealloc(tmem, C::TMC);
 }
 
-// M = sum over the K ranges of their partial stacks, in K-range order
-__global__ void mstack_reduce_kernel(const float* __restrict__ Mpart, int parts, size_t count, float* __restrict__ M) {
-    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+// M = sum of the partials in CTA order (FP32, rows (j, a), columns b), and Mq
+// = the same values as the quadratic-form operand: rows (j, b) in passes of
+// 256, K = a, canonical BF16 (M_j is symmetric, so row (j, b) column a is
+// D[(j, b), a]).
+template <int K_>
+__global__ void mstack_reduce_kernel(const float* __restrict__ Mpart, int parts, float* __restrict__ M,
+                                     uint8_t* __restrict__ Mq) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int count = S_ * K_ * K_;
     if (e >= count) return;
     float acc = 0.0f;
     for (int p = 0; p < parts; ++p) acc += Mpart[(size_t)p * count + e];
     M[e] = acc;
+    const int row = e / K_, col = e % K_;
+    const int pass = row / NP, rl = row % NP;
+    *reinterpret_cast<__nv_bfloat16*>(Mq + (size_t)pass * (NP * K_ * 2) + canon_off(rl, col, NP)) =
+        __float2bfloat16_rn(acc);
 }
 
-// grid: n/128 sample tiles; the s*k rows of the M stack in passes of NP rows
-template <int K_, int S_>
-__global__ void __launch_bounds__(TC_THREADS) quadform_tc_kernel(const float* __restrict__ A,
-                                                                const float* __restrict__ M, int n,
-                                                                float* __restrict__ T2, uint32_t* __restrict__ err) {
-    constexpr int NP = 256;                 // N per pass
-    constexpr int JP = NP / K_;             // j per pass
-    constexpr int PASSES = (S_ * K_) / NP;  // >= 1
-    constexpr uint32_t A_BYTES = 128 * K_ * 2, B_BYTES = NP * K_ * 2;
-    extern __shared__ __align__(1024) uint8_t sm[];  // A_BYTES + B_BYTES
-    __shared__ __align__(8) uint64_t mbar;
+// ---------------------------------------------------------------------------
+// Quadratic forms
+
+template <int K_>
+struct QfCfg {
+    static constexpr int PASSES = S_ * K_ / NP;  // 4 or 2
+    static constexpr int JP = NP / K_;           // j per pass
+    static constexpr uint32_t MQB = S_ * K_ * K_ * 2;
+    static constexpr uint32_t AQB = 128 * K_ * 2;
+    static constexpr int ST = 2;
+    static constexpr uint32_t SMEM = MQB + ST * AQB;
+};
+
+// 192 threads: warps 0-3 epilogue (tile rows 32w..32w+31), warp 4 lane 0
+// loads, warp 5 lane 0 issues the MMAs.  CTA b takes tiles b, b + grid, ...
+template <int K_>
+__global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __restrict__ Aq,
+                                                            const uint8_t* __restrict__ Mq,
+                                                            const float* __restrict__ A, int n, int ntiles,
+                                                            float* __restrict__ T2, uint32_t* __restrict__ err) {
+    using C = QfCfg<K_>;
+    extern __shared__ __align__(1024) uint8_t sm[];
+    __shared__ __align__(8) uint64_t mq_full, afull[C::ST], aempty[C::ST], tfull[2], tempty[2], done;
     __shared__ uint32_t tmem_base;
-    static_assert(K_ % 16 == 0 && (S_ * K_) % NP == 0, "tile shape");
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int i0 = blockIdx.x * 128;
-    uint8_t* As = sm;
-    uint8_t* Bs = sm + A_BYTES;
-    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), NP);
+    const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    if (warp == 0) tmem_alloc(smem_u32(&tmem_base), 2 * NP);
     if (tid == 0) {
-        mbar_init(smem_u32(&mbar), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;");
+        mbar_init(smem_u32(&mq_full), 1);
+        for (int s = 0; s < C::ST; ++s) {
+            mbar_init(smem_u32(&afull[s]), 1);
+            mbar_init(smem_u32(&aempty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&tfull[b]), 1);
+            mbar_init(smem_u32(&tempty[b]), 4);
+        }
+        mbar_init(smem_u32(&done), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // A tile: 128 samples x K_ (the a index is the reduction)
-    const int i = i0 + tid;
-    float arow[K_];
-#pragma unroll
-    for (int a = 0; a < K_; ++a) arow[a] = i < n ? A[(size_t)i * K_ + a] : 0.0f;
-    // tile_off assumes 64-wide K; with K_ < 64 only the first K_/16 steps exist
-#pragma unroll
-    for (int a = 0; a < K_; ++a)
-        *reinterpret_cast<__nv_bfloat16*>(As + tile_off(tid, a, 128)) = __float2bfloat16_rn(arow[a]);
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-    constexpr uint32_t idesc = idesc_bf16_f32(128, NP);
-    uint32_t phase = 0;
+    const uint32_t base = smem_u32(sm);
+    const uint32_t abase = base + C::MQB;
     bool ok = true;
-    for (int ps = 0; ps < PASSES; ++ps) {
-        // B tile: rows (j, b) of this pass, K = a: M[j][b][a]
-        for (int e = tid; e < NP * K_; e += TC_THREADS) {
-            const int row = e / K_, a = e % K_;
-            const int j = ps * JP + row / K_, b = row % K_;
-            *reinterpret_cast<__nv_bfloat16*>(Bs + tile_off(row, a, NP)) =
-                __float2bfloat16_rn(M[((size_t)j * K_ + b) * K_ + a]);
-        }
-        asm volatile("fence.proxy.async.shared::cta;");
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-#pragma unroll
-            for (int ks = 0; ks < K_ / 16; ++ks)
-                mma_bf16(tmem, umma_desc(smem_u32(As) + ks * 128 * 32), umma_desc(smem_u32(Bs) + ks * NP * 32), idesc,
-                         ks > 0 ? 1u : 0u);
-            mma_commit(smem_u32(&mbar));
-        }
-        __syncwarp();
-        ok = ok && mbar_wait(smem_u32(&mbar), phase);
-        phase ^= 1u;
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        if (ok) {
-            float t[JP];
-#pragma unroll
-            for (int jj = 0; jj < JP; ++jj) t[jj] = 0.0f;
-#pragma unroll
-            for (int c = 0; c < NP; c += 16) {
-                float v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c, v);
-                const int jj = c / K_, b0 = c % K_;
-#pragma unroll
-                for (int q = 0; q < 16; ++q) t[jj] = fmaf(v[q], arow[b0 + q], t[jj]);
+    if (warp == 4) {
+        if (lane == 0 && my_tiles > 0) {
+            mbar_expect_tx(smem_u32(&mq_full), C::MQB);
+            bulk_g2s(base, Mq, C::MQB, smem_u32(&mq_full));
+            int it = 0;
+            for (; it < my_tiles; ++it) {
+                const int s = it % C::ST;
+                if (it >= C::ST && !mbar_wait(smem_u32(&aempty[s]), (uint32_t)((it / C::ST - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                const int q = blockIdx.x + it * gridDim.x;
+                mbar_expect_tx(smem_u32(&afull[s]), C::AQB);
+                bulk_g2s(abase + s * C::AQB, Aq + (size_t)q * C::AQB, C::AQB, smem_u32(&afull[s]));
             }
-            if (i < n)
-#pragma unroll
-                for (int jj = 0; jj < JP; ++jj) T2[(size_t)i * S_ + ps * JP + jj] = t[jj];
+            mbar_wait(smem_u32(&mq_full), 0u);
+            for (int q = max(0, it - C::ST); q < it; ++q)
+                mbar_wait(smem_u32(&afull[q % C::ST]), (uint32_t)((q / C::ST) & 1));
         }
-        // all TMEM reads and B-tile reads of this pass are done before the next
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
+    } else if (warp == 5) {
+        if (lane == 0 && my_tiles > 0) {
+            constexpr uint32_t idesc = idesc_bf16_f32(128, NP);
+            ok = mbar_wait(smem_u32(&mq_full), 0u);
+            int pc = 0;  // passes issued
+            for (int it = 0; it < my_tiles && ok; ++it) {
+                const int s = it % C::ST;
+                if (!mbar_wait(smem_u32(&afull[s]), (uint32_t)((it / C::ST) & 1))) {
+                    ok = false;
+                    break;
+                }
+                for (int p = 0; p < C::PASSES && ok; ++p, ++pc) {
+                    const int b = pc & 1;
+                    if (pc >= 2 && !mbar_wait(smem_u32(&tempty[b]), (uint32_t)((pc / 2 - 1) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+                    for (int ks = 0; ks < K_ / 16; ++ks)
+                        mma_bf16(tmem + b * NP, umma_desc(abase + s * C::AQB + ks * (128 * 32)),
+                                 umma_desc(base + p * (NP * K_ * 2) + ks * (NP * 32)), idesc, ks > 0 ? 1u : 0u);
+                    mma_commit(smem_u32(&tfull[b]));
+                }
+                if (ok) mma_commit(smem_u32(&aempty[s]));  // the A tile is free once these MMAs finish
+            }
+        }
+        if (lane == 0) mma_commit(smem_u32(&done));  // arrives once every MMA issued above has finished
+    } else {
+        int pc = 0;
+        for (int it = 0; it < my_tiles && ok; ++it) {
+            const int q = blockIdx.x + it * gridDim.x;
+            const int i = q * 128 + warp * 32 + lane;
+            float arow[K_];
+            const float4* ar = reinterpret_cast<const float4*>(A + (size_t)i * K_);
+#pragma unroll
+            for (int c = 0; c < K_ / 4; ++c) {
+                const float4 v = i < n ? __ldg(ar + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+                arow[4 * c] = v.x;
+                arow[4 * c + 1] = v.y;
+                arow[4 * c + 2] = v.z;
+                arow[4 * c + 3] = v.w;
+            }
+#pragma unroll 1
+            for (int p = 0; p < C::PASSES; ++p, ++pc) {
+                const int b = pc & 1;
+                if (!mbar_wait(smem_u32(&tfull[b]), (uint32_t)((pc / 2) & 1))) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll 1
+                for (int jj = 0; jj < C::JP; ++jj) {
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int c = 0; c < K_; c += 32) {
+                        uint32_t v0[16], v1[16];
+                        const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + b * NP + jj * K_ + c;
+                        tmem_ld16_nw(ta, v0);
+                        tmem_ld16_nw(ta + 16, v1);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) acc = fmaf(__uint_as_float(v0[e]), arow[c + e], acc);
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) acc = fmaf(__uint_as_float(v1[e]), arow[c + 16 + e], acc);
+                    }
+                    if (i < n) T2[(size_t)i * S_ + p * C::JP + jj] = acc;
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&tempty[b]));
+            }
+        }
     }
-    if (!ok && lane == 0) atomicOr(err, ERR_WAIT_LIMIT);
-    if (warp == 0) tmem_dealloc(tmem, NP);
+    if (!ok && (lane == 0)) atomicOr(err, ERR_WAIT_LIMIT);
+    __syncthreads();
+    // every MMA has finished before TMEM is freed (bounded wait)
+    if (warp == 5 && lane == 0) mbar_wait(smem_u32(&done), 0u);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 2 * NP);
 }
 
 }  // namespace
 
-// M (S x k x k, zeroed here) and T2 (n x S) for the factor A (n x k) and the
-// centred block u (n x S), on the tensor cores.
-rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const float* u32, float* M, float* T2) {
+// Packed forms of the factor A for one MDS call (pack_factor_tc) and the
+// products with them.
+rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* At) {
+    const int n = c->n;
+    const int ntiles = (n + 127) / 128, nch = (n + CH - 1) / CH;
+    cudaStream_t s = c->stream;
+    const size_t tq = (size_t)ntiles * 128 * (k / 8), ta = (size_t)nch * k * (CH / 8);
+    if (k == 64) {
+        pack_aq_kernel<64><<<(unsigned)((tq + 255) / 256), 256, 0, s>>>(dA, n, ntiles, Aq);
+        pack_at_kernel<64><<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(dA, n, nch, At);
+    } else if (k == 32) {
+        pack_aq_kernel<32><<<(unsigned)((tq + 255) / 256), 256, 0, s>>>(dA, n, ntiles, Aq);
+        pack_at_kernel<32><<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(dA, n, nch, At);
+    } else {
+        set_error("tensor-core factor MDS supports rank 32 or 64");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    c->launches += 2;
+    RFX_CUDA(cudaGetLastError());
+    return RFX_OK;
+}
+
+size_t factor_tc_aq_bytes(int n, int k) { return (size_t)((n + 127) / 128) * 128 * k * 2; }
+size_t factor_tc_at_bytes(int n, int k) { return (size_t)((n + CH - 1) / CH) * CH * k * 2; }
+
+// M (S x k x k) and T2 (n x S) for the factor A (n x k, with its packed forms
+// Aq / At from pack_factor_tc) and the centred block u (n x S), on the tensor
+// cores.
+rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const uint8_t* Aq, const uint8_t* At,
+                                const float* u32, float* M, float* T2) {
     cudaStream_t s = c->stream;
     const int n = c->n;
-    constexpr int S = 16;
-    const int ksplit = 37;  // 296 CTAs for rank 64: two per SM
+    const int ntiles = (n + 127) / 128, nch = (n + CH - 1) / CH;
+    int sms = 148;
+    RFX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    const int per = (nch + sms - 1) / sms;
+    const int parts = (nch + per - 1) / per;
+    const int qgrid = std::min(ntiles, sms);
     Scratch sc(c);
-    const size_t count = (size_t)S * k * k;
-    float* Mpart = sc.get<float>(count * ksplit);
-    if (!Mpart) {
+    const size_t count = (size_t)S_ * k * k;
+    float* Mpart = sc.get<float>(count * parts);
+    float* uT = sc.get<float>((size_t)nch * CH * S_);
+    uint8_t* Mq = sc.get<uint8_t>(count * 2);
+    if (!Mpart || !uT || !Mq) {
         set_error("tensor-core factor MDS: scratch allocation failed");
         return RFX_ERR_OOM;
     }
-    auto run = [&](auto mk, auto qk, int K) -> rfx_status {
-        const int sm_m = 2 * (128 * KCH * 2 + K * KCH * 2);
-        const int sm_q = 128 * K * 2 + 256 * K * 2;
-        RFX_CUDA(cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_m));
-        RFX_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, sm_q));
-        mk<<<dim3(S * K / 128, ksplit), TC_THREADS, sm_m, s>>>(dA, u32, n, Mpart, c->d_err);
-        mstack_reduce_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(Mpart, ksplit, count, M);
-        qk<<<(n + 127) / 128, TC_THREADS, sm_q, s>>>(dA, M, n, T2, c->d_err);
+    pack_ut_kernel<<<(unsigned)(((size_t)nch * CH * S_ + 255) / 256), 256, 0, s>>>(u32, n, nch, uT);
+    auto run = [&](auto mk, auto rk, auto qk, uint32_t sm_m, uint32_t sm_q) -> rfx_status {
+        RFX_CUDA(cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_m));
+        RFX_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_q));
+        mk<<<parts, 192, sm_m, s>>>(At, uT, nch, per, Mpart, c->d_err);
+        rk<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(Mpart, parts, M, Mq);
+        qk<<<qgrid, 192, sm_q, s>>>(Aq, Mq, dA, n, ntiles, T2, c->d_err);
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
-    rfx_status st = RFX_OK;
-    switch (k) {
-        case 64:
-            st = run(mstack_tc_kernel<64, S>, quadform_tc_kernel<64, S>, 64);
-            break;
-        case 32:
-            st = run(mstack_tc_kernel<32, S>, quadform_tc_kernel<32, S>, 32);
-            break;
-        default:
-            set_error("tensor-core factor MDS supports rank 32 or 64");
-            return RFX_ERR_UNSUPPORTED;
+    rfx_status st;
+    if (k == 64)
+        st = run(mstack_tc_kernel<64>, mstack_reduce_kernel<64>, quadform_tc_kernel<64>, MsCfg<64>::SMEM,
+                 QfCfg<64>::SMEM);
+    else if (k == 32)
+        st = run(mstack_tc_kernel<32>, mstack_reduce_kernel<32>, quadform_tc_kernel<32>, MsCfg<32>::SMEM,
+                 QfCfg<32>::SMEM);
+    else {
+        set_error("tensor-core factor MDS supports rank 32 or 64");
+        return RFX_ERR_UNSUPPORTED;
     }
     if (st != RFX_OK) return st;
-    c->launches += 3;
+    c->launches += 4;
     return RFX_OK;
 }
 
