@@ -265,14 +265,8 @@ route_leaf_staged_kernel(const float* __restrict__ X, int n, int p, int nclass, 
     const int q = blockIdx.x * RT + threadIdx.x;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int i = q < n ? __ldg(memb + (size_t)t * n + q) : -1;
-    // each warp stages its 32 rows, one row at a time across the lanes
-    for (int r = 0; r < 32; ++r) {
-        const int ir = __shfl_sync(0xffffffffu, i, r);
-        if (ir < 0) continue;
-        float* dst = xs + (size_t)(w * 32 + r) * ps;
-        const float* src = X + (size_t)ir * p;
-        for (int m = lane; m < p; m += 32) dst[m] = __ldg(src + m);
-    }
+    // each warp stages its 32 rows
+    stage_warp_rows(xs + (size_t)(w * 32) * ps, ps, X, p, i, lane);
     __syncwarp();
     if (q >= n) return;
     const SharedRow xrow{xs + (size_t)threadIdx.x * ps};

@@ -194,17 +194,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     float* xs_par = xs_own + (size_t)VW * ps;
     if (SX) {
         const int w = tid >> 5;
-        for (int r = 0; r < 32; ++r) {
-            const int ir = __shfl_sync(0xffffffffu, active ? i : -1, r);
-            const int pr = __shfl_sync(0xffffffffu, ip, r);
-            if (ir < 0) continue;
-            float* d0 = xs_own + (size_t)(w * 32 + r) * ps;
-            float* d1 = xs_par + (size_t)(w * 32 + r) * ps;
-            for (int m = lane; m < p; m += 32) {
-                d0[m] = __ldg(X + (size_t)ir * p + m);
-                d1[m] = __ldg(X + (size_t)pr * p + m);
-            }
-        }
+        stage_warp_rows(xs_own + (size_t)(w * 32) * ps, ps, X, p, active ? i : -1, lane);
+        stage_warp_rows(xs_par + (size_t)(w * 32) * ps, ps, X, p, active ? ip : -1, lane);
     }
     if (tid == 0) {
         s_red[0] = 0;
@@ -514,9 +505,14 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         // after the counters (offset rounded to 16 bytes)
         const size_t cnt_bytes = sizeof(int32_t) * (((size_t)c->p + 3) & ~(size_t)3);
         auto staged_smem = [&](int vw) { return cnt_bytes + 2 * sizeof(float) * (size_t)vw * (size_t)(c->p | 1); };
+        // the staged kernels may take up to the device maximum (set once, so a
+        // captured launch of another forest's size stays valid)
+        int dev_smem = 0;
+        RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+        if (rfx_status s0 = allow_dyn_smem(varimp_walk_kernel<W, 64, false, true>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(varimp_walk_kernel<W, 128, false, true>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(varimp_walk_kernel<W, 256, false, true>, dev_smem)) return s0;
         auto go = [&](auto kernel, int vw, size_t sm) -> rfx_status {
-            if (sm > 48 * 1024)
-                RFX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             dim3 grid(((ordered ? c->n : max_noob) + vw - 1) / vw, c->T);
             kernel<<<grid, vw, sm, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
                                                  c->d_nnode, c->d_noob, c->d_cat, c->d_catgoleft, c->maxcat,

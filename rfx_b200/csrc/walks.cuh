@@ -44,6 +44,36 @@ struct SharedRow {
     __device__ __forceinline__ float operator()(int m) const { return r[m]; }
 };
 
+// Stage the feature rows of the 32 samples of a warp (lane l's sample id in
+// `id`, -1 for none) into dst + r * ps (row r = lane r's sample), 16 rows per
+// batch with every load of a batch in flight at once.  All 32 lanes call it.
+__device__ __forceinline__ void stage_warp_rows(float* dst, int ps, const float* __restrict__ X, int p, int id,
+                                                int lane) {
+    for (int mb = 0; mb < p; mb += 64) {
+        const int m0 = mb + lane, m1 = mb + 32 + lane;
+#pragma unroll
+        for (int r0 = 0; r0 < 32; r0 += 16) {
+            int ids[16];
+            float v0[16], v1[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) ids[q] = __shfl_sync(0xffffffffu, id, r0 + q);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const float* src = X + (size_t)(ids[q] < 0 ? 0 : ids[q]) * p;
+                v0[q] = (ids[q] >= 0 && m0 < p) ? __ldg(src + m0) : 0.0f;
+                v1[q] = (ids[q] >= 0 && m1 < p) ? __ldg(src + m1) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                if (ids[q] < 0) continue;
+                float* d = dst + (size_t)(r0 + q) * ps;
+                if (m0 < p) d[m0] = v0[q];
+                if (m1 < p) d[m1] = v1[q];
+            }
+        }
+    }
+}
+
 // Returns the node id; *cls receives the class (nodeclass of the final node,
 // or of the root on the fallback path).
 template <typename Src, typename XR>
