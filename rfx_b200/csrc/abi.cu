@@ -115,7 +115,7 @@ void free_forest(Ctx* c) {
     dfree(c, c->d_leafidx); dfree(c, c->d_catgoleft); dfree(c, c->d_offs); dfree(c, c->d_nnode);
     dfree(c, c->d_inbag); dfree(c, c->d_segbase); dfree(c, c->d_iv); dfree(c, c->d_noob); dfree(c, c->d_permoff);
     dfree(c, c->d_invnoob); dfree(c, c->d_key); dfree(c, c->d_segoff); dfree(c, c->d_memb);
-    dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_partner); dfree(c, c->d_vflags); dfree(c, c->d_flips);
+    dfree(c, c->d_votes); dfree(c, c->d_nout); dfree(c, c->d_joob); dfree(c, c->d_partner); dfree(c, c->d_oobord); dfree(c, c->d_vflags); dfree(c, c->d_flips);
     dfree(c, c->d_right); dfree(c, c->d_rightimp); dfree(c, c->d_qimp); dfree(c, c->d_qimpm); dfree(c, c->d_avimp);
     dfree(c, c->d_sqsd); dfree(c, c->d_opp); dfree(c, c->d_order);
     dfree(c, c->d_hubflag); dfree(c, c->d_hubtiles); dfree(c, c->d_hubstate);
@@ -978,6 +978,7 @@ rfx_status rfx_varimp(rfx_ctx* ctx, int impn, float* avimp, float* sqsd, float* 
     if (st == RFX_OK) st = dalloc(c, &c->ptr, (size_t)(cnt));
     ALLOC(d_joob, (size_t)T * n);
     ALLOC(d_partner, (size_t)T * n);
+    ALLOC(d_oobord, (size_t)T * n);
     ALLOC(d_vflags, (size_t)T * n);
     ALLOC(d_flips, (size_t)T * n * W);
     ALLOC(d_right, 2 * (size_t)T);

@@ -58,6 +58,7 @@ rfx_status varimp_buffers(Ctx* c) {
     rfx_status st = RFX_OK;
     if (st == RFX_OK) st = dalloc(c, &c->d_joob, (size_t)T * n);
     if (st == RFX_OK) st = dalloc(c, &c->d_partner, (size_t)T * n);
+    if (st == RFX_OK) st = dalloc(c, &c->d_oobord, (size_t)T * n);
     if (st == RFX_OK) st = dalloc(c, &c->d_vflags, (size_t)T * n);
     if (st == RFX_OK) st = dalloc(c, &c->d_flips, (size_t)T * n * W);
     if (st == RFX_OK) st = dalloc(c, &c->d_right, 2 * (size_t)T);

@@ -698,26 +698,26 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         nv = (len - head) >> 2;
     }
     for (int h = tid; h < head; h += NT) srow[h] = (int32_t)a16[i + h];
+    // four counters per 16-byte store: counter j is half (j & 1) of word
+    // j >> 1; each is zero-extended by one byte permute (the parity of the
+    // first counter is the same for the whole row)
     int4* s4 = reinterpret_cast<int4*>(srow + head);
     const int jg = i + head;
-    const int sh = (jg & 3) * 16;
-    const int gb = jg >> 2;
-    const int ngroups = words >> 1;
-    const uint2* a64 = reinterpret_cast<const uint2*>(acc);
-    for (int v0 = w * 32; v0 < nv; v0 += NT) {
-        const int v = v0 + lane;
-        const int g = gb + v;
-        const uint2 cg = g < ngroups ? a64[g] : make_uint2(0u, 0u);
-        uint2 nx;
-        nx.x = __shfl_down_sync(0xffffffffu, cg.x, 1);
-        nx.y = __shfl_down_sync(0xffffffffu, cg.y, 1);
-        if (lane == 31) nx = g + 1 < ngroups ? a64[g + 1] : make_uint2(0u, 0u);
-        const unsigned long long lo = ((unsigned long long)cg.y << 32) | cg.x;
-        const unsigned long long hi = ((unsigned long long)nx.y << 32) | nx.x;
-        const unsigned long long e = sh ? (lo >> sh) | (hi << (64 - sh)) : lo;
-        if (v < nv)
-            s4[v] = make_int4((int)(e & 0xffffu), (int)((e >> 16) & 0xffffu), (int)((e >> 32) & 0xffffu),
-                              (int)(e >> 48));
+    const int wb = jg >> 1;
+    if (jg & 1) {
+        for (int v = tid; v < nv; v += NT) {
+            const int wd = wb + 2 * v;
+            const uint32_t x0 = acc[wd], x1 = acc[wd + 1], x2 = acc[wd + 2];
+            s4[v] = make_int4((int)__byte_perm(x0, 0u, 0x4432u), (int)__byte_perm(x1, 0u, 0x4410u),
+                              (int)__byte_perm(x1, 0u, 0x4432u), (int)__byte_perm(x2, 0u, 0x4410u));
+        }
+    } else {
+        for (int v = tid; v < nv; v += NT) {
+            const int wd = wb + 2 * v;
+            const uint32_t x0 = acc[wd], x1 = acc[wd + 1];
+            s4[v] = make_int4((int)__byte_perm(x0, 0u, 0x4410u), (int)__byte_perm(x0, 0u, 0x4432u),
+                              (int)__byte_perm(x1, 0u, 0x4410u), (int)__byte_perm(x1, 0u, 0x4432u));
+        }
     }
     for (int j = i + head + 4 * nv + tid; j < n; j += NT) srow[j - i] = (int32_t)a16[j];
     if (pairs) {

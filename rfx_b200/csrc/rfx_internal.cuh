@@ -107,6 +107,7 @@ struct Ctx {
     // varimp scratch
     int32_t* d_joob = nullptr;          // T*n
     int32_t* d_partner = nullptr;       // T*n: permutation partner of each OOB sample
+    int32_t* d_oobord = nullptr;        // T*n: each tree's OOB samples in member-list (leaf) order
     uint8_t* d_vflags = nullptr;        // T*n: bit1 testreebag correct, bit2 testreeimp correct
     uint64_t* d_flips = nullptr;        // T*n*varimp_flip_words(iv_words)
     int32_t* d_right = nullptr;         // 2T: per tree #correct (testreebag), #correct (testreeimp)

@@ -15,9 +15,13 @@
 //   features, from which
 //   rightimp[t][k] = #testreeimp-correct + sum of signed flips (exact integers).
 //
-// joob_kernel        - one CTA per tree: OOB list (joob, ascending).
-// varimp_walk_kernel - one thread per (tree, OOB sample) over the whole grid:
-//                       walks, flip masks, per-tree integer counts.
+// joob_kernel        - one CTA per tree: OOB list (joob, ascending), the
+//                       permutation partners and, once member lists exist,
+//                       the OOB samples in leaf order (oobord).
+// varimp_walk_kernel - one thread per (tree, OOB sample) over the whole grid
+//                       (in leaf order when oobord exists, so a warp's main
+//                       paths coincide): walks, flip masks, per-tree integer
+//                       counts.
 // varimp_sample_kernel- one thread per sample: qimp / qimpm float sums in tree
 //                       order, 1/noob per correct OOB tree (the reference adds
 //                       each tree's temporaries in tree order,
@@ -78,7 +82,8 @@ __device__ __forceinline__ int imp_side_walk(const XR& xrow, const XR& xperm, in
 __global__ void __launch_bounds__(VT)
 joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all,
             const int32_t* __restrict__ permoff, const int32_t* __restrict__ perm_all,
-            int32_t* __restrict__ partner_all) {
+            int32_t* __restrict__ partner_all, const int32_t* __restrict__ memb = nullptr,
+            int32_t* __restrict__ oobord = nullptr) {
     __shared__ int wsum[VT / 32];
     __shared__ int s_base;
     const int t = blockIdx.x;
@@ -125,6 +130,44 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
     const int32_t* perm = perm_all + permoff[t];
     int32_t* partner = partner_all + (size_t)t * n;
     for (int r = tid; r < noob; r += VT) partner[joob[r]] = joob[__ldg(perm + r)];
+    if (!memb) return;
+    // the OOB samples in member-list order (by leaf): the walk's thread order
+    const int32_t* mt = memb + (size_t)t * n;
+    int32_t* ord = oobord + (size_t)t * n;
+    __syncthreads();
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += JB * VT) {
+        const int q0 = base + JB * tid;
+        int mv[JB];
+        unsigned fl = 0;
+#pragma unroll
+        for (int u = 0; u < JB; ++u) {
+            mv[u] = q0 + u < n ? __ldg(mt + q0 + u) : 0;
+            if (q0 + u < n && ib[mv[u]] == 0) fl |= 1u << u;
+        }
+        const int cnt = __popc(fl);
+        int incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        int woff = 0, tot = 0;
+        for (int q = 0; q < VT / 32; ++q) {
+            if (q < wid) woff += wsum[q];
+            tot += wsum[q];
+        }
+        int pos = s_base + woff + incl - cnt;
+#pragma unroll
+        for (int u = 0; u < JB; ++u)
+            if ((fl >> u) & 1u) ord[pos++] = mv[u];
+        __syncthreads();
+        if (tid == 0) s_base += tot;
+        __syncthreads();
+    }
 }
 
 // One thread per (tree, OOB position r): grid = (ceil(max noob / VW), T),
@@ -141,7 +184,7 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                    const int32_t* __restrict__ noob_arr, const int32_t* __restrict__ cat,
                    const int32_t* __restrict__ catgoleft, int maxcat, const int32_t* __restrict__ permoff,
                    const int32_t* __restrict__ perm_all, const int32_t* __restrict__ joob_all,
-                   const int32_t* __restrict__ memb, const int32_t* __restrict__ partner_all,
+                   const int32_t* __restrict__ oobord, const int32_t* __restrict__ partner_all,
                    const uint8_t* __restrict__ inbag, uint8_t* __restrict__ vflags, uint64_t* __restrict__ flips,
                    int32_t* __restrict__ counts, int32_t* __restrict__ delta_out, uint32_t* __restrict__ err,
                    int fb) {
@@ -160,21 +203,19 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     const int noob = noob_arr[t];
     const int r0 = blockIdx.x * VW;
     const int tid = threadIdx.x, lane = tid & 31;
-    // This thread's OOB sample i and its permutation partner ip.  With member
-    // lists (memb != null) the threads run over all samples of the tree in
-    // leaf order, so neighbouring threads share their main path; in-bag ones
-    // idle and CTAs without an OOB sample leave at once.  Otherwise thread r
-    // takes joob position r.
+    // This thread's OOB sample i and its permutation partner ip.  With the
+    // OOB samples in leaf order (oobord != null: the member lists' order, in
+    // the bag dropped) neighbouring threads share their main path.  Otherwise
+    // thread r takes joob position r.
     int i = 0, ip = 0;
     bool active;
-    if (memb) {
-        active = false;
-        if (r0 + tid < n) {
-            i = __ldg(memb + (size_t)t * n + r0 + tid);
-            active = __ldg(inbag + (size_t)t * n + i) == 0;
-            if (active) ip = __ldg(partner_all + (size_t)t * n + i);
+    if (oobord) {
+        if (r0 >= noob) return;
+        active = r0 + tid < noob;
+        if (active) {
+            i = __ldg(oobord + (size_t)t * n + r0 + tid);
+            ip = __ldg(partner_all + (size_t)t * n + i);
         }
-        if (!__syncthreads_or(active)) return;
     } else {
         if (r0 >= noob) return;
         active = r0 + tid < noob;
@@ -497,7 +538,8 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         StageTimer st(c, ST_VARIMP_TREE, 2);
         const bool ordered = c->csr_built && c->d_partner;
         joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, c->d_permoff, c->d_perm,
-                                                ordered ? c->d_partner : nullptr);
+                                                ordered ? c->d_partner : nullptr, ordered ? c->d_memb : nullptr,
+                                                c->d_oobord);
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
@@ -513,11 +555,11 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         if (rfx_status s0 = allow_dyn_smem(varimp_walk_kernel<W, 128, false, true>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(varimp_walk_kernel<W, 256, false, true>, dev_smem)) return s0;
         auto go = [&](auto kernel, int vw, size_t sm) -> rfx_status {
-            dim3 grid(((ordered ? c->n : max_noob) + vw - 1) / vw, c->T);
+            dim3 grid((max_noob + vw - 1) / vw, c->T);
             kernel<<<grid, vw, sm, c->stream>>>(c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs,
                                                  c->d_nnode, c->d_noob, c->d_cat, c->d_catgoleft, c->maxcat,
                                                  c->d_permoff, c->d_perm, c->d_joob,
-                                                 ordered ? c->d_memb : nullptr, c->d_partner, c->d_inbag,
+                                                 ordered ? c->d_oobord : nullptr, c->d_partner, c->d_inbag,
                                                  c->d_vflags, c->d_flips,
                                                  c->d_right, c->d_rightimp, c->d_err, 0);
             return RFX_OK;
@@ -573,19 +615,20 @@ rfx_status launch_varimp_blocked(Ctx* c, int impn) {
         StageTimer st(c, ST_VARIMP_TREE, 1 + (impn ? 2 : 1) * ((c->p + FW - 1) / FW));
         const bool ordered = c->csr_built && c->d_partner;
         joob_kernel<<<c->T, VT, 0, c->stream>>>(c->d_inbag, c->n, c->d_joob, c->d_permoff, c->d_perm,
-                                                ordered ? c->d_partner : nullptr);
+                                                ordered ? c->d_partner : nullptr, ordered ? c->d_memb : nullptr,
+                                                c->d_oobord);
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
         RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
         RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
-        const dim3 grid(((ordered ? c->n : max_noob) + VW - 1) / VW, c->T);
+        const dim3 grid((max_noob + VW - 1) / VW, c->T);
         for (int fb = 0; fb < c->p; fb += FW) {
             const int pw = std::min(FW, c->p - fb);
             const long long threads = (long long)c->n * ((pw + VS_FEAT - 1) / VS_FEAT);
             varimp_walk_kernel<W, VW, true><<<grid, VW, sizeof(int32_t) * pw, c->stream>>>(
                 c->d_X, c->d_y, c->n, c->p, c->d_nodes, c->d_nodeclass, c->d_offs, c->d_nnode, c->d_noob, c->d_cat,
-                c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, ordered ? c->d_memb : nullptr,
+                c->d_catgoleft, c->maxcat, c->d_permoff, c->d_perm, c->d_joob, ordered ? c->d_oobord : nullptr,
                 c->d_partner, c->d_inbag, c->d_vflags, c->d_flips, c->d_right, c->d_rightimp, c->d_err, fb);
             RFX_CUDA(cudaGetLastError());
             if (impn) {
