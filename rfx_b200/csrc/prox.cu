@@ -557,6 +557,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ long long lbase[V2_LIST];
     __shared__ int llen[V2_LIST];
     __shared__ int s_nlong, s_chunk;
+    __shared__ uint8_t s_lid[NW][32];  // per warp: lanes with a non-empty short range
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (hubt && hub_state[1] > 0) {
@@ -571,10 +572,11 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
             const uint4 v = __ldg(reinterpret_cast<const uint4*>(rowt + (size_t)J * 32768u + slot * 16));
             const uint32_t b[4] = {v.x, v.y, v.z, v.w};
             uint32_t o[8];
+            // bytes (b0 b1 b2 b3) -> u16 pairs (b0, b1) and (b2, b3): one byte permute each
 #pragma unroll
             for (int h = 0; h < 4; ++h) {
-                o[2 * h] = (b[h] & 0xffu) | ((b[h] & 0xff00u) << 8);
-                o[2 * h + 1] = ((b[h] >> 16) & 0xffu) | ((b[h] >> 8) & 0xff0000u);
+                o[2 * h] = __byte_perm(b[h], 0u, 0x4140u);
+                o[2 * h + 1] = __byte_perm(b[h], 0u, 0x4342u);
             }
             uint4* dst = reinterpret_cast<uint4*>(acc + (size_t)J * 128 + q * 8);
             dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
@@ -633,7 +635,12 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
             for (; off < ml; off += 32) count16(acc, __ldg(mp + off));
         }
         if (len >= 32) len = 0;
-        // the short ranges, element by element over the warp
+        // the short ranges, element by element over the warp: element e of
+        // the concatenated ranges belongs to the last non-empty range that
+        // starts at or before e; the warp lists its non-empty ranges (lane
+        // ids, in lane order) and, per window of 64 elements, ORs the range
+        // starts into a 64-bit mask, so an element finds its range with two
+        // population counts instead of a binary search
         int incl = len;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -641,25 +648,33 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
             if (lane >= d) incl += u;
         }
         const int total = __shfl_sync(0xffffffffu, incl, 31);
-        const int xoff = v.x - (incl - len);  // member index = tree base + xoff + element
-        for (int base = 0; base < total; base += 64) {
-            int e[2], j[2];
+        if (total > 0) {
+            const int ex = incl - len;  // this range's first element
+            const int xoff = v.x - ex;  // member index = tree base + xoff + element
+            const unsigned ne = __ballot_sync(0xffffffffu, len > 0);
+            if (len > 0) s_lid[w][__popc(ne & ((1u << lane) - 1u))] = (uint8_t)lane;
+            __syncwarp();
+            for (int base = 0; base < total; base += 64) {
+                const int sb = ex - base;
+                const bool st = len > 0 && sb >= 0 && sb < 64;
+                const unsigned lo = __reduce_or_sync(0xffffffffu, st && sb < 32 ? 1u << (sb & 31) : 0u);
+                const unsigned hi = __reduce_or_sync(0xffffffffu, st && sb >= 32 ? 1u << (sb & 31) : 0u);
+                const int before = __popc(__ballot_sync(0xffffffffu, len > 0 && sb < 0));
+                const unsigned upto = 0xffffffffu >> (31 - lane);  // bits 0..lane
+                int j[2];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                e[u] = base + (u << 5) + lane;
-                const int ec = min(e[u], total - 1);
-                int c = 0;  // number of lanes whose inclusive end is <= ec
-#pragma unroll
-                for (int d = 16; d > 0; d >>= 1) {
-                    const int x = __shfl_sync(0xffffffffu, incl, c + d - 1);
-                    if (x <= ec) c += d;
+                for (int u = 0; u < 2; ++u) {
+                    const int e = base + (u << 5) + lane;
+                    const int cnt = u == 0 ? __popc(lo & upto) : __popc(lo) + __popc(hi & upto);
+                    const int c = s_lid[w][max(0, before + cnt - 1)];
+                    const int xo = __shfl_sync(0xffffffffu, xoff, c);
+                    j[u] = e < total ? __ldg(memb + (size_t)((ch << 5) + c) * n + (xo + e)) : -1;
                 }
-                const int xo = __shfl_sync(0xffffffffu, xoff, c);
-                j[u] = e[u] < total ? __ldg(memb + (size_t)((ch << 5) + c) * n + (xo + e[u])) : -1;
-            }
 #pragma unroll
-            for (int u = 0; u < 2; ++u)
-                if (j[u] >= 0) count16(acc, j[u]);
+                for (int u = 0; u < 2; ++u)
+                    if (j[u] >= 0) count16(acc, j[u]);
+            }
+            __syncwarp();  // the list is rewritten by this warp's next chunk
         }
     }
     __syncthreads();
