@@ -196,7 +196,8 @@ TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "25
                 1: ["row16 256", "row16 512", "row16 1024", "row2 256", "row2 512", "row2 1024"],
                 2: ["64", "128", "256", "64 staged rows", "128 staged rows", "256 staged rows"],
                 3: ["128", "256", "512", "64 staged rows", "128 staged rows", "256 staged rows"],
-                4: ["row2 256", "row2 512", "row2 1024"]}
+                4: ["row2 256", "row2 512", "row2 1024", "row2 256 start-mask", "row2 512 start-mask",
+                    "row2 1024 start-mask"]}
 
 
 def _shape_name(kernel: int, shape: int) -> str:

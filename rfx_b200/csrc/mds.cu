@@ -88,16 +88,25 @@ __global__ void mds_grand_kernel(const double* __restrict__ rowmean, int n, doub
     }
 }
 
-// B with leading dimension npad (>= n); the pad rows and columns are zero.
-__global__ void mds_b_kernel(const float* __restrict__ P, const int32_t* __restrict__ nout, int n, int npad,
+// B in 64 x 64 tiles, tile (I, K) at (I * nt + K) * TILE_D doubles, rows of
+// TILE_LD doubles (64 values and 4 of padding, so that one bulk copy brings a
+// tile straight into the product kernel's bank-conflict-free layout); values
+// outside the n x n matrix and the padding are zero.
+constexpr int TILE_LD = 68;
+constexpr int TILE_D = 64 * TILE_LD;
+
+__global__ void mds_b_kernel(const float* __restrict__ P, const int32_t* __restrict__ nout, int n, int nt,
                              const unsigned long long* __restrict__ maxbits, const double* __restrict__ rowmean,
                              const double* __restrict__ grand, double* __restrict__ B) {
     const double mx = __longlong_as_double((long long)*maxbits);
     const double g = *grand;
-    const size_t total = (size_t)npad * npad;
+    const size_t total = (size_t)nt * nt * TILE_D;
     for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e / npad), j = (int)(e % npad);
-        if (i >= n || j >= n) {
+        const size_t tile = e / TILE_D;
+        const int within = (int)(e % TILE_D);
+        const int r = within / TILE_LD, cc = within % TILE_LD;
+        const int i = (int)(tile / nt) * 64 + r, j = (int)(tile % nt) * 64 + cc;
+        if (cc >= 64 || i >= n || j >= n) {
             B[e] = 0.0;
             continue;
         }
@@ -108,14 +117,13 @@ __global__ void mds_b_kernel(const float* __restrict__ P, const int32_t* __restr
 }
 
 // W[n x S] = B[n x n] V[n x S] in FP64 on the tensor cores (mma.sync
-// m16n8k4 .f64; Blackwell's tcgen05 has no FP64 kind).  B is stored with a
-// padded leading dimension npad (a multiple of 64, pads zero), so every
-// 64 x 64 tile row is one 512-byte bulk copy.  A CTA of four warps owns 64
-// rows and one range of kchunk columns; each 64-column step brings the B tile
-// (64 row copies into rows 544 bytes apart, which makes the fragment reads
-// conflict-free) and the matching 64 x 16 block of V (pre-arranged in
-// fragment order by bv_pack_kernel) through a DB_STAGES-deep mbarrier
-// pipeline.  Warp w multiplies rows 16w..16w+15 by both 8-column halves of V.
+// m16n8k4 .f64; Blackwell's tcgen05 has no FP64 kind).  B is stored in
+// 64 x 64 tiles with rows 544 bytes apart (mds_b_kernel), so a tile is one
+// contiguous bulk copy that lands in a layout whose fragment reads are free
+// of bank conflicts.  A CTA of four warps owns 64 rows and one range of
+// kchunk columns; each 64-column step brings the B tile and the matching
+// 64 x 16 block of V (pre-arranged in fragment order by bv_pack_kernel)
+// through a DB_STAGES-deep mbarrier pipeline, two bulk copies per step.  Warp w multiplies rows 16w..16w+15 by both 8-column halves of V.
 // The partial products go to Wpart[range] and are added in range order.
 constexpr int GT = 64;
 constexpr int BV_KSPLIT = 8;  // column ranges per row tile (enough CTAs to fill the GPU in several waves)
@@ -123,6 +131,7 @@ constexpr int DB_STAGES = 4;
 constexpr int DB_RS = GT * 8 + 32;                          // bytes between tile rows in shared memory
 constexpr int DB_VBYTES = GT * S_BLK * 8;                   // one 64 x 16 block of V
 constexpr int DB_STAGE = GT * DB_RS + DB_VBYTES;            // 43,008 bytes
+static_assert(DB_RS == TILE_LD * 8, "a bulk-copied B tile keeps its row stride in shared memory");
 constexpr size_t DB_SMEM = (size_t)DB_STAGES * DB_STAGE;    // 172,032 bytes
 constexpr int DB_WAIT_LIMIT = 1 << 24;
 
@@ -179,7 +188,7 @@ __global__ void bv_pack_kernel(const double* __restrict__ V, int n, int npad, do
     Vf[dst] = k < n ? V[idx] : 0.0;
 }
 
-__global__ void __launch_bounds__(128, 1) dgemm_bv_kernel(const double* __restrict__ B, int ldb,
+__global__ void __launch_bounds__(128, 1) dgemm_bv_kernel(const double* __restrict__ B, int nt,
                                                          const double* __restrict__ Vf, int n, int kchunk,
                                                          double* __restrict__ Wpart, uint32_t* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t dsm[];
@@ -203,11 +212,11 @@ __global__ void __launch_bounds__(128, 1) dgemm_bv_kernel(const double* __restri
         const int k0 = kbeg + it * GT;
         const uint32_t dst = base + (uint32_t)(s * DB_STAGE);
         const uint32_t bar = su32(&full[s]);
-        if (lane == 0) db_expect_tx(bar, GT * GT * 8 + DB_VBYTES);
-        __syncwarp();
-        for (int r = lane; r < GT; r += 32)
-            db_g2s(dst + (uint32_t)(r * DB_RS), B + (size_t)(r0 + r) * ldb + k0, GT * 8, bar);
-        if (lane == 0) db_g2s(dst + (uint32_t)(GT * DB_RS), Vf + (size_t)k0 * S_BLK, DB_VBYTES, bar);
+        if (lane == 0) {
+            db_expect_tx(bar, GT * DB_RS + DB_VBYTES);
+            db_g2s(dst, B + ((size_t)blockIdx.x * nt + k0 / GT) * TILE_D, GT * DB_RS, bar);
+            db_g2s(dst + (uint32_t)(GT * DB_RS), Vf + (size_t)k0 * S_BLK, DB_VBYTES, bar);
+        }
     };
     int issued = 0;
     if (warp == 0)
@@ -1038,8 +1047,9 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
         return RFX_ERR_UNSUPPORTED;
     }
     Scratch d(c);
-    const int npad = (n + GT - 1) / GT * GT;
-    double* B = d.get<double>((size_t)npad * npad);
+    const int nt = (n + GT - 1) / GT;
+    const int npad = nt * GT;
+    double* B = d.get<double>((size_t)nt * nt * TILE_D);
     double* rowmean = d.get<double>(n);
     double* grand = d.get<double>(1);
     unsigned long long* mx = d.get<unsigned long long>(1);
@@ -1051,7 +1061,7 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
     mds_max_kernel<<<1024, 256, 0, s>>>(dP, c->d_nout, n, mx);
     mds_rowsum_kernel<<<n, 256, 0, s>>>(dP, c->d_nout, n, mx, rowmean);
     mds_grand_kernel<<<1, 1024, 0, s>>>(rowmean, n, grand);
-    mds_b_kernel<<<2048, 256, 0, s>>>(dP, c->d_nout, n, npad, mx, rowmean, grand, B);
+    mds_b_kernel<<<2048, 256, 0, s>>>(dP, c->d_nout, n, nt, mx, rowmean, grand, B);
     c->launches += 4;
     RFX_CUDA(cudaGetLastError());
     const int kchunk = ((n + BV_KSPLIT - 1) / BV_KSPLIT + GT - 1) / GT * GT;
@@ -1065,7 +1075,7 @@ rfx_status launch_mds3d_full(Ctx* c, const float* dP, double* d_coords, double* 
     RFX_CUDA(cudaFuncSetAttribute(dgemm_bv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DB_SMEM));
     auto apply = [&](const double* V, double* W) -> rfx_status {
         bv_pack_kernel<<<(unsigned)(((size_t)npad * S_BLK + 255) / 256), 256, 0, s>>>(V, n, npad, Vf);
-        dgemm_bv_kernel<<<dim3(npad / GT, ksn), 128, DB_SMEM, s>>>(B, npad, Vf, n, kchunk, Wpart, c->d_err);
+        dgemm_bv_kernel<<<dim3(nt, ksn), 128, DB_SMEM, s>>>(B, nt, Vf, n, kchunk, Wpart, c->d_err);
         bv_reduce_kernel<<<(unsigned)(((size_t)n * S_BLK + 255) / 256), 256, 0, s>>>(Wpart, n, ksn, W);
         c->launches += 3;
         RFX_CUDA(cudaGetLastError());

@@ -547,7 +547,7 @@ constexpr int V2_LIST = 256;   // listed long ranges per row (more are walked in
 
 __device__ __forceinline__ void count16(uint32_t* acc, int j) { atomicAdd(acc + (j >> 1), 1u << ((j & 1) << 4)); }
 
-template <int NT>
+template <int NT, int SV>
 __global__ void __launch_bounds__(NT)
 pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                   int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
@@ -635,12 +635,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
             for (; off < ml; off += 32) count16(acc, __ldg(mp + off));
         }
         if (len >= 32) len = 0;
-        // the short ranges, element by element over the warp: element e of
-        // the concatenated ranges belongs to the last non-empty range that
-        // starts at or before e; the warp lists its non-empty ranges (lane
-        // ids, in lane order) and, per window of 64 elements, ORs the range
-        // starts into a 64-bit mask, so an element finds its range with two
-        // population counts instead of a binary search
+        // the short ranges, element by element over the warp
         int incl = len;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
@@ -648,9 +643,36 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
             if (lane >= d) incl += u;
         }
         const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (total > 0) {
+        const int xoff = v.x - (incl - len);  // member index = tree base + xoff + element
+        if constexpr (SV == 0) {
+            // a lane finds the range of its element by a binary search over
+            // the warp's inclusive length scan
+            for (int base = 0; base < total; base += 64) {
+                int j[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int e = base + (u << 5) + lane;
+                    const int ec = min(e, total - 1);
+                    int c = 0;  // number of lanes whose inclusive end is <= ec
+#pragma unroll
+                    for (int d = 16; d > 0; d >>= 1) {
+                        const int x = __shfl_sync(0xffffffffu, incl, c + d - 1);
+                        if (x <= ec) c += d;
+                    }
+                    const int xo = __shfl_sync(0xffffffffu, xoff, c);
+                    j[u] = e < total ? __ldg(memb + (size_t)((ch << 5) + c) * n + (xo + e)) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+                    if (j[u] >= 0) count16(acc, j[u]);
+            }
+        } else if (total > 0) {
+            // element e belongs to the last non-empty range starting at or
+            // before e: the warp lists its non-empty ranges (lane ids, in lane
+            // order) and, per window of 64 elements, ORs the range starts into
+            // a 64-bit mask, so an element finds its range with population
+            // counts
             const int ex = incl - len;  // this range's first element
-            const int xoff = v.x - ex;  // member index = tree base + xoff + element
             const unsigned ne = __ballot_sync(0xffffffffu, len > 0);
             if (len > 0) s_lid[w][__popc(ne & ((1u << lane) - 1u))] = (uint8_t)lane;
             __syncwarp();
@@ -713,26 +735,40 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         nv = (len - head) >> 2;
     }
     for (int h = tid; h < head; h += NT) srow[h] = (int32_t)a16[i + h];
-    // four counters per 16-byte store: counter j is half (j & 1) of word
-    // j >> 1; each is zero-extended by one byte permute (the parity of the
-    // first counter is the same for the whole row)
+    // body: lane L of a warp stores group v = v0 + L (entries jg + 4v ..+3);
+    // it reads the aligned 4-counter group holding its first entry (one
+    // 8-byte shared load), takes the next group from lane L + 1, and picks its
+    // four 16-bit counters with byte permutes (the offset o of jg in its group
+    // is the same for the whole row)
     int4* s4 = reinterpret_cast<int4*>(srow + head);
     const int jg = i + head;
-    const int wb = jg >> 1;
-    if (jg & 1) {
-        for (int v = tid; v < nv; v += NT) {
-            const int wd = wb + 2 * v;
-            const uint32_t x0 = acc[wd], x1 = acc[wd + 1], x2 = acc[wd + 2];
-            s4[v] = make_int4((int)__byte_perm(x0, 0u, 0x4432u), (int)__byte_perm(x1, 0u, 0x4410u),
-                              (int)__byte_perm(x1, 0u, 0x4432u), (int)__byte_perm(x2, 0u, 0x4410u));
+    const int o = jg & 3;
+    const int gb = jg >> 2;
+    const int ngroups = words >> 1;  // 4-counter groups in the array (the last one is padding)
+    const uint2* a64 = reinterpret_cast<const uint2*>(acc);
+    for (int v0 = w * 32; v0 < nv; v0 += NT) {
+        const int v = v0 + lane;
+        const int g = gb + v;
+        const uint2 cg = g < ngroups ? a64[g] : make_uint2(0u, 0u);
+        uint2 nx;
+        nx.x = __shfl_down_sync(0xffffffffu, cg.x, 1);
+        nx.y = __shfl_down_sync(0xffffffffu, cg.y, 1);
+        if (lane == 31) nx = g + 1 < ngroups ? a64[g + 1] : make_uint2(0u, 0u);
+        uint32_t q0, q1, q2, q3;
+        if (o == 0) {
+            q0 = __byte_perm(cg.x, 0u, 0x4410u); q1 = __byte_perm(cg.x, 0u, 0x4432u);
+            q2 = __byte_perm(cg.y, 0u, 0x4410u); q3 = __byte_perm(cg.y, 0u, 0x4432u);
+        } else if (o == 1) {
+            q0 = __byte_perm(cg.x, 0u, 0x4432u); q1 = __byte_perm(cg.y, 0u, 0x4410u);
+            q2 = __byte_perm(cg.y, 0u, 0x4432u); q3 = __byte_perm(nx.x, 0u, 0x4410u);
+        } else if (o == 2) {
+            q0 = __byte_perm(cg.y, 0u, 0x4410u); q1 = __byte_perm(cg.y, 0u, 0x4432u);
+            q2 = __byte_perm(nx.x, 0u, 0x4410u); q3 = __byte_perm(nx.x, 0u, 0x4432u);
+        } else {
+            q0 = __byte_perm(cg.y, 0u, 0x4432u); q1 = __byte_perm(nx.x, 0u, 0x4410u);
+            q2 = __byte_perm(nx.x, 0u, 0x4432u); q3 = __byte_perm(nx.y, 0u, 0x4410u);
         }
-    } else {
-        for (int v = tid; v < nv; v += NT) {
-            const int wd = wb + 2 * v;
-            const uint32_t x0 = acc[wd], x1 = acc[wd + 1];
-            s4[v] = make_int4((int)__byte_perm(x0, 0u, 0x4410u), (int)__byte_perm(x0, 0u, 0x4432u),
-                              (int)__byte_perm(x1, 0u, 0x4410u), (int)__byte_perm(x1, 0u, 0x4432u));
-        }
+        if (v < nv) s4[v] = make_int4((int)q0, (int)q1, (int)q2, (int)q3);
     }
     for (int j = i + head + 4 * nv + tid; j < n; j += NT) srow[j - i] = (int32_t)a16[j];
     if (pairs) {
@@ -883,15 +919,17 @@ bool use_row16(const Ctx* c, int dev_smem) {
     return c->T < 65536 && words * 4 + 20 * 1024 <= (size_t)dev_smem;
 }
 
-// Hub leaves on the tensor cores (hubs.cu): by default from n = 16,384 (at
-// smaller n the dense n x n tiles cost more than the few hub updates they
-// save); RFX_PAIRS_HUBS=0 turns the part off, =1 forces it on at any n.  The
-// counts are the same either way.
+// Hub leaves on the tensor cores (hubs.cu): by default from n = 16,384 and
+// 512 trees.  The tiles cost a fixed n x n pass (the GEMM and the row
+// kernel's read of the tiles) while the updates they take over grow with the
+// number of trees: 64 forests of 300 trees at n <= 50,000 ran 1.3x slower
+// with them.  RFX_PAIRS_HUBS=0 turns the part off, =1 forces it on at any
+// size.  The counts are the same either way.
 bool use_hubs(const Ctx* c) {
     const char* e = getenv("RFX_PAIRS_HUBS");
     if (e && std::string(e) == "0") return false;
     if (e && std::string(e) == "1") return true;
-    return c->n >= 16384 && c->T >= 16;
+    return c->n >= 16384 && c->T >= 512;
 }
 
 rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
@@ -928,13 +966,16 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<256>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<512>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row16_kernel<1024>, dev_smem)) return s0;
-        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<256>, dev_smem)) return s0;
-        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<512>, dev_smem)) return s0;
-        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<1024>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<256, 0>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<512, 0>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<1024, 0>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<256, 1>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<512, 1>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<1024, 1>, dev_smem)) return s0;
         StageTimer st(c, ST_PAIRS, 1);
         // with hub tiles only the second row kernel (which starts from them) runs
         const int tk = hubs ? TK_PAIRS_HUB : TK_PAIRS16;
-        const int nshape = hubs ? 3 : PAIRS_SHAPES;
+        const int nshape = hubs ? 6 : PAIRS_SHAPES;
         const int defshape = hubs ? 1 : PAIRS_DEFAULT_SHAPE;
         return autotune(c, tk, nshape, defshape, [&](int shape) -> rfx_status {
             // the pair counter restarts from the hub leaves' pair updates
@@ -943,11 +984,19 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
                                          c->stream));
             else
                 RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
-            if (hubs) shape += 3;
+            // hub shapes 0-2: row2 with 256/512/1024 threads, binary-search
+            // short ranges; 3-5: the same with the start-mask lookup
+            int sv = 0;
+            if (hubs) {
+                sv = shape >= 3;
+                shape = 3 + shape % 3;
+            }
             if (shape >= 3) {
                 const int nt = 256 << (shape - 3);
-                auto kern = shape == 3 ? pairs_row2_kernel<256> : shape == 4 ? pairs_row2_kernel<512>
-                                                                             : pairs_row2_kernel<1024>;
+                auto kern = sv ? (shape == 3 ? pairs_row2_kernel<256, 1> : shape == 4 ? pairs_row2_kernel<512, 1>
+                                                                                        : pairs_row2_kernel<1024, 1>)
+                               : (shape == 3 ? pairs_row2_kernel<256, 0> : shape == 4 ? pairs_row2_kernel<512, 0>
+                                                                                        : pairs_row2_kernel<1024, 0>);
                 kern<<<c->n, nt, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, words,
                                                     hubs ? c->d_hubtiles : nullptr, c->d_hubstate, dS, c->d_pairs);
             } else if (shape == 0)

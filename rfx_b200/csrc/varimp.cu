@@ -22,10 +22,10 @@
 //                       (in leaf order when oobord exists, so a warp's main
 //                       paths coincide): walks, flip masks, per-tree integer
 //                       counts.
-// varimp_sample_tiled_kernel - one thread per (sample, 16 features): qimp /
-//                       qimpm float sums in tree order, 1/noob per correct
-//                       OOB tree (the reference adds each tree's temporaries
-//                       in tree order, src/rf_random_forest.cpp:1217-1230).
+// varimp_sample_kernel - one thread per (sample, 16 features): qimp / qimpm
+//                       float sums in tree order, 1/noob per correct OOB
+//                       tree (the reference adds each tree's temporaries in
+//                       tree order, src/rf_random_forest.cpp:1217-1230).
 // varimp_feature_kernel - one thread per feature: avimp / sqsd sums of
 //                       rr = (right - rightimp) / noob in tree order.
 #include "walks.cuh"
@@ -412,125 +412,74 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
 // features come in blocks); iv rows are ivw words long.
 constexpr int VS_FEAT = 16;  // features per thread (a group never straddles a 64-bit word)
 
-// The (tree, sample) flags and flip words come through
-// shared memory in tiles of tcn trees x VS_SB samples: every thread of the
-// CTA issues its share of the next tile's loads (all independent, at most
-// VS_PER flip words and VS_PER flags per thread, which fixes tcn = nthreads /
-// (8 W) up to VS_TC) before the sums of the current tile, so the loads
-// stream instead of waiting one tree at a time.  Thread (s, g) = (tid % VS_SB,
-// tid / VS_SB) owns sample i0 + s and feature group g (blockDim = VS_SB x
-// groups).  vflags must be zero for in-bag units (bit 0 marks an OOB unit).
-constexpr int VS_SB = 64;   // samples per CTA
-constexpr int VS_TC = 32;   // most trees per tile
-constexpr int VS_PER = 8;   // tile loads per thread and kind
-
-__host__ __device__ inline int vs_tile_trees(int nth, int W) { return min(VS_TC, nth / (8 * W)); }
-
 template <int W>
-__global__ void __launch_bounds__(1024)
-varimp_sample_tiled_kernel(const uint8_t* __restrict__ vflags, const uint64_t* __restrict__ flips,
-                           const uint64_t* __restrict__ iv, const float* __restrict__ invnoob, int n, int p, int T,
-                           float* __restrict__ qimp, float* __restrict__ qimpm, int fb, int pw, int ivw) {
-    extern __shared__ __align__(16) uint8_t vs_sm[];
-    const int nth = blockDim.x;
-    const int tcn = vs_tile_trees(nth, W);
-    // two tile buffers: flip words [tcn][VS_SB * W], then flags [tcn][VS_SB]
-    const int FWN = tcn * VS_SB * W;
-    uint64_t* sflip = reinterpret_cast<uint64_t*>(vs_sm);
-    uint8_t* sflag = vs_sm + 2 * (size_t)FWN * sizeof(uint64_t);
-    const int tid = threadIdx.x;
-    const int s = tid % VS_SB, g = tid / VS_SB;
-    const int i0 = blockIdx.x * VS_SB;
-    const int i = i0 + s;
-    const int ns = min(VS_SB, n - i0);
-    const int kl = g * VS_FEAT;
+__global__ void __launch_bounds__(256, 3)
+varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restrict__ vflags,
+                     const uint64_t* __restrict__ flips, const uint64_t* __restrict__ iv,
+                     const float* __restrict__ invnoob, int n, int p, int T, float* __restrict__ qimp,
+                     float* __restrict__ qimpm, int fb, int pw, int ivw) {
+    const int G = (pw + VS_FEAT - 1) / VS_FEAT;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * G) return;
+    const int i = (int)(idx / G);
+    const int g = (int)(idx % G);
+    const int kl = g * VS_FEAT;  // first feature of the group within the block
     const int k0 = fb + kl;
-    const int wq = kl >> 6, sh = kl & 63;
-    const int iq = k0 >> 6;
-    uint64_t fv[VS_PER];
-    uint8_t bv[VS_PER];
-    // this thread's elements of tile t0: flip e = tid + q * nth -> (tree e /
-    // (ns W), slot e % (ns W)); flag e -> (tree e / ns, sample e % ns)
-    auto load_tile = [&](int t0) {
-        const int tc = min(tcn, T - t0);
-        const int cf = tc * ns * W, cb = tc * ns;
-#pragma unroll
-        for (int q = 0; q < VS_PER; ++q) {
-            const int e = tid + q * nth;
-            if (e < cf) {
-                const int r = e / (ns * W), cw = e - r * (ns * W);
-                fv[q] = __ldg(flips + ((size_t)(t0 + r) * n + i0) * W + cw);
-            }
-            if (e < cb) {
-                const int r = e / ns, c = e - r * ns;
-                bv[q] = __ldg(vflags + (size_t)(t0 + r) * n + i0 + c);
-            }
-        }
-    };
-    auto store_tile = [&](int buf, int t0) {
-        const int tc = min(tcn, T - t0);
-        const int cf = tc * ns * W, cb = tc * ns;
-        uint64_t* df = sflip + (size_t)buf * FWN;
-        uint8_t* db = sflag + (size_t)buf * tcn * VS_SB;
-#pragma unroll
-        for (int q = 0; q < VS_PER; ++q) {
-            const int e = tid + q * nth;
-            if (e < cf) {
-                const int r = e / (ns * W), cw = e - r * (ns * W);
-                df[r * VS_SB * W + cw] = fv[q];
-            }
-            if (e < cb) {
-                const int r = e / ns, c = e - r * ns;
-                db[r * VS_SB + c] = bv[q];
-            }
-        }
-    };
+    const int wq = kl >> 6, sh = kl & 63;  // groups never straddle a 64-bit word
+    const int iq = k0 >> 6;                // the group's word of the iv row
     float acc[VS_FEAT];
 #pragma unroll
     for (int u = 0; u < VS_FEAT; ++u) acc[u] = 0.0f;
     float q = 0.0f;
-    load_tile(0);
-    store_tile(0, 0);
-    __syncthreads();
-    int buf = 0;
-    for (int t0 = 0; t0 < T; t0 += tcn) {
-        const bool more = t0 + tcn < T;
-        if (more) load_tile(t0 + tcn);  // in flight during the sums below
-        const int tc = min(tcn, T - t0);
-        const uint64_t* df = sflip + (size_t)buf * FWN;
-        const uint8_t* db = sflag + (size_t)buf * tcn * VS_SB;
-        if (s < ns && kl < pw) {
-            for (int r = 0; r < tc; ++r) {
-                const uint8_t fl = db[r * VS_SB + s];
-                if (!(fl & 1u)) continue;  // in bag
-                const int t = t0 + r;
-                const float inv = __ldg(invnoob + t);
-                const bool btb = (fl >> 1) & 1, bimp = (fl >> 2) & 1;
-                if (btb) q = __fadd_rn(q, inv);
-                const uint64_t fw = df[r * VS_SB * W + s * W + wq];
-                const uint64_t ivt = __ldg(iv + (size_t)t * ivw + iq);
-                const uint64_t corr = (ivt & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivt & (btb ? ~0ull : 0ull));
-                const uint32_t cbits = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
+    // trees in blocks of TB: all loads of a block are issued before its sums
+    // (the flip words of in-bag units are read but not used), then the sums
+    // are added in tree order
+    constexpr int TB = 8;
+    int t0 = 0;
+    for (; t0 + TB <= T; t0 += TB) {
+        uint8_t ib[TB], fl[TB];
+        float inv[TB];
+        uint64_t fw[TB], ivv[TB];
 #pragma unroll
-                for (int u = 0; u < VS_FEAT; ++u)
-                    if ((cbits >> u) & 1u) acc[u] = __fadd_rn(acc[u], inv);
-            }
+        for (int u = 0; u < TB; ++u) {
+            const size_t ti = (size_t)(t0 + u) * n + i;
+            ib[u] = __ldg(inbag + ti);
+            fl[u] = __ldg(vflags + ti);
+            inv[u] = __ldg(invnoob + t0 + u);
+            fw[u] = __ldg(flips + ti * W + wq);
+            ivv[u] = __ldg(iv + (size_t)(t0 + u) * ivw + iq);
         }
-        __syncthreads();  // every thread is done with the other buffer's previous tile
-        if (more) store_tile(buf ^ 1, t0 + tcn);
-        __syncthreads();
-        buf ^= 1;
+#pragma unroll
+        for (int u = 0; u < TB; ++u) {
+            if (ib[u] != 0) continue;
+            const bool btb = (fl[u] >> 1) & 1, bimp = (fl[u] >> 2) & 1;
+            if (btb) q = __fadd_rn(q, inv[u]);
+            const uint64_t corr = (ivv[u] & ((bimp ? ~0ull : 0ull) ^ fw[u])) | (~ivv[u] & (btb ? ~0ull : 0ull));
+            const uint32_t cb = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
+#pragma unroll
+            for (int v = 0; v < VS_FEAT; ++v)
+                if ((cb >> v) & 1u) acc[v] = __fadd_rn(acc[v], inv[u]);
+        }
     }
-    if (s >= ns || kl >= pw) return;
+    for (int t = t0; t < T; ++t) {
+        const size_t ti = (size_t)t * n + i;
+        if (__ldg(inbag + ti) != 0) continue;
+        const uint8_t fl = __ldg(vflags + ti);
+        const float inv = __ldg(invnoob + t);
+        const bool btb = (fl >> 1) & 1, bimp = (fl >> 2) & 1;
+        if (btb) q = __fadd_rn(q, inv);
+        const uint64_t fw = __ldg(flips + ti * W + wq);
+        const uint64_t ivt = __ldg(iv + (size_t)t * ivw + iq);
+        const uint64_t corr = (ivt & ((bimp ? ~0ull : 0ull) ^ fw)) | (~ivt & (btb ? ~0ull : 0ull));
+        const uint32_t cb = (uint32_t)(corr >> sh) & ((1u << VS_FEAT) - 1u);
+#pragma unroll
+        for (int u = 0; u < VS_FEAT; ++u)
+            if ((cb >> u) & 1u) acc[u] = __fadd_rn(acc[u], inv);
+    }
     if (g == 0 && fb == 0) qimp[i] = q;
 #pragma unroll
     for (int u = 0; u < VS_FEAT; ++u)
         if (kl + u < pw) qimpm[(size_t)i * p + k0 + u] = acc[u];
-}
-
-inline size_t vs_smem(int nth, int W) {
-    const int tcn = vs_tile_trees(nth, W);
-    return 2 * ((size_t)tcn * VS_SB * W * sizeof(uint64_t) + (size_t)tcn * VS_SB);
 }
 
 // counts[2t] = #OOB correct by testreebag (right), counts[2t+1] = #OOB correct
@@ -582,22 +531,6 @@ __global__ void localimp_kernel(const float* __restrict__ qimp, const float* __r
     out[idx] = __fdiv_rn(__fmul_rn(100.0f, __fsub_rn(qimp[nn], qimpm[idx])), (float)T);
 }
 
-// qimp / qimpm over features [fb, fb + pw): one CTA per 64 samples, one
-// 64-thread group per 16 features
-template <int W>
-rfx_status launch_sample_tiled(Ctx* c, int fb, int pw, int ivw) {
-    const int G = (pw + VS_FEAT - 1) / VS_FEAT;
-    const int nth = VS_SB * G;
-    const size_t sm = vs_smem(nth, W);
-    int dev_smem = 0;
-    RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
-    if (rfx_status s0 = allow_dyn_smem(varimp_sample_tiled_kernel<W>, dev_smem)) return s0;
-    varimp_sample_tiled_kernel<W><<<(c->n + VS_SB - 1) / VS_SB, nth, sm, c->stream>>>(
-        c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp, c->d_qimpm, fb, pw, ivw);
-    RFX_CUDA(cudaGetLastError());
-    return RFX_OK;
-}
-
 template <int W>
 rfx_status launch_varimp_w(Ctx* c, int impn) {
     const size_t smem = (size_t)c->p * sizeof(int32_t);
@@ -608,8 +541,6 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
                                                 ordered ? c->d_partner : nullptr, ordered ? c->d_memb : nullptr,
                                                 c->d_oobord);
         RFX_CUDA(cudaGetLastError());
-        // the walk flags OOB units only; in-bag units read as zero
-        RFX_CUDA(cudaMemsetAsync(c->d_vflags, 0, (size_t)c->T * c->n, c->stream));
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
         // staged shapes hold VW own rows and VW partner rows of p | 1 floats
@@ -660,7 +591,12 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
     }
     if (impn) {
         StageTimer st(c, ST_VARIMP_SAMPLE, 1);
-        if (rfx_status s0 = launch_sample_tiled<W>(c, 0, c->p, W)) return s0;
+        const long long G = (c->p + VS_FEAT - 1) / VS_FEAT;
+        const long long threads = (long long)c->n * G;
+        varimp_sample_kernel<W><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp, c->d_qimpm, 0,
+            c->p, W);
+        RFX_CUDA(cudaGetLastError());
     }
     StageTimer st(c, ST_VARIMP_FEATURE, 1);
     varimp_feature_kernel<<<(c->p + 3) / 4, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,
@@ -684,7 +620,6 @@ rfx_status launch_varimp_blocked(Ctx* c, int impn) {
         RFX_CUDA(cudaGetLastError());
         int max_noob = 1;
         for (int t = 0; t < c->T; ++t) max_noob = std::max(max_noob, c->h_noob[t]);
-        RFX_CUDA(cudaMemsetAsync(c->d_vflags, 0, (size_t)c->T * c->n, c->stream));
         RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
         RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
         const dim3 grid((max_noob + VW - 1) / VW, c->T);
@@ -696,7 +631,11 @@ rfx_status launch_varimp_blocked(Ctx* c, int impn) {
                 c->d_partner, c->d_inbag, c->d_vflags, c->d_flips, c->d_right, c->d_rightimp, c->d_err, fb);
             RFX_CUDA(cudaGetLastError());
             if (impn) {
-                if (rfx_status s0 = launch_sample_tiled<W>(c, fb, pw, c->iv_words)) return s0;
+                const long long threads = (long long)c->n * ((pw + VS_FEAT - 1) / VS_FEAT);
+                varimp_sample_kernel<W><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+                    c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp,
+                    c->d_qimpm, fb, pw, c->iv_words);
+                RFX_CUDA(cudaGetLastError());
             }
         }
     }
