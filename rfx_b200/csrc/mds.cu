@@ -283,8 +283,10 @@ __global__ void bv_reduce_kernel(const double* __restrict__ Wpart, int n, int ks
 }
 
 // G[S x S] += X^T Y over rows (atomics into a zeroed G).
+// Per-CTA partial Gram matrices X^T Y (16 x 16) into part[blockIdx.x], added
+// by gram_sum_kernel in a fixed order (reproducible run to run).
 __global__ void __launch_bounds__(256) dgram_kernel(const double* __restrict__ X, const double* __restrict__ Y, int n,
-                                                    double* __restrict__ G) {
+                                                    double* __restrict__ part) {
     __shared__ double Xs[64][S_BLK], Ys[64][S_BLK];
     const int tid = threadIdx.x;
     const int a = tid / S_BLK, b = tid % S_BLK;  // 16 x 16 outputs
@@ -299,7 +301,20 @@ __global__ void __launch_bounds__(256) dgram_kernel(const double* __restrict__ X
         for (int r = 0; r < 64; ++r) acc = fma(Xs[r][a], Ys[r][b], acc);
         __syncthreads();
     }
-    atomicAdd(G + a * S_BLK + b, acc);
+    part[(size_t)blockIdx.x * (S_BLK * S_BLK) + a * S_BLK + b] = acc;
+}
+
+// G[e] = sum over the partials, one warp per entry (lane l the partials l,
+// l + 32, ..., then a fixed shuffle tree)
+__global__ void gram_sum_kernel(const double* __restrict__ part, int nparts, double* __restrict__ G) {
+    const int e = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (e >= S_BLK * S_BLK) return;
+    double v = 0.0;
+    for (int q = lane; q < nparts; q += 32) v += part[(size_t)q * (S_BLK * S_BLK) + e];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    if (lane == 0) G[e] = v;
 }
 
 // One CTA: Cholesky of G and the inverse of its factor, T = L^{-T} (S x S).
@@ -428,19 +443,26 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
         set_error("MDS: device allocation failed");
         return RFX_ERR_OOM;
     }
+    const int gb = std::min(1024, (n + 63) / 64);
+    double* gpart = d.get<double>((size_t)gb * S_BLK * S_BLK);
+    if (!gpart) {
+        set_error("MDS: device allocation failed");
+        return RFX_ERR_OOM;
+    }
+    auto gram = [&](const double* X, const double* Y) {
+        dgram_kernel<<<gb, 256, 0, s>>>(X, Y, n, gpart);
+        gram_sum_kernel<<<S_BLK * S_BLK * 32 / 256, 256, 0, s>>>(gpart, gb, G);
+    };
     // CholeskyQR2: Out = (src L1^{-T}) L2^{-T}, through the temporary Xt
     auto orth = [&](const double* src, double* Out) -> rfx_status {
-        const unsigned gb = (unsigned)std::min(1024, (n + 63) / 64);
         const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
-        RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * S_BLK * S_BLK, s));
-        dgram_kernel<<<gb, 256, 0, s>>>(src, src, n, G);
+        gram(src, src);
         chol_inv_kernel<<<1, 128, 0, s>>>(G, Tm, bad);
         dright_kernel<<<gr, 256, 0, s>>>(src, Tm, n, Xt);
-        RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * S_BLK * S_BLK, s));
-        dgram_kernel<<<gb, 256, 0, s>>>(Xt, Xt, n, G);
+        gram(Xt, Xt);
         chol_inv_kernel<<<1, 128, 0, s>>>(G, Tm, bad);
         dright_kernel<<<gr, 256, 0, s>>>(Xt, Tm, n, Out);
-        c->launches += 6;
+        c->launches += 8;
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
@@ -451,10 +473,9 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
     // Rayleigh-Ritz on span(V) with W = B V: eigenvalues into cur, change of
     // the k largest against the previous check into *delta
     auto ritz = [&](double* delta) -> rfx_status {
-        RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * S_BLK * S_BLK, s));
-        dgram_kernel<<<std::min(1024, (n + 63) / 64), 256, 0, s>>>(V, W, n, G);
+        gram(V, W);
         rr_kernel<<<1, 128, 0, s>>>(G, ev, U);
-        c->launches += 2;
+        c->launches += 3;
         RFX_CUDA(cudaMemcpyAsync(cur.data(), ev, sizeof(double) * S_BLK, cudaMemcpyDeviceToHost, s));
         RFX_CUDA(cudaStreamSynchronize(s));
         std::vector<double> a = cur, b = prev;
@@ -533,10 +554,9 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
         const bool check = (it % 10 == 0) || it == max_iter;
         if (check) {
             // Rayleigh-Ritz on span(V): H = V^T (B V)
-            RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(double) * S_BLK * S_BLK, s));
-            dgram_kernel<<<std::min(1024, (n + 63) / 64), 256, 0, s>>>(V, W, n, G);
+            gram(V, W);
             rr_kernel<<<1, 128, 0, s>>>(G, ev, U);
-            c->launches += 2;
+            c->launches += 3;
             RFX_CUDA(cudaMemcpyAsync(cur.data(), ev, sizeof(double) * S_BLK, cudaMemcpyDeviceToHost, s));
             RFX_CUDA(cudaStreamSynchronize(s));
             std::vector<double> a = cur, b = prev;
@@ -609,9 +629,23 @@ rfx_status subspace_topk(Ctx* c, int n, int k, Apply apply, int max_iter, double
 namespace {
 
 // Column means of an n x 16 FP64 block in a fixed summation order: per-CTA
-// partial sums over a strided row set, then one CTA adds the partials in CTA
-// order (reproducible run to run).
-constexpr int RED_CTAS = 296;
+// partial sums over a strided row set, then one warp per output adds the
+// partials (lane l the partials l, l + 32, ..., then a fixed shuffle tree), so
+// the result is reproducible run to run.
+constexpr int RED_CTAS = 1184;  // eight CTAs per SM
+
+// out[e] = scale * sum over p of part[p * cnt + e], one warp per e
+template <typename TV>
+__global__ void part_sum_kernel(const TV* __restrict__ part, int nparts, int cnt, TV scale, TV* __restrict__ out) {
+    const int e = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (e >= cnt) return;
+    TV s = 0;
+    for (int q = lane; q < nparts; q += 32) s += part[(size_t)q * cnt + e];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+    if (lane == 0) out[e] = s * scale;
+}
 
 __global__ void __launch_bounds__(256) colsum_part_kernel(const double* __restrict__ V, int n,
                                                           double* __restrict__ part) {
@@ -626,14 +660,6 @@ __global__ void __launch_bounds__(256) colsum_part_kernel(const double* __restri
         for (int q = 0; q < 16; ++q) t += red[q][threadIdx.x];
         part[(size_t)blockIdx.x * S_BLK + threadIdx.x] = t;
     }
-}
-
-__global__ void colmean_final_kernel(const double* __restrict__ part, int nparts, int n, double* __restrict__ mean) {
-    const int j = threadIdx.x;
-    if (j >= S_BLK) return;
-    double s = 0.0;
-    for (int q = 0; q < nparts; ++q) s += part[(size_t)q * S_BLK + j];
-    mean[j] = s / (double)n;
 }
 
 // u = V - mean (FP64), also as FP32
@@ -679,16 +705,9 @@ __global__ void __launch_bounds__(256) atu_part_kernel(const float* __restrict__
     }
 }
 
-__global__ void atu_final_kernel(const double* __restrict__ part, int nparts, int k, double* __restrict__ AtU) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= k * S_BLK) return;
-    double s = 0.0;
-    for (int q = 0; q < nparts; ++q) s += part[(size_t)q * k * S_BLK + e];
-    AtU[e] = s;
-}
-
-// M[j][a][b] += sum over a row chunk of u[i][j] A[i][a] A[i][b]; one CTA per
-// (row chunk, j); each thread a 4 x 4 block of (a, b).  k <= 64.
+// Partial M[j][a][b] = sum over the CTA's row chunks of u[i][j] A[i][a]
+// A[i][b]; one CTA per (row-chunk set, j); each thread a 4 x 4 block of
+// (a, b).  k <= 64.
 constexpr int MS_ROWS = 128;
 __global__ void __launch_bounds__(256) mstack_f32_kernel(const float* __restrict__ A, const float* __restrict__ u,
                                                          int n, int k, float* __restrict__ M) {
@@ -721,11 +740,22 @@ __global__ void __launch_bounds__(256) mstack_f32_kernel(const float* __restrict
         }
         __syncthreads();
     }
+    // this CTA's partial of M_j (added over the CTAs by part_sum_kernel)
+    float* Mp = M + (size_t)blockIdx.x * S_BLK * k * k;
 #pragma unroll
     for (int p = 0; p < 4; ++p)
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-            if (a0 + p < k && b0 + q < k) atomicAdd(M + ((size_t)j * k + a0 + p) * k + b0 + q, acc[p][q]);
+            if (a0 + p < k && b0 + q < k) Mp[((size_t)j * k + a0 + p) * k + b0 + q] = acc[p][q];
+}
+
+// M = the stack of the FP32 form: per-CTA partials, then a fixed-order sum
+constexpr int MSF_CTAS = 148;
+void mstack_f32(const float* dA, const float* u32, int n, int k, float* Mpart, float* M, cudaStream_t s) {
+    const int gx = std::min(MSF_CTAS, (n + MS_ROWS - 1) / MS_ROWS);
+    mstack_f32_kernel<<<dim3(gx, S_BLK), 256, 0, s>>>(dA, u32, n, k, Mpart);
+    const int cnt = S_BLK * k * k;
+    part_sum_kernel<float><<<(unsigned)(((size_t)cnt * 32 + 255) / 256), 256, 0, s>>>(Mpart, gx, cnt, 1.0f, M);
 }
 
 // T2[i][j] = a_i^T M_j a_i for 4 consecutive j per CTA (M slices in shared memory)
@@ -830,12 +860,31 @@ __global__ void __launch_bounds__(256) factor_combine_kernel(const float* __rest
 #pragma unroll
     for (int j = 0; j < S_BLK; ++j) t1[j] = 0.0;
     double nrm = 0.0;
-    for (int a = 0; a < k; ++a) {
-        const double x = A[(size_t)i * k + a];
+    const float* arow = A + (size_t)i * k;
+    auto step = [&](double x, int a) {
         nrm += x * x;
         const double* ar = s_atu + a * S_BLK;
 #pragma unroll
         for (int j = 0; j < S_BLK; ++j) t1[j] += x * ar[j];
+    };
+    if ((k & 3) == 0) {
+        // the row as 16-byte loads, four in flight
+        for (int a = 0; a < k; a += 16) {
+            float4 q[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+                q[h] = a + 4 * h < k ? __ldg(reinterpret_cast<const float4*>(arow + a) + h) : make_float4(0, 0, 0, 0);
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+                if (a + 4 * h < k) {
+                    step(q[h].x, a + 4 * h);
+                    step(q[h].y, a + 4 * h + 1);
+                    step(q[h].z, a + 4 * h + 2);
+                    step(q[h].w, a + 4 * h + 3);
+                }
+        }
+    } else {
+        for (int a = 0; a < k; ++a) step(A[(size_t)i * k + a], a);
     }
     const double cc = (1.0 - nrm) * (1.0 - nrm);
     const size_t o = (size_t)i * S_BLK;
@@ -869,13 +918,15 @@ __global__ void outlier_raw_kernel(const float* __restrict__ A, const double* __
     out[i] = (float)(1.0 / ss);
 }
 
-__global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __restrict__ AtA) {
+// Partial A^T A over the rows blockIdx.x, blockIdx.x + gridDim.x, ... into
+// part[blockIdx.x] (k x k), added by part_sum_kernel in a fixed order.
+__global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __restrict__ part) {
     const int e = blockIdx.y * blockDim.x + threadIdx.x;  // output index
     if (e >= k * k) return;
     const int a = e / k, b = e % k;
     double s = 0.0;
     for (int i = blockIdx.x; i < n; i += gridDim.x) s += (double)A[(size_t)i * k + a] * (double)A[(size_t)i * k + b];
-    atomicAdd(AtA + e, s);
+    part[(size_t)blockIdx.x * k * k + e] = s;
 }
 
 }  // namespace
@@ -889,11 +940,11 @@ size_t factor_tc_at_bytes(int n, int k);
 namespace {
 void col_mean(const double* V, int n, double* part, double* mean, cudaStream_t s) {
     colsum_part_kernel<<<RED_CTAS, 256, 0, s>>>(V, n, part);
-    colmean_final_kernel<<<1, 32, 0, s>>>(part, RED_CTAS, n, mean);
+    part_sum_kernel<double><<<(S_BLK * 32 + 255) / 256, 256, 0, s>>>(part, RED_CTAS, S_BLK, 1.0 / (double)n, mean);
 }
 void at_u(const float* A, const float* u, int n, int k, double* part, double* AtU, cudaStream_t s) {
     atu_part_kernel<<<RED_CTAS, 256, 0, s>>>(A, u, n, k, part);
-    atu_final_kernel<<<(k * S_BLK + 255) / 256, 256, 0, s>>>(part, RED_CTAS, k, AtU);
+    part_sum_kernel<double><<<(k * S_BLK * 32 + 255) / 256, 256, 0, s>>>(part, RED_CTAS, k * S_BLK, 1.0, AtU);
 }
 }  // namespace
 
@@ -911,9 +962,10 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     float* u32 = d.get<float>((size_t)n * S_BLK);
     double* AtU = d.get<double>((size_t)k * S_BLK);
     float* M = d.get<float>((size_t)S_BLK * k * k);
+    float* Mpart = d.get<float>((size_t)MSF_CTAS * S_BLK * k * k);
     float* T2 = d.get<float>((size_t)n * S_BLK);
     double* part = d.get<double>((size_t)RED_CTAS * k * S_BLK);
-    if (!mean || !u || !u32 || !AtU || !M || !T2 || !part) {
+    if (!mean || !u || !u32 || !AtU || !M || !Mpart || !T2 || !part) {
         set_error("compute_mds_from_factors: device allocation failed");
         return RFX_ERR_OOM;
     }
@@ -932,8 +984,7 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
             rfx_status st = launch_factor_ops_tc(c, dA, k, Aq, At, u32, M, T2);
             if (st != RFX_OK) return st;
         } else {
-            RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
-            mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
+            mstack_f32(dA, u32, n, k, Mpart, M, s);
             quadform_f32(dA, M, n, k, T2, s);
             c->launches += 2;
         }
@@ -989,9 +1040,10 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
     float* u32 = d.get<float>((size_t)n * S_BLK);
     double* AtU = d.get<double>((size_t)k * S_BLK);
     float* M = d.get<float>((size_t)S_BLK * k * k);
+    float* Mpart = d.get<float>((size_t)MSF_CTAS * S_BLK * k * k);
     float* T2 = d.get<float>((size_t)n * S_BLK);
     double* part = d.get<double>((size_t)RED_CTAS * k * S_BLK);
-    if (!mean || !u || !u32 || !AtU || !M || !T2 || !part) return RFX_ERR_OOM;
+    if (!mean || !u || !u32 || !AtU || !M || !Mpart || !T2 || !part) return RFX_ERR_OOM;
     const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
     col_mean(V, n, part, mean, s);
     center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
@@ -1006,8 +1058,7 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
     } else {
         const size_t qsm = 4 * (size_t)k * k * sizeof(float);
         RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));
-        RFX_CUDA(cudaMemsetAsync(M, 0, sizeof(float) * S_BLK * k * k, s));
-        mstack_f32_kernel<<<dim3(std::min(592, (n + MS_ROWS - 1) / MS_ROWS), S_BLK), 256, 0, s>>>(dA, u32, n, k, M);
+        mstack_f32(dA, u32, n, k, Mpart, M, s);
         quadform_f32(dA, M, n, k, T2, s);
     }
     if (st != RFX_OK) return st;
@@ -1024,11 +1075,12 @@ rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out) {
     cudaStream_t s = c->stream;
     Scratch d(c);
     double* AtA = d.get<double>((size_t)k * k);
-    if (!AtA) return RFX_ERR_OOM;
-    RFX_CUDA(cudaMemsetAsync(AtA, 0, sizeof(double) * k * k, s));
-    ata_kernel<<<dim3(256, (k * k + 255) / 256), 256, 0, s>>>(dA, n, k, AtA);
+    double* apart = d.get<double>((size_t)256 * k * k);
+    if (!AtA || !apart) return RFX_ERR_OOM;
+    ata_kernel<<<dim3(256, (k * k + 255) / 256), 256, 0, s>>>(dA, n, k, apart);
+    part_sum_kernel<double><<<(k * k * 32 + 255) / 256, 256, 0, s>>>(apart, 256, k * k, 1.0, AtA);
     outlier_raw_kernel<<<(n + 255) / 256, 256, 0, s>>>(dA, AtA, n, k, d_out);
-    c->launches += 2;
+    c->launches += 3;
     RFX_CUDA(cudaGetLastError());
     RFX_CUDA(cudaStreamSynchronize(s));
     return RFX_OK;
