@@ -216,6 +216,15 @@ typedef struct rfx_lowrank_opts {
 } rfx_lowrank_opts;
 rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* opts, float* A, float* evals);
 
+/* One product MV = M V of the low-rank path's operator M = P - I (P the
+ * finishprox proximity of the loaded forest, never formed) with a block V
+ * (n x w, w a multiple of 8 up to 120, row-major), computed as rfx_lowrank's
+ * range finder computes it (precision 0: FP32 storage, 1: BF16 storage of the
+ * sketch rows and leaf sums, FP32 accumulation).  No reference counterpart:
+ * it exposes the range finder's product so that callers (and tests) can apply
+ * M without the n x n matrix.  V and MV may be host or device pointers. */
+rfx_status rfx_lowrank_operator(rfx_ctx* ctx, int w, int precision, const float* V, float* MV);
+
 /* Quantised factors with one scale per column (format 1: INT8, q = round(A/s),
  * s = max|A[:,c]|/127; format 2: FP8 e4m3, s = max|A[:,c]|/448; format 3:
  * NF4, the reference's 16-level code of A/s with s = max|A[:,c]|, two codes

@@ -26,7 +26,7 @@ STATUS_NAMES = {0: "RFX_OK", 1: "RFX_ERR_INVALID", 2: "RFX_ERR_CUDA", 3: "RFX_ER
 # Every symbol include/rfx_b200.h declares (checked by the CPU tests).
 EXPORTS = ["rfx_last_error", "rfx_ctx_create", "rfx_ctx_destroy", "rfx_ctx_stream", "rfx_synchronize",
            "rfx_forest_load", "rfx_forest_load_device", "rfx_route_oob", "rfx_oob_summary", "rfx_proximity_upper_i32", "rfx_pair_updates",
-           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank",
+           "rfx_finishprox", "rfx_varimp", "rfx_localimp", "rfx_predict", "rfx_mds3d_full", "rfx_lowrank", "rfx_lowrank_operator",
            "rfx_lowrank_quantize", "rfx_mds_from_factors", "rfx_factor_mds_operator", "rfx_outlier_scores", "rfx_pair_counts_noalloc",
            "rfx_profile_enable", "rfx_profile_read", "rfx_grow_forest", "rfx_free_forest", "rfx_graph_capture_batch",
            "rfx_graph_launch", "rfx_graph_destroy", "rfx_tuned_shapes", "rfx_casewise_votes",
@@ -406,6 +406,14 @@ class Context:
         o = _LowrankOpts(rank=rank, oversample=oversample, power_iters=power_iters, precision=precision, seed=seed)
         _check(lib().rfx_lowrank(self._h, ctypes.byref(o), _vp(A), _vp(ev)))
         return A, ev
+
+    def lowrank_operator(self, V, precision=0):
+        """M V for the low-rank operator M = P - I (V: n x w float32, w a
+        multiple of 8 up to 120), as the range finder computes it."""
+        V = np.ascontiguousarray(V, dtype=np.float32)
+        MV = np.zeros_like(V)
+        _check(lib().rfx_lowrank_operator(self._h, int(V.shape[1]), int(precision), _vp(V), _vp(MV)))
+        return MV
 
     def lowrank_quantize(self, fmt):
         """fmt 1 = INT8, 2 = FP8 e4m3 (q: n x rank bytes), 3 = NF4 (q:

@@ -1172,6 +1172,51 @@ rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* o, float* A, float*
     return check_device_errors(c);
 }
 
+rfx_status rfx_lowrank_operator(rfx_ctx* ctx, int w, int precision, const float* V, float* MV) {
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    rfx_status st = need_forest(c);
+    if (st) return st;
+    if (!V || !MV) {
+        set_error("rfx_lowrank_operator: null argument");
+        return RFX_ERR_INVALID;
+    }
+    if (w < 8 || w > 120 || w % 8 != 0 || w > c->n || precision < 0 || precision > 1) {
+        set_error("rfx_lowrank_operator: w must be a multiple of 8 in 8..min(120, n) and precision 0 or 1");
+        return RFX_ERR_INVALID;
+    }
+    const size_t bytes = sizeof(float) * (size_t)c->n * w;
+    const float* dV = V;
+    float* sV = nullptr;
+    float* dMV = MV;
+    float* sMV = nullptr;
+    if (!is_device_ptr(V)) {
+        cudaError_t e = ctx_malloc(c, (void**)&sV, bytes);
+        if (e != cudaSuccess) return cuda_fail(e, "rfx_lowrank_operator staging");
+        e = cudaMemcpyAsync(sV, V, bytes, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) {
+            cudaFree(sV);
+            return cuda_fail(e, "rfx_lowrank_operator H2D");
+        }
+        dV = sV;
+    }
+    const bool mdev = is_device_ptr(MV);
+    if (!mdev) {
+        cudaError_t e = ctx_malloc(c, (void**)&sMV, bytes);
+        if (e != cudaSuccess) {
+            if (sV) cudaFree(sV);
+            return cuda_fail(e, "rfx_lowrank_operator staging");
+        }
+        dMV = sMV;
+    }
+    st = lowrank_compute(c, w, 0, 0, precision, 1ull, dMV, nullptr, dV);
+    if (st == RFX_OK && !mdev) st = copy_out(c, MV, dMV, bytes);
+    cudaStreamSynchronize(c->stream);
+    if (sV) cudaFree(sV);
+    if (sMV) cudaFree(sMV);
+    if (st) return st;
+    return check_device_errors(c);
+}
+
 rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     rfx_status st = need_forest(c);

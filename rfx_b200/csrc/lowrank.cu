@@ -22,6 +22,7 @@
 #include <cuda_fp8.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <type_traits>
 #include <cstdlib>
@@ -33,8 +34,6 @@
 namespace rfx {
 namespace {
 
-__device__ __forceinline__ float ld_val(const float* p) { return __ldg(p); }
-__device__ __forceinline__ float ld_val(const __nv_bfloat16* p) { return __bfloat162float(*p); }
 __device__ __forceinline__ void st_val(float* p, float v) { *p = v; }
 __device__ __forceinline__ void st_val(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 
@@ -186,13 +185,24 @@ __device__ __forceinline__ void add_partial(const float* in, int lane, bool c0ok
     }
 }
 
+// The warp first builds the chunk's key map without walking the keys one by
+// one: the tree's segment starts inside the chunk are read 32 at a time and
+// each marks its position (the largest key wins, so empty keys give way to
+// the key that holds the position), and a prefix maximum over the 64
+// positions gives every member its key.  The members' rows are then summed in
+// order with four row loads in flight, and a key's sum is written when its
+// last member in the chunk has been added.
 template <typename T, int E>
-__global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
-                              const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
-                              int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
-                              float* __restrict__ Pf, float* __restrict__ Pl, int32_t* __restrict__ fk) {
+__global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, int n, int W,
+                                                     const int32_t* __restrict__ memb,
+                                                     const int32_t* __restrict__ segoff,
+                                                     const int64_t* __restrict__ segbase, int t0, int t1, int cpt,
+                                                     const int64_t* __restrict__ gofs, T* __restrict__ G,
+                                                     float* __restrict__ Pf, float* __restrict__ Pl,
+                                                     int32_t* __restrict__ fk) {
+    __shared__ int keyat[8][SEG_CH];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     if (warp >= (int64_t)(t1 - t0) * cpt) return;
     const int tb = (int)(warp / cpt), ch = (int)(warp % cpt);
     const int t = t0 + tb;
@@ -205,6 +215,7 @@ __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32
         return;
     }
     const int ce = min(cs + SEG_CH, ntot);
+    const int cnt = ce - cs;
     // key holding position cs: the largest k with so[k] <= cs (so[0] = 0)
     int lo = 0, hi = K;
     while (hi - lo > 1) {
@@ -212,37 +223,87 @@ __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32
         if (__ldg(so + mid) <= cs) lo = mid;
         else hi = mid;
     }
-    int key = lo;
-    if (lane == 0) fk[warp] = key;
+    const int key0 = lo;
+    if (lane == 0) fk[warp] = key0;
+    // key map: keyat[p] = largest key starting at cs + p, -1 where none starts
+    int* ka = keyat[wl];
+    ka[lane] = -1;
+    ka[lane + 32] = -1;
+    __syncwarp();
+    int klast = key0;  // the key holding position ce - 1
+    for (int kb = key0 + 1; kb <= K; kb += 32) {
+        const int k = kb + lane;
+        const int st = k <= K ? __ldg(so + k) : INT_MAX;
+        const bool in = k < K && st < ce;  // key k starts inside the chunk (so[K] = ntot ends the keys)
+        if (in) atomicMax(ka + (st - cs), k);
+        const unsigned any = __ballot_sync(0xffffffffu, in);
+        if (any) klast = max(klast, kb + 31 - __clz(any));
+        if (__ballot_sync(0xffffffffu, st >= ce)) break;  // the starts are ascending: the rest lie beyond
+    }
+    __syncwarp();
+    // prefix maximum: key of positions lane and lane + 32
+    int ka0 = ka[lane], ka1 = ka[lane + 32];
+    if (lane == 0) ka0 = max(ka0, key0);
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, ka0, d);
+        if (lane >= d) ka0 = max(ka0, u);
+    }
+    ka1 = max(ka1, __shfl_sync(0xffffffffu, ka0, 31));
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, ka1, d);
+        if (lane >= d) ka1 = max(ka1, u);
+    }
+    // first key incomplete when it began before the chunk; last key
+    // incomplete when it runs past the chunk
+    const bool first_part = __ldg(so + key0) < cs;
+    const bool last_part = __ldg(so + klast + 1) > ce;
     const int32_t* mt = memb + (size_t)t * n;
     const int m0 = cs + lane < ce ? __ldg(mt + cs + lane) : 0;
     const int m1 = cs + 32 + lane < ce ? __ldg(mt + cs + 32 + lane) : 0;
     const int CH = W / E;
-    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
-    int pos = cs;
-    while (pos < ce) {
-        const int kbeg = __ldg(so + key), kend = __ldg(so + key + 1);
-        const int e = min(kend, ce);
-        float a0[E], a1[E];
+    // rows of at most 240 values: 8-value chunks never need a second lane pass
+    const bool c0ok = lane < CH, c1ok = E == 4 && lane + 32 < CH;
+    float a0[E], a1[E];
 #pragma unroll
-        for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
-#pragma unroll 4
-        for (int q = pos; q < e; ++q) {
-            const int r = q - cs;  // warp-uniform
-            const int j = __shfl_sync(0xffffffffu, r < 32 ? m0 : m1, r & 31);
-            add_row<T, E>(X + (size_t)j * W, lane, c0ok, c1ok, a0, a1);
+    for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
+    for (int q0 = 0; q0 < cnt; q0 += 4) {
+        float v0[4][E], v1[4][E];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int q = q0 + u;  // warp-uniform
+            const int j = __shfl_sync(0xffffffffu, q < 32 ? m0 : m1, q & 31);
+            const T* xr = X + (size_t)j * W;
+            if (q < cnt && c0ok) Chunk<T, E>::load(xr + lane * E, v0[u]);
+            if (q < cnt && c1ok) Chunk<T, E>::load(xr + (lane + 32) * E, v1[u]);
         }
-        if (kbeg >= cs && kend <= ce) {
-            store_row<T, E>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
-        } else if (pos == cs) {
-            store_partial<T, E>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
-        } else {
-            store_partial<T, E>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
-        }
-        pos = e;
-        if (pos < ce) {
-            ++key;
-            while (__ldg(so + key + 1) <= pos) ++key;  // skip empty keys; pos < ntot = so[K] bounds key < K
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int q = q0 + u;
+            if (q >= cnt) break;
+            if (c0ok)
+#pragma unroll
+                for (int e = 0; e < E; ++e) a0[e] += v0[u][e];
+            if (c1ok)
+#pragma unroll
+                for (int e = 0; e < E; ++e) a1[e] += v1[u][e];
+            const int kq = __shfl_sync(0xffffffffu, q < 32 ? ka0 : ka1, q & 31);
+            const int kn = q + 1 < cnt ? __shfl_sync(0xffffffffu, q + 1 < 32 ? ka0 : ka1, (q + 1) & 31) : -1;
+            if (kn != kq) {  // the last member of key kq in this chunk
+                // a key cut by a chunk edge leaves a partial: the chunk's
+                // first key in Pf, its last key in Pl (segsum_fix_kernel
+                // reads them so)
+                const bool cut = (kq == key0 && first_part) || (kq == klast && last_part);
+                if (!cut)
+                    store_row<T, E>(G + (size_t)(gofs[tb] + kq) * W, lane, c0ok, c1ok, a0, a1);
+                else if (kq == key0)
+                    store_partial<T, E>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+                else
+                    store_partial<T, E>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+#pragma unroll
+                for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
+            }
         }
     }
 }
@@ -349,37 +410,66 @@ __global__ void dinv_kernel(const int32_t* __restrict__ nout, int n, float* __re
 // G[w x w] (FP64) += X^T Y over rows; X, Y n x w FP32.  Block: 256 threads,
 // 64-row chunks, each thread accumulates (w*w)/256 entries.
 constexpr int GW = 128;  // maximum width
-__global__ void __launch_bounds__(256) gram_f32_kernel(const float* __restrict__ X, const float* __restrict__ Y,
-                                                       int n, int w, double* __restrict__ G) {
+
+// Per-CTA partial Gram matrices part[cta] = X^T Y over the CTA's rows (FP32
+// inputs, FP64 products and sums), w x w with w a multiple of 4: thread
+// (ta, tb) owns the 4 x 4 block of rows 4ta.. and columns 4tb.. of the
+// result; rows arrive in shared-memory tiles of 32.  gram_sum_w_kernel adds
+// the partials in CTA order (reproducible).
+constexpr int GRAM_CTAS = 296;
+__global__ void __launch_bounds__(1024) gram_f32_kernel(const float* __restrict__ X, const float* __restrict__ Y,
+                                                        int n, int w, double* __restrict__ part) {
     __shared__ float Xs[32][GW], Ys[32][GW];
-    const int tid = threadIdx.x;
-    const int ww = w * w;
-    double acc[64];
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int qw = w / 4;
+    const int ta = tid / qw, tb = tid % qw;
+    const bool own = tid < qw * qw;
+    double acc[4][4];
 #pragma unroll
-    for (int q = 0; q < 64; ++q) acc[q] = 0.0;
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
     for (int r0 = blockIdx.x * 32; r0 < n; r0 += gridDim.x * 32) {
-        for (int e = tid; e < 32 * w; e += 256) {
+        for (int e = tid; e < 32 * w; e += nth) {
             const int r = e / w, c = e % w;
             Xs[r][c] = (r0 + r < n) ? X[(size_t)(r0 + r) * w + c] : 0.0f;
             Ys[r][c] = (r0 + r < n) ? Y[(size_t)(r0 + r) * w + c] : 0.0f;
         }
         __syncthreads();
-#pragma unroll 1
-        for (int q = 0; q < 64; ++q) {
-            const int e = tid + q * 256;
-            if (e >= ww) break;
-            const int a = e / w, b = e % w;
-            double s = 0.0;
-            for (int r = 0; r < 32; ++r) s += (double)Xs[r][a] * (double)Ys[r][b];
-            acc[q] += s;
+        if (own) {
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) {
+                const float4 xa = *reinterpret_cast<const float4*>(&Xs[r][4 * ta]);
+                const float4 yb = *reinterpret_cast<const float4*>(&Ys[r][4 * tb]);
+                const double x[4] = {xa.x, xa.y, xa.z, xa.w}, y[4] = {yb.x, yb.y, yb.z, yb.w};
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[p][q] = fma(x[p], y[q], acc[p][q]);
+            }
         }
         __syncthreads();
     }
-    for (int q = 0; q < 64; ++q) {
-        const int e = tid + q * 256;
-        if (e >= ww) break;
-        atomicAdd(G + e, acc[q]);
+    if (own) {
+        double* pp = part + (size_t)blockIdx.x * w * w;
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) pp[(size_t)(4 * ta + p) * w + 4 * tb + q] = acc[p][q];
     }
+}
+
+// G[e] = sum over the partials, one warp per entry (lane l the partials l,
+// l + 32, ..., then a fixed shuffle tree)
+__global__ void gram_sum_w_kernel(const double* __restrict__ part, int nparts, int cnt, double* __restrict__ G) {
+    const int e = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (e >= cnt) return;
+    double v = 0.0;
+    for (int q = lane; q < nparts; q += 32) v += part[(size_t)q * cnt + e];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    if (lane == 0) G[e] = v;
 }
 
 // One CTA: T = L^{-T} for G = L L^T (w x w), in shared memory (dynamic).
@@ -398,19 +488,65 @@ __global__ void chol_inv_w_kernel(const double* __restrict__ G, int w, double* _
     }
 }
 
-// out[n x m] = X[n x w] T[w x m] (FP32 X, FP64 T)
-__global__ void right_mul_kernel(const float* __restrict__ X, const double* __restrict__ Tm, int n, int w, int m,
-                                 float* __restrict__ out) {
-    extern __shared__ double Ts[];
-    for (int e = threadIdx.x; e < w * m; e += blockDim.x) Ts[e] = Tm[e];
+// out[n x m] = X[n x w] T[w x m] (FP32 X, FP64 T and sums), m a multiple of
+// 4: a CTA takes 64 rows (staged in shared memory with T); thread (ra, cb)
+// owns the 4 x 4 block of rows 4ra.. and columns 4cb.. .
+constexpr int RM_ROWS = 64;
+__global__ void __launch_bounds__(1024) right_mul_kernel(const float* __restrict__ X, const double* __restrict__ Tm,
+                                                         int n, int w, int m, float* __restrict__ out) {
+    const int mp = (m + 3) & ~3;                                            // columns padded to 4
+    extern __shared__ double Ts[];                                          // w x mp
+    float* Xs = reinterpret_cast<float*>(Ts + (size_t)w * mp);             // RM_ROWS x (w + 1)
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int r0 = blockIdx.x * RM_ROWS;
+    for (int e = tid; e < w * mp; e += nth) {
+        const int kk = e / mp, c = e % mp;
+        Ts[e] = c < m ? Tm[(size_t)kk * m + c] : 0.0;
+    }
+    for (int e = tid; e < RM_ROWS * w; e += nth) {
+        const int r = e / w, c = e % w;
+        Xs[r * (w + 1) + c] = r0 + r < n ? X[(size_t)(r0 + r) * w + c] : 0.0f;
+    }
     __syncthreads();
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)n * m) return;
-    const int i = (int)(idx / m), c = (int)(idx % m);
-    double v = 0.0;
-    for (int k = 0; k < w; ++k) v += (double)X[(size_t)i * w + k] * Ts[k * m + c];
-    out[idx] = (float)v;
+    const int qm = mp / 4;
+    const int ra = tid / qm, cb = tid % qm;
+    if (ra >= RM_ROWS / 4) return;
+    double acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = 0.0;
+#pragma unroll 4
+    for (int kk = 0; kk < w; ++kk) {
+        double x[4], t[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) x[p] = Xs[(4 * ra + p) * (w + 1) + kk];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = Ts[(size_t)kk * mp + 4 * cb + q];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[p][q] = fma(x[p], t[q], acc[p][q]);
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int r = r0 + 4 * ra + p;
+        if (r >= n) continue;
+        if (mp == m) {
+            *reinterpret_cast<float4*>(out + (size_t)r * m + 4 * cb) =
+                make_float4((float)acc[p][0], (float)acc[p][1], (float)acc[p][2], (float)acc[p][3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (4 * cb + q < m) out[(size_t)r * m + 4 * cb + q] = (float)acc[p][q];
+        }
+    }
 }
+
+inline size_t right_mul_smem(int w, int m) {
+    return sizeof(double) * (size_t)w * ((m + 3) & ~3) + sizeof(float) * RM_ROWS * (size_t)(w + 1);
+}
+inline int right_mul_threads(int m) { return std::max(32, (RM_ROWS / 4) * (((m + 3) & ~3) / 4)); }
 
 // One CTA: eigen-decomposition of the symmetrised w x w H.
 __global__ void eig_w_kernel(const double* __restrict__ H, int w, double* __restrict__ evals,
@@ -425,9 +561,9 @@ __global__ void eig_w_kernel(const double* __restrict__ H, int w, double* __rest
         A[i * ld + j] = 0.5 * (H[i * w + j] + H[j * w + i]);
     }
     __syncthreads();
-    // the top k of w eigenpairs are kept: an absolute stop at 1e-15 of the
-    // largest eigenvalue
-    cta_jacobi(A, U, w, ld, 30, pairs, 1e-15);
+    // the top k of w eigenpairs are kept (and stored in FP32): an absolute
+    // stop at 1e-12 of the largest eigenvalue
+    cta_jacobi(A, U, w, ld, 30, pairs, 1e-12);
     for (int e = threadIdx.x; e < w * w; e += blockDim.x) evecs[e] = U[(e / w) * ld + (e % w)];
     for (int i = threadIdx.x; i < w; i += blockDim.x) evals[i] = A[i * ld + i];
 }
@@ -570,7 +706,7 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
 }
 
 rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int precision, uint64_t seed,
-                           float* d_A_out, float* h_evals) {
+                           float* d_A_out, float* h_evals, const float* d_apply_in) {
     cudaStream_t s = c->stream;
     const int n = c->n, T = c->T;
     const int w = (k + oversample + 7) / 8 * 8;  // rows of whole 16-byte chunks
@@ -667,24 +803,42 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
         return apply_m<__nv_bfloat16, __nv_bfloat16>(c, V, w, MV, dinv, (__nv_bfloat16*)X, (__nv_bfloat16*)G, Ybig,
                                                      batch_start, d_gofs, pref_at, Pf, Pl, fk);
     };
+    if (d_apply_in) {
+        // one product MV = M V of the block V (n x w) in the chosen storage
+        // form, into d_A_out (n x w)
+        if ((st = apply(d_apply_in, d_A_out, precision == 0 || precision == 2)) != RFX_OK) return st;
+        RFX_CUDA(cudaStreamSynchronize(s));
+        return RFX_OK;
+    }
     const size_t sm2 = 2 * (size_t)w * w * sizeof(double);
     RFX_CUDA(cudaFuncSetAttribute(chol_inv_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
     const size_t sm_eig = 2 * (size_t)w * (w + 1) * sizeof(double);
     RFX_CUDA(cudaFuncSetAttribute(eig_w_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_eig));
     RFX_CUDA(cudaFuncSetAttribute(right_mul_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * w * w)));
+                                  (int)right_mul_smem(GW, GW)));
+    const int gram_ctas = std::min(GRAM_CTAS, (n + 31) / 32);
+    const int gram_threads = std::max(32, (w / 4) * (w / 4));
+    double* gpart = d.get<double>((size_t)gram_ctas * w * w);
+    if (!gpart) {
+        set_error("rfx_lowrank: device allocation failed");
+        return RFX_ERR_OOM;
+    }
+    auto gram = [&](const float* Xa, const float* Ya) {
+        gram_f32_kernel<<<gram_ctas, gram_threads, 0, s>>>(Xa, Ya, n, w, gpart);
+        gram_sum_w_kernel<<<(unsigned)(((size_t)w * w * 32 + 255) / 256), 256, 0, s>>>(gpart, gram_ctas, w * w, Gm);
+    };
     auto orth = [&](const float* src, float* out) -> rfx_status {
         // CholeskyQR2 with FP64 Gram and FP64 triangular factors
         StageTimer stt(c, ST_LR_ORTH, 0);
         const float* cur = src;
         float* tmp = Z;
         for (int pass = 0; pass < 2; ++pass) {
-            RFX_CUDA(cudaMemsetAsync(Gm, 0, sizeof(double) * w * w, s));
-            gram_f32_kernel<<<std::min(1024, (n + 31) / 32), 256, 0, s>>>(cur, cur, n, w, Gm);
+            gram(cur, cur);
             chol_inv_w_kernel<<<1, 256, sm2, s>>>(Gm, w, Tm, bad);
             float* dst = pass == 0 ? tmp : out;
-            right_mul_kernel<<<nblk((int64_t)n * w), 256, sizeof(double) * w * w, s>>>(cur, Tm, n, w, w, dst);
-            c->launches += 3;
+            right_mul_kernel<<<(n + RM_ROWS - 1) / RM_ROWS, right_mul_threads(w), right_mul_smem(w, w), s>>>(
+                cur, Tm, n, w, w, dst);
+            c->launches += 4;
             RFX_CUDA(cudaGetLastError());
             cur = dst;
         }
@@ -700,10 +854,9 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     if ((st = orth(Yw, Q)) != RFX_OK) return st;
     // Rayleigh-Ritz projection; precision 2 recomputes this last product in FP32
     if ((st = apply(Q, Yw, !mixed || precision == 2)) != RFX_OK) return st;
-    RFX_CUDA(cudaMemsetAsync(Gm, 0, sizeof(double) * w * w, s));
-    gram_f32_kernel<<<std::min(1024, (n + 31) / 32), 256, 0, s>>>(Q, Yw, n, w, Gm);
+    gram(Q, Yw);
     eig_w_kernel<<<1, 256, sm_eig, s>>>(Gm, w, ev, U);
-    c->launches += 2;
+    c->launches += 3;
     RFX_CUDA(cudaGetLastError());
     std::vector<double> hev(w), hU((size_t)w * w);
     RFX_CUDA(cudaMemcpyAsync(hev.data(), ev, sizeof(double) * w, cudaMemcpyDeviceToHost, s));
@@ -727,7 +880,8 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
         for (int r = 0; r < w; ++r) Tk[(size_t)r * k + col] = hU[(size_t)r * w + idx[col]] * sc;
     }
     RFX_CUDA(cudaMemcpyAsync(Tm, Tk.data(), sizeof(double) * w * k, cudaMemcpyHostToDevice, s));
-    right_mul_kernel<<<nblk((int64_t)n * k), 256, sizeof(double) * w * k, s>>>(Q, Tm, n, w, k, d_A_out);
+    right_mul_kernel<<<(n + RM_ROWS - 1) / RM_ROWS, right_mul_threads(k), right_mul_smem(w, k), s>>>(Q, Tm, n, w, k,
+                                                                                                   d_A_out);
     c->launches += 1;
     RFX_CUDA(cudaGetLastError());
     RFX_CUDA(cudaStreamSynchronize(s));

@@ -55,6 +55,20 @@ def best_err(M, k):
     return rel_err(M, A)
 
 
+@pytest.mark.parametrize("w", [8, 40, 80])
+def test_range_finder_operator_matches_dense(setup, w):
+    """One product of the range finder (leaf sums through the member lists,
+    sums back to the samples) against the dense FP64 M V: FP32 storage to
+    1e-5 relative, BF16 storage to 1e-2."""
+    ctx, f, P, M = setup
+    V = np.random.default_rng(w).standard_normal((f.n, w)).astype(np.float32)
+    ref = M @ V.astype(np.float64)
+    nr = np.linalg.norm(ref)
+    for prec, tol in ((0, 1e-5), (1, 1e-2)):
+        MV = ctx.lowrank_operator(V, precision=prec)
+        assert np.linalg.norm(MV.astype(np.float64) - ref) <= tol * nr, (prec, w)
+
+
 @pytest.mark.parametrize("k", [8, 24])
 def test_factor_error_near_optimal(setup, k):
     ctx, f, P, M = setup
