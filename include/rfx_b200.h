@@ -204,7 +204,8 @@ rfx_status rfx_mds3d_full(rfx_ctx* ctx, const float* P, double* coords, double* 
  * power_iters power iterations, CholeskyQR2 in FP64, FP64
  * Rayleigh-Ritz).  precision 0 = FP32 throughout; 1 = BF16 storage of the
  * sketch inputs and leaf sums with FP32 accumulation; 2 = as 1 with the last
- * product (the Rayleigh-Ritz projection) in FP32.
+ * product (the Rayleigh-Ritz projection) in FP32; 3 = FP8 e4m3 storage of the
+ * sketch rows and leaf sums, one FP32 scale per row, FP32 accumulation.
  * The context keeps the factors for the calls below; A and evals (host, the
  * rank eigenvalues) may be NULL. */
 typedef struct rfx_lowrank_opts {
@@ -220,7 +221,8 @@ rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* opts, float* A, flo
  * finishprox proximity of the loaded forest, never formed) with a block V
  * (n x w, w a multiple of 8 up to 120, row-major), computed as rfx_lowrank's
  * range finder computes it (precision 0: FP32 storage, 1: BF16 storage of the
- * sketch rows and leaf sums, FP32 accumulation).  No reference counterpart:
+ * sketch rows and leaf sums, 3: FP8 e4m3 rows with a scale each; FP32
+ * accumulation).  No reference counterpart:
  * it exposes the range finder's product so that callers (and tests) can apply
  * M without the n x n matrix.  V and MV may be host or device pointers. */
 rfx_status rfx_lowrank_operator(rfx_ctx* ctx, int w, int precision, const float* V, float* MV);

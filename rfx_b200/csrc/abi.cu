@@ -1147,7 +1147,8 @@ rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* o, float* A, float*
     if (st) return st;
     if (!o) return RFX_ERR_INVALID;
     const int k = o->rank;
-    if (k < 1 || o->oversample < 0 || o->power_iters < 0 || o->power_iters > 8) {
+    if (k < 1 || o->oversample < 0 || o->power_iters < 0 || o->power_iters > 8 || o->precision < 0 ||
+        o->precision > 3) {
         set_error("rfx_lowrank: invalid options");
         return RFX_ERR_INVALID;
     }
@@ -1180,8 +1181,8 @@ rfx_status rfx_lowrank_operator(rfx_ctx* ctx, int w, int precision, const float*
         set_error("rfx_lowrank_operator: null argument");
         return RFX_ERR_INVALID;
     }
-    if (w < 8 || w > 120 || w % 8 != 0 || w > c->n || precision < 0 || precision > 1) {
-        set_error("rfx_lowrank_operator: w must be a multiple of 8 in 8..min(120, n) and precision 0 or 1");
+    if (w < 8 || w > 120 || w % 8 != 0 || w > c->n || (precision != 0 && precision != 1 && precision != 3)) {
+        set_error("rfx_lowrank_operator: w must be a multiple of 8 in 8..min(120, n) and precision 0, 1 or 3");
         return RFX_ERR_INVALID;
     }
     const size_t bytes = sizeof(float) * (size_t)c->n * w;

@@ -15,7 +15,9 @@
 //   FP32  - X, leaf sums and products in FP32;
 //   mixed - X and leaf sums stored in BF16, FP32 accumulation (precision 1);
 //           precision 2 also recomputes the last product M Q, which builds the
-//           Rayleigh-Ritz projection, in FP32.
+//           Rayleigh-Ritz projection, in FP32; precision 3 stores X and the
+//           leaf sums as FP8 e4m3 rows, each with its own FP32 scale (the
+//           row's largest magnitude maps to 448), FP32 accumulation.
 // FP64 is used for the k' x k' Gram (CholeskyQR2) and the eigensolve only.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -123,6 +125,66 @@ struct Chunk<__nv_bfloat16, 4> {
     }
 };
 
+// FP8 e4m3 rows (precision 3): 8 codes per lane chunk; the row's FP32 scale
+// lives beside it (values = code x scale).
+template <>
+struct Chunk<uint8_t, 8> {
+    __device__ static void load(const uint8_t* p, float* v) {
+        const uint2 x = __ldg(reinterpret_cast<const uint2*>(p));
+        const uint32_t w[2] = {x.x, x.y};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2(
+                    (__nv_fp8x2_storage_t)((w[h] >> (16 * q)) & 0xffffu), __NV_E4M3);
+                const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&hr));
+                v[4 * h + 2 * q] = f.x;
+                v[4 * h + 2 * q + 1] = f.y;
+            }
+        }
+    }
+    __device__ static void store(uint8_t* p, const float* v) {
+        uint32_t w[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t lo = __nv_cvt_float2_to_fp8x2(make_float2(v[4 * h], v[4 * h + 1]), __NV_SATFINITE, __NV_E4M3);
+            const uint32_t hi =
+                __nv_cvt_float2_to_fp8x2(make_float2(v[4 * h + 2], v[4 * h + 3]), __NV_SATFINITE, __NV_E4M3);
+            w[h] = lo | (hi << 16);
+        }
+        *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
+    }
+};
+
+template <typename T>
+constexpr bool is_fp8() { return std::is_same<T, uint8_t>::value; }
+
+// X = [V | D V] as FP8 rows with one scale per row (448 = the largest e4m3
+// value maps to the row's largest magnitude); one warp per row.
+__global__ void pack_x_fp8_kernel(const float* __restrict__ V, const float* __restrict__ dinv, int n, int w,
+                                  uint8_t* __restrict__ X, float* __restrict__ xs) {
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const int i = (int)warp;
+    const float di = dinv[i];
+    float amax = 0.0f;
+    for (int c = lane; c < w; c += 32) amax = fmaxf(amax, fmaxf(fabsf(V[(size_t)i * w + c]), fabsf(V[(size_t)i * w + c] * di)));
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, d));
+    const float sc = amax > 0.0f ? 448.0f / amax : 1.0f;
+    for (int c = lane; c < w; c += 32) {
+        const float v = V[(size_t)i * w + c];
+        X[(size_t)i * 2 * w + c] = (uint8_t)(__nv_cvt_float2_to_fp8x2(make_float2(v * sc, 0.0f), __NV_SATFINITE,
+                                                                      __NV_E4M3) & 0xffu);
+        X[(size_t)i * 2 * w + w + c] = (uint8_t)(__nv_cvt_float2_to_fp8x2(
+                                                     make_float2(__fmul_rn(v, di) * sc, 0.0f), __NV_SATFINITE,
+                                                     __NV_E4M3) & 0xffu);
+    }
+    if (lane == 0) xs[i] = 1.0f / sc;
+}
+
 // Leaf-key sums of X rows for trees [t0, t1): G[gofs[t-t0] + key][:] = sum
 // over members j of key of X[j][:].  The member list of each tree (keys in
 // order, members of a key contiguous) is cut into chunks of SEG_CH positions,
@@ -153,6 +215,36 @@ template <typename TO, int E>
 __device__ __forceinline__ void store_row(TO* out, int lane, bool c0ok, bool c1ok, const float* a0, const float* a1) {
     if (c0ok) Chunk<TO, E>::store(out + lane * E, a0);
     if (c1ok) Chunk<TO, E>::store(out + (lane + 32) * E, a1);
+}
+
+// A finished G row: FP8 rows get their own scale (the warp's largest
+// magnitude maps to 448), written beside the row; other types store as is.
+// Called by the whole warp.
+template <typename TO, int E>
+__device__ __forceinline__ void store_grow(TO* out, float* scale_out, int lane, bool c0ok, bool c1ok, const float* a0,
+                                           const float* a1) {
+    if constexpr (is_fp8<TO>()) {
+        float amax = 0.0f;
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            if (c0ok) amax = fmaxf(amax, fabsf(a0[e]));
+            if (c1ok) amax = fmaxf(amax, fabsf(a1[e]));
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, d));
+        const float sc = amax > 0.0f ? 448.0f / amax : 1.0f;
+        float b0[E], b1[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            b0[e] = a0[e] * sc;
+            b1[e] = a1[e] * sc;
+        }
+        store_row<TO, E>(out, lane, c0ok, c1ok, b0, b1);
+        if (lane == 0) *scale_out = 1.0f / sc;
+    } else {
+        (void)scale_out;
+        store_row<TO, E>(out, lane, c0ok, c1ok, a0, a1);
+    }
 }
 
 // FP32 partial rows use 4-float chunks; a lane chunk of E values is stored as
@@ -199,7 +291,8 @@ __global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, in
                                                      const int64_t* __restrict__ segbase, int t0, int t1, int cpt,
                                                      const int64_t* __restrict__ gofs, T* __restrict__ G,
                                                      float* __restrict__ Pf, float* __restrict__ Pl,
-                                                     int32_t* __restrict__ fk) {
+                                                     int32_t* __restrict__ fk, const float* __restrict__ xs,
+                                                     float* __restrict__ gs) {
     __shared__ int keyat[8][SEG_CH];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
@@ -269,12 +362,14 @@ __global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, in
 #pragma unroll
     for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
     for (int q0 = 0; q0 < cnt; q0 += 4) {
-        float v0[4][E], v1[4][E];
+        float v0[4][E], v1[4][E], sc[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int q = q0 + u;  // warp-uniform
             const int j = __shfl_sync(0xffffffffu, q < 32 ? m0 : m1, q & 31);
             const T* xr = X + (size_t)j * W;
+            sc[u] = 1.0f;
+            if constexpr (is_fp8<T>()) sc[u] = q < cnt ? __ldg(xs + j) : 0.0f;
             if (q < cnt && c0ok) Chunk<T, E>::load(xr + lane * E, v0[u]);
             if (q < cnt && c1ok) Chunk<T, E>::load(xr + (lane + 32) * E, v1[u]);
         }
@@ -284,10 +379,10 @@ __global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, in
             if (q >= cnt) break;
             if (c0ok)
 #pragma unroll
-                for (int e = 0; e < E; ++e) a0[e] += v0[u][e];
+                for (int e = 0; e < E; ++e) a0[e] = is_fp8<T>() ? fmaf(v0[u][e], sc[u], a0[e]) : a0[e] + v0[u][e];
             if (c1ok)
 #pragma unroll
-                for (int e = 0; e < E; ++e) a1[e] += v1[u][e];
+                for (int e = 0; e < E; ++e) a1[e] = is_fp8<T>() ? fmaf(v1[u][e], sc[u], a1[e]) : a1[e] + v1[u][e];
             const int kq = __shfl_sync(0xffffffffu, q < 32 ? ka0 : ka1, q & 31);
             const int kn = q + 1 < cnt ? __shfl_sync(0xffffffffu, q + 1 < 32 ? ka0 : ka1, (q + 1) & 31) : -1;
             if (kn != kq) {  // the last member of key kq in this chunk
@@ -296,7 +391,7 @@ __global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, in
                 // reads them so)
                 const bool cut = (kq == key0 && first_part) || (kq == klast && last_part);
                 if (!cut)
-                    store_row<T, E>(G + (size_t)(gofs[tb] + kq) * W, lane, c0ok, c1ok, a0, a1);
+                    store_grow<T, E>(G + (size_t)(gofs[tb] + kq) * W, gs + gofs[tb] + kq, lane, c0ok, c1ok, a0, a1);
                 else if (kq == key0)
                     store_partial<T, E>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
                 else
@@ -314,7 +409,7 @@ template <typename T, int E>
 __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase,
                                   int t0, int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
                                   const float* __restrict__ Pf, const float* __restrict__ Pl,
-                                  const int32_t* __restrict__ fk) {
+                                  const int32_t* __restrict__ fk, float* __restrict__ gs) {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= (int64_t)(t1 - t0) * cpt) return;
@@ -334,14 +429,15 @@ __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ sego
     add_partial<T, E>((kbeg == cs - SEG_CH ? Pf : Pl) + (size_t)(warp - 1) * W, lane, c0ok, c1ok, a0, a1);
     for (int c2 = ch; c2 * SEG_CH < kend; ++c2)
         add_partial<T, E>(Pf + (size_t)(warp - ch + c2) * W, lane, c0ok, c1ok, a0, a1);
-    store_row<T, E>(G + (size_t)(gofs[tb] + key) * W, lane, c0ok, c1ok, a0, a1);
+    store_grow<T, E>(G + (size_t)(gofs[tb] + key) * W, gs + gofs[tb] + key, lane, c0ok, c1ok, a0, a1);
 }
 
 // Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample,
 // 16-byte chunks per lane, 32 trees' keys fetched at once.
 template <typename T, int E>
 __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
-                            const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate) {
+                            const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate,
+                            const float* __restrict__ gs) {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
@@ -365,15 +461,24 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
             if (r < 0) continue;
             const T* gr = G + (size_t)r * W;
             float v[E];
-            if (c0ok) {
-                Chunk<T, E>::load(gr + lane * E, v);
+            if constexpr (is_fp8<T>()) {
+                const float sc = __ldg(gs + r);
+                if (c0ok) {
+                    Chunk<T, E>::load(gr + lane * E, v);
 #pragma unroll
-                for (int e = 0; e < E; ++e) a0[e] += v[e];
-            }
-            if (c1ok) {
-                Chunk<T, E>::load(gr + (lane + 32) * E, v);
+                    for (int e = 0; e < E; ++e) a0[e] = fmaf(v[e], sc, a0[e]);
+                }
+            } else {
+                if (c0ok) {
+                    Chunk<T, E>::load(gr + lane * E, v);
 #pragma unroll
-                for (int e = 0; e < E; ++e) a1[e] += v[e];
+                    for (int e = 0; e < E; ++e) a0[e] += v[e];
+                }
+                if (c1ok) {
+                    Chunk<T, E>::load(gr + (lane + 32) * E, v);
+#pragma unroll
+                    for (int e = 0; e < E; ++e) a1[e] += v[e];
+                }
             }
         }
     }
@@ -663,11 +768,14 @@ inline unsigned nblk(int64_t count, int b = 256) { return (unsigned)((count + b 
 template <typename TX, typename TG>
 rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, TX* X, TG* G, float* Y,
                    const std::vector<int64_t>& batch_start, int64_t* d_gofs, const std::vector<int64_t>& h_gofs_all,
-                   float* Pf, float* Pl, int32_t* fk) {
+                   float* Pf, float* Pl, int32_t* fk, float* xs = nullptr, float* gs = nullptr) {
     cudaStream_t s = c->stream;
     const int n = c->n, W = 2 * w;
     StageTimer stt(c, ST_LR_PRODUCT, 0);
-    pack_x_kernel<TX><<<nblk((int64_t)n * w), 256, 0, s>>>(V, dinv, n, w, X);
+    if constexpr (is_fp8<TX>())
+        pack_x_fp8_kernel<<<nblk((int64_t)n * 32), 256, 0, s>>>(V, dinv, n, w, X, xs);
+    else
+        pack_x_kernel<TX><<<nblk((int64_t)n * w), 256, 0, s>>>(V, dinv, n, w, X);
     RFX_CUDA(cudaGetLastError());
     c->launches += 1;
     for (size_t b = 0; b + 1 < batch_start.size(); ++b) {
@@ -681,17 +789,20 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
         const int cpt = (n + SEG_CH - 1) / SEG_CH;
         const int64_t chunks = (int64_t)(t1 - t0) * cpt;
         RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(TG) * (size_t)total_keys * W, s));
+        if constexpr (is_fp8<TG>()) RFX_CUDA(cudaMemsetAsync(gs, 0, sizeof(float) * (size_t)total_keys, s));
         auto run = [&](auto e_tag) {
             constexpr int E = decltype(e_tag)::value;
             segsum_kernel<TX, E><<<nblk(chunks * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0,
-                                                                   t1, cpt, gofs, G, Pf, Pl, fk);
+                                                                   t1, cpt, gofs, G, Pf, Pl, fk, xs, gs);
             segsum_fix_kernel<TG, E><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt,
-                                                                       gofs, G, Pf, Pl, fk);
-            pull_kernel<TG, E><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0);
+                                                                       gofs, G, Pf, Pl, fk, gs);
+            pull_kernel<TG, E><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0, gs);
         };
         // BF16 rows narrower than 32 16-byte chunks use 8-byte chunks, so more lanes carry data
         if constexpr (std::is_same<TX, float>::value) {
             run(std::integral_constant<int, 4>{});
+        } else if constexpr (is_fp8<TX>()) {
+            run(std::integral_constant<int, 8>{});
         } else {
             if (W / 8 > 16) run(std::integral_constant<int, 8>{});
             else run(std::integral_constant<int, 4>{});
@@ -726,7 +837,8 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     const int W = 2 * w;
     // tree batches: leaf sums of up to 4 GB per batch (fewer passes over the
     // n x 2w accumulator beat L2-sized batches; RFX_LR_BATCH_MB overrides)
-    const size_t gbytes_row = (size_t)W * (precision ? 2 : 4);
+    const bool f8 = precision == 3;  // FP8 e4m3 rows with one scale each
+    const size_t gbytes_row = f8 ? (size_t)W + 4 : (size_t)W * (precision ? 2 : 4);
     size_t batch_budget = (size_t)4 << 30;
     if (const char* e = std::getenv("RFX_LR_BATCH_MB")) {
         const long v = std::atol(e);
@@ -775,9 +887,13 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     double* ev = d.get<double>(w);
     double* U = d.get<double>((size_t)w * w);
     int* bad = d.get<int>(1);
-    void* X = precision ? (void*)d.get<__nv_bfloat16>((size_t)n * W) : (void*)d.get<float>((size_t)n * W);
-    void* G = precision ? (void*)d.get<__nv_bfloat16>((size_t)max_batch_keys * W)
-                        : (void*)d.get<float>((size_t)max_batch_keys * W);
+    void* X = f8 ? (void*)d.get<uint8_t>((size_t)n * W)
+              : precision ? (void*)d.get<__nv_bfloat16>((size_t)n * W) : (void*)d.get<float>((size_t)n * W);
+    void* G = f8 ? (void*)d.get<uint8_t>((size_t)max_batch_keys * W)
+              : precision ? (void*)d.get<__nv_bfloat16>((size_t)max_batch_keys * W)
+                          : (void*)d.get<float>((size_t)max_batch_keys * W);
+    float* xs = f8 ? d.get<float>(n) : nullptr;
+    float* gs = f8 ? d.get<float>((size_t)max_batch_keys) : nullptr;
     void* X32 = precision == 2 ? (void*)d.get<float>((size_t)n * W) : X;
     void* G32 = precision == 2 ? (void*)d.get<float>((size_t)max_batch_keys * W) : G;
     const size_t nchunks = (size_t)max_batch_trees * ((n + SEG_CH - 1) / SEG_CH);
@@ -785,7 +901,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     float* Pl = d.get<float>(nchunks * W);
     int32_t* fk = d.get<int32_t>(nchunks);
     if (!dinv || !Om || !Yw || !Q || !Z || !Ybig || !d_gofs || !Gm || !Tm || !ev || !U || !bad || !X || !G || !X32 ||
-        !G32 || !Pf || !Pl || !fk) {
+        !G32 || !Pf || !Pl || !fk || (f8 && (!xs || !gs))) {
         set_error("rfx_lowrank: device allocation failed");
         return RFX_ERR_OOM;
     }
@@ -800,6 +916,9 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
         if (fp32)
             return apply_m<float, float>(c, V, w, MV, dinv, (float*)X32, (float*)G32, Ybig, batch_start, d_gofs,
                                          pref_at, Pf, Pl, fk);
+        if (f8)
+            return apply_m<uint8_t, uint8_t>(c, V, w, MV, dinv, (uint8_t*)X, (uint8_t*)G, Ybig, batch_start, d_gofs,
+                                             pref_at, Pf, Pl, fk, xs, gs);
         return apply_m<__nv_bfloat16, __nv_bfloat16>(c, V, w, MV, dinv, (__nv_bfloat16*)X, (__nv_bfloat16*)G, Ybig,
                                                      batch_start, d_gofs, pref_at, Pf, Pl, fk);
     };
