@@ -378,7 +378,11 @@ def run_lowrank(args):
     ctx.load(f, X, y)
     ctx.route_oob()
 
-    phases = {0: {}, 1: {}}
+    # forms: 0 = FP32, 1 = mixed with BF16 sketch storage, 3 = mixed with FP8
+    # e4m3 sketch storage (both mixed forms run the factor-MDS products on
+    # the tensor cores with one FP32 refinement step)
+    forms = (0, 1, 3)
+    phases = {p: {} for p in forms}
 
     def run(precision):
         torch.cuda.synchronize()
@@ -403,15 +407,16 @@ def run_lowrank(args):
         return t4 - t, A, C, o
 
     run(1)  # warm-up (module load, allocations; builds the leaf keys and member lists once)
-    run(0)
     once_ms = {key: phases[1][key] for key in ("route_ms", "leaf_lists_ms")}
-    times = {0: [], 1: []}
-    best = {0: None, 1: None}
+    run(0)
+    run(3)
+    times = {p: [] for p in forms}
+    best = {p: None for p in forms}
     res = {}
     clocks = Clocks(0)
     clocks.start()
     for rep in range(max(1, args.steps)):
-        for prec in (0, 1):
+        for prec in forms:
             dt, A, C, o = run(prec)
             times[prec].append(dt)
             res[prec] = (A, C, o)
@@ -447,7 +452,7 @@ def run_lowrank(args):
         R.fill_diagonal_(0.0)
         return float(torch.linalg.norm(R)) / nrm
 
-    for prec in (0, 1):
+    for prec in forms:
         errs[prec] = sub_err(res[prec][0])
     # rank truncation against algorithm error: the best rank-k approximation of
     # the subsample's own exact matrix (top-k positive eigenpairs, FP64) in the
@@ -470,16 +475,24 @@ def run_lowrank(args):
     for q_it in (1, 2, 3):
         Aq, _ = ctx.lowrank(k, oversample=16, power_iters=q_it, precision=0)
         sweep[str(q_it)] = sub_err(Aq)
-    C32, Cm = res[0][1], res[1][1]
-    U, _, Vt = np.linalg.svd(Cm.T @ C32)
-    proc = float(np.sqrt(np.mean((Cm @ (U @ Vt) - C32) ** 2)) / np.sqrt(np.mean(C32 ** 2)))
+    def procrustes(Cm, C32):
+        U, _, Vt = np.linalg.svd(Cm.T @ C32)
+        return float(np.sqrt(np.mean((Cm @ (U @ Vt) - C32) ** 2)) / np.sqrt(np.mean(C32 ** 2)))
+
+    procs = {p: procrustes(res[p][1], res[0][1]) for p in (1, 3)}
     ctx_s.close()
     ctx.close()
-    t32, tmx = min(times[0]), min(times[1])
+    t32 = min(times[0])
+    # the headline mixed form: the faster of the two whose factor error is
+    # the FP32 form's to 1 % (relative)
+    same = [p for p in (1, 3) if abs(errs[p] - errs[0]) <= 0.01 * errs[0]]
+    mix = min(same, key=lambda p: min(times[p])) if same else 1
+    tmx = min(times[mix])
+    proc = procs[mix]
     qname = "FP8 e4m3" if fmt == 2 else "INT8"
     line = {"metric": f"n={n // 1000}K rank-{k} prox+MDS sec, mixed vs FP32 form @same err", "value": tmx,
             "unit": "s", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
-            "dtype": "bf16+fp32 (mixed) / fp32", "data": f"synthetic ({gen})",
+            "dtype": ("fp8+fp32" if mix == 3 else "bf16+fp32") + " (mixed) / fp32", "data": f"synthetic ({gen})",
             "config": {"workload": f"low-rank proximity + 3D MDS{' + outlier scores' if large else ''}: n={n} "
                                    f"p={X.shape[1]} c={nclass} ntree={T} mtry={mtry} nodesize={minnd} rank={k} "
                                    f"oversample=16 power_iters=1, {qname} per-column factors",
@@ -488,7 +501,11 @@ def run_lowrank(args):
                                 f"{', outlier scores' if large else ''}; leaf keys and member lists are built once "
                                 "per loaded forest (per_forest_once_ms)"},
             "fp32_seconds": t32, "mixed_seconds": tmx, "speedup_mixed_vs_fp32": t32 / tmx,
-            "rel_frobenius_err_fp32": errs[0], "rel_frobenius_err_mixed": errs[1],
+            "mixed_form": "FP8 e4m3 sketch storage" if mix == 3 else "BF16 sketch storage",
+            "rel_frobenius_err_fp32": errs[0], "rel_frobenius_err_mixed": errs[mix],
+            "mixed_bf16_seconds": min(times[1]), "mixed_fp8_seconds": min(times[3]),
+            "rel_frobenius_err_mixed_bf16": errs[1], "rel_frobenius_err_mixed_fp8": errs[3],
+            "mds_procrustes_rel_mixed_bf16_vs_fp32": procs[1], "mds_procrustes_rel_mixed_fp8_vs_fp32": procs[3],
             "err_subsample_rows": m, "rel_frobenius_err_best_rank_k_on_subsample": floor_k,
             "rank_for_1e-2_on_subsample_eigen_tail": rank_1e2,
             "rel_frobenius_err_fp32_by_power_iters": sweep,
@@ -497,9 +514,10 @@ def run_lowrank(args):
                          "bound for any rank-k factors restricted to the subsample); rank_for_1e-2 from the "
                          "eigenvalue tail (diagonal kept)"),
             "mds_procrustes_rel_mixed_vs_fp32": proc,
-            "phases_fp32": phases[0], "phases_mixed": phases[1]}
+            "phases_fp32": phases[0], "phases_mixed": phases[mix], "phases_mixed_bf16": phases[1],
+            "phases_mixed_fp8": phases[3]}
     if large:
-        o = res[1][2]
+        o = res[mix][2]
         top = np.argsort(-o)[: len(outl)]
         line["outlier_recall_top1pct"] = float(np.isin(top, outl).mean())
     if clk:
