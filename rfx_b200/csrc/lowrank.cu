@@ -196,18 +196,19 @@ __global__ void pack_x_fp8_kernel(const float* __restrict__ V, const float* __re
 // must be zero beforehand.
 constexpr int SEG_CH = 64;
 
+// adds the row (times its scale sc, for FP8 rows) to the lane's sums
 template <typename T, int E>
-__device__ __forceinline__ void add_row(const T* xr, int lane, bool c0ok, bool c1ok, float* a0, float* a1) {
+__device__ __forceinline__ void add_row(const T* xr, float sc, int lane, bool c0ok, bool c1ok, float* a0, float* a1) {
     float v[E];
     if (c0ok) {
         Chunk<T, E>::load(xr + lane * E, v);
 #pragma unroll
-        for (int e = 0; e < E; ++e) a0[e] += v[e];
+        for (int e = 0; e < E; ++e) a0[e] = is_fp8<T>() ? fmaf(v[e], sc, a0[e]) : a0[e] + v[e];
     }
     if (c1ok) {
         Chunk<T, E>::load(xr + (lane + 32) * E, v);
 #pragma unroll
-        for (int e = 0; e < E; ++e) a1[e] += v[e];
+        for (int e = 0; e < E; ++e) a1[e] = is_fp8<T>() ? fmaf(v[e], sc, a1[e]) : a1[e] + v[e];
     }
 }
 
@@ -277,25 +278,14 @@ __device__ __forceinline__ void add_partial(const float* in, int lane, bool c0ok
     }
 }
 
-// The warp first builds the chunk's key map without walking the keys one by
-// one: the tree's segment starts inside the chunk are read 32 at a time and
-// each marks its position (the largest key wins, so empty keys give way to
-// the key that holds the position), and a prefix maximum over the 64
-// positions gives every member its key.  The members' rows are then summed in
-// order with four row loads in flight, and a key's sum is written when its
-// last member in the chunk has been added.
 template <typename T, int E>
-__global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, int n, int W,
-                                                     const int32_t* __restrict__ memb,
-                                                     const int32_t* __restrict__ segoff,
-                                                     const int64_t* __restrict__ segbase, int t0, int t1, int cpt,
-                                                     const int64_t* __restrict__ gofs, T* __restrict__ G,
-                                                     float* __restrict__ Pf, float* __restrict__ Pl,
-                                                     int32_t* __restrict__ fk, const float* __restrict__ xs,
-                                                     float* __restrict__ gs) {
-    __shared__ int keyat[8][SEG_CH];
+__global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
+                              const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
+                              int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
+                              float* __restrict__ Pf, float* __restrict__ Pl, int32_t* __restrict__ fk,
+                              const float* __restrict__ xs, float* __restrict__ gs) {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     if (warp >= (int64_t)(t1 - t0) * cpt) return;
     const int tb = (int)(warp / cpt), ch = (int)(warp % cpt);
     const int t = t0 + tb;
@@ -308,7 +298,6 @@ __global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, in
         return;
     }
     const int ce = min(cs + SEG_CH, ntot);
-    const int cnt = ce - cs;
     // key holding position cs: the largest k with so[k] <= cs (so[0] = 0)
     int lo = 0, hi = K;
     while (hi - lo > 1) {
@@ -316,89 +305,37 @@ __global__ void __launch_bounds__(256) segsum_kernel(const T* __restrict__ X, in
         if (__ldg(so + mid) <= cs) lo = mid;
         else hi = mid;
     }
-    const int key0 = lo;
-    if (lane == 0) fk[warp] = key0;
-    // key map: keyat[p] = largest key starting at cs + p, -1 where none starts
-    int* ka = keyat[wl];
-    ka[lane] = -1;
-    ka[lane + 32] = -1;
-    __syncwarp();
-    int klast = key0;  // the key holding position ce - 1
-    for (int kb = key0 + 1; kb <= K; kb += 32) {
-        const int k = kb + lane;
-        const int st = k <= K ? __ldg(so + k) : INT_MAX;
-        const bool in = k < K && st < ce;  // key k starts inside the chunk (so[K] = ntot ends the keys)
-        if (in) atomicMax(ka + (st - cs), k);
-        const unsigned any = __ballot_sync(0xffffffffu, in);
-        if (any) klast = max(klast, kb + 31 - __clz(any));
-        if (__ballot_sync(0xffffffffu, st >= ce)) break;  // the starts are ascending: the rest lie beyond
-    }
-    __syncwarp();
-    // prefix maximum: key of positions lane and lane + 32
-    int ka0 = ka[lane], ka1 = ka[lane + 32];
-    if (lane == 0) ka0 = max(ka0, key0);
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, ka0, d);
-        if (lane >= d) ka0 = max(ka0, u);
-    }
-    ka1 = max(ka1, __shfl_sync(0xffffffffu, ka0, 31));
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, ka1, d);
-        if (lane >= d) ka1 = max(ka1, u);
-    }
-    // first key incomplete when it began before the chunk; last key
-    // incomplete when it runs past the chunk
-    const bool first_part = __ldg(so + key0) < cs;
-    const bool last_part = __ldg(so + klast + 1) > ce;
+    int key = lo;
+    if (lane == 0) fk[warp] = key;
     const int32_t* mt = memb + (size_t)t * n;
     const int m0 = cs + lane < ce ? __ldg(mt + cs + lane) : 0;
     const int m1 = cs + 32 + lane < ce ? __ldg(mt + cs + 32 + lane) : 0;
     const int CH = W / E;
-    // rows of at most 240 values: 8-value chunks never need a second lane pass
-    const bool c0ok = lane < CH, c1ok = E == 4 && lane + 32 < CH;
-    float a0[E], a1[E];
+    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
+    int pos = cs;
+    while (pos < ce) {
+        const int kbeg = __ldg(so + key), kend = __ldg(so + key + 1);
+        const int e = min(kend, ce);
+        float a0[E], a1[E];
 #pragma unroll
-    for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
-    for (int q0 = 0; q0 < cnt; q0 += 4) {
-        float v0[4][E], v1[4][E], sc[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int q = q0 + u;  // warp-uniform
-            const int j = __shfl_sync(0xffffffffu, q < 32 ? m0 : m1, q & 31);
-            const T* xr = X + (size_t)j * W;
-            sc[u] = 1.0f;
-            if constexpr (is_fp8<T>()) sc[u] = q < cnt ? __ldg(xs + j) : 0.0f;
-            if (q < cnt && c0ok) Chunk<T, E>::load(xr + lane * E, v0[u]);
-            if (q < cnt && c1ok) Chunk<T, E>::load(xr + (lane + 32) * E, v1[u]);
+        for (int q = 0; q < E; ++q) a0[q] = a1[q] = 0.0f;
+#pragma unroll 4
+        for (int q = pos; q < e; ++q) {
+            const int r = q - cs;  // warp-uniform
+            const int j = __shfl_sync(0xffffffffu, r < 32 ? m0 : m1, r & 31);
+            add_row<T, E>(X + (size_t)j * W, is_fp8<T>() ? __ldg(xs + j) : 1.0f, lane, c0ok, c1ok, a0, a1);
         }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int q = q0 + u;
-            if (q >= cnt) break;
-            if (c0ok)
-#pragma unroll
-                for (int e = 0; e < E; ++e) a0[e] = is_fp8<T>() ? fmaf(v0[u][e], sc[u], a0[e]) : a0[e] + v0[u][e];
-            if (c1ok)
-#pragma unroll
-                for (int e = 0; e < E; ++e) a1[e] = is_fp8<T>() ? fmaf(v1[u][e], sc[u], a1[e]) : a1[e] + v1[u][e];
-            const int kq = __shfl_sync(0xffffffffu, q < 32 ? ka0 : ka1, q & 31);
-            const int kn = q + 1 < cnt ? __shfl_sync(0xffffffffu, q + 1 < 32 ? ka0 : ka1, (q + 1) & 31) : -1;
-            if (kn != kq) {  // the last member of key kq in this chunk
-                // a key cut by a chunk edge leaves a partial: the chunk's
-                // first key in Pf, its last key in Pl (segsum_fix_kernel
-                // reads them so)
-                const bool cut = (kq == key0 && first_part) || (kq == klast && last_part);
-                if (!cut)
-                    store_grow<T, E>(G + (size_t)(gofs[tb] + kq) * W, gs + gofs[tb] + kq, lane, c0ok, c1ok, a0, a1);
-                else if (kq == key0)
-                    store_partial<T, E>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
-                else
-                    store_partial<T, E>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
-#pragma unroll
-                for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
-            }
+        if (kbeg >= cs && kend <= ce) {
+            store_grow<T, E>(G + (size_t)(gofs[tb] + key) * W, gs + gofs[tb] + key, lane, c0ok, c1ok, a0, a1);
+        } else if (pos == cs) {
+            store_partial<T, E>(Pf + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+        } else {
+            store_partial<T, E>(Pl + (size_t)warp * W, lane, c0ok, c1ok, a0, a1);
+        }
+        pos = e;
+        if (pos < ce) {
+            ++key;
+            while (__ldg(so + key + 1) <= pos) ++key;  // skip empty keys; pos < ntot = so[K] bounds key < K
         }
     }
 }
@@ -432,9 +369,14 @@ __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ sego
     store_grow<T, E>(G + (size_t)(gofs[tb] + key) * W, gs + gofs[tb] + key, lane, c0ok, c1ok, a0, a1);
 }
 
-// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample,
-// 16-byte chunks per lane, 32 trees' keys fetched at once.
-template <typename T, int E>
+// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per
+// sample.  A row of W values is CPR chunks of E values; a lane owns CPL
+// chunks, so LPR = ceil(CPR / CPL) lanes hold a row and the warp's 32 / LPR
+// slots gather that many trees' rows at once (narrow storage types fill more
+// slots, so they need fewer instructions per (tree, sample)).  The 32 trees'
+// keys are fetched at once; at the end the slots' sums are added in slot
+// order (reproducible) and slot 0 writes the row.
+template <typename T, int E, int CPL>
 __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
                             const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate,
                             const float* __restrict__ gs) {
@@ -442,11 +384,16 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
     const int i = (int)warp;
-    const int CH = W / E;
-    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
-    float a0[E], a1[E];
+    const int CPR = W / E;
+    const int LPR = (CPR + CPL - 1) / CPL;
+    const int SL = 32 / LPR;
+    const int slot = lane / LPR, lr = lane % LPR;
+    const bool live = slot < SL;
+    float acc[CPL][E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
+    for (int c = 0; c < CPL; ++c)
+#pragma unroll
+        for (int e = 0; e < E; ++e) acc[c][e] = 0.0f;
     for (int tb = t0; tb < t1; tb += 32) {
         const int t = tb + lane;
         long long gi = -1;
@@ -455,46 +402,47 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
             if (k >= 0) gi = gofs[t - t0] + (k ^ 1);
         }
         const int cnt = min(32, t1 - tb);
-#pragma unroll 4
-        for (int q = 0; q < cnt; ++q) {
-            const long long r = __shfl_sync(0xffffffffu, gi, q);
-            if (r < 0) continue;
+#pragma unroll 2
+        for (int q0 = 0; q0 < cnt; q0 += SL) {
+            const int src = q0 + slot;
+            const long long r = __shfl_sync(0xffffffffu, gi, live && src < cnt ? src : 0);
+            if (!live || src >= cnt || r < 0) continue;
             const T* gr = G + (size_t)r * W;
-            float v[E];
-            if constexpr (is_fp8<T>()) {
-                const float sc = __ldg(gs + r);
-                if (c0ok) {
-                    Chunk<T, E>::load(gr + lane * E, v);
+            const float sc = is_fp8<T>() ? __ldg(gs + r) : 1.0f;
 #pragma unroll
-                    for (int e = 0; e < E; ++e) a0[e] = fmaf(v[e], sc, a0[e]);
-                }
-            } else {
-                if (c0ok) {
-                    Chunk<T, E>::load(gr + lane * E, v);
+            for (int c = 0; c < CPL; ++c) {
+                const int ci = lr * CPL + c;
+                if (ci < CPR) {
+                    float v[E];
+                    Chunk<T, E>::load(gr + ci * E, v);
 #pragma unroll
-                    for (int e = 0; e < E; ++e) a0[e] += v[e];
-                }
-                if (c1ok) {
-                    Chunk<T, E>::load(gr + (lane + 32) * E, v);
-#pragma unroll
-                    for (int e = 0; e < E; ++e) a1[e] += v[e];
+                    for (int e = 0; e < E; ++e) acc[c][e] = is_fp8<T>() ? fmaf(v[e], sc, acc[c][e]) : acc[c][e] + v[e];
                 }
             }
         }
     }
+    // slots 1.. add into slot 0, in slot order
+    for (int sl = 1; sl < SL; ++sl) {
+#pragma unroll
+        for (int c = 0; c < CPL; ++c)
+#pragma unroll
+            for (int e = 0; e < E; ++e) {
+                const float o = __shfl_sync(0xffffffffu, acc[c][e], min(31, lane + sl * LPR));
+                if (slot == 0) acc[c][e] += o;
+            }
+    }
+    if (slot != 0) return;
     float* y = Y + (size_t)i * W;
-    if (c0ok)
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) {
+        const int ci = lr * CPL + c;
+        if (ci >= CPR) continue;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int c = lane * E + e;
-            y[c] = accumulate ? y[c] + a0[e] : a0[e];
+            const int col = ci * E + e;
+            y[col] = accumulate ? y[col] + acc[c][e] : acc[c][e];
         }
-    if (c1ok)
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-            const int c = (lane + 32) * E + e;
-            y[c] = accumulate ? y[c] + a1[e] : a1[e];
-        }
+    }
 }
 
 // MV = 1/4 (D Y[:, :w] + Y[:, w:])
@@ -796,7 +744,7 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
                                                                    t1, cpt, gofs, G, Pf, Pl, fk, xs, gs);
             segsum_fix_kernel<TG, E><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt,
                                                                        gofs, G, Pf, Pl, fk, gs);
-            pull_kernel<TG, E><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0, gs);
+            pull_kernel<TG, E, 4><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0, gs);
         };
         // BF16 rows narrower than 32 16-byte chunks use 8-byte chunks, so more lanes carry data
         if constexpr (std::is_same<TX, float>::value) {
