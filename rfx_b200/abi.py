@@ -188,7 +188,8 @@ class BatchGraph:
             pass
 
 
-TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order", 4: "pair_counts_hub"}
+TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order", 4: "pair_counts_hub",
+                5: "lowrank_leaf_sums_fp32", 6: "lowrank_leaf_sums_bf16", 7: "lowrank_leaf_sums_fp8"}
 # launch shapes per stage, in the library's shape order
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
                     "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight",
@@ -197,7 +198,8 @@ TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "25
                 2: ["64", "128", "256", "64 staged rows", "128 staged rows", "256 staged rows"],
                 3: ["128", "256", "512", "64 staged rows", "128 staged rows", "256 staged rows"],
                 4: ["row2 256", "row2 512", "row2 1024", "row2 256 start-mask", "row2 512 start-mask",
-                    "row2 1024 start-mask"]}
+                    "row2 1024 start-mask"],
+                5: ["warp per key", "slots"], 6: ["warp per key", "slots"], 7: ["warp per key", "slots"]}
 
 
 def _shape_name(kernel: int, shape: int) -> str:

@@ -340,6 +340,129 @@ __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32
     }
 }
 
+// The same sums with the warp split into slots (as pull_kernel): a row is
+// held by LPR = ceil(CPR / CPL) lanes of CPL chunks each, and the warp's
+// 32 / LPR slots take that many of the chunk's keys at once, each slot adding
+// its key's member rows in order.  Keys are short (a few members), so the
+// slots replace the per-key turns of the whole warp.
+template <typename T, int E, int CPL>
+__global__ void segsum_slot_kernel(const T* __restrict__ X, int n, int W, const int32_t* __restrict__ memb,
+                                   const int32_t* __restrict__ segoff, const int64_t* __restrict__ segbase, int t0,
+                                   int t1, int cpt, const int64_t* __restrict__ gofs, T* __restrict__ G,
+                                   float* __restrict__ Pf, float* __restrict__ Pl, int32_t* __restrict__ fk,
+                                   const float* __restrict__ xs, float* __restrict__ gs) {
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= (int64_t)(t1 - t0) * cpt) return;
+    const int tb = (int)(warp / cpt), ch = (int)(warp % cpt);
+    const int t = t0 + tb;
+    const int32_t* so = segoff + segbase[t];
+    const int K = (int)(segbase[t + 1] - segbase[t]) - 1;
+    const int ntot = __ldg(so + K);
+    const int cs = ch * SEG_CH;
+    if (cs >= ntot) {
+        if (lane == 0) fk[warp] = -1;
+        return;
+    }
+    const int ce = min(cs + SEG_CH, ntot);
+    // first key: the largest k with so[k] <= cs; last key: the largest k with
+    // so[k] <= ce - 1 (so[0] = 0, so[K] = ntot > ce - 1)
+    int lo = 0, hi = K;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(so + mid) <= cs) lo = mid;
+        else hi = mid;
+    }
+    const int key0 = lo;
+    hi = K;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(so + mid) <= ce - 1) lo = mid;
+        else hi = mid;
+    }
+    const int nkeys = lo - key0 + 1;
+    if (lane == 0) fk[warp] = key0;
+    const int32_t* mt = memb + (size_t)t * n;
+    const int m0 = cs + lane < ce ? __ldg(mt + cs + lane) : 0;
+    const int m1 = cs + 32 + lane < ce ? __ldg(mt + cs + 32 + lane) : 0;
+    const int CPR = W / E;
+    const int LPR = (CPR + CPL - 1) / CPL;
+    const int SL = 32 / LPR;
+    const int slot = lane / LPR, lr = lane % LPR;
+    const bool live = slot < SL;
+    for (int kb = 0; kb < nkeys; kb += SL) {
+        const int k = key0 + kb + slot;
+        const bool act = live && kb + slot < nkeys;
+        const int kbeg = act ? __ldg(so + k) : 0, kend = act ? __ldg(so + k + 1) : 0;
+        const int p0 = max(kbeg, cs), p1 = min(kend, ce);
+        const int cntm = act ? max(0, p1 - p0) : 0;
+        const int maxc = __reduce_max_sync(0xffffffffu, cntm);
+        float acc[CPL][E];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c)
+#pragma unroll
+            for (int e = 0; e < E; ++e) acc[c][e] = 0.0f;
+        for (int m = 0; m < maxc; ++m) {
+            const int q = p0 - cs + m;  // this slot's member position in the chunk
+            const int j0 = __shfl_sync(0xffffffffu, m0, q & 31);
+            const int j1 = __shfl_sync(0xffffffffu, m1, q & 31);
+            if (m >= cntm) continue;
+            const int j = q < 32 ? j0 : j1;
+            const T* xr = X + (size_t)j * W;
+            const float sc = is_fp8<T>() ? __ldg(xs + j) : 1.0f;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int ci = lr * CPL + c;
+                if (ci < CPR) {
+                    float v[E];
+                    Chunk<T, E>::load(xr + ci * E, v);
+#pragma unroll
+                    for (int e = 0; e < E; ++e) acc[c][e] = is_fp8<T>() ? fmaf(v[e], sc, acc[c][e]) : acc[c][e] + v[e];
+                }
+            }
+        }
+        // a key cut by the chunk edges leaves a partial: the chunk's first
+        // key in Pf, its last in Pl (segsum_fix_kernel reads them so)
+        const bool whole = kbeg >= cs && kend <= ce;
+        float scale = 1.0f;
+        if constexpr (is_fp8<T>()) {
+            // the row's largest magnitude over the slot's lanes maps to 448
+            float amax = 0.0f;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c)
+#pragma unroll
+                for (int e = 0; e < E; ++e) amax = fmaxf(amax, fabsf(acc[c][e]));
+            for (int d = 1; d < LPR; ++d)
+                amax = fmaxf(amax, __shfl_sync(0xffffffffu, amax, min(31, slot * LPR + (lr + d) % LPR)));
+            scale = amax > 0.0f ? 448.0f / amax : 1.0f;
+        }
+        if (cntm == 0) continue;  // empty key: its zero row was cleared beforehand
+        if (whole) {
+            T* gr = G + (size_t)(gofs[tb] + k) * W;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int ci = lr * CPL + c;
+                if (ci < CPR) {
+                    float v[E];
+#pragma unroll
+                    for (int e = 0; e < E; ++e) v[e] = acc[c][e] * scale;
+                    Chunk<T, E>::store(gr + ci * E, v);
+                }
+            }
+            if (is_fp8<T>() && lr == 0) gs[gofs[tb] + k] = 1.0f / scale;
+        } else {
+            float* pr = (p0 == cs ? Pf : Pl) + (size_t)warp * W;
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+                const int ci = lr * CPL + c;
+                if (ci < CPR)
+#pragma unroll
+                    for (int h = 0; h < E / 4; ++h) Chunk<float, 4>::store(pr + ci * E + 4 * h, &acc[c][4 * h]);
+            }
+        }
+    }
+}
+
 // Keys that cross chunk boundaries: the chunk after the one a key starts in
 // sums the key's partial rows in chunk order and writes its G row.
 template <typename T, int E>
@@ -738,23 +861,39 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
         const int64_t chunks = (int64_t)(t1 - t0) * cpt;
         RFX_CUDA(cudaMemsetAsync(G, 0, sizeof(TG) * (size_t)total_keys * W, s));
         if constexpr (is_fp8<TG>()) RFX_CUDA(cudaMemsetAsync(gs, 0, sizeof(float) * (size_t)total_keys, s));
-        auto run = [&](auto e_tag) {
+        auto run = [&](auto e_tag) -> rfx_status {
             constexpr int E = decltype(e_tag)::value;
-            segsum_kernel<TX, E><<<nblk(chunks * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0,
-                                                                   t1, cpt, gofs, G, Pf, Pl, fk, xs, gs);
+            // shape 0: the warp takes the chunk's keys in turn; 1: slots of
+            // the warp take several keys at once
+            const int tk = is_fp8<TX>() ? TK_SEGSUM_FP8 : std::is_same<TX, float>::value ? TK_SEGSUM_F32 : TK_SEGSUM_BF16;
+            rfx_status st0 = autotune(c, tk, 2, 0, [&](int shape) -> rfx_status {
+                if (shape == 1)
+                    segsum_slot_kernel<TX, E, 4><<<nblk(chunks * 32), 256, 0, s>>>(
+                        X, n, W, c->d_memb, c->d_segoff, c->d_segbase, t0, t1, cpt, gofs, G, Pf, Pl, fk, xs, gs);
+                else
+                    segsum_kernel<TX, E><<<nblk(chunks * 32), 256, 0, s>>>(X, n, W, c->d_memb, c->d_segoff,
+                                                                           c->d_segbase, t0, t1, cpt, gofs, G, Pf,
+                                                                           Pl, fk, xs, gs);
+                RFX_CUDA(cudaGetLastError());
+                return RFX_OK;
+            });
+            if (st0 != RFX_OK) return st0;
             segsum_fix_kernel<TG, E><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt,
                                                                        gofs, G, Pf, Pl, fk, gs);
             pull_kernel<TG, E, 4><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0, gs);
+            return RFX_OK;
         };
         // BF16 rows narrower than 32 16-byte chunks use 8-byte chunks, so more lanes carry data
+        rfx_status rs;
         if constexpr (std::is_same<TX, float>::value) {
-            run(std::integral_constant<int, 4>{});
+            rs = run(std::integral_constant<int, 4>{});
         } else if constexpr (is_fp8<TX>()) {
-            run(std::integral_constant<int, 8>{});
+            rs = run(std::integral_constant<int, 8>{});
         } else {
-            if (W / 8 > 16) run(std::integral_constant<int, 8>{});
-            else run(std::integral_constant<int, 4>{});
+            if (W / 8 > 16) rs = run(std::integral_constant<int, 8>{});
+            else rs = run(std::integral_constant<int, 4>{});
         }
+        if (rs != RFX_OK) return rs;
         c->launches += 3;
         RFX_CUDA(cudaGetLastError());
     }

@@ -55,12 +55,14 @@ def best_err(M, k):
     return rel_err(M, A)
 
 
+@pytest.mark.parametrize("shape", [0, 1])
 @pytest.mark.parametrize("w", [8, 40, 80])
-def test_range_finder_operator_matches_dense(setup, w):
+def test_range_finder_operator_matches_dense(setup, monkeypatch, w, shape):
     """One product of the range finder (leaf sums through the member lists,
     sums back to the samples) against the dense FP64 M V: FP32 storage to
     1e-5 relative, BF16 storage to 1e-2, FP8 (per-row scales) to 6e-2."""
     ctx, f, P, M = setup
+    monkeypatch.setenv("RFX_TUNE_SEGSUM", str(shape))  # both leaf-sum kernel forms
     V = np.random.default_rng(w).standard_normal((f.n, w)).astype(np.float32)
     ref = M @ V.astype(np.float64)
     nr = np.linalg.norm(ref)
