@@ -412,7 +412,7 @@ __global__ void segsum_slot_kernel(const T* __restrict__ X, int n, int W, const 
             const float sc = is_fp8<T>() ? __ldg(xs + j) : 1.0f;
 #pragma unroll
             for (int c = 0; c < CPL; ++c) {
-                const int ci = lr * CPL + c;
+                const int ci = c * LPR + lr;
                 if (ci < CPR) {
                     float v[E];
                     Chunk<T, E>::load(xr + ci * E, v);
@@ -441,7 +441,7 @@ __global__ void segsum_slot_kernel(const T* __restrict__ X, int n, int W, const 
             T* gr = G + (size_t)(gofs[tb] + k) * W;
 #pragma unroll
             for (int c = 0; c < CPL; ++c) {
-                const int ci = lr * CPL + c;
+                const int ci = c * LPR + lr;
                 if (ci < CPR) {
                     float v[E];
 #pragma unroll
@@ -454,7 +454,7 @@ __global__ void segsum_slot_kernel(const T* __restrict__ X, int n, int W, const 
             float* pr = (p0 == cs ? Pf : Pl) + (size_t)warp * W;
 #pragma unroll
             for (int c = 0; c < CPL; ++c) {
-                const int ci = lr * CPL + c;
+                const int ci = c * LPR + lr;
                 if (ci < CPR)
 #pragma unroll
                     for (int h = 0; h < E / 4; ++h) Chunk<float, 4>::store(pr + ci * E + 4 * h, &acc[c][4 * h]);
@@ -494,7 +494,8 @@ __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ sego
 
 // Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per
 // sample.  A row of W values is CPR chunks of E values; a lane owns CPL
-// chunks, so LPR = ceil(CPR / CPL) lanes hold a row and the warp's 32 / LPR
+// chunks (chunks lr, lr + LPR, ..., so that each load instruction reads
+// contiguous bytes), LPR = ceil(CPR / CPL) lanes hold a row and the warp's 32 / LPR
 // slots gather that many trees' rows at once (narrow storage types fill more
 // slots, so they need fewer instructions per (tree, sample)).  The 32 trees'
 // keys are fetched at once; at the end the slots' sums are added in slot
@@ -534,7 +535,7 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
             const float sc = is_fp8<T>() ? __ldg(gs + r) : 1.0f;
 #pragma unroll
             for (int c = 0; c < CPL; ++c) {
-                const int ci = lr * CPL + c;
+                const int ci = c * LPR + lr;
                 if (ci < CPR) {
                     float v[E];
                     Chunk<T, E>::load(gr + ci * E, v);
@@ -558,7 +559,7 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
     float* y = Y + (size_t)i * W;
 #pragma unroll
     for (int c = 0; c < CPL; ++c) {
-        const int ci = lr * CPL + c;
+        const int ci = c * LPR + lr;
         if (ci >= CPR) continue;
 #pragma unroll
         for (int e = 0; e < E; ++e) {
