@@ -100,12 +100,16 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
                 pairs[2 * k + 1] = max(a, b);
             }
             __syncthreads();
+            int rot = 0;
             for (int k = tid; k < m / 2; k += nt) {
                 const int p = pairs[2 * k], q = pairs[2 * k + 1];
                 double c = 1.0, sn = 0.0;
                 if (q < s && p != q) {
                     const double apq = A[p * ld + q];
-                    if (fabs(apq) > 1e-300) {
+                    // entries already below the stop test are not rotated
+                    if (fabs(apq) > 1e-300 && apq * apq > 1e-32 * fabs(A[p * ld + p] * A[q * ld + q]) &&
+                        apq * apq > floor2) {
+                        rot = 1;
                         const double app = A[p * ld + p], aqq = A[q * ld + q];
                         const double tau = (aqq - app) / (2.0 * apq);
                         const double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
@@ -116,7 +120,8 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
                 cs[k][0] = c;
                 cs[k][1] = sn;
             }
-            __syncthreads();
+            // a round without a rotation leaves A and V as they are
+            if (!__syncthreads_or(rot)) continue;
             // A <- J^T A J applied as rows then columns; V <- V J
             for (int e = tid; e < (m / 2) * s; e += nt) {
                 const int k = e / s, r = e % s;
