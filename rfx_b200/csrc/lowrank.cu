@@ -340,7 +340,7 @@ __global__ void segsum_kernel(const T* __restrict__ X, int n, int W, const int32
     }
 }
 
-// The same sums with the warp split into slots (as pull_kernel): a row is
+// The same sums with the warp split into slots: a row is
 // held by LPR = ceil(CPR / CPL) lanes of CPL chunks each, and the warp's
 // 32 / LPR slots take that many of the chunk's keys at once, each slot adding
 // its key's member rows in order.  Keys are short (a few members), so the
@@ -492,15 +492,9 @@ __global__ void segsum_fix_kernel(int n, int W, const int32_t* __restrict__ sego
     store_grow<T, E>(G + (size_t)(gofs[tb] + key) * W, gs + gofs[tb] + key, lane, c0ok, c1ok, a0, a1);
 }
 
-// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per
-// sample.  A row of W values is CPR chunks of E values; a lane owns CPL
-// chunks (chunks lr, lr + LPR, ..., so that each load instruction reads
-// contiguous bytes), LPR = ceil(CPR / CPL) lanes hold a row and the warp's 32 / LPR
-// slots gather that many trees' rows at once (narrow storage types fill more
-// slots, so they need fewer instructions per (tree, sample)).  The 32 trees'
-// keys are fetched at once; at the end the slots' sums are added in slot
-// order (reproducible) and slot 0 writes the row.
-template <typename T, int E, int CPL>
+// Y[i] (+)= sum over trees [t0, t1) of G_t[key_t(i) ^ 1]; one warp per sample,
+// 16-byte chunks per lane, 32 trees' keys fetched at once.
+template <typename T, int E>
 __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__ key, int n, int W, int t0, int t1,
                             const int64_t* __restrict__ gofs, float* __restrict__ Y, int accumulate,
                             const float* __restrict__ gs) {
@@ -508,16 +502,11 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
     const int lane = threadIdx.x & 31;
     if (warp >= n) return;
     const int i = (int)warp;
-    const int CPR = W / E;
-    const int LPR = (CPR + CPL - 1) / CPL;
-    const int SL = 32 / LPR;
-    const int slot = lane / LPR, lr = lane % LPR;
-    const bool live = slot < SL;
-    float acc[CPL][E];
+    const int CH = W / E;
+    const bool c0ok = lane < CH, c1ok = lane + 32 < CH;
+    float a0[E], a1[E];
 #pragma unroll
-    for (int c = 0; c < CPL; ++c)
-#pragma unroll
-        for (int e = 0; e < E; ++e) acc[c][e] = 0.0f;
+    for (int e = 0; e < E; ++e) a0[e] = a1[e] = 0.0f;
     for (int tb = t0; tb < t1; tb += 32) {
         const int t = tb + lane;
         long long gi = -1;
@@ -526,47 +515,46 @@ __global__ void pull_kernel(const T* __restrict__ G, const int32_t* __restrict__
             if (k >= 0) gi = gofs[t - t0] + (k ^ 1);
         }
         const int cnt = min(32, t1 - tb);
-#pragma unroll 2
-        for (int q0 = 0; q0 < cnt; q0 += SL) {
-            const int src = q0 + slot;
-            const long long r = __shfl_sync(0xffffffffu, gi, live && src < cnt ? src : 0);
-            if (!live || src >= cnt || r < 0) continue;
+#pragma unroll 4
+        for (int q = 0; q < cnt; ++q) {
+            const long long r = __shfl_sync(0xffffffffu, gi, q);
+            if (r < 0) continue;
             const T* gr = G + (size_t)r * W;
-            const float sc = is_fp8<T>() ? __ldg(gs + r) : 1.0f;
+            float v[E];
+            if constexpr (is_fp8<T>()) {
+                const float sc = __ldg(gs + r);
+                if (c0ok) {
+                    Chunk<T, E>::load(gr + lane * E, v);
 #pragma unroll
-            for (int c = 0; c < CPL; ++c) {
-                const int ci = c * LPR + lr;
-                if (ci < CPR) {
-                    float v[E];
-                    Chunk<T, E>::load(gr + ci * E, v);
+                    for (int e = 0; e < E; ++e) a0[e] = fmaf(v[e], sc, a0[e]);
+                }
+            } else {
+                if (c0ok) {
+                    Chunk<T, E>::load(gr + lane * E, v);
 #pragma unroll
-                    for (int e = 0; e < E; ++e) acc[c][e] = is_fp8<T>() ? fmaf(v[e], sc, acc[c][e]) : acc[c][e] + v[e];
+                    for (int e = 0; e < E; ++e) a0[e] += v[e];
+                }
+                if (c1ok) {
+                    Chunk<T, E>::load(gr + (lane + 32) * E, v);
+#pragma unroll
+                    for (int e = 0; e < E; ++e) a1[e] += v[e];
                 }
             }
         }
     }
-    // slots 1.. add into slot 0, in slot order
-    for (int sl = 1; sl < SL; ++sl) {
-#pragma unroll
-        for (int c = 0; c < CPL; ++c)
-#pragma unroll
-            for (int e = 0; e < E; ++e) {
-                const float o = __shfl_sync(0xffffffffu, acc[c][e], min(31, lane + sl * LPR));
-                if (slot == 0) acc[c][e] += o;
-            }
-    }
-    if (slot != 0) return;
     float* y = Y + (size_t)i * W;
-#pragma unroll
-    for (int c = 0; c < CPL; ++c) {
-        const int ci = c * LPR + lr;
-        if (ci >= CPR) continue;
+    if (c0ok)
 #pragma unroll
         for (int e = 0; e < E; ++e) {
-            const int col = ci * E + e;
-            y[col] = accumulate ? y[col] + acc[c][e] : acc[c][e];
+            const int c = lane * E + e;
+            y[c] = accumulate ? y[c] + a0[e] : a0[e];
         }
-    }
+    if (c1ok)
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+            const int c = (lane + 32) * E + e;
+            y[c] = accumulate ? y[c] + a1[e] : a1[e];
+        }
 }
 
 // MV = 1/4 (D Y[:, :w] + Y[:, w:])
@@ -881,7 +869,7 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
             if (st0 != RFX_OK) return st0;
             segsum_fix_kernel<TG, E><<<nblk(chunks * 32), 256, 0, s>>>(n, W, c->d_segoff, c->d_segbase, t0, t1, cpt,
                                                                        gofs, G, Pf, Pl, fk, gs);
-            pull_kernel<TG, E, 4><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0, gs);
+            pull_kernel<TG, E><<<nblk((int64_t)n * 32), 256, 0, s>>>(G, c->d_key, n, W, t0, t1, gofs, Y, b > 0, gs);
             return RFX_OK;
         };
         // BF16 rows narrower than 32 16-byte chunks use 8-byte chunks, so more lanes carry data
