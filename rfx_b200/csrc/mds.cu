@@ -674,7 +674,7 @@ __global__ void center_kernel(const double* __restrict__ V, const double* __rest
 
 // AtU[a][j] = sum_i A[i][a] u[i][j] in FP64: per-CTA partials (64 columns x
 // 4 row groups per CTA, all 16 j per thread), then a fixed-order sum over CTAs.
-__global__ void __launch_bounds__(256) atu_part_kernel(const float* __restrict__ A, const float* __restrict__ u, int n,
+__global__ void __launch_bounds__(256) atu_part_kernel(const float* __restrict__ A, const double* __restrict__ u, int n,
                                                        int k, double* __restrict__ part) {
     const int a = threadIdx.x % 64, rg = threadIdx.x / 64;
     double acc[S_BLK];
@@ -684,14 +684,13 @@ __global__ void __launch_bounds__(256) atu_part_kernel(const float* __restrict__
 #pragma unroll 4
         for (int i = blockIdx.x * 4 + rg; i < n; i += gridDim.x * 4) {
             const double x = (double)__ldg(A + (size_t)i * k + a);
-            const float4* ur = reinterpret_cast<const float4*>(u + (size_t)i * S_BLK);
+            // the FP64 row of u (shared by the CTA's 64 columns): no conversions per product
+            const double2* ur = reinterpret_cast<const double2*>(u + (size_t)i * S_BLK);
 #pragma unroll
-            for (int q = 0; q < S_BLK / 4; ++q) {
-                const float4 v = __ldg(ur + q);
-                acc[4 * q] = fma(x, (double)v.x, acc[4 * q]);
-                acc[4 * q + 1] = fma(x, (double)v.y, acc[4 * q + 1]);
-                acc[4 * q + 2] = fma(x, (double)v.z, acc[4 * q + 2]);
-                acc[4 * q + 3] = fma(x, (double)v.w, acc[4 * q + 3]);
+            for (int q = 0; q < S_BLK / 2; ++q) {
+                const double2 v = __ldg(ur + q);
+                acc[2 * q] = fma(x, v.x, acc[2 * q]);
+                acc[2 * q + 1] = fma(x, v.y, acc[2 * q + 1]);
             }
         }
     }
@@ -851,7 +850,7 @@ __global__ void __launch_bounds__(256) factor_combine_kernel(const float* __rest
                                                              double* __restrict__ W) {
     // one thread per row: the row of A is read once for all 16 columns and
     // for |a_i|^2; A^T u sits in shared memory
-    __shared__ double s_atu[64 * S_BLK];
+    __shared__ __align__(16) double s_atu[64 * S_BLK];
     for (int e = threadIdx.x; e < k * S_BLK; e += blockDim.x) s_atu[e] = AtU[e];
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -863,9 +862,13 @@ __global__ void __launch_bounds__(256) factor_combine_kernel(const float* __rest
     const float* arow = A + (size_t)i * k;
     auto step = [&](double x, int a) {
         nrm += x * x;
-        const double* ar = s_atu + a * S_BLK;
+        const double2* ar = reinterpret_cast<const double2*>(s_atu + a * S_BLK);
 #pragma unroll
-        for (int j = 0; j < S_BLK; ++j) t1[j] += x * ar[j];
+        for (int j = 0; j < S_BLK / 2; ++j) {
+            const double2 v = ar[j];
+            t1[2 * j] += x * v.x;
+            t1[2 * j + 1] += x * v.y;
+        }
     };
     if ((k & 3) == 0) {
         // the row as 16-byte loads, four in flight
@@ -942,7 +945,7 @@ void col_mean(const double* V, int n, double* part, double* mean, cudaStream_t s
     colsum_part_kernel<<<RED_CTAS, 256, 0, s>>>(V, n, part);
     part_sum_kernel<double><<<(S_BLK * 32 + 255) / 256, 256, 0, s>>>(part, RED_CTAS, S_BLK, 1.0 / (double)n, mean);
 }
-void at_u(const float* A, const float* u, int n, int k, double* part, double* AtU, cudaStream_t s) {
+void at_u(const float* A, const double* u, int n, int k, double* part, double* AtU, cudaStream_t s) {
     atu_part_kernel<<<RED_CTAS, 256, 0, s>>>(A, u, n, k, part);
     part_sum_kernel<double><<<(k * S_BLK * 32 + 255) / 256, 256, 0, s>>>(part, RED_CTAS, k * S_BLK, 1.0, AtU);
 }
@@ -979,7 +982,7 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
         const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
         col_mean(V, n, part, mean, s);
         center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
-        at_u(dA, u32, n, k, part, AtU, s);
+        at_u(dA, u, n, k, part, AtU, s);
         if (tensor) {
             rfx_status st = launch_factor_ops_tc(c, dA, k, Aq, At, u32, M, T2);
             if (st != RFX_OK) return st;
@@ -1047,7 +1050,7 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
     const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
     col_mean(V, n, part, mean, s);
     center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
-    at_u(dA, u32, n, k, part, AtU, s);
+    at_u(dA, u, n, k, part, AtU, s);
     rfx_status st = RFX_OK;
     if (precision) {
         uint8_t* Aq = d.get<uint8_t>(factor_tc_aq_bytes(n, k));
