@@ -556,7 +556,8 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     extern __shared__ uint32_t acc[];  // `words` words, two u16 counters each
     __shared__ long long lbase[V2_LIST];
     __shared__ int llen[V2_LIST];
-    __shared__ int s_nlong, s_chunk;
+    __shared__ int s_nlong, s_chunk, s_np;
+    __shared__ int lpre[V2_LIST];       // first piece number of each listed long range
     __shared__ uint8_t s_lid[NW][32];  // per warp: lanes with a non-empty short range
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -700,29 +701,62 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         }
     }
     __syncthreads();
-    // phase B: the listed long ranges, pieces dealt round-robin over the warps
+    // phase B: the listed long ranges cut into pieces of V2_PIECE members;
+    // piece g of the list (ranges in list order) goes to warp g % NW, two
+    // pieces in flight per warp, and finds its range by a binary search over
+    // the ranges' first-piece numbers (lpre)
     const int L = min(s_nlong, V2_LIST);
-    int run = 0;
-    for (int c = 0; c < L; ++c) {
-        const long long b = lbase[c];
-        const int len = llen[c];
-        const int np = (len + V2_PIECE - 1) / V2_PIECE;
-        int k = w - run;
-        if (k < 0) k += NW;
-        for (; k < np; k += NW) {
-            const int32_t* mp = memb + b + (long long)k * V2_PIECE;
-            const int lim = min(V2_PIECE, len - k * V2_PIECE);
-            int j[V2_PIECE / 32];
+    if (w == 0) {
+        constexpr int PL = V2_LIST / 32;  // ranges per lane
+        int loc[PL];
+        int sum = 0;
+#pragma unroll
+        for (int u = 0; u < PL; ++u) {
+            const int c = lane * PL + u;
+            loc[u] = sum;
+            sum += c < L ? (llen[c] + V2_PIECE - 1) / V2_PIECE : 0;
+        }
+        int incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += u;
+        }
+#pragma unroll
+        for (int u = 0; u < PL; ++u) lpre[lane * PL + u] = incl - sum + loc[u];
+        if (lane == 31) s_np = incl;
+    }
+    __syncthreads();
+    const int P = s_np;
+    for (int g0 = w; g0 < P; g0 += 2 * NW) {
+        int j[2][V2_PIECE / 32];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int g = g0 + h * NW;
+            int c = 0;
+            if (g < P) {
+                int lo = 0, hi = L;  // the last range whose first piece is <= g
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (lpre[mid] <= g) lo = mid;
+                    else hi = mid;
+                }
+                c = lo;
+            }
+            const int k = g - lpre[c];
+            const int32_t* mp = memb + lbase[c] + (long long)k * V2_PIECE;
+            const int lim = g < P ? min(V2_PIECE, llen[c] - k * V2_PIECE) : 0;
 #pragma unroll
             for (int u = 0; u < V2_PIECE / 32; ++u) {
                 const int o = (u << 5) + lane;
-                j[u] = o < lim ? __ldg(mp + o) : -1;
+                j[h][u] = o < lim ? __ldg(mp + o) : -1;
             }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
 #pragma unroll
             for (int u = 0; u < V2_PIECE / 32; ++u)
-                if (j[u] >= 0) count16(acc, j[u]);
-        }
-        run = (run + np) % NW;
+                if (j[h][u] >= 0) count16(acc, j[h][u]);
     }
     __syncthreads();
     const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
