@@ -214,6 +214,12 @@ typedef struct rfx_lowrank_opts {
     int32_t power_iters;
     int32_t precision;
     uint64_t seed;
+    /* trees per pass of the leaf sums: 0 = as many as 4 GB of leaf sums hold
+     * (the batched form); 1 = one tree per pass, the per-tree structure of the
+     * reference's GPU accumulation (slower: every pass re-reads the n x 2w
+     * accumulator) */
+    int32_t trees_per_pass;
+    int32_t reserved;
 } rfx_lowrank_opts;
 rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* opts, float* A, float* evals);
 

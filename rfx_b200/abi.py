@@ -66,7 +66,8 @@ class _ForestDeviceView(ctypes.Structure):
 
 class _LowrankOpts(ctypes.Structure):
     _fields_ = [("rank", ctypes.c_int32), ("oversample", ctypes.c_int32), ("power_iters", ctypes.c_int32),
-                ("precision", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+                ("precision", ctypes.c_int32), ("seed", ctypes.c_uint64), ("trees_per_pass", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class _BatchItem(ctypes.Structure):
@@ -399,13 +400,14 @@ class Context:
         _check(lib().rfx_mds3d_full(self._h, _vp(P), _vp(coords), _vp(ev)))
         return coords, ev
 
-    def lowrank(self, rank, oversample=16, power_iters=1, precision=0, seed=12345, A=None):
+    def lowrank(self, rank, oversample=16, power_iters=1, precision=0, seed=12345, A=None, trees_per_pass=0):
         """Factors A (n x rank float32, P ~= I + A A^T) and the rank eigenvalues."""
         self._rank_guess = rank
         if A is None:
             A = np.zeros((self.n, rank), np.float32)
         ev = np.zeros(rank, np.float32)
-        o = _LowrankOpts(rank=rank, oversample=oversample, power_iters=power_iters, precision=precision, seed=seed)
+        o = _LowrankOpts(rank=rank, oversample=oversample, power_iters=power_iters, precision=precision, seed=seed,
+                         trees_per_pass=trees_per_pass)
         _check(lib().rfx_lowrank(self._h, ctypes.byref(o), _vp(A), _vp(ev)))
         return A, ev
 

@@ -1162,7 +1162,7 @@ rfx_status rfx_lowrank(rfx_ctx* ctx, const rfx_lowrank_opts* o, float* A, float*
     if ((st = dalloc(c, &c->d_lrA, (size_t)c->n * k))) return st;
     std::vector<float> ev(k);
     st = lowrank_compute(c, k, o->oversample, o->power_iters, o->precision, o->seed ? o->seed : 12345ull, c->d_lrA,
-                         ev.data());
+                         ev.data(), nullptr, std::max(0, o->trees_per_pass));
     if (st) return st;
     c->lr_rank = k;
     if (evals) std::copy(ev.begin(), ev.end(), evals);

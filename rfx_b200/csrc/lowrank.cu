@@ -893,7 +893,7 @@ rfx_status apply_m(Ctx* c, const float* V, int w, float* MV, const float* dinv, 
 }
 
 rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int precision, uint64_t seed,
-                           float* d_A_out, float* h_evals, const float* d_apply_in) {
+                           float* d_A_out, float* h_evals, const float* d_apply_in, int trees_per_pass) {
     cudaStream_t s = c->stream;
     const int n = c->n, T = c->T;
     const int w = (k + oversample + 7) / 8 * 8;  // rows of whole 16-byte chunks
@@ -932,7 +932,9 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
             int t1 = t;
             while (t1 < T) {
                 const int64_t kt = c->h_segbase[t1 + 1] - c->h_segbase[t1] - 1;
-                if (t1 > t && (size_t)(keys + kt) * gbytes_row > batch_budget) break;
+                if (t1 > t && ((size_t)(keys + kt) * gbytes_row > batch_budget ||
+                               (trees_per_pass > 0 && t1 - t >= trees_per_pass)))
+                    break;
                 keys += kt;
                 ++t1;
             }

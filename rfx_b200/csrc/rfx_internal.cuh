@@ -332,7 +332,8 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
 rfx_status launch_outlier_scores(Ctx* c, const float* dA, int k, float* d_out);
 rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* V, double* W, int precision);
 rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int precision, uint64_t seed,
-                           float* d_A_out, float* h_evals, const float* d_apply_in = nullptr);
+                           float* d_A_out, float* h_evals, const float* d_apply_in = nullptr,
+                           int trees_per_pass = 0);
 rfx_status lowrank_quantize(Ctx* c, const float* dA, int k, int format, void* dq, float* dscale);
 rfx_status lowrank_dequantize(Ctx* c, const void* dq, const float* dscale, int k, int format, float* dA);
 
