@@ -92,17 +92,16 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
         for (int round = 0; round < m - 1; ++round) {
             // round-robin tournament: index 0 stays, indices 1..m-1 rotate;
             // pair k joins positions k and m-1-k
+            // (the thread that numbers pair k also computes its rotation; the
+            // barrier below publishes both)
+            int rot = 0;
             for (int k = tid; k < m / 2; k += nt) {
                 const int pa = k, pb = m - 1 - k;
                 const int a = (pa == 0) ? 0 : ((pa - 1 + round) % (m - 1)) + 1;
                 const int b = ((pb - 1 + round) % (m - 1)) + 1;
-                pairs[2 * k] = min(a, b);
-                pairs[2 * k + 1] = max(a, b);
-            }
-            __syncthreads();
-            int rot = 0;
-            for (int k = tid; k < m / 2; k += nt) {
-                const int p = pairs[2 * k], q = pairs[2 * k + 1];
+                const int p = min(a, b), q = max(a, b);
+                pairs[2 * k] = p;
+                pairs[2 * k + 1] = q;
                 double c = 1.0, sn = 0.0;
                 if (q < s && p != q) {
                     const double apq = A[p * ld + q];
@@ -122,7 +121,8 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
             }
             // a round without a rotation leaves A and V as they are
             if (!__syncthreads_or(rot)) continue;
-            // A <- J^T A J applied as rows then columns; V <- V J
+            // A <- J^T A J applied as rows then columns; V <- V J goes with the
+            // row pass, so both passes move two pairs of entries per element
             for (int e = tid; e < (m / 2) * s; e += nt) {
                 const int k = e / s, r = e % s;
                 const int p = pairs[2 * k], q = pairs[2 * k + 1];
@@ -131,6 +131,9 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
                 const double ap = A[p * ld + r], aq = A[q * ld + r];
                 A[p * ld + r] = c * ap - sn * aq;
                 A[q * ld + r] = sn * ap + c * aq;
+                const double vp = V[r * ld + p], vq = V[r * ld + q];
+                V[r * ld + p] = c * vp - sn * vq;
+                V[r * ld + q] = sn * vp + c * vq;
             }
             __syncthreads();
             for (int e = tid; e < (m / 2) * s; e += nt) {
@@ -141,9 +144,6 @@ __device__ inline void cta_jacobi(double* A, double* V, int s, int ld, int sweep
                 const double ap = A[r * ld + p], aq = A[r * ld + q];
                 A[r * ld + p] = c * ap - sn * aq;
                 A[r * ld + q] = sn * ap + c * aq;
-                const double vp = V[r * ld + p], vq = V[r * ld + q];
-                V[r * ld + p] = c * vp - sn * vq;
-                V[r * ld + q] = sn * vp + c * vq;
             }
             __syncthreads();
         }

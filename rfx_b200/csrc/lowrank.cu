@@ -714,7 +714,7 @@ inline size_t right_mul_smem(int w, int m) {
 inline int right_mul_threads(int m) { return std::max(32, (RM_ROWS / 4) * (((m + 3) & ~3) / 4)); }
 
 // One CTA: eigen-decomposition of the symmetrised w x w H.
-__global__ void eig_w_kernel(const double* __restrict__ H, int w, double* __restrict__ evals,
+__global__ void __launch_bounds__(1024, 1) eig_w_kernel(const double* __restrict__ H, int w, double* __restrict__ evals,
                              double* __restrict__ evecs) {
     extern __shared__ double sm[];  // two w x (w + 1) arrays
     const int ld = w + 1;
@@ -1052,7 +1052,7 @@ rfx_status lowrank_compute(Ctx* c, int k, int oversample, int power_iters, int p
     // Rayleigh-Ritz projection; precision 2 recomputes this last product in FP32
     if ((st = apply(Q, Yw, !mixed || precision == 2)) != RFX_OK) return st;
     gram(Q, Yw);
-    eig_w_kernel<<<1, 256, sm_eig, s>>>(Gm, w, ev, U);
+    eig_w_kernel<<<1, 1024, sm_eig, s>>>(Gm, w, ev, U);
     c->launches += 3;
     RFX_CUDA(cudaGetLastError());
     std::vector<double> hev(w), hU((size_t)w * w);
