@@ -548,7 +548,7 @@ constexpr int V2_LIST = 256;   // listed long ranges per row (more are walked in
 __device__ __forceinline__ void count16(uint32_t* acc, int j) { atomicAdd(acc + (j >> 1), 1u << ((j & 1) << 4)); }
 
 template <int NT, int SV>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 2048 / NT)
 pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                   int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
                   int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
