@@ -528,22 +528,20 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
 // Stage 2, full-row form without per-round block barriers (pairs_row2_kernel).
 //   One CTA per row, u16 counters for the whole row as in pairs_row16_kernel.
 //   Phase A: warps claim chunks of 32 trees from a CTA counter (lane = tree)
-//     and count the chunk's ranges themselves: ranges shorter than 32 members
-//     are expanded element by element over the warp (a lane finds its range
-//     by a binary search over the warp's inclusive length scan, so no lane
-//     idles on a short range), ranges of 32..V2_LONG-1 members are walked by
-//     the whole warp with four loads in flight per lane, and ranges of
-//     V2_LONG or more are put on a per-CTA list.
-//   Phase B (after one barrier): the listed ranges are cut into pieces of
-//     V2_PIECE members dealt round-robin over the warps (the running piece
-//     count of the ranges before a range fixes where its first piece goes),
-//     eight loads in flight per lane.
+//     and count the chunk's short ranges themselves: ranges shorter than 32
+//     members are expanded element by element over the warp (a lane finds
+//     its range by a binary search over the warp's inclusive length scan, so
+//     no lane idles on a short range).  Ranges of 32 members or more are put
+//     on a per-CTA list (those beyond its capacity are walked by the whole
+//     warp, four loads in flight per lane).
+//   Phase B (after one barrier): the listed ranges are cut into pieces of 32
+//     members dealt round-robin over the warps, so every warp gets the same
+//     share of them whatever the chunks held; four loads in flight per lane.
 //   Three barriers per row: after zeroing, between the phases, before the
 //   write-out.
 // ---------------------------------------------------------------------------
-constexpr int V2_LONG = 256;
-constexpr int V2_PIECE = 256;  // 8 members per lane
-constexpr int V2_LIST = 256;   // listed long ranges per row (more are walked in phase A)
+constexpr int V2_LONG = 32;   // ranges of this many members or more go on the CTA list
+constexpr int V2_LIST = 256;  // listed ranges per row (more are walked in phase A)
 
 __device__ __forceinline__ void count16(uint32_t* acc, int j) { atomicAdd(acc + (j >> 1), 1u << ((j & 1) << 4)); }
 
@@ -701,10 +699,11 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         }
     }
     __syncthreads();
-    // phase B: the listed long ranges cut into pieces of V2_PIECE members;
-    // piece g of the list (ranges in list order) goes to warp g % NW, two
-    // pieces in flight per warp, and finds its range by a binary search over
-    // the ranges' first-piece numbers (lpre)
+    // phase B: the listed ranges cut into pieces of 32 members; piece g (ranges
+    // in list order) goes to warp g % NW.  Lane l of warp w looks up piece
+    // w + NW * (32 r + l) of round r (a binary search over the ranges' first
+    // piece numbers, lpre) and the warp then takes its pieces four at a time,
+    // the piece's start and length broadcast from the lane that found it.
     const int L = min(s_nlong, V2_LIST);
     if (w == 0) {
         constexpr int PL = V2_LIST / 32;  // ranges per lane
@@ -714,7 +713,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         for (int u = 0; u < PL; ++u) {
             const int c = lane * PL + u;
             loc[u] = sum;
-            sum += c < L ? (llen[c] + V2_PIECE - 1) / V2_PIECE : 0;
+            sum += c < L ? (llen[c] + 31) >> 5 : 0;
         }
         int incl = sum;
 #pragma unroll
@@ -728,35 +727,34 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     }
     __syncthreads();
     const int P = s_np;
-    for (int g0 = w; g0 < P; g0 += 2 * NW) {
-        int j[2][V2_PIECE / 32];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int g = g0 + h * NW;
-            int c = 0;
-            if (g < P) {
-                int lo = 0, hi = L;  // the last range whose first piece is <= g
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (lpre[mid] <= g) lo = mid;
-                    else hi = mid;
-                }
-                c = lo;
+    for (int r0 = w; r0 < P; r0 += NW * 32) {
+        const int g = r0 + NW * lane;
+        long long ps = 0;
+        int lim = 0;
+        if (g < P) {
+            int lo = 0, hi = L;  // the last range whose first piece is <= g
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (lpre[mid] <= g) lo = mid;
+                else hi = mid;
             }
-            const int k = g - lpre[c];
-            const int32_t* mp = memb + lbase[c] + (long long)k * V2_PIECE;
-            const int lim = g < P ? min(V2_PIECE, llen[c] - k * V2_PIECE) : 0;
-#pragma unroll
-            for (int u = 0; u < V2_PIECE / 32; ++u) {
-                const int o = (u << 5) + lane;
-                j[h][u] = o < lim ? __ldg(mp + o) : -1;
-            }
+            const int k = g - lpre[lo];
+            ps = lbase[lo] + ((long long)k << 5);
+            lim = min(32, llen[lo] - (k << 5));
         }
+        const int cnt = min(32, (P - r0 + NW - 1) / NW);  // pieces of this warp in this round
+        for (int u0 = 0; u0 < cnt; u0 += 4) {
+            int j[4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+            for (int v = 0; v < 4; ++v) {
+                const long long pv = __shfl_sync(0xffffffffu, ps, (u0 + v) & 31);
+                const int lv = __shfl_sync(0xffffffffu, lim, (u0 + v) & 31);
+                j[v] = (u0 + v < cnt && lane < lv) ? __ldg(memb + pv + lane) : -1;
+            }
 #pragma unroll
-            for (int u = 0; u < V2_PIECE / 32; ++u)
-                if (j[h][u] >= 0) count16(acc, j[h][u]);
+            for (int v = 0; v < 4; ++v)
+                if (j[v] >= 0) count16(acc, j[v]);
+        }
     }
     __syncthreads();
     const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
