@@ -195,11 +195,12 @@ TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_o
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
                     "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight",
                     "256x8 samples, 2048 staged nodes", "256x4 samples, 1024 staged nodes"],
-                1: ["row16 256", "row16 512", "row16 1024", "row2 256", "row2 512", "row2 1024"],
+                1: ["row16 256", "row16 512", "row16 1024", "row2 256", "row2 512", "row2 1024", "row3 512",
+                    "row3 1024"],
                 2: ["64", "128", "256", "64 staged rows", "128 staged rows", "256 staged rows"],
                 3: ["128", "256", "512", "64 staged rows", "128 staged rows", "256 staged rows"],
                 4: ["row2 256", "row2 512", "row2 1024", "row2 256 start-mask", "row2 512 start-mask",
-                    "row2 1024 start-mask"],
+                    "row2 1024 start-mask", "row3 512", "row3 1024"],
                 5: ["warp per key", "slots"], 6: ["warp per key", "slots"], 7: ["warp per key", "slots"]}
 
 

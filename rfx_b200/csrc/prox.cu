@@ -347,7 +347,7 @@ row_order_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ se
 // pairs_row16_kernel with 256/512/1024 threads, 3..5 pairs_row2_kernel with
 // 256/512/1024 threads.
 constexpr int R16_THREADS = 512;
-constexpr int PAIRS_SHAPES = 6;
+constexpr int PAIRS_SHAPES = 8;
 constexpr int PAIRS_DEFAULT_SHAPE = 4;
 
 template <int NW>
@@ -524,6 +524,96 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
     }
 }
 
+// Row i's counters start from the hub leaves' counts when the hub tiles exist:
+// row i of the S_hub tiles (row block I = i / 128, column tiles J = i / 256 ..
+// NJ - 1; 16-byte chunk q of a tile row stored at slot q ^ (row % 16)),
+// u8 -> u16; otherwise from zero.
+template <int NT>
+__device__ __forceinline__ void row_counters_init(uint32_t* acc, int words, int n, int i,
+                                                  const uint8_t* __restrict__ hubt,
+                                                  const int32_t* __restrict__ hub_state, int tid) {
+    if (hubt && hub_state[1] > 0) {
+        const int NJ = (n + 255) >> 8, I = i >> 7, r = i & 127, J0 = i >> 8;
+        const uint8_t* rowt = hubt + (size_t)(hub_row_start(I, NJ) - (I >> 1)) * 32768u + (size_t)r * 256u;
+        const int nch = (NJ - J0) * 16;
+        for (int k = tid; k < nch; k += NT) {
+            const int J = J0 + (k >> 4), slot = k & 15, q = slot ^ (r & 15);
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(rowt + (size_t)J * 32768u + slot * 16));
+            const uint32_t b[4] = {v.x, v.y, v.z, v.w};
+            uint32_t o[8];
+            // bytes (b0 b1 b2 b3) -> u16 pairs (b0, b1) and (b2, b3): one byte permute each
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                o[2 * h] = __byte_perm(b[h], 0u, 0x4140u);
+                o[2 * h + 1] = __byte_perm(b[h], 0u, 0x4342u);
+            }
+            uint4* dst = reinterpret_cast<uint4*>(acc + (size_t)J * 128 + q * 8);
+            dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+            dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+        }
+        for (int k = NJ * 128 + tid; k < words; k += NT) acc[k] = 0u;
+    } else {
+        uint4* a4 = reinterpret_cast<uint4*>(acc);
+        const int w4 = words >> 2;
+        for (int k = tid; k < w4; k += NT) a4[k] = make_uint4(0u, 0u, 0u, 0u);
+        for (int k = (w4 << 2) + tid; k < words; k += NT) acc[k] = 0u;
+    }
+}
+
+// Row i of S (entries j >= i of the packed upper triangle) from the u16
+// counters.
+template <int NT>
+__device__ __forceinline__ void row_write_out(const uint32_t* acc, int words, int n, int i, int32_t* __restrict__ S,
+                                              int tid) {
+    const int lane = tid & 31, w = tid >> 5;
+    const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
+    const uint16_t* a16 = reinterpret_cast<const uint16_t*>(acc);
+    int32_t* srow = S + rowoff + i;
+    const int len = n - i;
+    int head = len, nv = 0;
+    if ((reinterpret_cast<uintptr_t>(S) & 15) == 0) {
+        head = min(len, (int)((4 - ((rowoff + i) & 3)) & 3));
+        nv = (len - head) >> 2;
+    }
+    for (int h = tid; h < head; h += NT) srow[h] = (int32_t)a16[i + h];
+    // body: lane L of a warp stores group v = v0 + L (entries jg + 4v ..+3);
+    // it reads the aligned 4-counter group holding its first entry (one
+    // 8-byte shared load), takes the next group from lane L + 1, and picks its
+    // four 16-bit counters with byte permutes (the offset o of jg in its group
+    // is the same for the whole row)
+    int4* s4 = reinterpret_cast<int4*>(srow + head);
+    const int jg = i + head;
+    const int o = jg & 3;
+    const int gb = jg >> 2;
+    const int ngroups = words >> 1;  // 4-counter groups in the array (the last one is padding)
+    const uint2* a64 = reinterpret_cast<const uint2*>(acc);
+    for (int v0 = w * 32; v0 < nv; v0 += NT) {
+        const int v = v0 + lane;
+        const int g = gb + v;
+        const uint2 cg = g < ngroups ? a64[g] : make_uint2(0u, 0u);
+        uint2 nx;
+        nx.x = __shfl_down_sync(0xffffffffu, cg.x, 1);
+        nx.y = __shfl_down_sync(0xffffffffu, cg.y, 1);
+        if (lane == 31) nx = g + 1 < ngroups ? a64[g + 1] : make_uint2(0u, 0u);
+        uint32_t q0, q1, q2, q3;
+        if (o == 0) {
+            q0 = __byte_perm(cg.x, 0u, 0x4410u); q1 = __byte_perm(cg.x, 0u, 0x4432u);
+            q2 = __byte_perm(cg.y, 0u, 0x4410u); q3 = __byte_perm(cg.y, 0u, 0x4432u);
+        } else if (o == 1) {
+            q0 = __byte_perm(cg.x, 0u, 0x4432u); q1 = __byte_perm(cg.y, 0u, 0x4410u);
+            q2 = __byte_perm(cg.y, 0u, 0x4432u); q3 = __byte_perm(nx.x, 0u, 0x4410u);
+        } else if (o == 2) {
+            q0 = __byte_perm(cg.y, 0u, 0x4410u); q1 = __byte_perm(cg.y, 0u, 0x4432u);
+            q2 = __byte_perm(nx.x, 0u, 0x4410u); q3 = __byte_perm(nx.x, 0u, 0x4432u);
+        } else {
+            q0 = __byte_perm(cg.y, 0u, 0x4432u); q1 = __byte_perm(nx.x, 0u, 0x4410u);
+            q2 = __byte_perm(nx.x, 0u, 0x4432u); q3 = __byte_perm(nx.y, 0u, 0x4410u);
+        }
+        if (v < nv) s4[v] = make_int4((int)q0, (int)q1, (int)q2, (int)q3);
+    }
+    for (int j = i + head + 4 * nv + tid; j < n; j += NT) srow[j - i] = (int32_t)a16[j];
+}
+
 // ---------------------------------------------------------------------------
 // Stage 2, full-row form without per-round block barriers (pairs_row2_kernel).
 //   One CTA per row, u16 counters for the whole row as in pairs_row16_kernel.
@@ -559,35 +649,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ uint8_t s_lid[NW][32];  // per warp: lanes with a non-empty short range
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (hubt && hub_state[1] > 0) {
-        // counters start from the hub leaves' counts: row i of the S_hub tiles
-        // (row block I = i / 128, column tiles J = i / 256 .. NJ - 1; 16-byte
-        // chunk q of a tile row stored at slot q ^ (row % 16)), u8 -> u16
-        const int NJ = (n + 255) >> 8, I = i >> 7, r = i & 127, J0 = i >> 8;
-        const uint8_t* rowt = hubt + (size_t)(hub_row_start(I, NJ) - (I >> 1)) * 32768u + (size_t)r * 256u;
-        const int nch = (NJ - J0) * 16;
-        for (int k = tid; k < nch; k += NT) {
-            const int J = J0 + (k >> 4), slot = k & 15, q = slot ^ (r & 15);
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(rowt + (size_t)J * 32768u + slot * 16));
-            const uint32_t b[4] = {v.x, v.y, v.z, v.w};
-            uint32_t o[8];
-            // bytes (b0 b1 b2 b3) -> u16 pairs (b0, b1) and (b2, b3): one byte permute each
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                o[2 * h] = __byte_perm(b[h], 0u, 0x4140u);
-                o[2 * h + 1] = __byte_perm(b[h], 0u, 0x4342u);
-            }
-            uint4* dst = reinterpret_cast<uint4*>(acc + (size_t)J * 128 + q * 8);
-            dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-            dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
-        }
-        for (int k = NJ * 128 + tid; k < words; k += NT) acc[k] = 0u;
-    } else {
-        uint4* a4 = reinterpret_cast<uint4*>(acc);
-        const int w4 = words >> 2;
-        for (int k = tid; k < w4; k += NT) a4[k] = make_uint4(0u, 0u, 0u, 0u);
-        for (int k = (w4 << 2) + tid; k < words; k += NT) acc[k] = 0u;
-    }
+    row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
     if (tid == 0) {
         s_nlong = 0;
         s_chunk = 0;
@@ -757,52 +819,124 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         }
     }
     __syncthreads();
-    const int64_t rowoff = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 - i;  // + j gives S[i][j]
-    const uint16_t* a16 = reinterpret_cast<const uint16_t*>(acc);
-    int32_t* srow = S + rowoff + i;
-    const int len = n - i;
-    int head = len, nv = 0;
-    if ((reinterpret_cast<uintptr_t>(S) & 15) == 0) {
-        head = min(len, (int)((4 - ((rowoff + i) & 3)) & 3));
-        nv = (len - head) >> 2;
+    row_write_out<NT>(acc, words, n, i, S, tid);
+    if (pairs) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
+        if (lane == 0 && my_pairs) atomicAdd(pairs, my_pairs);
     }
-    for (int h = tid; h < head; h += NT) srow[h] = (int32_t)a16[i + h];
-    // body: lane L of a warp stores group v = v0 + L (entries jg + 4v ..+3);
-    // it reads the aligned 4-counter group holding its first entry (one
-    // 8-byte shared load), takes the next group from lane L + 1, and picks its
-    // four 16-bit counters with byte permutes (the offset o of jg in its group
-    // is the same for the whole row)
-    int4* s4 = reinterpret_cast<int4*>(srow + head);
-    const int jg = i + head;
-    const int o = jg & 3;
-    const int gb = jg >> 2;
-    const int ngroups = words >> 1;  // 4-counter groups in the array (the last one is padding)
-    const uint2* a64 = reinterpret_cast<const uint2*>(acc);
-    for (int v0 = w * 32; v0 < nv; v0 += NT) {
-        const int v = v0 + lane;
-        const int g = gb + v;
-        const uint2 cg = g < ngroups ? a64[g] : make_uint2(0u, 0u);
-        uint2 nx;
-        nx.x = __shfl_down_sync(0xffffffffu, cg.x, 1);
-        nx.y = __shfl_down_sync(0xffffffffu, cg.y, 1);
-        if (lane == 31) nx = g + 1 < ngroups ? a64[g + 1] : make_uint2(0u, 0u);
-        uint32_t q0, q1, q2, q3;
-        if (o == 0) {
-            q0 = __byte_perm(cg.x, 0u, 0x4410u); q1 = __byte_perm(cg.x, 0u, 0x4432u);
-            q2 = __byte_perm(cg.y, 0u, 0x4410u); q3 = __byte_perm(cg.y, 0u, 0x4432u);
-        } else if (o == 1) {
-            q0 = __byte_perm(cg.x, 0u, 0x4432u); q1 = __byte_perm(cg.y, 0u, 0x4410u);
-            q2 = __byte_perm(cg.y, 0u, 0x4432u); q3 = __byte_perm(nx.x, 0u, 0x4410u);
-        } else if (o == 2) {
-            q0 = __byte_perm(cg.y, 0u, 0x4410u); q1 = __byte_perm(cg.y, 0u, 0x4432u);
-            q2 = __byte_perm(nx.x, 0u, 0x4410u); q3 = __byte_perm(nx.x, 0u, 0x4432u);
-        } else {
-            q0 = __byte_perm(cg.y, 0u, 0x4432u); q1 = __byte_perm(nx.x, 0u, 0x4410u);
-            q2 = __byte_perm(nx.x, 0u, 0x4432u); q3 = __byte_perm(nx.y, 0u, 0x4410u);
+}
+
+// ---------------------------------------------------------------------------
+// Stage 2, balanced full-row form (pairs_row3_kernel).
+//   One CTA per row with the u16 counters, start values and write-out of
+//   pairs_row2_kernel.  The row's ranges are taken in rounds of NT trees:
+//   thread t loads the range of tree t of the round, a CTA-wide scan of the
+//   lengths lists the non-empty ranges (s_pre: the first element of each in
+//   the round's element sequence; s_off: its member-list position minus that
+//   element number), and the E elements of the round are cut into NW
+//   contiguous slices, one per warp, so every warp gets the same count
+//   whatever the lengths.  A warp walks its slice in windows of 32 elements
+//   (lane x takes element W + x): the ranges that start inside a window are
+//   the next listed ones after the range r holding element W - 1, so one
+//   shared-memory load of the next 32 starts and an OR of the bits
+//   (start - W) give each lane its range by a population count.  The member
+//   loads of R3_BATCH windows are issued before their counts.  Member-list
+//   positions are 32-bit here (ntree x n < 2^31, checked by the launcher).
+// ---------------------------------------------------------------------------
+constexpr int R3_BATCH = 4;
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 2048 / NT)
+pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
+                  int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
+                  int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+    constexpr int NW = NT / 32;
+    extern __shared__ uint32_t acc[];  // `words` words, two u16 counters each
+    __shared__ int s_off[NT];
+    __shared__ int s_pre[NT + 32];     // INT_MAX after the last listed range
+    __shared__ int s_wf[NW], s_wl[NW];  // per-warp totals: non-empty ranges, elements
+    const int i = order[blockIdx.x];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
+    unsigned long long my_pairs = 0;
+    const int2* orow = opp + (size_t)i * T;
+    for (int tb = 0; tb < T; tb += NT) {
+        const int t = tb + tid;
+        const int2 v = t < T ? __ldg(orow + t) : make_int2(0, 0);
+        const int len = v.y;
+        const int f = len > 0 ? 1 : 0;
+        my_pairs += (unsigned long long)len;
+        int fi = f, li = len;  // inclusive warp scans
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, fi, d);
+            const int b = __shfl_up_sync(0xffffffffu, li, d);
+            if (lane >= d) {
+                fi += a;
+                li += b;
+            }
         }
-        if (v < nv) s4[v] = make_int4((int)q0, (int)q1, (int)q2, (int)q3);
+        if (lane == 31) {
+            s_wf[w] = fi;
+            s_wl[w] = li;
+        }
+        // (also: every warp has finished the previous round's element phase
+        // before its list is overwritten below)
+        __syncthreads();
+        int wf = lane < NW ? s_wf[lane] : 0, wl = lane < NW ? s_wl[lane] : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, wf, d);
+            const int b = __shfl_up_sync(0xffffffffu, wl, d);
+            if (lane >= d) {
+                wf += a;
+                wl += b;
+            }
+        }
+        const int R = __shfl_sync(0xffffffffu, wf, 31);
+        const int E = __shfl_sync(0xffffffffu, wl, 31);
+        const int fb = __shfl_sync(0xffffffffu, wf, (w + 31) & 31);
+        const int lb = __shfl_sync(0xffffffffu, wl, (w + 31) & 31);
+        if (f) {
+            const int c = (w > 0 ? fb : 0) + fi - 1;
+            const int e0 = (w > 0 ? lb : 0) + li - len;
+            s_pre[c] = e0;
+            s_off[c] = t * n + v.x - e0;
+        }
+        if (tid < 32) s_pre[R + tid] = 0x7fffffff;
+        __syncthreads();
+        const int per = (E + NW - 1) / NW;
+        const int e_beg = w * per, e_end = min(E, e_beg + per);
+        if (e_beg < e_end) {
+            int lo = 0, hi = R;  // r: the listed range holding element e_beg
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pre[mid] <= e_beg) lo = mid;
+                else hi = mid;
+            }
+            int r = lo;
+            for (int W = e_beg; W < e_end; W += 32 * R3_BATCH) {
+                int j[R3_BATCH];
+#pragma unroll
+                for (int u = 0; u < R3_BATCH; ++u) {
+                    const int Wu = W + 32 * u;
+                    // ranges r + 1 ... start at or after Wu; those before Wu + 32 set bit (start - Wu)
+                    const int nl = s_pre[r + 1 + lane];
+                    const unsigned P = __reduce_or_sync(0xffffffffu, nl < Wu + 32 ? 1u << (nl - Wu) : 0u);
+                    const int x = Wu + lane;
+                    const int rc = r + __popc(P & (0xffffffffu >> (31 - lane)));
+                    j[u] = x < e_end ? __ldg(memb + (unsigned)(s_off[rc] + x)) : -1;
+                    r += __popc(P);
+                }
+#pragma unroll
+                for (int u = 0; u < R3_BATCH; ++u)
+                    if (j[u] >= 0) count16(acc, j[u]);
+            }
+        }
     }
-    for (int j = i + head + 4 * nv + tid; j < n; j += NT) srow[j - i] = (int32_t)a16[j];
+    __syncthreads();
+    row_write_out<NT>(acc, words, n, i, S, tid);
     if (pairs) {
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) my_pairs += __shfl_down_sync(0xffffffffu, my_pairs, d);
@@ -1004,10 +1138,14 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
         if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<256, 1>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<512, 1>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(pairs_row2_kernel<1024, 1>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row3_kernel<512>, dev_smem)) return s0;
+        if (rfx_status s0 = allow_dyn_smem(pairs_row3_kernel<1024>, dev_smem)) return s0;
+        // the balanced row kernel keeps member-list positions in 32 bits
+        const bool row3_ok = (long long)c->T * c->n < (1ll << 31);
         StageTimer st(c, ST_PAIRS, 1);
         // with hub tiles only the second row kernel (which starts from them) runs
         const int tk = hubs ? TK_PAIRS_HUB : TK_PAIRS16;
-        const int nshape = hubs ? 6 : PAIRS_SHAPES;
+        const int nshape = PAIRS_SHAPES;
         const int defshape = hubs ? 1 : PAIRS_DEFAULT_SHAPE;
         return autotune(c, tk, nshape, defshape, [&](int shape) -> rfx_status {
             // the pair counter restarts from the hub leaves' pair updates
@@ -1016,8 +1154,20 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
                                          c->stream));
             else
                 RFX_CUDA(cudaMemsetAsync(c->d_pairs, 0, sizeof(unsigned long long), c->stream));
-            // hub shapes 0-2: row2 with 256/512/1024 threads, binary-search
-            // short ranges; 3-5: the same with the start-mask lookup
+            // shapes 6-7 (with or without hub tiles): row3 with 512 / 1024
+            // threads (row2 1024 where row3 does not apply); hub shapes 0-2:
+            // row2 with 256/512/1024 threads, binary-search short ranges, 3-5:
+            // the same with the start-mask lookup; otherwise 0-2 row16 and
+            // 3-5 row2 with 256/512/1024 threads
+            if (shape >= 6 && row3_ok) {
+                auto kern = shape == 6 ? pairs_row3_kernel<512> : pairs_row3_kernel<1024>;
+                kern<<<c->n, shape == 6 ? 512 : 1024, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n,
+                                                                         c->T, words, hubs ? c->d_hubtiles : nullptr,
+                                                                         c->d_hubstate, dS, c->d_pairs);
+                RFX_CUDA(cudaGetLastError());
+                return RFX_OK;
+            }
+            if (shape >= 6) shape = 5;
             int sv = 0;
             if (hubs) {
                 sv = shape >= 3;

@@ -210,6 +210,16 @@ def test_bench_workload_matches_oracle(built):
     assert ctx.pair_updates() == U
     S_orc = torch.from_numpy(O["S"]).to(dev)
     assert torch.equal(S, S_orc)
+    # the same counts through the hub GEMM + row kernel (the bench's 1,000-tree
+    # path; 200 trees alone stay below the hub stage's switch-on)
+    os.environ["RFX_PAIRS_HUBS"] = "1"
+    try:
+        S.fill_(-1)
+        ctx.proximity_upper(S)
+        ctx.synchronize()
+    finally:
+        del os.environ["RFX_PAIRS_HUBS"]
+    assert torch.equal(S, S_orc)
     # finishprox on 2,000 rows: the members of the forest's largest leaves plus
     # seeded others, against the oracle's finishprox of the same rows
     P = torch.empty(L, dtype=torch.float32, device=dev)

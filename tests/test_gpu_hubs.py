@@ -35,7 +35,7 @@ def test_hub_counts_match_oracle(built, monkeypatch, n, T, seed, hub_min):
     monkeypatch.setenv("RFX_PAIRS_HUBS", "1")
     if hub_min is not None:
         monkeypatch.setenv("RFX_PAIRS_HUB_MIN", hub_min)
-    for shape in range(6):
+    for shape in range(8):
         monkeypatch.setenv("RFX_TUNE_PAIRS_HUB", str(shape))
         ctx = abi.Context(0)
         ctx.load(f, X, y)

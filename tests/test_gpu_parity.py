@@ -233,19 +233,24 @@ def test_window_crossing_rows(built, monkeypatch):
     ctx.close()
 
 
-def test_many_trees_two_rounds(built):
-    """More trees than one expansion round of the row kernel (1024)."""
+def test_many_trees_two_rounds(built, monkeypatch):
+    """More trees than one expansion round of the row kernels (512 / 1024
+    trees per round): the tuner's pick, and each balanced row kernel forced."""
     from oracle import oracle as orc
     from rfx_b200 import abi
 
     X, y, f = _grow(*synth.gaussian_classes(700, 6, 3, seed=4, mean_scale=0.7), 1100, 2)
     O = orc.analyse(X, y, f, do_imp=True)
-    ctx = abi.Context(0)
-    ctx.load(f, X, y)
-    assert np.array_equal(ctx.proximity_upper(), O["S"])
-    avimp, sqsd, qimp, qimpm = ctx.varimp(True)
-    assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"])
-    ctx.close()
+    for shape in (None, 6, 7):
+        if shape is not None:
+            monkeypatch.setenv("RFX_TUNE_PAIRS", str(shape))
+        ctx = abi.Context(0)
+        ctx.load(f, X, y)
+        assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
+        assert ctx.pair_updates() == int(O["S"].astype(np.int64).sum()), shape
+        avimp, sqsd, qimp, qimpm = ctx.varimp(True)
+        assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
+        ctx.close()
 
 
 def test_windowed_pair_kernel(built, monkeypatch):
@@ -315,7 +320,7 @@ def ok_leaf(term, f, t, node):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("stage,count", [("ROUTE", 10), ("PAIRS", 6), ("VWALK", 6), ("ROUTE_LEAF", 6)])
+@pytest.mark.parametrize("stage,count", [("ROUTE", 10), ("PAIRS", 8), ("VWALK", 6), ("ROUTE_LEAF", 6)])
 def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
     """Each launch shape the autotuner can pick gives the oracle's results."""
     from oracle import oracle as orc
