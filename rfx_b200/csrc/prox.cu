@@ -844,7 +844,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
 //   loads of R3_BATCH windows are issued before their counts.  Member-list
 //   positions are 32-bit here (ntree x n < 2^31, checked by the launcher).
 // ---------------------------------------------------------------------------
-constexpr int R3_BATCH = 4;
+constexpr int R3_BATCH = 8;
 
 template <int NT>
 __global__ void __launch_bounds__(NT, 2048 / NT)
@@ -858,12 +858,15 @@ pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ int s_wf[NW], s_wl[NW];  // per-warp totals: non-empty ranges, elements
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // the first round's ranges are loaded before the counters are set up, so
+    // the two loads are in flight together
+    const int2* orow = opp + (size_t)i * T;
+    const int2 v0 = tid < T ? __ldg(orow + tid) : make_int2(0, 0);
     row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
     unsigned long long my_pairs = 0;
-    const int2* orow = opp + (size_t)i * T;
     for (int tb = 0; tb < T; tb += NT) {
         const int t = tb + tid;
-        const int2 v = t < T ? __ldg(orow + t) : make_int2(0, 0);
+        const int2 v = tb == 0 ? v0 : t < T ? __ldg(orow + t) : make_int2(0, 0);
         const int len = v.y;
         const int f = len > 0 ? 1 : 0;
         my_pairs += (unsigned long long)len;
