@@ -78,64 +78,6 @@ __device__ __forceinline__ int imp_side_walk(const XR& xrow, const XR& xperm, in
     return -1;
 }
 
-// Two side walks advanced in lock step (walk b only if has_b), so the node
-// and feature loads of both are in flight together; each gives the result
-// imp_side_walk would give for it.
-// The permuted feature's value (the partner's) is the same at every node of
-// a walk, so it is passed in (qa, qb) rather than read per step.
-template <typename Src, typename XR>
-__device__ __forceinline__ void imp_side_walk2(const XR& xa, int ma, float qa, int ka, int ba, const XR& xb, int mb,
-                                               float qb, int kb, int bb, bool has_b, int p, const Src& nodes,
-                                               const int32_t* __restrict__ nclass_of, const int32_t* __restrict__ cgl,
-                                               int maxcat, int& ca, int& cb) {
-    bool ra = ba > 0, rb = has_b && bb > 0;  // still walking
-    ca = -1;
-    cb = -1;
-    int sa = 0, sb = 0;
-    while (ra || rb) {
-        const DNode na = nodes(ra ? ka : 0);
-        const DNode nb = nodes(rb ? kb : 0);
-        const int sta = node_status(na.meta), stb = node_status(nb.meta);
-        const int va = node_var(na.meta), vb = node_var(nb.meta);
-        const bool fa = ra && sta != -1 && va < p, fb = rb && stb != -1 && vb < p;
-        float xva = 0.0f, xvb = 0.0f;
-        if (fa) xva = va == ma ? qa : xa(va);
-        if (fb) xvb = vb == mb ? qb : xb(vb);
-        if (ra) {
-            if (sta == -1) {
-                ca = __ldg(nclass_of + ka);
-                ra = false;
-            } else if (!fa) {
-                ra = false;
-            } else {
-                const int nx = imp_decide(na, ka, xva, cgl, maxcat);
-                if (nx == DIR_BREAK) {
-                    ra = false;
-                } else {
-                    ka = nx;
-                    if (++sa >= ba) ra = false;
-                }
-            }
-        }
-        if (rb) {
-            if (stb == -1) {
-                cb = __ldg(nclass_of + kb);
-                rb = false;
-            } else if (!fb) {
-                rb = false;
-            } else {
-                const int nx = imp_decide(nb, kb, xvb, cgl, maxcat);
-                if (nx == DIR_BREAK) {
-                    rb = false;
-                } else {
-                    kb = nx;
-                    if (++sb >= bb) rb = false;
-                }
-            }
-        }
-    }
-}
-
 // OOB samples of every tree in ascending order (joob of cpu_varimp).
 __global__ void __launch_bounds__(VT)
 joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all,
@@ -409,25 +351,17 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         base_imp = (ok && jvr0 == yi);
     }
     __syncthreads();
-    // shared phase: every queued side walk, spread over the CTA's threads,
-    // entries e and e + VW walked together by thread e % VW
+    // shared phase: every queued side walk, spread over the CTA's threads
     const int qn = min(q_n, QCAP);
-    for (int e = tid; e < qn; e += 2 * VW) {
-        const bool has_b = e + VW < qn;
-        const int4 ea = q_ent[e];
-        const int4 eb = has_b ? q_ent[e + VW] : ea;
-        const int la = ea.x, lb = eb.x;
-        const float qa = RowSel<SX>{X + (size_t)s_ip[la] * p, xs_par + (size_t)la * ps}(ea.y);
-        const float qb = RowSel<SX>{X + (size_t)s_ip[lb] * p, xs_par + (size_t)lb * ps}(eb.y);
-        int ca, cb;
-        imp_side_walk2(RowSel<SX>{X + (size_t)s_i[la] * p, xs_own + (size_t)la * ps}, ea.y, qa, ea.z, ea.w,
-                       RowSel<SX>{X + (size_t)s_i[lb] * p, xs_own + (size_t)lb * ps}, eb.y, qb, eb.z, eb.w, has_b, p,
-                       src, tc, cgl, maxcat, ca, cb);
-        if (ca < 0 || (has_b && cb < 0)) my_err |= ERR_STALE_JVR;
-        const int ma = FB ? ea.y - fb : ea.y;
-        if (ca >= 0 && ca == s_y[la]) atomicOr(&s_pcorr[la][ma >> 6], 1ull << (ma & 63));
-        const int mb = FB ? eb.y - fb : eb.y;
-        if (has_b && cb >= 0 && cb == s_y[lb]) atomicOr(&s_pcorr[lb][mb >> 6], 1ull << (mb & 63));
+    for (int e = tid; e < qn; e += VW) {
+        const int4 en = q_ent[e];
+        const int lt = en.x, m = en.y;
+        const int cls_m = imp_side_walk(RowSel<SX>{X + (size_t)s_i[lt] * p, xs_own + (size_t)lt * ps},
+                                        RowSel<SX>{X + (size_t)s_ip[lt] * p, xs_par + (size_t)lt * ps}, m, p, en.z, en.w, src,
+                                        tc, cgl, maxcat);
+        if (cls_m < 0) my_err |= ERR_STALE_JVR;
+        const int mb = FB ? m - fb : m;
+        if (cls_m >= 0 && cls_m == s_y[lt]) atomicOr(&s_pcorr[lt][mb >> 6], 1ull << (mb & 63));
     }
     __syncthreads();
     if (active) {
