@@ -524,6 +524,24 @@ pairs_row16_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ mem
     }
 }
 
+// L2 prefetch of the inputs of row `ip`, which a CTA of a later wave takes
+// (the CTA ahead = resident CTAs after this one): its range row (T x 8 bytes)
+// and its hub tile row (256 bytes per column tile), one 128-byte line per
+// thread, so that row's first loads find them in L2 rather than DRAM.
+__device__ __forceinline__ void prefetch_row_l2(const int2* __restrict__ opp, int T, int n, int ip,
+                                                const uint8_t* __restrict__ hubt, int tid, int nt) {
+    const char* orow = reinterpret_cast<const char*>(opp + (size_t)ip * T);
+    const int olines = (T * 8 + 127) >> 7;
+    int k = tid;
+    for (; k < olines; k += nt)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(orow + ((size_t)k << 7)));
+    if (!hubt) return;
+    const int NJ = (n + 255) >> 8, I = ip >> 7, r = ip & 127, J0 = ip >> 8;
+    const uint8_t* rowt = hubt + (size_t)(hub_row_start(I, NJ) - (I >> 1)) * 32768u + (size_t)r * 256u;
+    for (k -= olines; k < (NJ - J0) * 2; k += nt)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(rowt + (size_t)(J0 + (k >> 1)) * 32768u + (k & 1) * 128));
+}
+
 // Row i's counters start from the hub leaves' counts when the hub tiles exist:
 // row i of the S_hub tiles (row block I = i / 128, column tiles J = i / 256 ..
 // NJ - 1; 16-byte chunk q of a tile row stored at slot q ^ (row % 16)),
@@ -639,7 +657,7 @@ template <int NT, int SV>
 __global__ void __launch_bounds__(NT, 2048 / NT)
 pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                   int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
-                  int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+                  int32_t* __restrict__ S, unsigned long long* __restrict__ pairs, int ahead) {
     constexpr int NW = NT / 32;
     extern __shared__ uint32_t acc[];  // `words` words, two u16 counters each
     __shared__ long long lbase[V2_LIST];
@@ -649,6 +667,10 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ uint8_t s_lid[NW][32];  // per warp: lanes with a non-empty short range
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (blockIdx.x + ahead < n) {
+        const bool hubs_on = hubt && hub_state[1] > 0;
+        prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubs_on ? hubt : nullptr, tid, NT);
+    }
     row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
     if (tid == 0) {
         s_nlong = 0;
@@ -850,7 +872,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT, 2048 / NT)
 pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                   int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
-                  int32_t* __restrict__ S, unsigned long long* __restrict__ pairs) {
+                  int32_t* __restrict__ S, unsigned long long* __restrict__ pairs, int ahead) {
     constexpr int NW = NT / 32;
     extern __shared__ uint32_t acc[];  // `words` words, two u16 counters each
     __shared__ int s_off[NT];
@@ -858,6 +880,10 @@ pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ int s_wf[NW], s_wl[NW];  // per-warp totals: non-empty ranges, elements
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (blockIdx.x + ahead < n) {
+        const bool hubs_on = hubt && hub_state[1] > 0;
+        prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubs_on ? hubt : nullptr, tid, NT);
+    }
     // the first round's ranges are loaded before the counters are set up, so
     // the two loads are in flight together
     const int2* orow = opp + (size_t)i * T;
@@ -924,13 +950,16 @@ pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
 #pragma unroll
                 for (int u = 0; u < R3_BATCH; ++u) {
                     const int Wu = W + 32 * u;
-                    // ranges r + 1 ... start at or after Wu; those before Wu + 32 set bit (start - Wu)
-                    const int nl = s_pre[r + 1 + lane];
-                    const unsigned P = __reduce_or_sync(0xffffffffu, nl < Wu + 32 ? 1u << (nl - Wu) : 0u);
-                    const int x = Wu + lane;
-                    const int rc = r + __popc(P & (0xffffffffu >> (31 - lane)));
-                    j[u] = x < e_end ? __ldg(memb + (unsigned)(s_off[rc] + x)) : -1;
-                    r += __popc(P);
+                    j[u] = -1;
+                    if (Wu < e_end) {  // the same for the whole warp: windows past the slice are skipped
+                        // ranges r + 1 ... start at or after Wu; those before Wu + 32 set bit (start - Wu)
+                        const int nl = s_pre[r + 1 + lane];
+                        const unsigned P = __reduce_or_sync(0xffffffffu, nl < Wu + 32 ? 1u << (nl - Wu) : 0u);
+                        const int x = Wu + lane;
+                        const int rc = r + __popc(P & (0xffffffffu >> (31 - lane)));
+                        if (x < e_end) j[u] = __ldg(memb + (unsigned)(s_off[rc] + x));
+                        r += __popc(P);
+                    }
                 }
 #pragma unroll
                 for (int u = 0; u < R3_BATCH; ++u)
@@ -1162,11 +1191,20 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
             // row2 with 256/512/1024 threads, binary-search short ranges, 3-5:
             // the same with the start-mask lookup; otherwise 0-2 row16 and
             // 3-5 row2 with 256/512/1024 threads
+            // a CTA prefetches into L2 the inputs of the row that the CTA one
+            // wave of resident CTAs later takes
+            auto ahead_of = [&](auto kern, int nt) -> int {
+                int occ = 1, sms = 148;
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nt, smem);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+                return std::max(1, occ) * sms;
+            };
             if (shape >= 6 && row3_ok) {
                 auto kern = shape == 6 ? pairs_row3_kernel<512> : pairs_row3_kernel<1024>;
-                kern<<<c->n, shape == 6 ? 512 : 1024, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n,
-                                                                         c->T, words, hubs ? c->d_hubtiles : nullptr,
-                                                                         c->d_hubstate, dS, c->d_pairs);
+                const int nt = shape == 6 ? 512 : 1024;
+                kern<<<c->n, nt, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, words,
+                                                    hubs ? c->d_hubtiles : nullptr, c->d_hubstate, dS, c->d_pairs,
+                                                    ahead_of(kern, nt));
                 RFX_CUDA(cudaGetLastError());
                 return RFX_OK;
             }
@@ -1183,7 +1221,8 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
                                : (shape == 3 ? pairs_row2_kernel<256, 0> : shape == 4 ? pairs_row2_kernel<512, 0>
                                                                                         : pairs_row2_kernel<1024, 0>);
                 kern<<<c->n, nt, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T, words,
-                                                    hubs ? c->d_hubtiles : nullptr, c->d_hubstate, dS, c->d_pairs);
+                                                    hubs ? c->d_hubtiles : nullptr, c->d_hubstate, dS, c->d_pairs,
+                                                    ahead_of(kern, nt));
             } else if (shape == 0)
                 pairs_row16_kernel<256><<<c->n, 256, smem, c->stream>>>(c->d_opp, c->d_memb, c->d_order, c->n, c->T,
                                                                        dS, c->d_pairs);
