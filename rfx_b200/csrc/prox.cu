@@ -542,33 +542,49 @@ __device__ __forceinline__ void prefetch_row_l2(const int2* __restrict__ opp, in
         asm volatile("prefetch.global.L2 [%0];" ::"l"(rowt + (size_t)(J0 + (k >> 1)) * 32768u + (k & 1) * 128));
 }
 
-// Row i's counters start from the hub leaves' counts when the hub tiles exist:
-// row i of the S_hub tiles (row block I = i / 128, column tiles J = i / 256 ..
-// NJ - 1; 16-byte chunk q of a tile row stored at slot q ^ (row % 16)),
-// u8 -> u16; otherwise from zero.
+// Row i's counters start from the hub leaves' counts when the hub tiles exist
+// and hold a hub: row i of the S_hub tiles (row block I = i / 128, column
+// tiles J = i / 256 .. NJ - 1; 16-byte chunk q of a tile row stored at slot
+// q ^ (row % 16)), u8 -> u16; otherwise from zero.
 template <int NT>
 __device__ __forceinline__ void row_counters_init(uint32_t* acc, int words, int n, int i,
                                                   const uint8_t* __restrict__ hubt,
                                                   const int32_t* __restrict__ hub_state, int tid) {
-    if (hubt && hub_state[1] > 0) {
+    if (hubt) {
+        // the tile loads go out with the load of the hub count (the tiles are
+        // allocated whether or not any hub was found), two per thread at a time
+        const int nh = __ldg(hub_state + 1);
         const int NJ = (n + 255) >> 8, I = i >> 7, r = i & 127, J0 = i >> 8;
         const uint8_t* rowt = hubt + (size_t)(hub_row_start(I, NJ) - (I >> 1)) * 32768u + (size_t)r * 256u;
         const int nch = (NJ - J0) * 16;
-        for (int k = tid; k < nch; k += NT) {
-            const int J = J0 + (k >> 4), slot = k & 15, q = slot ^ (r & 15);
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(rowt + (size_t)J * 32768u + slot * 16));
-            const uint32_t b[4] = {v.x, v.y, v.z, v.w};
-            uint32_t o[8];
-            // bytes (b0 b1 b2 b3) -> u16 pairs (b0, b1) and (b2, b3): one byte permute each
+        for (int k0 = tid; k0 < nch; k0 += 2 * NT) {
+            uint4 v[2];
 #pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                o[2 * h] = __byte_perm(b[h], 0u, 0x4140u);
-                o[2 * h + 1] = __byte_perm(b[h], 0u, 0x4342u);
+            for (int u = 0; u < 2; ++u) {
+                const int k = k0 + u * NT;
+                const int J = J0 + (k >> 4), slot = k & 15;
+                v[u] = k < nch ? __ldg(reinterpret_cast<const uint4*>(rowt + (size_t)J * 32768u + slot * 16))
+                               : make_uint4(0u, 0u, 0u, 0u);
             }
-            uint4* dst = reinterpret_cast<uint4*>(acc + (size_t)J * 128 + q * 8);
-            dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-            dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int k = k0 + u * NT;
+                if (k >= nch) break;
+                const int J = J0 + (k >> 4), q = (k & 15) ^ (r & 15);
+                const uint32_t b[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+                uint32_t o[8];
+                // bytes (b0 b1 b2 b3) -> u16 pairs (b0, b1) and (b2, b3): one byte permute each
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    o[2 * h] = nh > 0 ? __byte_perm(b[h], 0u, 0x4140u) : 0u;
+                    o[2 * h + 1] = nh > 0 ? __byte_perm(b[h], 0u, 0x4342u) : 0u;
+                }
+                uint4* dst = reinterpret_cast<uint4*>(acc + (size_t)J * 128 + q * 8);
+                dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+                dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+            }
         }
+        // (words below J0 * 128 hold columns before i: never counted or written)
         for (int k = NJ * 128 + tid; k < words; k += NT) acc[k] = 0u;
     } else {
         uint4* a4 = reinterpret_cast<uint4*>(acc);
@@ -667,11 +683,8 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ uint8_t s_lid[NW][32];  // per warp: lanes with a non-empty short range
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (blockIdx.x + ahead < n) {
-        const bool hubs_on = hubt && hub_state[1] > 0;
-        prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubs_on ? hubt : nullptr, tid, NT);
-    }
     row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
+    if (blockIdx.x + ahead < n) prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubt, tid, NT);
     if (tid == 0) {
         s_nlong = 0;
         s_chunk = 0;
@@ -868,8 +881,10 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
 // ---------------------------------------------------------------------------
 constexpr int R3_BATCH = 8;
 
+// (two CTAs per SM: a row's counters take up to half the shared memory at the
+// sizes this form serves, so 512 threads get 64 registers and 1024 get 32)
 template <int NT>
-__global__ void __launch_bounds__(NT, 2048 / NT)
+__global__ void __launch_bounds__(NT, 2)
 pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb, const int32_t* __restrict__ order,
                   int n, int T, int words, const uint8_t* __restrict__ hubt, const int32_t* __restrict__ hub_state,
                   int32_t* __restrict__ S, unsigned long long* __restrict__ pairs, int ahead) {
@@ -880,15 +895,12 @@ pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ int s_wf[NW], s_wl[NW];  // per-warp totals: non-empty ranges, elements
     const int i = order[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (blockIdx.x + ahead < n) {
-        const bool hubs_on = hubt && hub_state[1] > 0;
-        prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubs_on ? hubt : nullptr, tid, NT);
-    }
     // the first round's ranges are loaded before the counters are set up, so
     // the two loads are in flight together
     const int2* orow = opp + (size_t)i * T;
     const int2 v0 = tid < T ? __ldg(orow + tid) : make_int2(0, 0);
     row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
+    if (blockIdx.x + ahead < n) prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubt, tid, NT);
     unsigned long long my_pairs = 0;
     for (int tb = 0; tb < T; tb += NT) {
         const int t = tb + tid;
