@@ -682,9 +682,10 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ int lpre[V2_LIST];       // first piece number of each listed long range
     __shared__ uint8_t s_lid[NW][32];  // per warp: lanes with a non-empty short range
     const int i = order[blockIdx.x];
+    const int ipf = blockIdx.x + ahead < n ? order[blockIdx.x + ahead] : -1;  // the row prefetched below
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
-    if (blockIdx.x + ahead < n) prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubt, tid, NT);
+    if (ipf >= 0) prefetch_row_l2(opp, T, n, ipf, hubt, tid, NT);
     if (tid == 0) {
         s_nlong = 0;
         s_chunk = 0;
@@ -879,7 +880,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
 //   loads of R3_BATCH windows are issued before their counts.  Member-list
 //   positions are 32-bit here (ntree x n < 2^31, checked by the launcher).
 // ---------------------------------------------------------------------------
-constexpr int R3_BATCH = 8;
+constexpr int R3_BATCH = 12;
 
 // (two CTAs per SM: a row's counters take up to half the shared memory at the
 // sizes this form serves, so 512 threads get 64 registers and 1024 get 32)
@@ -894,13 +895,14 @@ pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
     __shared__ int s_pre[NT + 32];     // INT_MAX after the last listed range
     __shared__ int s_wf[NW], s_wl[NW];  // per-warp totals: non-empty ranges, elements
     const int i = order[blockIdx.x];
+    const int ipf = blockIdx.x + ahead < n ? order[blockIdx.x + ahead] : -1;  // the row prefetched below
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     // the first round's ranges are loaded before the counters are set up, so
     // the two loads are in flight together
     const int2* orow = opp + (size_t)i * T;
     const int2 v0 = tid < T ? __ldg(orow + tid) : make_int2(0, 0);
     row_counters_init<NT>(acc, words, n, i, hubt, hub_state, tid);
-    if (blockIdx.x + ahead < n) prefetch_row_l2(opp, T, n, order[blockIdx.x + ahead], hubt, tid, NT);
+    if (ipf >= 0) prefetch_row_l2(opp, T, n, ipf, hubt, tid, NT);
     unsigned long long my_pairs = 0;
     for (int tb = 0; tb < T; tb += NT) {
         const int t = tb + tid;
