@@ -880,7 +880,7 @@ pairs_row2_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
 //   loads of R3_BATCH windows are issued before their counts.  Member-list
 //   positions are 32-bit here (ntree x n < 2^31, checked by the launcher).
 // ---------------------------------------------------------------------------
-constexpr int R3_BATCH = 12;
+constexpr int R3_BATCH = 8;
 
 // (two CTAs per SM: a row's counters take up to half the shared memory at the
 // sizes this form serves, so 512 threads get 64 registers and 1024 get 32)
