@@ -253,13 +253,16 @@ rfx_status rfx_lowrank_quantize(rfx_ctx* ctx, int format, void* q, float* scales
  * operator in FP32; precision 1 (rank 32 or 64) runs tcgen05 BF16 GEMMs with
  * FP32 accumulation until the iteration stalls at the BF16 rounding level, then
  * takes one FP32 step (an FP32 operator product and Rayleigh-Ritz) from that
- * basis. */
+ * basis; precision 3 does the same with FP8 E4M3 operands (tcgen05
+ * kind::f8f6f4, a scale per factor column, per stack row and per block
+ * column, FP32 accumulation).  Other non-zero values mean 1. */
 rfx_status rfx_mds_from_factors(rfx_ctx* ctx, int k, int use_quantized, int precision, double* coords,
                                 double* evals);
 
 /* One application W = B V of the double-centred factor-space MDS operator of
  * rfx_mds_from_factors to an n x 16 FP64 block V (row-major; host or device);
- * precision 0 = FP32 products, 1 = tcgen05 BF16 products (rank 32 or 64). */
+ * precision 0 = FP32 products, 1 = tcgen05 BF16 products, 3 = tcgen05 FP8
+ * E4M3 products (rank 32 or 64 for either). */
 rfx_status rfx_factor_mds_operator(rfx_ctx* ctx, int use_quantized, int precision, const double* V, double* W);
 
 /* Outlier scores from the factors (compute_outlier_scores,

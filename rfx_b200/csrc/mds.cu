@@ -935,8 +935,8 @@ __global__ void ata_kernel(const float* __restrict__ A, int n, int k, double* __
 }  // namespace
 
 rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const uint8_t* Aq, const uint8_t* At,
-                                const float* u32, float* M, float* T2);
-rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* At);
+                                const float* sA, const float* u32, float* M, float* T2);
+rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* At, float* sA);
 size_t factor_tc_aq_bytes(int n, int k);
 size_t factor_tc_at_bytes(int n, int k);
 
@@ -978,13 +978,14 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     bool tensor = false;
     uint8_t* Aq = nullptr;
     uint8_t* At = nullptr;
+    float* sA = nullptr;  // FP8 column scales (precision 3)
     auto apply = [&](const double* V, double* W) -> rfx_status {
         const unsigned gr = (unsigned)(((size_t)n * S_BLK + 255) / 256);
         col_mean(V, n, part, mean, s);
         center_kernel<<<gr, 256, 0, s>>>(V, mean, n, u, u32);
         at_u(dA, u, n, k, part, AtU, s);
         if (tensor) {
-            rfx_status st = launch_factor_ops_tc(c, dA, k, Aq, At, u32, M, T2);
+            rfx_status st = launch_factor_ops_tc(c, dA, k, Aq, At, sA, u32, M, T2);
             if (st != RFX_OK) return st;
         } else {
             mstack_f32(dA, u32, n, k, Mpart, M, s);
@@ -1000,17 +1001,18 @@ rfx_status launch_mds_factors(Ctx* c, const float* dA, int k, int ndim, int max_
     };
     if (precision == 0 || (k != 32 && k != 64))
         return subspace_topk(c, n, ndim, apply, max_iter, d_coords, evals, 12345, tol, nullptr, nullptr, iters, true);
-    // mixed: BF16 tensor-core iterations to the BF16 rounding floor, then one
-    // FP32 refinement step from that basis
+    // mixed: tensor-core iterations (BF16, or FP8 E4M3 for precision 3) to
+    // their rounding floor, then one FP32 refinement step from that basis
     double* basis = d.get<double>((size_t)n * S_BLK);
     Aq = d.get<uint8_t>(factor_tc_aq_bytes(n, k));
     At = d.get<uint8_t>(factor_tc_at_bytes(n, k));
-    if (!basis || !Aq || !At) {
+    if (precision == 3) sA = d.get<float>((size_t)k);
+    if (!basis || !Aq || !At || (precision == 3 && !sA)) {
         set_error("compute_mds_from_factors: device allocation failed");
         return RFX_ERR_OOM;
     }
-    // the factor's BF16 tensor-core operands, packed once for every product
-    if (rfx_status pst = pack_factor_tc(c, dA, k, Aq, At)) return pst;
+    // the factor's tensor-core operands, packed once for every product
+    if (rfx_status pst = pack_factor_tc(c, dA, k, Aq, At, sA)) return pst;
     tensor = true;
     int it1 = 0, it2 = 0;
     rfx_status st =
@@ -1055,9 +1057,10 @@ rfx_status launch_factor_operator(Ctx* c, const float* dA, int k, const double* 
     if (precision) {
         uint8_t* Aq = d.get<uint8_t>(factor_tc_aq_bytes(n, k));
         uint8_t* At = d.get<uint8_t>(factor_tc_at_bytes(n, k));
-        if (!Aq || !At) return RFX_ERR_OOM;
-        st = pack_factor_tc(c, dA, k, Aq, At);
-        if (st == RFX_OK) st = launch_factor_ops_tc(c, dA, k, Aq, At, u32, M, T2);
+        float* sA = precision == 3 ? d.get<float>((size_t)k) : nullptr;
+        if (!Aq || !At || (precision == 3 && !sA)) return RFX_ERR_OOM;
+        st = pack_factor_tc(c, dA, k, Aq, At, sA);
+        if (st == RFX_OK) st = launch_factor_ops_tc(c, dA, k, Aq, At, sA, u32, M, T2);
     } else {
         const size_t qsm = 4 * (size_t)k * k * sizeof(float);
         RFX_CUDA(cudaFuncSetAttribute(quadform_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)qsm));

@@ -31,6 +31,7 @@
 // raises ERR_WAIT_LIMIT, and the CTA drains its copies and MMAs (again with
 // bounded waits) before it frees TMEM and returns.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include "rfx_internal.cuh"
 
@@ -53,17 +54,50 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// byte offset of (row r, k) in a canonical tile of R rows: 16-wide K steps of
-// R * 32 bytes each
-__host__ __device__ __forceinline__ uint32_t canon_off(int r, int k, int R) {
-    return (uint32_t)((k >> 4) * (R * 32) + (r >> 3) * 256 + ((k >> 3) & 1) * 128 + (r & 7) * 16 + (k & 7) * 2);
+__host__ __device__ constexpr uint32_t idesc_e4m3_f32(int M, int N) {
+    // kind::f8f6f4 with A and B both E4M3 (type code 0), FP32 accumulation
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
+
+// byte offset of (row r, K byte kb) in a canonical tile of R rows: K steps of
+// 32 bytes (16 BF16 or 32 FP8 elements, one MMA's K), R * 32 bytes each
+__host__ __device__ __forceinline__ uint32_t canon_off_b(int r, int kb, int R) {
+    return (uint32_t)((kb >> 5) * (R * 32) + (r >> 3) * 256 + ((kb >> 4) & 1) * 128 + (r & 7) * 16 + (kb & 15));
+}
+
+// the same for the BF16 element k
+__host__ __device__ __forceinline__ uint32_t canon_off(int r, int k, int R) { return canon_off_b(r, 2 * k, R); }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
         "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_e4m3(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+template <bool F8>
+__device__ __forceinline__ void mma_op(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    if constexpr (F8) mma_e4m3(tmem_d, a, b, idesc, acc);
+    else mma_bf16(tmem_d, a, b, idesc, acc);
+}
+
+// FP8 E4M3 conversions (round to nearest, saturating to +-448)
+__device__ __forceinline__ uint32_t pack_e4m3x4(float a, float b, float c, float d) {
+    const uint32_t lo = __nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t hi = __nv_cvt_float2_to_fp8x2(make_float2(c, d), __NV_SATFINITE, __NV_E4M3);
+    return lo | (hi << 16);
+}
+
+__device__ __forceinline__ float2 e4m3x2_to_float2(uint32_t two) {
+    const __half2_raw h = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)two, __NV_E4M3);
+    return __half22float2(*reinterpret_cast<const __half2*>(&h));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t mbar) {
@@ -179,25 +213,96 @@ __global__ void pack_at_kernel(const float* __restrict__ A, int n, int nch, uint
     *reinterpret_cast<uint4*>(At + ch * (size_t)(K_ * CH * 2) + canon_off(a, g * 8, K_)) = o;
 }
 
-// uT: 32-sample chunks of u^T in FP32, [chunk][j][32], samples >= n zero.
-__global__ void pack_ut_kernel(const float* __restrict__ u, int n, int nch, float* __restrict__ uT) {
+// uT: 32-sample chunks of u^T in FP32, [chunk][j][32], samples >= n zero;
+// with umax (the FP8 form) every column j divided by its largest magnitude.
+__global__ void pack_ut_kernel(const float* __restrict__ u, int n, int nch, const unsigned* __restrict__ umax,
+                               float* __restrict__ uT) {
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (size_t)nch * CH * S_) return;
     const size_t i = idx / S_;
     const int j = (int)(idx % S_);
     const size_t ch = i / CH;
     const int w = (int)(i % CH);
-    uT[(ch * S_ + j) * CH + w] = i < (size_t)n ? u[idx] : 0.0f;
+    float v = i < (size_t)n ? u[idx] : 0.0f;
+    if (umax) {
+        const float m = __uint_as_float(umax[j]);
+        v = m > 0.0f ? v / m : 0.0f;
+    }
+    uT[(ch * S_ + j) * CH + w] = v;
+}
+
+// largest |x| of every column of an n x cols FP32 matrix (bit patterns of
+// non-negative floats order like the values), into zeroed mx
+__global__ void col_absmax_kernel(const float* __restrict__ X, int64_t count, int cols, unsigned* __restrict__ mx) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= count) return;
+    const float v = fabsf(X[idx]);
+    if (v > 0.0f) atomicMax(mx + (idx % cols), __float_as_uint(v));
+}
+
+// FP8 operands of the factor (the FP8 form): column scales sA[a] = max |A[:, a]| / 448,
+// Aq8 as Aq with E4M3(A / sA) bytes (K = rank bytes), At8 as At (K = 32
+// samples = one 32-byte K step).
+__global__ void col_scale_kernel(const unsigned* __restrict__ mx, int k, float* __restrict__ sA) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= k) return;
+    const float m = __uint_as_float(mx[a]);
+    sA[a] = m > 0.0f ? m / 448.0f : 1.0f;
+}
+
+template <int K_>
+__global__ void pack_aq8_kernel(const float* __restrict__ A, const float* __restrict__ sA, int n, int ntiles,
+                                uint8_t* __restrict__ Aq) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // one (tile row, 16-wide K group)
+    const size_t total = (size_t)ntiles * 128 * (K_ / 16);
+    if (idx >= total) return;
+    const int kg = (int)(idx % (K_ / 16));
+    const size_t row = idx / (K_ / 16);
+    const int tile = (int)(row / 128), r = (int)(row % 128);
+    float v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = row < (size_t)n ? A[row * K_ + kg * 16 + q] / sA[kg * 16 + q] : 0.0f;
+    uint4 o;
+    o.x = pack_e4m3x4(v[0], v[1], v[2], v[3]);
+    o.y = pack_e4m3x4(v[4], v[5], v[6], v[7]);
+    o.z = pack_e4m3x4(v[8], v[9], v[10], v[11]);
+    o.w = pack_e4m3x4(v[12], v[13], v[14], v[15]);
+    *reinterpret_cast<uint4*>(Aq + (size_t)tile * (128 * K_) + canon_off_b(r, kg * 16, 128)) = o;
+}
+
+template <int K_>
+__global__ void pack_at8_kernel(const float* __restrict__ A, const float* __restrict__ sA, int n, int nch,
+                                uint8_t* __restrict__ At) {
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // one (chunk, a, 16-sample group)
+    const size_t total = (size_t)nch * K_ * (CH / 16);
+    if (idx >= total) return;
+    const int g = (int)(idx % (CH / 16));
+    const int a = (int)((idx / (CH / 16)) % K_);
+    const size_t ch = idx / ((size_t)(CH / 16) * K_);
+    const float inv = 1.0f / sA[a];
+    float v[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const size_t i = ch * CH + g * 16 + q;
+        v[q] = i < (size_t)n ? A[i * K_ + a] * inv : 0.0f;
+    }
+    uint4 o;
+    o.x = pack_e4m3x4(v[0], v[1], v[2], v[3]);
+    o.y = pack_e4m3x4(v[4], v[5], v[6], v[7]);
+    o.z = pack_e4m3x4(v[8], v[9], v[10], v[11]);
+    o.w = pack_e4m3x4(v[12], v[13], v[14], v[15]);
+    *reinterpret_cast<uint4*>(At + ch * (size_t)(K_ * CH) + canon_off_b(a, g * 16, K_)) = o;
 }
 
 // ---------------------------------------------------------------------------
 // M stack
 
-template <int K_>
+template <int K_, bool F8>
 struct MsCfg {
+    static constexpr int EB = F8 ? 1 : 2;                  // bytes per operand element
     static constexpr int MT = S_ * K_ / 128;               // M tiles
-    static constexpr uint32_t AOP = MT * 128 * CH * 2;     // scaled operand per stage
-    static constexpr uint32_t ATB = K_ * CH * 2;           // A^T chunk
+    static constexpr uint32_t AOP = MT * 128 * CH * EB;    // scaled operand per stage
+    static constexpr uint32_t ATB = K_ * CH * EB;          // A^T chunk
     static constexpr uint32_t UTB = S_ * CH * 4;           // u^T chunk
     static constexpr uint32_t STB = AOP + ATB + UTB;
     static constexpr int ST = K_ == 64 ? 3 : 4;            // stages
@@ -208,11 +313,11 @@ struct MsCfg {
 // 192 threads: warps 0-3 build the scaled operand and run the epilogue, warp 4
 // lane 0 loads, warp 5 lane 0 issues the MMAs.  CTA b owns chunks
 // [b * per, min(nch, (b + 1) * per)) and writes partial b.
-template <int K_>
+template <int K_, bool F8>
 __global__ void __launch_bounds__(192, 1) mstack_tc_kernel(const uint8_t* __restrict__ At, const float* __restrict__ uT,
                                                           int nch, int per, float* __restrict__ Mpart,
                                                           uint32_t* __restrict__ err) {
-    using C = MsCfg<K_>;
+    using C = MsCfg<K_, F8>;
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ __align__(8) uint64_t full[C::ST], aready[C::ST], empty[C::ST], done;
     __shared__ uint32_t tmem_base;
@@ -257,7 +362,7 @@ __global__ void __launch_bounds__(192, 1) mstack_tc_kernel(const uint8_t* __rest
         }
     } else if (warp == 5) {
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_bf16_f32(128, K_);
+            constexpr uint32_t idesc = F8 ? idesc_e4m3_f32(128, K_) : idesc_bf16_f32(128, K_);
             for (int it = 0; it < cnt && ok; ++it) {
                 const int s = it % C::ST;
                 if (!mbar_wait(smem_u32(&aready[s]), (uint32_t)((it / C::ST) & 1))) {
@@ -269,9 +374,9 @@ __global__ void __launch_bounds__(192, 1) mstack_tc_kernel(const uint8_t* __rest
 #pragma unroll
                 for (int m = 0; m < C::MT; ++m)
 #pragma unroll
-                    for (int ks = 0; ks < CH / 16; ++ks)
-                        mma_bf16(tmem + m * K_, umma_desc(st + m * (128 * CH * 2) + ks * (128 * 32)),
-                                 umma_desc(st + C::AOP + ks * (K_ * 32)), idesc, (it > 0 || ks > 0) ? 1u : 0u);
+                    for (int ks = 0; ks < CH * C::EB / 32; ++ks)
+                        mma_op<F8>(tmem + m * K_, umma_desc(st + m * (128 * CH * C::EB) + ks * (128 * 32)),
+                                   umma_desc(st + C::AOP + ks * (K_ * 32)), idesc, (it > 0 || ks > 0) ? 1u : 0u);
                 mma_commit(smem_u32(&empty[s]));
             }
             mma_commit(smem_u32(&done));  // arrives once every MMA issued above has finished
@@ -290,28 +395,59 @@ __global__ void __launch_bounds__(192, 1) mstack_tc_kernel(const uint8_t* __rest
             uint8_t* st = sm + s * C::STB;
             const uint8_t* at = st + C::AOP;
             const float* ut = reinterpret_cast<const float*>(st + C::AOP + C::ATB);
+            if constexpr (F8) {
+                // 16 samples per 16-byte store; u^T arrives divided by its
+                // column's largest magnitude, so every product fits E4M3
 #pragma unroll
-            for (int g = 0; g < CH / 8; ++g) {
-                const uint4 av = *reinterpret_cast<const uint4*>(at + canon_off(a, g * 8, K_));
-                const __nv_bfloat162* ab = reinterpret_cast<const __nv_bfloat162*>(&av);
-                float x[8];
+                for (int g = 0; g < CH / 16; ++g) {
+                    const uint4 av = *reinterpret_cast<const uint4*>(at + canon_off_b(a, g * 16, K_));
+                    const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+                    float x[16];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float2 f = __bfloat1622float2(ab[q]);
-                    x[2 * q] = f.x;
-                    x[2 * q + 1] = f.y;
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 lo = e4m3x2_to_float2(aw[q] & 0xffffu), hi = e4m3x2_to_float2(aw[q] >> 16);
+                        x[4 * q] = lo.x;
+                        x[4 * q + 1] = lo.y;
+                        x[4 * q + 2] = hi.x;
+                        x[4 * q + 3] = hi.y;
+                    }
+#pragma unroll
+                    for (int m = 0; m < C::MT; ++m) {
+                        const int j = m * (128 / K_) + jr;
+                        const float4* up = reinterpret_cast<const float4*>(ut + j * CH + g * 16);
+                        const float4 u0 = up[0], u1 = up[1], u2 = up[2], u3 = up[3];
+                        uint4 o;
+                        o.x = pack_e4m3x4(u0.x * x[0], u0.y * x[1], u0.z * x[2], u0.w * x[3]);
+                        o.y = pack_e4m3x4(u1.x * x[4], u1.y * x[5], u1.z * x[6], u1.w * x[7]);
+                        o.z = pack_e4m3x4(u2.x * x[8], u2.y * x[9], u2.z * x[10], u2.w * x[11]);
+                        o.w = pack_e4m3x4(u3.x * x[12], u3.y * x[13], u3.z * x[14], u3.w * x[15]);
+                        *reinterpret_cast<uint4*>(st + m * (128 * CH) + canon_off_b(r, g * 16, 128)) = o;
+                    }
                 }
+            } else {
 #pragma unroll
-                for (int m = 0; m < C::MT; ++m) {
-                    const int j = m * (128 / K_) + jr;
-                    const float4 u0 = *reinterpret_cast<const float4*>(ut + j * CH + g * 8);
-                    const float4 u1 = *reinterpret_cast<const float4*>(ut + j * CH + g * 8 + 4);
-                    uint4 o;
-                    o.x = pack_bf16x2(u0.x * x[0], u0.y * x[1]);
-                    o.y = pack_bf16x2(u0.z * x[2], u0.w * x[3]);
-                    o.z = pack_bf16x2(u1.x * x[4], u1.y * x[5]);
-                    o.w = pack_bf16x2(u1.z * x[6], u1.w * x[7]);
-                    *reinterpret_cast<uint4*>(st + m * (128 * CH * 2) + canon_off(r, g * 8, 128)) = o;
+                for (int g = 0; g < CH / 8; ++g) {
+                    const uint4 av = *reinterpret_cast<const uint4*>(at + canon_off(a, g * 8, K_));
+                    const __nv_bfloat162* ab = reinterpret_cast<const __nv_bfloat162*>(&av);
+                    float x[8];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 f = __bfloat1622float2(ab[q]);
+                        x[2 * q] = f.x;
+                        x[2 * q + 1] = f.y;
+                    }
+#pragma unroll
+                    for (int m = 0; m < C::MT; ++m) {
+                        const int j = m * (128 / K_) + jr;
+                        const float4 u0 = *reinterpret_cast<const float4*>(ut + j * CH + g * 8);
+                        const float4 u1 = *reinterpret_cast<const float4*>(ut + j * CH + g * 8 + 4);
+                        uint4 o;
+                        o.x = pack_bf16x2(u0.x * x[0], u0.y * x[1]);
+                        o.y = pack_bf16x2(u0.z * x[2], u0.w * x[3]);
+                        o.z = pack_bf16x2(u1.x * x[4], u1.y * x[5]);
+                        o.w = pack_bf16x2(u1.z * x[6], u1.w * x[7]);
+                        *reinterpret_cast<uint4*>(st + m * (128 * CH * 2) + canon_off(r, g * 8, 128)) = o;
+                    }
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -378,27 +514,72 @@ __global__ void mstack_reduce_kernel(const float* __restrict__ Mpart, int parts,
         __float2bfloat16_rn(acc);
 }
 
+// FP8 form: one warp per row R = (j, x) of the stack.  M[R][y] = U_j s_x s_y
+// D[R][y] (the partials summed in CTA order; U_j = the largest |u| of column
+// j, s = the factor's column scales), and the quadratic-form operand row
+// (j, x), K = y: E4M3(M[R][y] s_y / t_R) with t_R = max_y |M[R][y] s_y| / 448
+// kept in tq.
+template <int K_>
+__global__ void mstack_reduce8_kernel(const float* __restrict__ Mpart, int parts, const unsigned* __restrict__ umax,
+                                      const float* __restrict__ sA, float* __restrict__ M, uint8_t* __restrict__ Mq,
+                                      float* __restrict__ tq) {
+    const int R = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    constexpr int count = S_ * K_ * K_;
+    constexpr int PL = K_ / 32;  // columns per lane
+    if (R >= S_ * K_) return;
+    const int j = R / K_, x = R % K_;
+    const float sc = __uint_as_float(umax[j]) * sA[x];
+    float v[PL];
+    float amax = 0.0f;
+#pragma unroll
+    for (int q = 0; q < PL; ++q) {
+        const int y = q * 32 + lane;
+        float acc = 0.0f;
+        for (int p = 0; p < parts; ++p) acc += Mpart[(size_t)p * count + (size_t)R * K_ + y];
+        const float m = acc * sc * sA[y];
+        M[(size_t)R * K_ + y] = m;
+        v[q] = m * sA[y];
+        amax = fmaxf(amax, fabsf(v[q]));
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, d));
+    const float t = amax > 0.0f ? amax / 448.0f : 1.0f;
+    const int pass = R / NP, rl = R % NP;
+#pragma unroll
+    for (int q = 0; q < PL; ++q) {
+        const int y = q * 32 + lane;
+        Mq[(size_t)pass * (NP * K_) + canon_off_b(rl, y, NP)] =
+            (uint8_t)(__nv_cvt_float2_to_fp8x2(make_float2(v[q] / t, 0.0f), __NV_SATFINITE, __NV_E4M3) & 0xffu);
+    }
+    if (lane == 0) tq[R] = t;
+}
+
 // ---------------------------------------------------------------------------
 // Quadratic forms
 
-template <int K_>
+template <int K_, bool F8>
 struct QfCfg {
+    static constexpr int EB = F8 ? 1 : 2;        // bytes per operand element
     static constexpr int PASSES = S_ * K_ / NP;  // 4 or 2
     static constexpr int JP = NP / K_;           // j per pass
-    static constexpr uint32_t MQB = S_ * K_ * K_ * 2;
-    static constexpr uint32_t AQB = 128 * K_ * 2;
+    static constexpr uint32_t MQB = S_ * K_ * K_ * EB;
+    static constexpr uint32_t AQB = 128 * K_ * EB;
     static constexpr int ST = 2;
     static constexpr uint32_t SMEM = MQB + ST * AQB;
 };
 
 // 192 threads: warps 0-3 epilogue (tile rows 32w..32w+31), warp 4 lane 0
 // loads, warp 5 lane 0 issues the MMAs.  CTA b takes tiles b, b + grid, ...
-template <int K_>
+template <int K_, bool F8>
 __global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __restrict__ Aq,
                                                             const uint8_t* __restrict__ Mq,
                                                             const float* __restrict__ A, int n, int ntiles,
-                                                            float* __restrict__ T2, uint32_t* __restrict__ err) {
-    using C = QfCfg<K_>;
+                                                            const float* __restrict__ tq, float* __restrict__ T2,
+                                                            uint32_t* __restrict__ err) {
+    using C = QfCfg<K_, F8>;
+    __shared__ float s_tq[F8 ? S_ * K_ : 1];  // FP8 form: the stack rows' scales
+    if constexpr (F8)
+        for (int e = threadIdx.x; e < S_ * K_; e += blockDim.x) s_tq[e] = tq[e];
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ __align__(8) uint64_t mq_full, afull[C::ST], aempty[C::ST], tfull[2], tempty[2], done;
     __shared__ uint32_t tmem_base;
@@ -446,7 +627,7 @@ __global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __re
         }
     } else if (warp == 5) {
         if (lane == 0 && my_tiles > 0) {
-            constexpr uint32_t idesc = idesc_bf16_f32(128, NP);
+            constexpr uint32_t idesc = F8 ? idesc_e4m3_f32(128, NP) : idesc_bf16_f32(128, NP);
             ok = mbar_wait(smem_u32(&mq_full), 0u);
             int pc = 0;  // passes issued
             for (int it = 0; it < my_tiles && ok; ++it) {
@@ -463,9 +644,9 @@ __global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __re
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-                    for (int ks = 0; ks < K_ / 16; ++ks)
-                        mma_bf16(tmem + b * NP, umma_desc(abase + s * C::AQB + ks * (128 * 32)),
-                                 umma_desc(base + p * (NP * K_ * 2) + ks * (NP * 32)), idesc, ks > 0 ? 1u : 0u);
+                    for (int ks = 0; ks < K_ * C::EB / 32; ++ks)
+                        mma_op<F8>(tmem + b * NP, umma_desc(abase + s * C::AQB + ks * (128 * 32)),
+                                   umma_desc(base + p * (NP * K_ * C::EB) + ks * (NP * 32)), idesc, ks > 0 ? 1u : 0u);
                     mma_commit(smem_u32(&tfull[b]));
                 }
                 if (ok) mma_commit(smem_u32(&aempty[s]));  // the A tile is free once these MMAs finish
@@ -498,6 +679,7 @@ __global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __re
 #pragma unroll 1
                 for (int jj = 0; jj < C::JP; ++jj) {
                     float acc = 0.0f;
+                    const float* tr = s_tq + (F8 ? (p * C::JP + jj) * K_ : 0);
 #pragma unroll
                     for (int c = 0; c < K_; c += 32) {
                         uint32_t v0[16], v1[16];
@@ -505,10 +687,20 @@ __global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __re
                         tmem_ld16_nw(ta, v0);
                         tmem_ld16_nw(ta + 16, v1);
                         tmem_wait_ld();
+                        if constexpr (F8) {
+                            // the FP8 stack rows carry a scale each (D = t D')
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) acc = fmaf(__uint_as_float(v0[e]), arow[c + e], acc);
+                            for (int e = 0; e < 16; ++e)
+                                acc = fmaf(__uint_as_float(v0[e]), arow[c + e] * tr[c + e], acc);
 #pragma unroll
-                        for (int e = 0; e < 16; ++e) acc = fmaf(__uint_as_float(v1[e]), arow[c + 16 + e], acc);
+                            for (int e = 0; e < 16; ++e)
+                                acc = fmaf(__uint_as_float(v1[e]), arow[c + 16 + e] * tr[c + 16 + e], acc);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < 16; ++e) acc = fmaf(__uint_as_float(v0[e]), arow[c + e], acc);
+#pragma unroll
+                            for (int e = 0; e < 16; ++e) acc = fmaf(__uint_as_float(v1[e]), arow[c + 16 + e], acc);
+                        }
                     }
                     if (i < n) T2[(size_t)i * S_ + p * C::JP + jj] = acc;
                 }
@@ -530,21 +722,46 @@ __global__ void __launch_bounds__(192, 1) quadform_tc_kernel(const uint8_t* __re
 }  // namespace
 
 // Packed forms of the factor A for one MDS call (pack_factor_tc) and the
-// products with them.
-rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* At) {
+// products with them.  With sA (the FP8 form) the operands are E4M3 bytes of
+// A / sA with sA = the column scales, written there; otherwise BF16.
+rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* At, float* sA) {
     const int n = c->n;
     const int ntiles = (n + 127) / 128, nch = (n + CH - 1) / CH;
     cudaStream_t s = c->stream;
+    if (k != 64 && k != 32) {
+        set_error("tensor-core factor MDS supports rank 32 or 64");
+        return RFX_ERR_UNSUPPORTED;
+    }
+    if (sA) {
+        Scratch sc(c);
+        unsigned* mx = sc.get<unsigned>((size_t)k);
+        if (!mx) {
+            set_error("tensor-core factor MDS: scratch allocation failed");
+            return RFX_ERR_OOM;
+        }
+        RFX_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned) * k, s));
+        const int64_t cnt = (int64_t)n * k;
+        col_absmax_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(dA, cnt, k, mx);
+        col_scale_kernel<<<1, 64, 0, s>>>(mx, k, sA);
+        const size_t tq = (size_t)ntiles * 128 * (k / 16), ta = (size_t)nch * k * (CH / 16);
+        if (k == 64) {
+            pack_aq8_kernel<64><<<(unsigned)((tq + 255) / 256), 256, 0, s>>>(dA, sA, n, ntiles, Aq);
+            pack_at8_kernel<64><<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(dA, sA, n, nch, At);
+        } else {
+            pack_aq8_kernel<32><<<(unsigned)((tq + 255) / 256), 256, 0, s>>>(dA, sA, n, ntiles, Aq);
+            pack_at8_kernel<32><<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(dA, sA, n, nch, At);
+        }
+        c->launches += 4;
+        RFX_CUDA(cudaGetLastError());
+        return RFX_OK;
+    }
     const size_t tq = (size_t)ntiles * 128 * (k / 8), ta = (size_t)nch * k * (CH / 8);
     if (k == 64) {
         pack_aq_kernel<64><<<(unsigned)((tq + 255) / 256), 256, 0, s>>>(dA, n, ntiles, Aq);
         pack_at_kernel<64><<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(dA, n, nch, At);
-    } else if (k == 32) {
+    } else {
         pack_aq_kernel<32><<<(unsigned)((tq + 255) / 256), 256, 0, s>>>(dA, n, ntiles, Aq);
         pack_at_kernel<32><<<(unsigned)((ta + 255) / 256), 256, 0, s>>>(dA, n, nch, At);
-    } else {
-        set_error("tensor-core factor MDS supports rank 32 or 64");
-        return RFX_ERR_UNSUPPORTED;
     }
     c->launches += 2;
     RFX_CUDA(cudaGetLastError());
@@ -555,10 +772,10 @@ size_t factor_tc_aq_bytes(int n, int k) { return (size_t)((n + 127) / 128) * 128
 size_t factor_tc_at_bytes(int n, int k) { return (size_t)((n + CH - 1) / CH) * CH * k * 2; }
 
 // M (S x k x k) and T2 (n x S) for the factor A (n x k, with its packed forms
-// Aq / At from pack_factor_tc) and the centred block u (n x S), on the tensor
-// cores.
+// Aq / At from pack_factor_tc; sA its FP8 column scales, null for BF16) and
+// the centred block u (n x S), on the tensor cores.
 rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const uint8_t* Aq, const uint8_t* At,
-                                const float* u32, float* M, float* T2) {
+                                const float* sA, const float* u32, float* M, float* T2) {
     cudaStream_t s = c->stream;
     const int n = c->n;
     const int ntiles = (n + 127) / 128, nch = (n + CH - 1) / CH;
@@ -567,32 +784,54 @@ rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const uint8_t* A
     const int per = (nch + sms - 1) / sms;
     const int parts = (nch + per - 1) / per;
     const int qgrid = std::min(ntiles, sms);
+    const bool f8 = sA != nullptr;
     Scratch sc(c);
     const size_t count = (size_t)S_ * k * k;
     float* Mpart = sc.get<float>(count * parts);
     float* uT = sc.get<float>((size_t)nch * CH * S_);
     uint8_t* Mq = sc.get<uint8_t>(count * 2);
-    if (!Mpart || !uT || !Mq) {
+    unsigned* umax = f8 ? sc.get<unsigned>(S_) : nullptr;
+    float* tq = f8 ? sc.get<float>((size_t)S_ * k) : nullptr;
+    if (!Mpart || !uT || !Mq || (f8 && (!umax || !tq))) {
         set_error("tensor-core factor MDS: scratch allocation failed");
         return RFX_ERR_OOM;
     }
-    pack_ut_kernel<<<(unsigned)(((size_t)nch * CH * S_ + 255) / 256), 256, 0, s>>>(u32, n, nch, uT);
-    auto run = [&](auto mk, auto rk, auto qk, uint32_t sm_m, uint32_t sm_q) -> rfx_status {
+    if (f8) {
+        RFX_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned) * S_, s));
+        const int64_t cnt = (int64_t)n * S_;
+        col_absmax_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(u32, cnt, S_, umax);
+        c->launches += 1;
+    }
+    pack_ut_kernel<<<(unsigned)(((size_t)nch * CH * S_ + 255) / 256), 256, 0, s>>>(u32, n, nch, umax, uT);
+    auto run = [&](auto mk, auto qk, uint32_t sm_m, uint32_t sm_q, auto reduce) -> rfx_status {
         RFX_CUDA(cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_m));
         RFX_CUDA(cudaFuncSetAttribute(qk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_q));
         mk<<<parts, 192, sm_m, s>>>(At, uT, nch, per, Mpart, c->d_err);
-        rk<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(Mpart, parts, M, Mq);
-        qk<<<qgrid, 192, sm_q, s>>>(Aq, Mq, dA, n, ntiles, T2, c->d_err);
+        reduce();
+        qk<<<qgrid, 192, sm_q, s>>>(Aq, Mq, dA, n, ntiles, tq, T2, c->d_err);
         RFX_CUDA(cudaGetLastError());
         return RFX_OK;
     };
+    // BF16: M and Mq element by element; FP8: a warp per stack row (scales)
+    auto red16 = [&](auto rk) {
+        return [&, rk]() { rk<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(Mpart, parts, M, Mq); };
+    };
+    auto red8 = [&](auto rk) {
+        return [&, rk]() { rk<<<(unsigned)(((size_t)S_ * k * 32 + 255) / 256), 256, 0, s>>>(Mpart, parts, umax, sA, M, Mq, tq); };
+    };
     rfx_status st;
-    if (k == 64)
-        st = run(mstack_tc_kernel<64>, mstack_reduce_kernel<64>, quadform_tc_kernel<64>, MsCfg<64>::SMEM,
-                 QfCfg<64>::SMEM);
+    if (k == 64 && f8)
+        st = run(mstack_tc_kernel<64, true>, quadform_tc_kernel<64, true>, MsCfg<64, true>::SMEM,
+                 QfCfg<64, true>::SMEM, red8(mstack_reduce8_kernel<64>));
+    else if (k == 32 && f8)
+        st = run(mstack_tc_kernel<32, true>, quadform_tc_kernel<32, true>, MsCfg<32, true>::SMEM,
+                 QfCfg<32, true>::SMEM, red8(mstack_reduce8_kernel<32>));
+    else if (k == 64)
+        st = run(mstack_tc_kernel<64, false>, quadform_tc_kernel<64, false>, MsCfg<64, false>::SMEM,
+                 QfCfg<64, false>::SMEM, red16(mstack_reduce_kernel<64>));
     else if (k == 32)
-        st = run(mstack_tc_kernel<32>, mstack_reduce_kernel<32>, quadform_tc_kernel<32>, MsCfg<32>::SMEM,
-                 QfCfg<32>::SMEM);
+        st = run(mstack_tc_kernel<32, false>, quadform_tc_kernel<32, false>, MsCfg<32, false>::SMEM,
+                 QfCfg<32, false>::SMEM, red16(mstack_reduce_kernel<32>));
     else {
         set_error("tensor-core factor MDS supports rank 32 or 64");
         return RFX_ERR_UNSUPPORTED;
