@@ -341,7 +341,9 @@ rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count);
  * CUDA_MODULE_LOADING=EAGER); the device then holds the array until its
  * context is destroyed.  The first call on a device (and the first after the
  * device's context was reset) also looks up the array's device address with
- * cudaGetSymbolAddress, and should come before any stream capture.  Limits:
+ * cudaGetSymbolAddress.  Every call is synchronous (it reads its error flag
+ * back to the host and waits for `stream`), so it cannot be recorded into a
+ * CUDA graph by stream capture.  Limits:
  * n <= 32768, ntree <= 65535, ntree * n <= 1048576, 1 <= max_leaves <= n; larger
  * inputs are rejected with RFX_ERR_INVALID, as is a leaf index >= max_leaves
  * (those samples are left out of S).  Every call uses the same array and it
