@@ -231,13 +231,30 @@ __global__ void pack_ut_kernel(const float* __restrict__ u, int n, int nch, cons
     uT[(ch * S_ + j) * CH + w] = v;
 }
 
-// largest |x| of every column of an n x cols FP32 matrix (bit patterns of
-// non-negative floats order like the values), into zeroed mx
-__global__ void col_absmax_kernel(const float* __restrict__ X, int64_t count, int cols, unsigned* __restrict__ mx) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= count) return;
-    const float v = fabsf(X[idx]);
-    if (v > 0.0f) atomicMax(mx + (idx % cols), __float_as_uint(v));
+// largest |x| of every column of a rows x cols FP32 matrix (cols divides
+// 256; bit patterns of non-negative floats order like the values), into
+// zeroed mx: thread t keeps column t % cols over a stride of rows, the CTA
+// combines in shared memory, one global atomic per CTA and column
+constexpr int CAM_THREADS = 256;
+constexpr int CAM_CTAS = 592;
+__global__ void __launch_bounds__(CAM_THREADS) col_absmax_kernel(const float* __restrict__ X, int64_t rows, int cols,
+                                                                 unsigned* __restrict__ mx) {
+    __shared__ unsigned s_mx[CAM_THREADS];
+    const int c = threadIdx.x % cols;
+    const int rpb = CAM_THREADS / cols;  // rows per CTA step
+    unsigned m = 0u;
+    for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / cols; r < rows; r += (int64_t)gridDim.x * rpb)
+        m = max(m, __float_as_uint(fabsf(X[r * cols + c])));
+    if (threadIdx.x < cols) s_mx[threadIdx.x] = 0u;
+    __syncthreads();
+    atomicMax(s_mx + c, m);
+    __syncthreads();
+    if (threadIdx.x < cols && s_mx[threadIdx.x]) atomicMax(mx + threadIdx.x, s_mx[threadIdx.x]);
+}
+
+inline unsigned col_absmax_grid(int64_t rows, int cols) {
+    const int64_t need = (rows + CAM_THREADS / cols - 1) / (CAM_THREADS / cols);
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(CAM_CTAS, need));
 }
 
 // FP8 operands of the factor (the FP8 form): column scales sA[a] = max |A[:, a]| / 448,
@@ -740,8 +757,7 @@ rfx_status pack_factor_tc(Ctx* c, const float* dA, int k, uint8_t* Aq, uint8_t* 
             return RFX_ERR_OOM;
         }
         RFX_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned) * k, s));
-        const int64_t cnt = (int64_t)n * k;
-        col_absmax_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(dA, cnt, k, mx);
+        col_absmax_kernel<<<col_absmax_grid(n, k), CAM_THREADS, 0, s>>>(dA, n, k, mx);
         col_scale_kernel<<<1, 64, 0, s>>>(mx, k, sA);
         const size_t tq = (size_t)ntiles * 128 * (k / 16), ta = (size_t)nch * k * (CH / 16);
         if (k == 64) {
@@ -798,8 +814,7 @@ rfx_status launch_factor_ops_tc(Ctx* c, const float* dA, int k, const uint8_t* A
     }
     if (f8) {
         RFX_CUDA(cudaMemsetAsync(umax, 0, sizeof(unsigned) * S_, s));
-        const int64_t cnt = (int64_t)n * S_;
-        col_absmax_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(u32, cnt, S_, umax);
+        col_absmax_kernel<<<col_absmax_grid(n, S_), CAM_THREADS, 0, s>>>(u32, n, S_, umax);
         c->launches += 1;
     }
     pack_ut_kernel<<<(unsigned)(((size_t)nch * CH * S_ + 255) / 256), 256, 0, s>>>(u32, n, nch, umax, uT);
