@@ -1207,11 +1207,15 @@ rfx_status launch_pairs_upper(Ctx* c, int32_t* dS) {
             // 3-5 row2 with 256/512/1024 threads
             // a CTA prefetches into L2 the inputs of the row that the CTA one
             // wave of resident CTAs later takes
-            auto ahead_of = [&](auto kern, int nt) -> int {
-                int occ = 1, sms = 148;
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, nt, smem);
+            // (resident CTAs per SM from the thread count and the shared memory
+            // of a row, with 10 KB for the kernels' static arrays; device
+            // attributes only, so this also holds inside a graph capture)
+            auto ahead_of = [&](auto, int nt) -> int {
+                int sms = 148, smem_sm = 233472;
                 cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-                return std::max(1, occ) * sms;
+                cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device);
+                const int by_smem = smem_sm / (int)(smem + 10 * 1024);
+                return sms * std::max(1, std::min(2048 / nt, by_smem));
             };
             if (shape >= 6 && row3_ok) {
                 auto kern = shape == 6 ? pairs_row3_kernel<512> : pairs_row3_kernel<1024>;
