@@ -952,11 +952,17 @@ pairs_row3_kernel(const int2* __restrict__ opp, const int32_t* __restrict__ memb
         const int per = (E + NW - 1) / NW;
         const int e_beg = w * per, e_end = min(E, e_beg + per);
         if (e_beg < e_end) {
-            int lo = 0, hi = R;  // r: the listed range holding element e_beg
+            // r: the listed range holding element e_beg (the last c with
+            // s_pre[c] <= e_beg), by a 32-way search: lane l probes
+            // lo + l * step, the probes at or below e_beg are a prefix of the
+            // lanes (s_pre rises), two rounds for up to 1024 ranges
+            int lo = 0, hi = R;
             while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pre[mid] <= e_beg) lo = mid;
-                else hi = mid;
+                const int step = (hi - lo + 31) >> 5;
+                const int c = lo + lane * step;
+                const unsigned le = __ballot_sync(0xffffffffu, c < hi && s_pre[c] <= e_beg);
+                lo += (__popc(le) - 1) * step;
+                hi = min(hi, lo + step);
             }
             int r = lo;
             for (int W = e_beg; W < e_end; W += 32 * R3_BATCH) {
