@@ -588,6 +588,9 @@ def run_rows(args):
     S = torch.empty(L, dtype=torch.int32, device=dev)
     ctx.proximity_upper(S)
     ctx.synchronize()
+    # SM clocks and throttle reasons sampled over the n = 50,000 rows below
+    clocks = Clocks(0)
+    clocks.start()
     for full in (True, False):
         P = torch.empty((n, n) if full else (L,), dtype=torch.float32, device=dev)
         ms = timed(ctx, "finishprox", lambda: ctx.finishprox(S, P, full=full))
@@ -617,6 +620,7 @@ def run_rows(args):
                                                 "iteration for the top 3 eigenpairs"}
     del Pd, coords
     ctx.close()
+    clk = clocks.stop()  # (the n = 2,000 case below grows its forest on the host first)
     X1, y1 = synth.gaussian_classes(2000, 13, 3)
     f1 = abi.grow_forest(X1, y1, 500, 3, 1, nclass=3)
     ctx = abi.Context(0)
@@ -637,7 +641,7 @@ def run_rows(args):
             "config": {"workload": "rows a5/a7/a9: finishprox, predict at n=50000 ntree=1000; full-matrix 3-D MDS "
                                    "at n=50000 and n=2000", "forest_grow_s": round(grow_s, 2),
                        "peak_hbm_gbs": hbm, "peak_source": peak_src},
-            "rows": rows}
+            "rows": rows, "clocks": clk}
     print(json.dumps(line), flush=True)
     return 0
 
