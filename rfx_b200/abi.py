@@ -197,8 +197,10 @@ TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "25
                     "256x8 samples, 2048 staged nodes", "256x4 samples, 1024 staged nodes"],
                 1: ["row16 256", "row16 512", "row16 1024", "row2 256", "row2 512", "row2 1024", "row3 512",
                     "row3 1024"],
-                2: ["64", "128", "256", "64 staged rows", "128 staged rows", "256 staged rows"],
-                3: ["128", "256", "512", "64 staged rows", "128 staged rows", "256 staged rows"],
+                2: ["64", "128", "256", "64 staged rows", "128 staged rows", "256 staged rows",
+                    "64 child prefetch", "128 child prefetch", "256 child prefetch"],
+                3: ["128", "256", "512", "64 staged rows", "128 staged rows", "256 staged rows",
+                    "128 child prefetch", "256 child prefetch", "512 child prefetch"],
                 4: ["row2 256", "row2 512", "row2 1024", "row2 256 start-mask", "row2 512 start-mask",
                     "row2 1024 start-mask", "row3 512", "row3 1024"],
                 5: ["warp per key", "slots"], 6: ["warp per key", "slots"], 7: ["warp per key", "slots"]}

@@ -213,8 +213,10 @@ route2_kernel(const float* __restrict__ X, int n, int p, int T, int nclass, cons
 // earlier pass, tree t's samples are taken in that order (members of one leaf
 // and bag status together, then the samples without a terminal node), so the
 // threads of a warp follow the same path with the same walk rule.  Every
-// result is indexed by sample, so only the order of work changes.
-template <int RT>
+// result is indexed by sample, so only the order of work changes.  With PF
+// the walks load both children of each split node with the feature value
+// (walk_testreebag_pf / walk_terminal_pf).
+template <int RT, bool PF = false>
 __global__ void __launch_bounds__(RT)
 route_leaf_order_kernel(const float* __restrict__ X, int n, int p, int nclass, const DNode* __restrict__ nodes,
                         const int32_t* __restrict__ nodeclass, const int32_t* __restrict__ leafidx,
@@ -238,10 +240,12 @@ route_leaf_order_kernel(const float* __restrict__ X, int n, int p, int nclass, c
     int node;
     if (!ib) {
         int cls;
-        node = walk_testreebag(xrow, p, tn, tc, nn, cat, cgl, maxcat, &cls);
+        if constexpr (PF) node = walk_testreebag_pf(GlobalRow{xrow}, p, tn, tc, nn, cat, cgl, maxcat, &cls);
+        else node = walk_testreebag(xrow, p, tn, tc, nn, cat, cgl, maxcat, &cls);
         if (cls >= 0 && cls < nclass) atomicAdd(votes + (size_t)i * nclass + cls, 1);
     } else {
-        node = walk_terminal(xrow, p, tn, cat, cgl, maxcat, 2 * n + 1);
+        if constexpr (PF) node = walk_terminal_pf(GlobalRow{xrow}, p, tn, cat, cgl, maxcat, 2 * n + 1);
+        else node = walk_terminal(xrow, p, tn, cat, cgl, maxcat, 2 * n + 1);
     }
     const int li = (node >= 0 && node < nn) ? __ldg(leafidx + o + node) : -1;
     key_out[ti] = li >= 0 ? 2 * li + (ib ? 1 : 0) : -1;
@@ -446,14 +450,15 @@ rfx_status launch_route(Ctx* c) {
         // the member lists of an earlier pass over this forest give the order
         // shapes 0-2: 128 / 256 / 512 threads; 3-5: 64 / 128 / 256 threads
         // with the feature rows staged in shared memory (when they fit in
-        // 96 KB; otherwise the unstaged kernel of that width runs)
+        // 96 KB; otherwise the unstaged kernel of that width runs); 6-8:
+        // 128 / 256 / 512 threads with child-prefetching walks
         const size_t row_bytes = sizeof(float) * (size_t)(c->p | 1);
         int dev_smem = 0;
         RFX_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
         if (rfx_status s0 = allow_dyn_smem(route_leaf_staged_kernel<64>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(route_leaf_staged_kernel<128>, dev_smem)) return s0;
         if (rfx_status s0 = allow_dyn_smem(route_leaf_staged_kernel<256>, dev_smem)) return s0;
-        r = autotune(c, TK_ROUTE_LEAF, 6, 1, [&](int shape) -> rfx_status {
+        r = autotune(c, TK_ROUTE_LEAF, 9, 1, [&](int shape) -> rfx_status {
             RFX_CUDA(cudaMemsetAsync(c->d_votes, 0, sizeof(int32_t) * (size_t)c->n * c->nclass, c->stream));
             auto go = [&](auto kernel, int rt, size_t smem) {
                 dim3 grid((c->n + rt - 1) / rt, c->T);
@@ -462,8 +467,14 @@ rfx_status launch_route(Ctx* c) {
                                                       c->d_catgoleft, c->maxcat, c->d_memb, c->d_key, c->d_votes);
             };
             const int srt = shape == 3 ? 64 : shape == 4 ? 128 : 256;
-            const bool staged = shape >= 3 && (size_t)srt * row_bytes <= 96 * 1024;
-            if (staged) {
+            const bool staged = shape >= 3 && shape <= 5 && (size_t)srt * row_bytes <= 96 * 1024;
+            if (shape == 6) {
+                go(route_leaf_order_kernel<128, true>, 128, 0);
+            } else if (shape == 7) {
+                go(route_leaf_order_kernel<256, true>, 256, 0);
+            } else if (shape == 8) {
+                go(route_leaf_order_kernel<512, true>, 512, 0);
+            } else if (staged) {
                 const size_t sm = (size_t)srt * row_bytes;
                 if (srt == 64) go(route_leaf_staged_kernel<64>, 64, sm);
                 else if (srt == 128) go(route_leaf_staged_kernel<128>, 128, sm);

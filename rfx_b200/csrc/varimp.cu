@@ -78,6 +78,31 @@ __device__ __forceinline__ int imp_side_walk(const XR& xrow, const XR& xperm, in
     return -1;
 }
 
+// The same side walk with both children of each split node loaded together
+// with the feature value (walks.cuh, load_node_now): one round trip to memory
+// per step.  Children of nodes with status != -1 are in [0, nnode) (checked
+// at load), so the loads stay in bounds.
+template <typename XR>
+__device__ __forceinline__ int imp_side_walk_pf(const XR& xrow, const XR& xperm, int mr, int p, int kt, int budget,
+                                                const DNode* __restrict__ tn, const int32_t* __restrict__ nclass_of,
+                                                const int32_t* __restrict__ cgl, int maxcat) {
+    if (budget <= 0) return -1;
+    DNode nd = load_node_now(tn, kt);
+    for (int s = 0; s < budget; ++s) {
+        if (node_status(nd.meta) == -1) return __ldg(nclass_of + kt);
+        const int m = node_var(nd.meta);
+        if (m >= p) return -1;
+        const DNode cl = load_node_now(tn, nd.left);
+        const DNode cr = load_node_now(tn, nd.right);
+        const float x = m == mr ? xperm(m) : xrow(m);
+        const int nx = imp_decide(nd, kt, x, cgl, maxcat);
+        if (nx == DIR_BREAK) return -1;
+        nd = nx == nd.left ? cl : cr;
+        kt = nx;
+    }
+    return -1;
+}
+
 // OOB samples of every tree in ascending order (joob of cpu_varimp).
 __global__ void __launch_bounds__(VT)
 joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob_all,
@@ -175,9 +200,11 @@ joob_kernel(const uint8_t* __restrict__ inbag, int n, int32_t* __restrict__ joob
 // With FB (more than 64 W features) one launch decides the features of one
 // block [fb, fb + 64 W): flip bits and delta counters are block-local, other
 // features' splits are followed without a permuted decision, and the per-tree
-// correct counts are added by the fb == 0 launch only.
-template <int W, int VW, bool FB = false, bool SX = false>
-__global__ void __launch_bounds__(VW, 1536 / VW)
+// correct counts are added by the fb == 0 launch only.  With PF the main
+// path and the side walks load both children of each split node with the
+// feature values (one round trip to memory per step).
+template <int W, int VW, bool FB = false, bool SX = false, bool PF = false>
+__global__ void __launch_bounds__(VW, (PF ? 1024 : 1536) / VW)  // PF: room for the children's registers
 varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, int n, int p,
                    const DNode* __restrict__ nodes, const int32_t* __restrict__ nodeclass,
                    const int64_t* __restrict__ offs, const int32_t* __restrict__ nnode_arr,
@@ -275,8 +302,10 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
         int tb_steps = 0;
         int kt = 0, jvr0 = -1;
         bool ok = false;
+        DNode nd_next;
+        if constexpr (PF) nd_next = load_node_now(tn, 0);
         for (int step = 0; step < nnv; ++step) {
-            const DNode nd = src(kt);
+            const DNode nd = PF ? nd_next : src(kt);
             const int st = node_status(nd.meta);
             const int m = node_var(nd.meta);
             if (tb_sync && !tb_done) {
@@ -294,6 +323,11 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                 break;
             }
             if (m >= p) break;
+            DNode cl, cr;
+            if constexpr (PF) {
+                cl = load_node_now(tn, nd.left);
+                cr = load_node_now(tn, nd.right);
+            }
             const float xv = xi(m);
             const int dir_o = imp_decide(nd, kt, xv, cgl, maxcat);
             if (tb_sync && !tb_done) {
@@ -331,6 +365,8 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                         const int slot = atomicAdd(&q_n, 1);
                         if (slot < QCAP)
                             q_ent[slot] = make_int4(tid, m, dir_p, nnv - step - 1);
+                        else if constexpr (PF)
+                            cls_m = imp_side_walk_pf(xi, xp, m, p, dir_p, nnv - step - 1, tn, tc, cgl, maxcat);
                         else
                             cls_m = imp_side_walk(xi, xp, m, p, dir_p, nnv - step - 1, src, tc, cgl, maxcat);
                     }
@@ -343,6 +379,7 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
                         }
                 }
             }
+            if constexpr (PF) nd_next = dir_o == nd.left ? cl : cr;
             kt = dir_o;
         }
         if (!ok) my_err |= ERR_STALE_JVR;
@@ -356,9 +393,11 @@ varimp_walk_kernel(const float* __restrict__ X, const int32_t* __restrict__ y, i
     for (int e = tid; e < qn; e += VW) {
         const int4 en = q_ent[e];
         const int lt = en.x, m = en.y;
-        const int cls_m = imp_side_walk(RowSel<SX>{X + (size_t)s_i[lt] * p, xs_own + (size_t)lt * ps},
-                                        RowSel<SX>{X + (size_t)s_ip[lt] * p, xs_par + (size_t)lt * ps}, m, p, en.z, en.w, src,
-                                        tc, cgl, maxcat);
+        const RowSel<SX> xo{X + (size_t)s_i[lt] * p, xs_own + (size_t)lt * ps};
+        const RowSel<SX> xq{X + (size_t)s_ip[lt] * p, xs_par + (size_t)lt * ps};
+        int cls_m;
+        if constexpr (PF) cls_m = imp_side_walk_pf(xo, xq, m, p, en.z, en.w, tn, tc, cgl, maxcat);
+        else cls_m = imp_side_walk(xo, xq, m, p, en.z, en.w, src, tc, cgl, maxcat);
         if (cls_m < 0) my_err |= ERR_STALE_JVR;
         const int mb = FB ? m - fb : m;
         if (cls_m >= 0 && cls_m == s_y[lt]) atomicOr(&s_pcorr[lt][mb >> 6], 1ull << (mb & 63));
@@ -565,15 +604,20 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
             return RFX_OK;
         };
         // shapes 0-2: rows through the read-only cache at 64/128/256 threads;
-        // 3-5: the same with staged rows, where they fit in 96 KB
-        rfx_status r = autotune(c, TK_VWALK, 6, 1, [&](int shape) -> rfx_status {
+        // 3-5: the same with staged rows, where they fit in 96 KB; 6-8: rows
+        // through the read-only cache with child-prefetching walks
+        rfx_status r = autotune(c, TK_VWALK, 9, 1, [&](int shape) -> rfx_status {
             // the walk adds to the per-tree counts: clear them for every run
             RFX_CUDA(cudaMemsetAsync(c->d_right, 0, sizeof(int32_t) * 2 * (size_t)c->T, c->stream));
             RFX_CUDA(cudaMemsetAsync(c->d_rightimp, 0, sizeof(int32_t) * (size_t)c->T * c->p, c->stream));
             const int vw = (shape % 3) == 0 ? 64 : (shape % 3) == 2 ? 256 : 128;
-            const bool staged = shape >= 3 && staged_smem(vw) <= 96 * 1024;
+            const bool staged = shape >= 3 && shape <= 5 && staged_smem(vw) <= 96 * 1024;
             rfx_status g;
-            if (staged) {
+            if (shape >= 6) {
+                g = vw == 64 ? go(varimp_walk_kernel<W, 64, false, false, true>, 64, smem)
+                    : vw == 256 ? go(varimp_walk_kernel<W, 256, false, false, true>, 256, smem)
+                                : go(varimp_walk_kernel<W, 128, false, false, true>, 128, smem);
+            } else if (staged) {
                 const size_t sm = staged_smem(vw);
                 g = vw == 64 ? go(varimp_walk_kernel<W, 64, false, true>, 64, sm)
                     : vw == 256 ? go(varimp_walk_kernel<W, 256, false, true>, 256, sm)

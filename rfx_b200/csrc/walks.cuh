@@ -29,6 +29,19 @@ struct GlobalNodes {
     __device__ __forceinline__ DNode operator()(int k) const { return load_node(g, k); }
 };
 
+// A node record loaded by an explicit instruction.  The child-prefetching
+// walks below load both children of a split node before the decision picks
+// one; written as plain loads followed by a select, the compiler may turn the
+// pair into one load from the selected address, which waits for the decision
+// again.
+__device__ __forceinline__ DNode load_node_now(const DNode* __restrict__ nodes, int k) {
+    int4 v;
+    asm volatile("ld.global.nc.v4.s32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(reinterpret_cast<const int4*>(nodes) + k));
+    return as_node(v);
+}
+
 __device__ __forceinline__ int cgl_at(const int32_t* __restrict__ cgl, int maxcat, int node, int idx) {
     return cgl ? __ldg(cgl + (size_t)node * maxcat + idx) : 0;
 }
@@ -114,6 +127,79 @@ __device__ __forceinline__ int walk_testreebag_x(const XR& xrow, int p, const Sr
         return kt;
     }
     *cls = __ldg(nclass_of + 0);
+    return 0;
+}
+
+// Child-prefetching forms of the two routing walks.  At a split node both
+// children are loaded together with the feature value the decision needs, so
+// a step waits for one round trip to memory instead of two (node, then
+// feature).  The loads stay in bounds: pack_nodes_kernel (load.cu) checks
+// that every node with status != -1 has both children in [0, nnode).  The
+// decisions, stopping rules and results are those of walk_testreebag_x and
+// walk_terminal_x.
+template <typename XR>
+__device__ __forceinline__ int walk_testreebag_pf(const XR& xrow, int p, const DNode* __restrict__ nodes,
+                                                  const int32_t* __restrict__ nclass_of, int nnode,
+                                                  const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                  int maxcat, int* cls) {
+    int kt = 0;
+    int steps = 0;
+    DNode nd = load_node_now(nodes, 0);
+    while (node_status(nd.meta) == 1 && steps < 1000) {
+        steps++;
+        if (steps >= 1000) break;
+        const int m = node_var(nd.meta);
+        if (m >= p) break;
+        const DNode cl = load_node_now(nodes, nd.left);
+        const DNode cr = load_node_now(nodes, nd.right);
+        const float v = xrow(m);
+        bool go_left;
+        if (!node_cat(nd.meta)) {
+            go_left = v <= nd.split;
+        } else {
+            const int iv = __float2int_rz(v);
+            go_left = iv >= 0 && iv < __ldg(cat + m) && cgl_at(cgl, maxcat, kt, iv) == 1;
+        }
+        kt = go_left ? nd.left : nd.right;
+        nd = go_left ? cl : cr;
+        if (node_status(nd.meta) != 1) break;
+    }
+    const int st = node_status(nd.meta);
+    if (st == -1 || st == 2) {
+        *cls = __ldg(nclass_of + kt);
+        return kt;
+    }
+    *cls = __ldg(nclass_of + 0);
+    return 0;
+}
+
+template <typename XR>
+__device__ __forceinline__ int walk_terminal_pf(const XR& xrow, int p, const DNode* __restrict__ nodes,
+                                                const int32_t* __restrict__ cat, const int32_t* __restrict__ cgl,
+                                                int maxcat, int maxnode) {
+    int cur = 0;
+    DNode nd = load_node_now(nodes, 0);
+    for (int k = 0; k < maxnode; ++k) {
+        if (node_status(nd.meta) == -1) return cur;
+        const int m = node_var(nd.meta);
+        if (m >= p) return 0;
+        const DNode cl = load_node_now(nodes, nd.left);
+        const DNode cr = load_node_now(nodes, nd.right);
+        const float v = xrow(m);
+        bool go_left;
+        if (!node_cat(nd.meta)) {
+            go_left = v <= nd.split;
+        } else {
+            const int j = __double2int_rz(__dadd_rn((double)v, 0.5));
+            if (j >= 1 && j <= __ldg(cat + m)) {
+                go_left = cgl_at(cgl, maxcat, cur, j - 1) == 1;
+            } else {
+                return 0;
+            }
+        }
+        cur = go_left ? nd.left : nd.right;
+        nd = go_left ? cl : cr;
+    }
     return 0;
 }
 
