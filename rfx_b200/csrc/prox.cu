@@ -317,30 +317,34 @@ __global__ void __launch_bounds__(1024)
 row_order_kernel(const int32_t* __restrict__ key, const int32_t* __restrict__ segoff,
                  const int64_t* __restrict__ segbase, const int32_t* __restrict__ memb, int n,
                  int32_t* __restrict__ order) {
+    // thread t owns the samples [t * R, (t + 1) * R): it counts those
+    // without a tree-0 leaf, one block-wide scan places its run, and it
+    // writes them in ascending order after tree 0's keyed members
     __shared__ int wsum[32];
-    __shared__ int s_base;
     const int K0 = (int)(segbase[1] - segbase[0]) - 1;
     const int cnt0 = segoff[segbase[0] + K0];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int q = tid; q < cnt0; q += 1024) order[q] = memb[q];
-    if (tid == 0) s_base = cnt0;
-    __syncthreads();
-    for (int base = 0; base < n; base += 1024) {
-        const int i = base + tid;
-        const int f = (i < n && key[i] < 0) ? 1 : 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) wsum[wid] = __popc(bal);
-        __syncthreads();
-        int woff = 0, tot = 0;
-        for (int q = 0; q < 32; ++q) {
-            if (q < wid) woff += wsum[q];
-            tot += wsum[q];
-        }
-        if (f) order[s_base + woff + __popc(bal & ((1u << lane) - 1u))] = i;
-        __syncthreads();
-        if (tid == 0) s_base += tot;
-        __syncthreads();
+    const int R = (n + 1023) / 1024;
+    const int b = min(n, tid * R), e = min(n, b + R);
+    int f = 0;
+    for (int i = b; i < e; ++i) f += __ldg(key + i) < 0 ? 1 : 0;
+    int incl = f;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += u;
     }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    int woff = 0;
+    for (int q = 0; q < wid; ++q) woff += wsum[q];
+    int pos = cnt0 + woff + incl - f;
+    for (int i = b; i < e && f > 0; ++i)
+        if (__ldg(key + i) < 0) {
+            order[pos++] = i;
+            --f;
+        }
 }
 
 // Launch shapes of the row kernels the autotuner chooses from: 0..2
@@ -1003,67 +1007,92 @@ constexpr int FP_TILE = 32;
 constexpr int FP_JT = 8;  // column tiles per CTA
 
 // S/2 is exact for an integer S, so it is formed as S * 0.5 (the same double
-// as the reference's division by 2).
-template <typename TS>
-__device__ __forceinline__ double fp_value(TS s, double inv_i, double inv_j, bool sc_i, bool sc_j) {
-    const double h = __dmul_rn((double)s, 0.5);
-    const double a = sc_i ? __dmul_rn(h, inv_i) : h;
-    const double b = sc_j ? __dmul_rn(h, inv_j) : h;
-    return __dmul_rn(0.5, __dadd_rn(a, b));
+// as the reference's division by 2).  inv_i is 1/nout[i], or 1.0 where
+// nout[i] == 0: the reference then uses S/2 unscaled, and S/2 * 1.0 is
+// that same double, so one product covers both cases.
+__device__ __forceinline__ double fp_value(double s, double inv_i, double inv_j) {
+    const double h = __dmul_rn(s, 0.5);
+    return __dmul_rn(0.5, __dadd_rn(__dmul_rn(h, inv_i), __dmul_rn(h, inv_j)));
 }
 
-// One CTA per row tile I and a run of FP_JT column tiles J >= I; computes the
-// 32x32 values of each tile (I, J) from the packed S rows of tile I and writes
-// tile (I, J) and its mirror (J, I) of the full matrix, or tile (I, J) of the
-// packed triangle.  The row tile's 1/nout factors are formed once per CTA.
+// 1/nout per sample, formed once per call (1.0 where nout == 0).
+__global__ void finish_inv_kernel(const int32_t* __restrict__ nout, int n, double* __restrict__ inv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const int ni = nout[i];
+        inv[i] = ni > 0 ? __ddiv_rn(1.0, (double)ni) : 1.0;
+    }
+}
+
+// Runs of FP_JT column tiles J >= I of row tile I.
+__host__ __device__ __forceinline__ int fp_runs(int nt, int I) { return (nt - I + FP_JT - 1) / FP_JT; }
+
+// One CTA per run of FP_JT column tiles J >= I of one row tile I; computes
+// the 32x32 values of each tile (I, J) from the packed S rows of tile I and
+// writes tile (I, J) and its mirror (J, I) of the full matrix, or tile (I, J)
+// of the packed triangle.  Grid: y = row-tile pair (I, nt - 1 - I), whose run
+// counts add up to about nt / FP_JT, x = run within the pair, so no CTA lies
+// left of the diagonal.  The next tile's S values and column factors are
+// loaded before the current tile's values are formed.
 template <typename TS>
 __global__ void __launch_bounds__(FP_TILE * 8)
-finishprox_kernel(const TS* __restrict__ S, const int32_t* __restrict__ nout, int n, int full,
+finishprox_kernel(const TS* __restrict__ S, const double* __restrict__ inv, int n, int full,
                   float* __restrict__ P) {
     __shared__ float tile[FP_TILE][FP_TILE + 1];
     __shared__ double s_inv[FP_TILE];
-    __shared__ int s_ni[FP_TILE];
-    const int I = blockIdx.y;
     const int nt = (n + FP_TILE - 1) / FP_TILE;
-    const int J0 = blockIdx.x * FP_JT;
+    int I = blockIdx.y, run = blockIdx.x;
+    const int ra = fp_runs(nt, I);
+    if (run >= ra) {
+        I = nt - 1 - I;
+        run -= ra;
+        if (I <= (int)blockIdx.y || run >= fp_runs(nt, I)) return;
+    }
+    const int J0 = I + run * FP_JT;
     const int J1 = min(J0 + FP_JT, nt);
-    if (J1 <= I) return;  // the whole run lies left of the diagonal
     const int tx = threadIdx.x % FP_TILE, ty = threadIdx.x / FP_TILE;  // 32 x 8
     if (threadIdx.x < FP_TILE) {
         const int i = I * FP_TILE + threadIdx.x;
-        const int ni = i < n ? nout[i] : 0;
-        s_ni[threadIdx.x] = ni;
-        s_inv[threadIdx.x] = ni > 0 ? __ddiv_rn(1.0, (double)ni) : 1.0;
+        s_inv[threadIdx.x] = i < n ? __ldg(inv + i) : 1.0;
     }
-    __syncthreads();
-    for (int J = max(J0, I); J < J1; ++J) {
+    constexpr int RU = FP_TILE / 8;  // rows per thread
+    // row offsets of the packed triangle: S[i][j] = S[base_i + j]
+    int64_t base[RU];
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+        const int64_t i = I * FP_TILE + ty + 8 * u;
+        base[u] = i * n - (i * (i - 1)) / 2 - i;
+    }
+    auto load = [&](int J, TS* sv, double& invj) {
         const int j = J * FP_TILE + tx;
         const bool jv = j < n;
-        const int nj = jv ? nout[j] : 0;
-        const double inv_j = nj > 0 ? __ddiv_rn(1.0, (double)nj) : 1.0;
-        // the four rows' loads are issued before any value is formed (four
-        // 128-byte row segments in flight per warp)
-        TS sv[FP_TILE / 8];
-        int64_t ix[FP_TILE / 8];
+        invj = jv ? __ldg(inv + j) : 1.0;
 #pragma unroll
-        for (int u = 0; u < FP_TILE / 8; ++u) {
+        for (int u = 0; u < RU; ++u) {
             const int i = I * FP_TILE + ty + 8 * u;
-            ix[u] = (int64_t)i * n - ((int64_t)i * (i - 1)) / 2 + (j - i);
-            sv[u] = (i < n && jv && j > i) ? __ldg(S + ix[u]) : (TS)0;
+            sv[u] = (i < n && jv && j > i) ? __ldg(S + base[u] + j) : (TS)0;
         }
+    };
+    TS cur[RU], nxt[RU];
+    double inv_c = 1.0, inv_n = 1.0;
+    load(J0, cur, inv_c);
+    __syncthreads();
+    for (int J = J0; J < J1; ++J) {
+        if (J + 1 < J1) load(J + 1, nxt, inv_n);
+        const int j = J * FP_TILE + tx;
+        const bool jv = j < n;
 #pragma unroll
-        for (int u = 0; u < FP_TILE / 8; ++u) {
+        for (int u = 0; u < RU; ++u) {
             const int r = ty + 8 * u;
             const int i = I * FP_TILE + r;
             float v = 0.0f;
             if (i < n && jv && j >= i) {
-                const int ni = s_ni[r];
-                const double d = (j == i) ? 1.0 : fp_value(sv[u], s_inv[r], inv_j, ni > 0, nj > 0);
+                const double d = (j == i) ? 1.0 : fp_value((double)cur[u], s_inv[r], inv_c);
                 v = __double2float_rn(d);
                 if (full) P[(size_t)i * n + j] = v;
-                else P[ix[u]] = v;
+                else P[base[u] + j] = v;
             }
-            tile[r][tx] = v;
+            if (full) tile[r][tx] = v;
         }
         if (full) {
             __syncthreads();
@@ -1075,6 +1104,9 @@ finishprox_kernel(const TS* __restrict__ S, const int32_t* __restrict__ nout, in
             }
             __syncthreads();  // the tile is rewritten for the next J
         }
+#pragma unroll
+        for (int u = 0; u < RU; ++u) cur[u] = nxt[u];
+        inv_c = inv_n;
     }
 }
 
@@ -1304,24 +1336,43 @@ rfx_status launch_pairs_pipeline_raw(const PairsRawArgs& a, cudaStream_t stream)
     return RFX_OK;
 }
 
-rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full) {
-    StageTimer st(c, ST_FINISHPROX, 1);
-    const int nt = (c->n + FP_TILE - 1) / FP_TILE;
-    dim3 grid((nt + FP_JT - 1) / FP_JT, nt);
-    finishprox_kernel<int32_t><<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
+namespace {
+// Grid of the finishprox kernel: x = run within a row-tile pair, y = pair.
+dim3 finishprox_grid(int n) {
+    const int nt = (n + FP_TILE - 1) / FP_TILE;
+    int bx = 1;
+    for (int I = 0; I < (nt + 1) / 2; ++I) {
+        const int I2 = nt - 1 - I;
+        bx = std::max(bx, fp_runs(nt, I) + (I2 > I ? fp_runs(nt, I2) : 0));
+    }
+    return dim3(bx, (nt + 1) / 2);
+}
+
+template <typename TS>
+rfx_status finishprox_run(Ctx* c, const TS* dS, float* dP, int full) {
+    StageTimer st(c, ST_FINISHPROX, 2);
+    Scratch sc(c);
+    double* inv = sc.get<double>((size_t)c->n);
+    if (!inv) {
+        set_error("finishprox: scratch allocation failed");
+        return RFX_ERR_OOM;
+    }
+    finish_inv_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_nout, c->n, inv);
+    RFX_CUDA(cudaGetLastError());
+    finishprox_kernel<TS><<<finishprox_grid(c->n), FP_TILE * 8, 0, c->stream>>>(dS, inv, c->n, full, dP);
     RFX_CUDA(cudaGetLastError());
     return RFX_OK;
+}
+}  // namespace
+
+rfx_status launch_finishprox(Ctx* c, const int32_t* dS, float* dP, int full) {
+    return finishprox_run<int32_t>(c, dS, dP, full);
 }
 
 // finishprox of FP64 sums (case-wise weights): the same arithmetic on
 // S = C + C^T in double
 rfx_status launch_finishprox_f64(Ctx* c, const double* dS, float* dP, int full) {
-    StageTimer st(c, ST_FINISHPROX, 1);
-    const int nt = (c->n + FP_TILE - 1) / FP_TILE;
-    dim3 grid((nt + FP_JT - 1) / FP_JT, nt);
-    finishprox_kernel<double><<<grid, FP_TILE * 8, 0, c->stream>>>(dS, c->d_nout, c->n, full, dP);
-    RFX_CUDA(cudaGetLastError());
-    return RFX_OK;
+    return finishprox_run<double>(c, dS, dP, full);
 }
 
 }  // namespace rfx
