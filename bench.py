@@ -580,7 +580,8 @@ def run_rows(args):
         return tot / reps
 
     rows = {}
-    n, T = 50_000, 1000
+    n = args.n if args.n is not None else 50_000
+    T = args.trees if args.trees is not None else 1000
     X, y, f, grow_s = make_forest(n, T, 0, 1, lambda: None)
     ctx = abi.Context(0)
     ctx.load(f, X, y)
@@ -611,16 +612,27 @@ def run_rows(args):
     rows["predict"] = {"ms": ms, "walks_per_s": walks / ms * 1e3, "alg_bytes": nbytes,
                        "achieved_gbs": nbytes / ms / 1e6, "frac": nbytes / ms / 1e6 / hbm,
                        "unit": "walk = one (test row, tree); bytes: X rows + votes + one pass over the 16-byte nodes"}
-    Pd = torch.empty((n, n), dtype=torch.float32, device=dev)
-    ctx.finishprox(S, Pd, full=True)
-    del S
-    coords = torch.empty((n, 3), dtype=torch.float64, device=dev)
-    ms = timed(ctx, "mds_full", lambda: ctx.mds3d_full(Pd, coords))
-    rows["mds_full_n50000"] = {"ms": ms, "unit": "whole call: centring into an n x n FP64 matrix, subspace "
-                                                "iteration for the top 3 eigenpairs"}
-    del Pd, coords
+    if not args.no_mds:
+        Pd = torch.empty((n, n), dtype=torch.float32, device=dev)
+        ctx.finishprox(S, Pd, full=True)
+        del S
+        coords = torch.empty((n, 3), dtype=torch.float64, device=dev)
+        ms = timed(ctx, "mds_full", lambda: ctx.mds3d_full(Pd, coords))
+        rows[f"mds_full_n{n}"] = {"ms": ms, "unit": "whole call: centring into an n x n FP64 matrix, subspace "
+                                                    "iteration for the top 3 eigenpairs"}
+        del Pd, coords
     ctx.close()
     clk = clocks.stop()  # (the n = 2,000 case below grows its forest on the host first)
+    if args.no_mds:
+        line = {"metric": "per-row device time (finishprox, predict)", "value": rows["finishprox_full"]["ms"],
+                "unit": f"ms (finishprox full, n={n})", "higher_is_better": False, "n_gpus": 1, "steps": reps,
+                "warmup": warm, "dtype": "int32 counts, fp64 normalisation, fp32 outputs",
+                "data": "synthetic (seeded cover-shaped generator)",
+                "config": {"workload": f"rows a5/a9: finishprox, predict at n={n} ntree={T}",
+                           "forest_grow_s": round(grow_s, 2), "peak_hbm_gbs": hbm, "peak_source": peak_src},
+                "rows": rows, "clocks": clk}
+        print(json.dumps(line), flush=True)
+        return 0
     X1, y1 = synth.gaussian_classes(2000, 13, 3)
     f1 = abi.grow_forest(X1, y1, 500, 3, 1, nclass=3)
     ctx = abi.Context(0)
@@ -635,11 +647,11 @@ def run_rows(args):
     rows["mds_full_n2000"] = {"ms": ms, "unit": "whole call, n = 2,000, 500 trees"}
     ctx.close()
     line = {"metric": "per-row device time (finishprox, predict, full-matrix MDS)", "value": rows["finishprox_full"]["ms"],
-            "unit": "ms (finishprox full, n=50000)", "higher_is_better": False, "n_gpus": 1, "steps": reps,
+            "unit": f"ms (finishprox full, n={n})", "higher_is_better": False, "n_gpus": 1, "steps": reps,
             "warmup": warm, "dtype": "int32 counts, fp64 normalisation and MDS, fp32 outputs",
             "data": "synthetic (seeded cover-shaped and Gaussian generators)",
-            "config": {"workload": "rows a5/a7/a9: finishprox, predict at n=50000 ntree=1000; full-matrix 3-D MDS "
-                                   "at n=50000 and n=2000", "forest_grow_s": round(grow_s, 2),
+            "config": {"workload": f"rows a5/a7/a9: finishprox, predict at n={n} ntree={T}; full-matrix 3-D MDS "
+                                   f"at n={n} and n=2000", "forest_grow_s": round(grow_s, 2),
                        "peak_hbm_gbs": hbm, "peak_source": peak_src},
             "rows": rows, "clocks": clk}
     print(json.dumps(line), flush=True)
@@ -752,6 +764,7 @@ def main():
     ap.add_argument("--trees", type=int, default=None, help="trees (default 1000; 2000 for --workload lowrank)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mds", action="store_true", help="rows workload: finishprox and predict only")
     ap.add_argument("--workload", default="exact", choices=["exact", "lowrank", "large", "batch", "rows"])
     ap.add_argument("--forests", type=int, default=64, help="forests in the batch workload")
     ap.add_argument("--grow-forest", default=None, metavar="PATH",
