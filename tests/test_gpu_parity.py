@@ -346,3 +346,34 @@ def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
         avimp, sqsd, qimp, qimpm = ctx.varimp(True)
         assert np.array_equal(avimp, O["avimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
         ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["catgoleft", "cover_minnd5"])
+def test_child_prefetch_shapes_match_oracle(built, monkeypatch, name):
+    """The child-prefetching walks (leaf-order routing shapes 6-8, importance
+    walk shapes 6-8) on a forest with non-zero categorical go-left tables and
+    on one grown with minndsize 5: the oracle's votes, leaves, importances and
+    pair counts, in natural and in leaf order."""
+    from oracle import oracle as orc
+    from rfx_b200 import abi
+
+    X, y, f = CASES[name]()
+    O = orc.analyse(X, y, f, want_leaf=True)
+    for shape in (6, 7, 8):
+        monkeypatch.setenv("RFX_TUNE_VWALK", str(shape))
+        monkeypatch.setenv("RFX_TUNE_ROUTE_LEAF", str(shape))
+        ctx = abi.Context(0)
+        ctx.load(f, X, y)
+        ctx.route_oob()
+        assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
+        # routing and the walk now run in the leaf order of the pass above
+        leaf = np.zeros((f.ntree, f.n), np.int32)
+        q, nout, _ = ctx.route_oob(leaf=leaf)
+        assert np.array_equal(q.astype(np.float32), O["q_raw"]), shape
+        assert np.array_equal(leaf, O["leaf"]), shape
+        assert np.array_equal(ctx.proximity_upper(), O["S"]), shape
+        avimp, sqsd, qimp, qimpm = ctx.varimp(True)
+        assert np.array_equal(avimp, O["avimp"]) and np.array_equal(sqsd, O["sqsd"]), shape
+        assert np.array_equal(qimp, O["qimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
+        ctx.close()
