@@ -190,7 +190,8 @@ class BatchGraph:
 
 
 TUNED_STAGES = {0: "route", 1: "pair_counts", 2: "varimp_walk", 3: "route_leaf_order", 4: "pair_counts_hub",
-                5: "lowrank_leaf_sums_fp32", 6: "lowrank_leaf_sums_bf16", 7: "lowrank_leaf_sums_fp8"}
+                5: "lowrank_leaf_sums_fp32", 6: "lowrank_leaf_sums_bf16", 7: "lowrank_leaf_sums_fp8",
+                8: "varimp_sample"}
 # launch shapes per stage, in the library's shape order
 TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "256x2 trees, 2 walks in flight",
                     "256x4 trees, 2 walks in flight", "128x4 trees, 2 walks in flight",
@@ -203,7 +204,8 @@ TUNED_SHAPES = {0: ["256x1", "128x1", "512x1", "256x2 trees", "256x4 trees", "25
                     "128 child prefetch", "256 child prefetch", "512 child prefetch"],
                 4: ["row2 256", "row2 512", "row2 1024", "row2 256 start-mask", "row2 512 start-mask",
                     "row2 1024 start-mask", "row3 512", "row3 1024"],
-                5: ["warp per key", "slots"], 6: ["warp per key", "slots"], 7: ["warp per key", "slots"]}
+                5: ["warp per key", "slots"], 6: ["warp per key", "slots"], 7: ["warp per key", "slots"],
+                8: ["tree loop", "per-sample OOB tree lists"]}
 
 
 def _shape_name(kernel: int, shape: int) -> str:

@@ -278,7 +278,7 @@ rfx_status launch_build_csr(Ctx* c);
 
 // Autotuned stages: kernel ids and the launch shapes each offers.
 enum TuneKernel : int { TK_ROUTE = 0, TK_PAIRS16 = 1, TK_VWALK = 2, TK_ROUTE_LEAF = 3, TK_PAIRS_HUB = 4,
-                        TK_SEGSUM_F32 = 5, TK_SEGSUM_BF16 = 6, TK_SEGSUM_FP8 = 7 };
+                        TK_SEGSUM_F32 = 5, TK_SEGSUM_BF16 = 6, TK_SEGSUM_FP8 = 7, TK_VSAMPLE = 8 };
 rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<rfx_status(int)>& run);
 rfx_status launch_pack_forest(cudaStream_t s, int T, int n, int p, const int64_t* d_offs, const int32_t* status,
                               const int32_t* bestvar, const float* split, const int32_t* treemap,

@@ -38,12 +38,13 @@ bool tuning_enabled() {
 
 }  // namespace
 
-// RFX_TUNE_<STAGE>=<shape> (ROUTE, PAIRS, VWALK, ROUTE_LEAF, PAIRS_HUB, SEGSUM) forces a shape,
-// e.g. to test every shape against the oracle.
+// RFX_TUNE_<STAGE>=<shape> (ROUTE, PAIRS, VWALK, ROUTE_LEAF, PAIRS_HUB, SEGSUM, VSAMPLE) forces a
+// shape, e.g. to test every shape against the oracle.
 int forced_shape(int kernel, int nvar) {
-    static const char* names[] = {"RFX_TUNE_ROUTE", "RFX_TUNE_PAIRS", "RFX_TUNE_VWALK", "RFX_TUNE_ROUTE_LEAF",
-                                  "RFX_TUNE_PAIRS_HUB", "RFX_TUNE_SEGSUM", "RFX_TUNE_SEGSUM", "RFX_TUNE_SEGSUM"};
-    if (kernel < 0 || kernel > 7) return -1;
+    static const char* names[] = {"RFX_TUNE_ROUTE",  "RFX_TUNE_PAIRS",     "RFX_TUNE_VWALK",
+                                  "RFX_TUNE_ROUTE_LEAF", "RFX_TUNE_PAIRS_HUB", "RFX_TUNE_SEGSUM",
+                                  "RFX_TUNE_SEGSUM", "RFX_TUNE_SEGSUM",    "RFX_TUNE_VSAMPLE"};
+    if (kernel < 0 || kernel > 8) return -1;
     const char* e = std::getenv(names[kernel]);
     if (!e || !*e) return -1;
     const int v = std::atoi(e);

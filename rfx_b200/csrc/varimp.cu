@@ -521,6 +521,100 @@ varimp_sample_kernel(const uint8_t* __restrict__ inbag, const uint8_t* __restric
         if (kl + u < pw) qimpm[(size_t)i * p + k0 + u] = acc[u];
 }
 
+// The same sums from per-sample lists of OOB trees (the second launch shape
+// of the stage).  oob_trees_kernel lists, for every sample, the trees where it
+// is out of bag in ascending order (oobt[k * n + i] = k-th such tree, at most
+// 65,535 trees); varimp_sample_oob_kernel then visits only those trees, so a
+// thread does no work for its in-bag trees and the lanes of a warp do not wait
+// on each other's OOB trees.  The sums still run in tree order.  The flip word
+// and the used-feature mask are read as the 16-bit piece that holds the
+// thread's sixteen features.
+__global__ void __launch_bounds__(256)
+oob_trees_kernel(const uint8_t* __restrict__ inbag, int n, int T, uint16_t* __restrict__ oobt,
+                 int32_t* __restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int k = 0;
+    constexpr int TB = 16;
+    int t0 = 0;
+    for (; t0 + TB <= T; t0 += TB) {
+        uint8_t b[TB];
+#pragma unroll
+        for (int u = 0; u < TB; ++u) b[u] = __ldg(inbag + (size_t)(t0 + u) * n + i);
+#pragma unroll
+        for (int u = 0; u < TB; ++u)
+            if (b[u] == 0) oobt[(size_t)(k++) * n + i] = (uint16_t)(t0 + u);
+    }
+    for (int t = t0; t < T; ++t)
+        if (__ldg(inbag + (size_t)t * n + i) == 0) oobt[(size_t)(k++) * n + i] = (uint16_t)t;
+    cnt[i] = k;
+}
+
+template <int W>
+__global__ void __launch_bounds__(256, 4)
+varimp_sample_oob_kernel(const uint16_t* __restrict__ oobt, const int32_t* __restrict__ cnt,
+                         const uint8_t* __restrict__ vflags, const uint64_t* __restrict__ flips,
+                         const uint64_t* __restrict__ iv, const float* __restrict__ invnoob, int n, int p,
+                         float* __restrict__ qimp, float* __restrict__ qimpm, int fb, int pw, int ivw) {
+    const int G = (pw + VS_FEAT - 1) / VS_FEAT;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * G) return;
+    const int i = (int)(idx / G);
+    const int g = (int)(idx % G);
+    const int kl = g * VS_FEAT;  // first feature of the group within the block
+    const int k0 = fb + kl;
+    const int wq = kl >> 6, sh = kl & 63;  // groups never straddle a 64-bit word
+    const int iq = k0 >> 6;                // the group's word of the iv row
+    const int pc = sh >> 4;                // the 16-bit piece of those words
+    const uint16_t* fl16 = reinterpret_cast<const uint16_t*>(flips);
+    const uint16_t* iv16 = reinterpret_cast<const uint16_t*>(iv);
+    const int K = __ldg(cnt + i);
+    float acc[VS_FEAT];
+#pragma unroll
+    for (int u = 0; u < VS_FEAT; ++u) acc[u] = 0.0f;
+    float q = 0.0f;
+    constexpr int TB = 4;
+    // the next block's tree ids are loaded with the current block's data
+    int tn[TB];
+#pragma unroll
+    for (int u = 0; u < TB; ++u) tn[u] = u < K ? (int)__ldg(oobt + (size_t)u * n + i) : -1;
+    for (int kb = 0; kb < K; kb += TB) {
+        int tt[TB];
+#pragma unroll
+        for (int u = 0; u < TB; ++u) {
+            tt[u] = tn[u];
+            const int kn = kb + TB + u;
+            tn[u] = kn < K ? (int)__ldg(oobt + (size_t)kn * n + i) : -1;
+        }
+        uint8_t fl[TB];
+        float inv[TB];
+        uint32_t fw[TB], ivv[TB];
+#pragma unroll
+        for (int u = 0; u < TB; ++u) {
+            const int t = tt[u] < 0 ? 0 : tt[u];
+            const size_t ti = (size_t)t * n + i;
+            fl[u] = tt[u] < 0 ? 0 : __ldg(vflags + ti);
+            inv[u] = __ldg(invnoob + t);
+            fw[u] = tt[u] < 0 ? 0u : __ldg(fl16 + ((ti * W + wq) << 2) + pc);
+            ivv[u] = __ldg(iv16 + (((size_t)t * ivw + iq) << 2) + pc);
+        }
+#pragma unroll
+        for (int u = 0; u < TB; ++u) {
+            if (tt[u] < 0) break;
+            const bool btb = (fl[u] >> 1) & 1, bimp = (fl[u] >> 2) & 1;
+            if (btb) q = __fadd_rn(q, inv[u]);
+            const uint32_t corr = (ivv[u] & ((bimp ? 0xffffu : 0u) ^ fw[u])) | (~ivv[u] & (btb ? 0xffffu : 0u));
+#pragma unroll
+            for (int v = 0; v < VS_FEAT; ++v)
+                if ((corr >> v) & 1u) acc[v] = __fadd_rn(acc[v], inv[u]);
+        }
+    }
+    if (g == 0 && fb == 0) qimp[i] = q;
+#pragma unroll
+    for (int u = 0; u < VS_FEAT; ++u)
+        if (kl + u < pw) qimpm[(size_t)i * p + k0 + u] = acc[u];
+}
+
 // counts[2t] = #OOB correct by testreebag (right), counts[2t+1] = #OOB correct
 // by the unpermuted testreeimp walk; rightimp[t][k] = counts[2t+1] + delta[t][k].
 // One warp per feature: the lanes compute rr for 32 trees at once, then the
@@ -637,10 +731,37 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         StageTimer st(c, ST_VARIMP_SAMPLE, 1);
         const long long G = (c->p + VS_FEAT - 1) / VS_FEAT;
         const long long threads = (long long)c->n * G;
-        varimp_sample_kernel<W><<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
-            c->d_inbag, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->T, c->d_qimp, c->d_qimpm, 0,
-            c->p, W);
-        RFX_CUDA(cudaGetLastError());
+        const unsigned blocks = (unsigned)((threads + 255) / 256);
+        // shape 0: every thread loops over all trees; 1: over its sample's
+        // OOB trees from per-sample lists (tree ids in 16 bits; the lists
+        // live in per-call scratch, so a stream capture takes shape 0)
+        const int nshape = c->T < 65536 ? 2 : 1;
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        RFX_CUDA(cudaStreamIsCapturing(c->stream, &cap));
+        const bool capturing = cap != cudaStreamCaptureStatusNone;
+        rfx_status r = autotune(c, TK_VSAMPLE, nshape, 0, [&](int shape) -> rfx_status {
+            if (shape == 1 && !capturing) {
+                Scratch sc(c);
+                uint16_t* oobt = sc.get<uint16_t>((size_t)c->T * c->n);
+                int32_t* cnt = sc.get<int32_t>((size_t)c->n);
+                if (!oobt || !cnt) {
+                    set_error("varimp: scratch allocation failed");
+                    return RFX_ERR_OOM;
+                }
+                oob_trees_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_inbag, c->n, c->T, oobt, cnt);
+                RFX_CUDA(cudaGetLastError());
+                varimp_sample_oob_kernel<W><<<blocks, 256, 0, c->stream>>>(
+                    oobt, cnt, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->d_qimp, c->d_qimpm, 0,
+                    c->p, W);
+            } else {
+                varimp_sample_kernel<W><<<blocks, 256, 0, c->stream>>>(c->d_inbag, c->d_vflags, c->d_flips, c->d_iv,
+                                                                       c->d_invnoob, c->n, c->p, c->T, c->d_qimp,
+                                                                       c->d_qimpm, 0, c->p, W);
+            }
+            RFX_CUDA(cudaGetLastError());
+            return RFX_OK;
+        });
+        if (r != RFX_OK) return r;
     }
     StageTimer st(c, ST_VARIMP_FEATURE, 1);
     varimp_feature_kernel<<<(c->p + 3) / 4, 128, 0, c->stream>>>(c->d_right, c->d_rightimp, c->d_noob, c->d_iv,

@@ -320,7 +320,8 @@ def ok_leaf(term, f, t, node):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("stage,count", [("ROUTE", 10), ("PAIRS", 8), ("VWALK", 9), ("ROUTE_LEAF", 9)])
+@pytest.mark.parametrize("stage,count", [("ROUTE", 10), ("PAIRS", 8), ("VWALK", 9), ("ROUTE_LEAF", 9),
+                                         ("VSAMPLE", 2)])
 def test_every_launch_shape_matches_oracle(built, monkeypatch, stage, count):
     """Each launch shape the autotuner can pick gives the oracle's results."""
     from oracle import oracle as orc
