@@ -1,8 +1,8 @@
 // Launch-shape autotuner.  A tunable stage offers a few launch shapes that
 // all compute the same result; the first time a stage runs for a given
 // problem shape (device, kernel, and power-of-two buckets of n, ntree and p)
-// each shape is run once and timed with CUDA events on the context stream,
-// the fastest is remembered for the rest of the process, and the stage's
+// each shape is run once untimed and once timed with CUDA events on the
+// context stream, the fastest is remembered for the rest of the process, and the stage's
 // result is the one the last timed run left behind (every shape writes the
 // complete result).  Tuning is skipped, and the default shape used, while the
 // stream is being captured into a graph or when RFX_AUTOTUNE=0.
@@ -70,7 +70,11 @@ rfx_status autotune(Ctx* c, int kernel, int nvar, int def, const std::function<r
         cudaEventDestroy(e0);
         return cuda_fail(e, "autotune");
     }
-    rfx_status st = run(def);  // warm-up (caches, first-launch costs)
+    // warm-up: every shape runs once untimed, so no timed run pays a first
+    // launch (lazy module loading of its kernels) or a first scratch
+    // allocation that the others were spared
+    rfx_status st = RFX_OK;
+    for (int v = 0; v < nvar && st == RFX_OK; ++v) st = run(v);
     int best = def;
     float best_ms = 3.0e38f;
     for (int v = 0; v < nvar && st == RFX_OK; ++v) {
