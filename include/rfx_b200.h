@@ -305,16 +305,18 @@ rfx_status rfx_graph_launch(rfx_graph* g, void* stream);
 rfx_status rfx_graph_destroy(rfx_graph* g);
 
 /* Launch-shape autotuner (no counterpart in the reference).  The routing,
- * pair-count and varimp-walk stages each offer a few launch shapes with
- * identical results; the first run for a problem shape (device and
- * power-of-two buckets of n, ntree, p) times each once on the context stream
- * and keeps the fastest for the process.  Setting RFX_AUTOTUNE=0 keeps the
- * default shapes, and RFX_TUNE_ROUTE / RFX_TUNE_PAIRS / RFX_TUNE_VWALK /
- * RFX_TUNE_ROUTE_LEAF = <shape> force one shape; nothing is tuned while a
- * stream is being captured.
+ * pair-count, varimp-walk, per-sample importance and low-rank leaf-sum stages
+ * each offer a few launch shapes with identical results; the first run for a
+ * problem shape (device and power-of-two buckets of n, ntree, p) runs each
+ * once untimed, then times each once on the context stream and keeps the
+ * fastest for the process.  Setting RFX_AUTOTUNE=0 keeps the default shapes,
+ * and RFX_TUNE_ROUTE / RFX_TUNE_PAIRS / RFX_TUNE_VWALK / RFX_TUNE_ROUTE_LEAF /
+ * RFX_TUNE_PAIRS_HUB / RFX_TUNE_SEGSUM / RFX_TUNE_VSAMPLE = <shape> force one
+ * shape; nothing is tuned while a stream is being captured.
  * rfx_tuned_shapes copies up to `cap` records of 6 int32 {stage (0 routing,
- * 1 pair counts, 2 varimp walk, 3 routing in leaf order), device, log2 n,
- * log2 ntree, log2 p, shape}
+ * 1 pair counts, 2 varimp walk, 3 routing in leaf order, 4 pair counts with
+ * hub tiles, 5-7 low-rank leaf sums in FP32 / BF16 / FP8, 8 per-sample
+ * importance sums), device, log2 n, log2 ntree, log2 p, shape}
  * and sets *count to the number of records. */
 rfx_status rfx_tuned_shapes(int32_t* out, int32_t cap, int32_t* count);
 
