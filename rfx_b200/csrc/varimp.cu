@@ -1,6 +1,6 @@
-// Permutation importance for all trees and all features in four launches (with
-// more than 256 features the walk and the per-sample sums run once per block of
-// 256 features).
+// Permutation importance for all trees and all features in four or five
+// launches (with more than 256 features the walk and the per-sample sums run
+// once per block of 256 features).
 //
 // cpu_varimp (src/rf_varimp.cpp:106-302) re-routes every OOB sample once per
 // used feature k, with x[pjoob[r]][k] in place of x[joob[r]][k], where pjoob is
@@ -26,6 +26,9 @@
 //                       float sums in tree order, 1/noob per correct OOB
 //                       tree (the reference adds each tree's temporaries in
 //                       tree order, src/rf_random_forest.cpp:1217-1230).
+//                       Its other launch shape, oob_trees_kernel +
+//                       varimp_sample_oob_kernel, visits only each sample's
+//                       OOB trees, from per-sample lists, in the same order.
 // varimp_feature_kernel - one thread per feature: avimp / sqsd sums of
 //                       rr = (right - rightimp) / noob in tree order.
 #include "walks.cuh"
