@@ -378,3 +378,26 @@ def test_child_prefetch_shapes_match_oracle(built, monkeypatch, name):
         assert np.array_equal(avimp, O["avimp"]) and np.array_equal(sqsd, O["sqsd"]), shape
         assert np.array_equal(qimp, O["qimp"]) and np.array_equal(qimpm, O["qimpm"]), shape
         ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("p", [70, 130, 250])
+def test_sample_sum_shapes_multiword_flips(built, monkeypatch, p):
+    """Both launch shapes of the per-sample importance sums with two, three
+    and four 64-bit flip words per (tree, sample): the oracle's qimp, qimpm,
+    avimp and sqsd."""
+    from oracle import oracle as orc
+    from rfx_b200 import abi
+
+    X, y, f = _grow(*synth.gaussian_classes(600, p, 3, seed=p), 10, max(2, int(np.sqrt(p))))
+    O = orc.analyse(X, y, f)
+    for shape in (0, 1):
+        monkeypatch.setenv("RFX_TUNE_VSAMPLE", str(shape))
+        ctx = abi.Context(0)
+        ctx.load(f, X, y)
+        for _ in range(2):  # over the OOB lists, then in leaf order after the pair counts
+            avimp, sqsd, qimp, qimpm = ctx.varimp(True)
+            assert np.array_equal(avimp, O["avimp"]) and np.array_equal(sqsd, O["sqsd"]), (p, shape)
+            assert np.array_equal(qimp, O["qimp"]) and np.array_equal(qimpm, O["qimpm"]), (p, shape)
+            ctx.proximity_upper()
+        ctx.close()
