@@ -743,20 +743,22 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
         RFX_CUDA(cudaStreamIsCapturing(c->stream, &cap));
         const bool capturing = cap != cudaStreamCaptureStatusNone;
         rfx_status r = autotune(c, TK_VSAMPLE, nshape, 0, [&](int shape) -> rfx_status {
+            bool listed = false;
             if (shape == 1 && !capturing) {
+                // (where the lists do not fit in device memory the tree loop runs)
                 Scratch sc(c);
                 uint16_t* oobt = sc.get<uint16_t>((size_t)c->T * c->n);
-                int32_t* cnt = sc.get<int32_t>((size_t)c->n);
-                if (!oobt || !cnt) {
-                    set_error("varimp: scratch allocation failed");
-                    return RFX_ERR_OOM;
+                int32_t* cnt = oobt ? sc.get<int32_t>((size_t)c->n) : nullptr;
+                if (oobt && cnt) {
+                    oob_trees_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_inbag, c->n, c->T, oobt, cnt);
+                    RFX_CUDA(cudaGetLastError());
+                    varimp_sample_oob_kernel<W><<<blocks, 256, 0, c->stream>>>(
+                        oobt, cnt, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->d_qimp,
+                        c->d_qimpm, 0, c->p, W);
+                    listed = true;
                 }
-                oob_trees_kernel<<<(c->n + 255) / 256, 256, 0, c->stream>>>(c->d_inbag, c->n, c->T, oobt, cnt);
-                RFX_CUDA(cudaGetLastError());
-                varimp_sample_oob_kernel<W><<<blocks, 256, 0, c->stream>>>(
-                    oobt, cnt, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->d_qimp, c->d_qimpm, 0,
-                    c->p, W);
-            } else {
+            }
+            if (!listed) {
                 varimp_sample_kernel<W><<<blocks, 256, 0, c->stream>>>(c->d_inbag, c->d_vflags, c->d_flips, c->d_iv,
                                                                        c->d_invnoob, c->n, c->p, c->T, c->d_qimp,
                                                                        c->d_qimpm, 0, c->p, W);
