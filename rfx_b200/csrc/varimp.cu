@@ -755,6 +755,7 @@ rfx_status launch_varimp_w(Ctx* c, int impn) {
                     varimp_sample_oob_kernel<W><<<blocks, 256, 0, c->stream>>>(
                         oobt, cnt, c->d_vflags, c->d_flips, c->d_iv, c->d_invnoob, c->n, c->p, c->d_qimp,
                         c->d_qimpm, 0, c->p, W);
+                    c->launches += 1;  // the list kernel (the stage counts one kernel)
                     listed = true;
                 }
             }
